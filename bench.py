@@ -1,0 +1,335 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 subtask path on the imageFiltering configuration.
+
+Workload (one "step"): one imageFiltering task over a seeded synthetic
+8192 x 8192 RGB image (bytes uniform in [0,255]), 5x5 integer filter with
+weights uniform in [-4,4], output clamped to [0,255], split into 256 subtasks
+of 512 x 512 output pixels (with their 2-pixel halos), all run in ONE launch of
+the stencil kernel.  Input and output (201 MB each) exceed the 126 MB L2, so
+no flush is needed between steps.
+
+  value   : algorithmic bytes (read 3WH + write 3WH) per step / device time,
+            inputs resident in HBM, CUDA events on the launching stream.
+  e2e     : the same metric through the C ABI with host buffers: pinned host
+            input -> H2D -> kernel -> D2H -> pinned host output, per step.
+  roofline: the stencil kernel against the measured HBM copy bandwidth.
+  cpu_baseline: the reference's own imageFilter_cpu (oracle/_ref, compiled
+            from the reference sources) on the host cores, one worker per core.
+
+`--impl reference` times that reference CPU implementation alone (the
+reference has no runnable GPU path for this app: its texture-reference kernel
+does not compile for CUDA 12).
+
+Multi-GPU (torchrun): replicas only -- every rank filters its own image; value
+is the bytes of all ranks over the max-over-ranks time.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+W = H = 8192
+R = 2
+TILE = 512
+SEED = 3
+ALG_BYTES = 2 * 3 * W * H  # 402,653,184
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            p = json.load(fh)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """Per-launch DRAM bytes of the stencil kernel from the committed ncu summary."""
+    path = os.path.join(ROOT, "profiles", "image_filter_8192_r2.md")
+    try:
+        with open(path) as fh:
+            for line in fh:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return int(line.split(":")[1].strip())
+    except OSError:
+        pass
+    return None
+
+
+def make_inputs():
+    rng = np.random.default_rng(SEED)
+    img = rng.integers(0, 256, size=H * W * 3, dtype=np.uint8)
+    f = rng.integers(-4, 5, size=(2 * R + 1, 2 * R + 1)).astype(np.int8)
+    return img, f
+
+
+def tiles():
+    return [(r, min(r + TILE, H), c, min(c + TILE, W)) for r in range(0, H, TILE) for c in range(0, W, TILE)]
+
+
+class ClockSampler:
+    """Samples nvidia-smi clocks/throttle reasons while the timed region runs."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, dev: int):
+        self.dev = dev
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.dev), f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.lines:
+            return None
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline(img, f, threads: int, rows: int):
+    """Reference imageFilter_cpu on a band of `rows` image rows, all threads.
+
+    The reference computes the wrap (signed char) form; the cost per pixel is
+    the same as the clamp form the GPU line computes.
+    """
+    path = os.path.join(ROOT, "oracle", "_ref", "libref_imgf.so")
+    if not os.path.exists(path):
+        return None
+    ref = ctypes.CDLL(path)
+    fb = np.zeros((32, 32), np.int8)
+    fb[: 2 * R + 1, : 2 * R + 1] = f
+    band = np.ascontiguousarray(img[: rows * W * 3])
+    out = np.zeros_like(band)
+    P = ctypes.c_void_p
+    split = max(1, (2 * threads + 3) // 4)
+    t0 = time.perf_counter()
+    st = ref.ref_imgf_task(band.ctypes.data_as(P), out.ctypes.data_as(P), W, rows, R, fb.ctypes.data_as(P),
+                           threads, split)
+    dt = time.perf_counter() - t0
+    if st != 0:
+        return None
+    return {"value": round(2 * 3 * W * rows / dt / 1e9, 3), "unit": "GB/s", "cores": threads,
+            "kind": "reference",
+            "sample": f"imageFilter_cpu (reference source) on a {W}x{rows} band of the same image, "
+                      f"{threads} worker threads, each reference subtask split {split} ways",
+            "seconds": round(dt, 3)}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = os.cpu_count() or 1
+    img, f = make_inputs()
+    rows = 2048
+    samples = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(img, f, threads, rows)
+        if r is None:
+            print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_imgf.so not built"}))
+            return 0
+        if i >= args.warmup:
+            samples.append(r["value"])
+    v = statistics.median(samples)
+    line = {
+        "impl": "reference", "metric": "imageFilter throughput (algorithmic bytes)", "value": v, "unit": "GB/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(2 * 3 * W * rows / (v * 1e9) * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": f"imageFiltering {W}x{H} RGB, 5x5 filter, reference CPU callback, "
+                               f"band of {rows} rows per step", "threads": threads},
+        "cpu_baseline": {"value": v, "unit": "GB/s", "cores": threads, "kind": "reference",
+                         "sample": f"{W}x{rows} band per step"},
+        "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+def main():
+    args = parse()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import torch
+    from unicorn_b200 import capi
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    L = capi.lib()
+    img, f = make_inputs()
+    fb = np.zeros((32, 32), np.int8)
+    fb[: 2 * R + 1, : 2 * R + 1] = f
+    fp = fb.ctypes.data_as(ctypes.c_void_p)
+
+    d_in = torch.from_numpy(img).cuda()
+    d_out = torch.empty_like(d_in)
+    rects = tiles()
+    items = (capi.ImgfItem * len(rects))()
+    for k, (r0, r1, c0, c1) in enumerate(rects):
+        it = items[k]
+        it.in_, it.out = d_in.data_ptr(), d_out.data_ptr()
+        it.in_pitch = it.out_pitch = 3 * W
+        it.width, it.height = W, H
+        it.r0, it.r1, it.c0, it.c1 = r0, r1, c0, c1
+    stream = torch.cuda.Stream()
+    sp = ctypes.c_void_p(stream.cuda_stream)
+
+    def step():
+        capi.check(L.pmb_image_filter(items, len(rects), fp, R, capi.PMB_IMGF_CLAMP, sp))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident timing -----------------------------------------
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            step()
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        barrier()
+    dev_ms = max_over_ranks(ev0.elapsed_time(ev1))
+    ms_per_step = dev_ms / args.steps
+    value = world * ALG_BYTES * args.steps / (dev_ms / 1e3) / 1e9
+    kernel_gbs = ALG_BYTES / (ms_per_step / 1e3) / 1e9
+
+    # ---- end to end: host buffers, copies inside the timed region --------
+    h_in = torch.from_numpy(img).pin_memory()
+    h_out = torch.empty(h_in.numel(), dtype=torch.uint8).pin_memory()
+
+    def e2e_step():
+        d_in.copy_(h_in, non_blocking=True)
+        step()
+        h_out.copy_(d_out, non_blocking=True)
+
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            e2e_step()
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(stream):
+        e0.record(stream)
+        for _ in range(args.steps):
+            e2e_step()
+        e1.record(stream)
+    barrier()
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    e2e_value = world * ALG_BYTES * args.steps / (e2e_ms / 1e3) / 1e9
+
+    peak, peak_kind = peaks()
+    line = {
+        "metric": "imageFilter throughput (algorithmic bytes)", "value": round(value, 2), "unit": "GB/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": {"workload": "imageFiltering 8192x8192 RGB u8, 5x5 int filter [-4,4], clamp to [0,255], "
+                               "256 subtasks of 512x512 (+2 px halo) in one launch",
+                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (201 MB in + 201 MB out)"},
+        "roofline": {"bound": "hbm", "achieved": round(kernel_gbs, 1), "peak": peak, "unit": "GB/s",
+                     "frac": round(kernel_gbs / peak, 4), "traffic": profiled_traffic(),
+                     "peak_source": f"{peak_kind} hbm_gbs (burst, kernel timed alone)"},
+        "e2e": {"value": round(e2e_value, 2), "unit": "GB/s", "h2d_bytes_per_step": 3 * W * H,
+                "d2h_bytes_per_step": 3 * W * H, "path": "C ABI pmb_image_filter, pinned host buffers"},
+        "gpu_launches": args.steps,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(img, f, os.cpu_count() or 1, 2048)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

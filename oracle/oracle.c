@@ -1,0 +1,100 @@
+/*
+ * oracle.c -- TEST INFRASTRUCTURE ONLY.
+ *
+ * CPU restatements of the reference (iitd-plos/unicorn testSuite) algorithms
+ * on the B200 subtask path.  They exist to CHECK the CUDA kernels: only
+ * tests/, __graft_entry__.smoke() and the CPU-baseline leg of bench.py load
+ * this library.  Nothing in unicorn_b200/ links or calls it.
+ *
+ * Parity is pinned two ways: (1) against the reference's own CPU callbacks
+ * compiled from the reference sources into oracle/_ref (oracle/ref/Makefile),
+ * on identical seeded inputs; (2) against the golden fixtures committed under
+ * tests/golden/ (generated by tests/golden/make_golden.py from (1)).
+ */
+#include <stdint.h>
+#include <stddef.h>
+#include <stdlib.h>
+#include <string.h>
+#include <pthread.h>
+
+#define ORC_MAX_FILTER_DIM 32
+
+/* Number of worker threads the row-parallel oracles use (default 1). */
+static int g_threads = 1;
+void orc_set_threads(int n) { g_threads = n < 1 ? 1 : (n > 256 ? 256 : n); }
+
+/* Run body(lo, hi, arg) over [0, n) split into g_threads contiguous chunks. */
+typedef void (*orc_range_fn)(long lo, long hi, void* arg);
+struct orc_job { orc_range_fn fn; void* arg; long lo, hi; };
+static void* orc_thread_main(void* p) {
+    struct orc_job* j = (struct orc_job*)p;
+    j->fn(j->lo, j->hi, j->arg);
+    return NULL;
+}
+static void orc_parallel_for(long n, orc_range_fn fn, void* arg) {
+    int t = g_threads;
+    if (t > n) t = (int)(n > 0 ? n : 1);
+    if (t <= 1) { fn(0, n, arg); return; }
+    pthread_t th[256];
+    struct orc_job jobs[256];
+    for (int k = 0; k < t; ++k) {
+        jobs[k].fn = fn; jobs[k].arg = arg;
+        jobs[k].lo = n * k / t; jobs[k].hi = n * (k + 1) / t;
+        if (k > 0) pthread_create(&th[k], NULL, orc_thread_main, &jobs[k]);
+    }
+    orc_thread_main(&jobs[0]);
+    for (int k = 1; k < t; ++k) pthread_join(th[k], NULL);
+}
+
+static inline int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+/*
+ * imageFilter over an output rectangle, NATURAL views of the whole image.
+ * Follows imageFilter_cpu, testSuite/imageFiltering/source/code/src/
+ * imageFiltering.cpp:419-468: taps clamp to the image border (:433-434), the
+ * input address space holds image row m in buffer row H-1-m (:438), output
+ * byte 0 of a pixel accumulates input byte 2 and byte 2 accumulates input
+ * byte 0 (:457-467).  mode 0 (wrap): the accumulator is a char, so the result
+ * is the exact sum reduced mod 256 (two's complement); mode 1 (clamp):
+ * unsigned input bytes, exact int sum clamped to [0,255].
+ */
+struct imgf_args {
+    const uint8_t* in; uint8_t* out; int W, H, R; const int8_t* filter; int mode, r0, c0, c1;
+};
+
+static void imgf_rows(long lo, long hi, void* p) {
+    const struct imgf_args* a = (const struct imgf_args*)p;
+    const int W = a->W, H = a->H, R = a->R;
+    for (long ii = lo; ii < hi; ++ii) {
+        const int i = a->r0 + (int)ii;
+        for (int j = a->c0; j < a->c1; ++j) {
+            int acc[3] = {0, 0, 0};
+            for (int ky = 0; ky <= 2 * R; ++ky) {
+                const int m = clampi(i - R + ky, 0, H - 1);
+                const uint8_t* row = a->in + (size_t)(H - 1 - m) * 3 * W;
+                for (int kx = 0; kx <= 2 * R; ++kx) {
+                    const int n = clampi(j - R + kx, 0, W - 1);
+                    const int f = a->filter[ky * ORC_MAX_FILTER_DIM + kx];
+                    if (a->mode == 0) {
+                        acc[0] += (int8_t)row[3 * n + 2] * f;
+                        acc[1] += (int8_t)row[3 * n + 1] * f;
+                        acc[2] += (int8_t)row[3 * n + 0] * f;
+                    } else {
+                        acc[0] += row[3 * n + 2] * f;
+                        acc[1] += row[3 * n + 1] * f;
+                        acc[2] += row[3 * n + 0] * f;
+                    }
+                }
+            }
+            uint8_t* o = a->out + ((size_t)i * W + j) * 3;
+            for (int c = 0; c < 3; ++c)
+                o[c] = a->mode == 0 ? (uint8_t)(acc[c] & 0xff) : (uint8_t)clampi(acc[c], 0, 255);
+        }
+    }
+}
+
+void orc_image_filter(const uint8_t* in, uint8_t* out, int W, int H, int R, const int8_t* filter,
+                      int mode, int r0, int r1, int c0, int c1) {
+    struct imgf_args a = {in, out, W, H, R, filter, mode, r0, c0, c1};
+    orc_parallel_for(r1 - r0, imgf_rows, &a);
+}

@@ -1,0 +1,64 @@
+"""Generate the imageFilter golden fixtures from the reference's own CPU code.
+
+Runs the reference's imageFilterDataDistribution + imageFilter_cpu (compiled
+unchanged from testSuite/imageFiltering/source/code/src/imageFiltering.cpp into
+oracle/_ref/libref_imgf.so by oracle/ref/Makefile) on small seeded inputs and
+stores inputs, filters and outputs in imgf_golden.npz, plus the reference's
+subscription geometry for a few image shapes in imgf_subscriptions.json.
+
+Usage (in a tree where the reference is available):
+    make -C oracle/ref && python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+
+# (W, H, R, seed): odd sizes, heavy clamping (R larger than the image), and a
+# width that spans two reference subtasks (TILE_DIM 2048).
+CASES = [(37, 35, 1, 11), (67, 41, 2, 12), (130, 70, 3, 13), (20, 20, 15, 14), (5, 3, 2, 15),
+         (2050, 5, 2, 16)]
+SUB_SHAPES = [(8192, 8192, 2), (2100, 2050, 3), (4096, 2049, 1)]
+
+
+def main() -> None:
+    ref = ctypes.CDLL(os.path.join(ROOT, "oracle", "_ref", "libref_imgf.so"))
+    ref.ref_imgf_subtask_count.restype = ctypes.c_ulong
+    P = ctypes.c_void_p
+    out = {}
+    for idx, (W, H, R, seed) in enumerate(CASES):
+        rng = np.random.default_rng(seed)
+        img = rng.integers(0, 256, size=H * W * 3, dtype=np.uint8)
+        f = np.zeros((32, 32), np.int8)
+        f[: 2 * R + 1, : 2 * R + 1] = rng.integers(-128, 128, size=(2 * R + 1, 2 * R + 1))
+        res = np.zeros_like(img)
+        st = ref.ref_imgf_task(img.ctypes.data_as(P), res.ctypes.data_as(P), W, H, R,
+                               f.ctypes.data_as(P), 1, 0)
+        assert st == 0, st
+        out[f"c{idx}_meta"] = np.array([W, H, R, seed], np.int64)
+        out[f"c{idx}_in"] = img
+        out[f"c{idx}_filter"] = f
+        out[f"c{idx}_out"] = res
+    np.savez_compressed(os.path.join(HERE, "imgf_golden.npz"), **out)
+
+    subs = []
+    buf = (ctypes.c_ulonglong * 8)()
+    for (W, H, R) in SUB_SHAPES:
+        n = ref.ref_imgf_subtask_count(W, H)
+        rows = []
+        for sid in range(n):
+            assert ref.ref_imgf_subscriptions(W, H, R, ctypes.c_ulong(sid), buf) == 0
+            rows.append([int(x) for x in buf])
+        subs.append({"W": W, "H": H, "R": R, "tile_dim": ref.ref_imgf_tile_dim(), "subtasks": rows})
+    with open(os.path.join(HERE, "imgf_subscriptions.json"), "w") as fh:
+        json.dump(subs, fh)
+
+
+if __name__ == "__main__":
+    main()

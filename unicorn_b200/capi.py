@@ -1,0 +1,90 @@
+"""ctypes binding of libpmb.so, the C ABI of the B200 subtask path.
+
+Every function declared in include/pmb_capi.h is bound here with its exact
+argument types.  Loading fails loudly (ImportError) when the library has not
+been built: there is no fallback implementation.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libpmb.so")
+
+c_void_p = ctypes.c_void_p
+c_int = ctypes.c_int
+c_int64 = ctypes.c_int64
+c_size_t = ctypes.c_size_t
+
+PMB_SUCCESS = 0
+PMB_IMGF_WRAP = 0
+PMB_IMGF_CLAMP = 1
+PMB_IMGF_MAX_ITEMS = 256
+PMB_IMGF_MAX_FILTER_DIM = 32
+
+
+class PmbError(RuntimeError):
+    """A libpmb.so call returned a non-zero pmStatus."""
+
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"pmStatus {status}: {msg}")
+        self.status = status
+
+
+class ImgfItem(ctypes.Structure):
+    """Mirror of pmb_imgf_item (include/pmb_capi.h)."""
+
+    _fields_ = [
+        ("in_", c_void_p),
+        ("out", c_void_p),
+        ("in_pitch", c_int64),
+        ("out_pitch", c_int64),
+        ("width", ctypes.c_int32),
+        ("height", ctypes.c_int32),
+        ("in_row0", ctypes.c_int32),
+        ("in_col0", ctypes.c_int32),
+        ("out_row0", ctypes.c_int32),
+        ("out_col0", ctypes.c_int32),
+        ("r0", ctypes.c_int32),
+        ("r1", ctypes.c_int32),
+        ("c0", ctypes.c_int32),
+        ("c1", ctypes.c_int32),
+    ]
+
+
+# name -> (restype, argtypes)
+_SIGS = {
+    "pmb_last_error": (ctypes.c_char_p, []),
+    "pmb_version": (ctypes.c_char_p, []),
+    "pmb_device_supported": (c_int, [c_int]),
+    "pmb_image_filter": (c_int, [ctypes.POINTER(ImgfItem), c_int, c_void_p, c_int, c_int, c_void_p]),
+    "pmb_image_filter_full": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_int, c_int, c_void_p]),
+    "pmb_image_filter_plain": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_int, c_int, c_void_p]),
+}
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """Load libpmb.so once (raises ImportError if it is missing)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is not built; run `make -C unicorn_b200/csrc`")
+        l = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGS.items():
+            fn = getattr(l, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = l
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != PMB_SUCCESS:
+        raise PmbError(status, lib().pmb_last_error().decode())
+
+
+def declared_symbols() -> list[str]:
+    return list(_SIGS)

@@ -1,0 +1,398 @@
+// imageFiltering subtask kernel for sm_100a.
+//
+// Computes, for every output pixel (i, j) of a subtask rectangle and every
+// channel c, the (2R+1)^2 stencil of testSuite/imageFiltering/source/code/src/
+// imageFiltering.cpp:419-468 (imageFilter_cpu):
+//
+//     out[i][j][c] = sum_{ky,kx} img[clamp(i+ky-R)][clamp(j+kx-R)][2-c] * f[ky][kx]
+//
+// where img[m][n][ch] is byte ch of pixel n in buffer row H-1-m (the address
+// space stores the image bottom-up, :438) and clamp() is edge replication
+// (:433-434).  WRAP mode keeps the reference's signed-char accumulator (the
+// byte is the sum mod 256); CLAMP mode sums unsigned bytes exactly and clamps
+// to [0, 255].
+//
+// Design.  One CTA owns a 64 x 32 output tile.  It stages the tile plus halo
+// once into shared memory as three planar byte planes (one per output
+// channel), de-interleaving RGB with byte permutes while loading 12-byte pixel
+// quads with 32-bit loads.  Each thread then produces a 4-pixel x 4-row block:
+// for every staged row it reads a few aligned 32-bit words of a plane and
+// feeds them to dp4a (4 byte multiply-adds per instruction) against filter
+// "pattern" words precomputed on the host (filter row ky shifted so that tap
+// kx lines up with the byte it multiplies).  Every input byte is read from HBM
+// once per tile (halo re-reads hit L2), so the kernel's DRAM traffic is the
+// algorithmic 2 x 3WH bytes per pass.  The batch of subtasks (items) of one or
+// several tasks runs in ONE launch: blockIdx.x is mapped to (item, tile).
+#include <algorithm>
+
+#include "pmb_common.cuh"
+
+namespace {
+
+constexpr int kTW = 64;                    // tile width (pixels)
+constexpr int kTH = 32;                    // tile height (rows)
+constexpr int kV = 4;                      // output rows per thread
+constexpr int kGX = kTW / 4;               // 4-pixel groups per tile row
+constexpr int kThreads = kGX * (kTH / kV); // 128
+
+template <int R>
+struct Geo {
+    static constexpr int KD = 2 * R + 1;             // filter taps per row
+    static constexpr int PADL = ((R + 3) / 4) * 4;   // left halo, word aligned
+    static constexpr int OFF = PADL - R;             // first tap byte of pixel 0 in its window
+    static constexpr int NW = (OFF + 2 * R + 3) / 4 + 1;  // 32-bit words in a 4-pixel window
+    static constexpr int PW = kTW + PADL + 4 * NW;   // plane row width (bytes)
+    static constexpr int PH = kTH + 2 * R;           // plane rows
+    static constexpr int GPR = PW / 4;               // 4-pixel groups per plane row
+};
+
+// Does output pixel k (0..3) of a group have taps inside window word w?
+template <int R>
+__host__ __device__ constexpr bool tap_word_used(int k, int w) {
+    return 4 * w <= Geo<R>::OFF + k + 2 * R && 4 * w + 3 >= Geo<R>::OFF + k;
+}
+
+template <int R, int MAXI>
+struct ImgfParams {
+    uint32_t pat[Geo<R>::KD][4][Geo<R>::NW];
+    int n_items;
+    int tile_start[MAXI + 1];
+    int tiles_x[MAXI];
+    pmb_imgf_item items[MAXI];
+};
+
+__device__ __forceinline__ int dp4a_us(uint32_t a, uint32_t b, int c) {
+    int d;
+    asm("dp4a.u32.s32 %0, %1, %2, %3;" : "=r"(d) : "r"(a), "r"(b), "r"(c));
+    return d;
+}
+
+template <int R, int MODE, int MAXI>
+__global__ void __launch_bounds__(kThreads)
+imgf_kernel(const __grid_constant__ ImgfParams<R, MAXI> p) {
+    using G = Geo<R>;
+    __shared__ __align__(16) uint8_t planes[3][G::PH][G::PW];
+
+    // ---- which item / tile ------------------------------------------------
+    const int t = blockIdx.x;
+    int lo = 0, hi = p.n_items - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (p.tile_start[mid] <= t) lo = mid; else hi = mid - 1;
+    }
+    const pmb_imgf_item& it = p.items[lo];
+    const int local = t - p.tile_start[lo];
+    const int tx = local % p.tiles_x[lo];
+    const int ty = local / p.tiles_x[lo];
+    const int tile_c0 = it.c0 + tx * kTW;
+    const int tile_r0 = it.r0 + ty * kTH;
+    const int H = it.height;
+    const int mlo = max(0, it.r0 - R), mhi = min(H - 1, it.r1 - 1 + R);
+    const int clo = max(0, it.c0 - R), chi = min(it.width - 1, it.c1 - 1 + R);
+
+    // ---- stage tile + halo as planes: plane c holds input byte 2-c ---------
+    const uint8_t* inb = it.in;
+    const int64_t ip = it.in_pitch;
+    const bool al4 = ((reinterpret_cast<uintptr_t>(inb) | static_cast<uintptr_t>(ip)) & 3) == 0;
+    for (int g = threadIdx.x; g < G::PH * G::GPR; g += kThreads) {
+        const int yy = g / G::GPR;
+        const int xg = g - yy * G::GPR;
+        const int m = pmb::clampi(tile_r0 - R + yy, mlo, mhi);
+        const uint8_t* rowp = inb + static_cast<int64_t>(H - 1 - m - it.in_row0) * ip;
+        const int n0 = tile_c0 - G::PADL + 4 * xg;
+        uint32_t o0, o1, o2;
+        if (al4 && n0 >= clo && n0 + 3 <= chi && ((n0 - it.in_col0) & 3) == 0) {
+            const uint32_t* s = reinterpret_cast<const uint32_t*>(rowp + 3 * (n0 - it.in_col0));
+            const uint32_t w0 = __ldg(s), w1 = __ldg(s + 1), w2 = __ldg(s + 2);
+            // Pixel q's bytes b0 b1 b2 sit at 3q..3q+2 of the 12-byte quad.
+            o0 = __byte_perm(__byte_perm(w0, w1, 0x0052), w2, 0x7410);  // b2 of pixels 0..3
+            o1 = __byte_perm(__byte_perm(w0, w1, 0x0741), w2, 0x6210);  // b1
+            o2 = __byte_perm(__byte_perm(w0, w1, 0x0630), w2, 0x5210);  // b0
+        } else {
+            o0 = o1 = o2 = 0;
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int n = pmb::clampi(n0 + q, clo, chi);
+                const uint8_t* px = rowp + 3 * (n - it.in_col0);
+                o0 |= static_cast<uint32_t>(__ldg(px + 2)) << (8 * q);
+                o1 |= static_cast<uint32_t>(__ldg(px + 1)) << (8 * q);
+                o2 |= static_cast<uint32_t>(__ldg(px + 0)) << (8 * q);
+            }
+        }
+        *reinterpret_cast<uint32_t*>(&planes[0][yy][4 * xg]) = o0;
+        *reinterpret_cast<uint32_t*>(&planes[1][yy][4 * xg]) = o1;
+        *reinterpret_cast<uint32_t*>(&planes[2][yy][4 * xg]) = o2;
+    }
+    __syncthreads();
+
+    // ---- 4 pixels x kV rows per thread, dp4a over plane words -------------
+    const int gx = threadIdx.x % kGX;
+    const int gy = threadIdx.x / kGX;
+    uint32_t res[kV][4];
+#pragma unroll
+    for (int v = 0; v < kV; ++v)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) res[v][k] = 0;
+
+#pragma unroll 1
+    for (int ch = 0; ch < 3; ++ch) {
+        int acc[kV][4];
+#pragma unroll
+        for (int v = 0; v < kV; ++v)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) acc[v][k] = 0;
+
+        if constexpr (R <= 4) {
+#pragma unroll
+            for (int yy = 0; yy < kV + 2 * R; ++yy) {
+                const uint32_t* rp =
+                    reinterpret_cast<const uint32_t*>(&planes[ch][gy * kV + yy][4 * gx]);
+                uint32_t win[G::NW];
+#pragma unroll
+                for (int w = 0; w < G::NW; ++w) win[w] = rp[w];
+#pragma unroll
+                for (int v = 0; v < kV; ++v) {
+                    const int ky = yy - v;
+                    if (ky < 0 || ky >= G::KD) continue;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+#pragma unroll
+                        for (int w = 0; w < G::NW; ++w)
+                            if (tap_word_used<R>(k, w))
+                                acc[v][k] = dp4a_us(win[w], p.pat[ky][k][w], acc[v][k]);
+                }
+            }
+        } else {
+#pragma unroll 1
+            for (int yy = 0; yy < kV + 2 * R; ++yy) {
+                const uint32_t* rp =
+                    reinterpret_cast<const uint32_t*>(&planes[ch][gy * kV + yy][4 * gx]);
+                uint32_t win[G::NW];
+#pragma unroll
+                for (int w = 0; w < G::NW; ++w) win[w] = rp[w];
+#pragma unroll
+                for (int v = 0; v < kV; ++v) {
+                    const int ky = yy - v;
+                    if (ky < 0 || ky >= G::KD) continue;
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+#pragma unroll
+                        for (int w = 0; w < G::NW; ++w)
+                            if (tap_word_used<R>(k, w))
+                                acc[v][k] = dp4a_us(win[w], p.pat[ky][k][w], acc[v][k]);
+                }
+            }
+        }
+
+#pragma unroll
+        for (int v = 0; v < kV; ++v)
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int a = acc[v][k];
+                const uint32_t b = MODE == PMB_IMGF_WRAP ? static_cast<uint32_t>(a) & 0xffu
+                                                         : static_cast<uint32_t>(min(max(a, 0), 255));
+                res[v][k] |= b << (8 * ch);
+            }
+    }
+
+    // ---- write: pixel k's channels (c0 c1 c2) are bytes 3k..3k+2 -----------
+    const int j0 = tile_c0 + 4 * gx;
+    if (j0 >= it.c1) return;
+#pragma unroll
+    for (int v = 0; v < kV; ++v) {
+        const int i = tile_r0 + gy * kV + v;
+        if (i >= it.r1) break;
+        uint8_t* dst = it.out + static_cast<int64_t>(i - it.out_row0) * it.out_pitch +
+                       3 * (j0 - it.out_col0);
+        if (j0 + 3 < it.c1 && (reinterpret_cast<uintptr_t>(dst) & 3) == 0) {
+            uint32_t* d = reinterpret_cast<uint32_t*>(dst);
+            d[0] = res[v][0] | (res[v][1] << 24);
+            d[1] = (res[v][1] >> 8) | (res[v][2] << 16);
+            d[2] = (res[v][2] >> 16) | (res[v][3] << 8);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (j0 + k >= it.c1) break;
+                dst[3 * k + 0] = static_cast<uint8_t>(res[v][k]);
+                dst[3 * k + 1] = static_cast<uint8_t>(res[v][k] >> 8);
+                dst[3 * k + 2] = static_cast<uint8_t>(res[v][k] >> 16);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Plain GPU form: one thread per output pixel, byte loads straight from HBM.
+struct PlainFilter {
+    int8_t f[PMB_IMGF_MAX_FILTER_DIM][PMB_IMGF_MAX_FILTER_DIM];
+};
+
+template <int MODE>
+__global__ void imgf_plain_kernel(const uint8_t* __restrict__ in, uint8_t* __restrict__ out, int W,
+                                  int H, int R, const __grid_constant__ PlainFilter pf) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.y * blockDim.y + threadIdx.y;
+    if (j >= W || i >= H) return;
+    int s0 = 0, s1 = 0, s2 = 0;
+    for (int ky = 0; ky <= 2 * R; ++ky) {
+        const int m = pmb::clampi(i + ky - R, 0, H - 1);
+        const uint8_t* row = in + static_cast<int64_t>(H - 1 - m) * 3 * W;
+        for (int kx = 0; kx <= 2 * R; ++kx) {
+            const int n = pmb::clampi(j + kx - R, 0, W - 1);
+            const int f = pf.f[ky][kx];
+            s0 += row[3 * n + 2] * f;
+            s1 += row[3 * n + 1] * f;
+            s2 += row[3 * n + 0] * f;
+        }
+    }
+    uint8_t* o = out + (static_cast<int64_t>(i) * W + j) * 3;
+    if (MODE == PMB_IMGF_WRAP) {
+        o[0] = static_cast<uint8_t>(s0);
+        o[1] = static_cast<uint8_t>(s1);
+        o[2] = static_cast<uint8_t>(s2);
+    } else {
+        o[0] = static_cast<uint8_t>(min(max(s0, 0), 255));
+        o[1] = static_cast<uint8_t>(min(max(s1, 0), 255));
+        o[2] = static_cast<uint8_t>(min(max(s2, 0), 255));
+    }
+}
+
+// ---------------------------------------------------------------------------
+int validate_item(const pmb_imgf_item& it, int R, int idx) {
+    PMB_CHECK_ARG(it.in && it.out, "item %d: null pointer", idx);
+    PMB_CHECK_ARG(it.width > 0 && it.height > 0, "item %d: bad image size %dx%d", idx, it.width,
+                  it.height);
+    PMB_CHECK_ARG(0 <= it.r0 && it.r0 <= it.r1 && it.r1 <= it.height && 0 <= it.c0 &&
+                      it.c0 <= it.c1 && it.c1 <= it.width,
+                  "item %d: rectangle [%d,%d)x[%d,%d) outside %dx%d image", idx, it.r0, it.r1,
+                  it.c0, it.c1, it.width, it.height);
+    if (it.r0 == it.r1 || it.c0 == it.c1) return PMB_SUCCESS;
+    const int mhi = std::min(it.height - 1, it.r1 - 1 + R);
+    const int clo = std::max(0, it.c0 - R), chi = std::min(it.width - 1, it.c1 - 1 + R);
+    PMB_CHECK_ARG(it.in_row0 >= 0 && it.in_row0 <= it.height - 1 - mhi && it.in_col0 >= 0 &&
+                      it.in_col0 <= clo,
+                  "item %d: input view origin (%d,%d) does not cover the subscription", idx,
+                  it.in_row0, it.in_col0);
+    PMB_CHECK_ARG(it.in_pitch >= 3LL * (chi - it.in_col0 + 1), "item %d: input pitch too small",
+                  idx);
+    PMB_CHECK_ARG(it.out_row0 >= 0 && it.out_row0 <= it.r0 && it.out_col0 >= 0 &&
+                      it.out_col0 <= it.c0,
+                  "item %d: output view origin does not cover the rectangle", idx);
+    PMB_CHECK_ARG(it.out_pitch >= 3LL * (it.c1 - it.out_col0), "item %d: output pitch too small",
+                  idx);
+    return PMB_SUCCESS;
+}
+
+template <int R, int MODE, int MAXI>
+int launch_t(const pmb_imgf_item* items, int n, const int8_t* filter, cudaStream_t s) {
+    using G = Geo<R>;
+    ImgfParams<R, MAXI> p;
+    for (int ky = 0; ky < G::KD; ++ky)
+        for (int k = 0; k < 4; ++k)
+            for (int w = 0; w < G::NW; ++w) {
+                uint32_t word = 0;
+                for (int b = 0; b < 4; ++b) {
+                    const int kx = 4 * w + b - G::OFF - k;
+                    if (kx >= 0 && kx < G::KD)
+                        word |= static_cast<uint32_t>(
+                                    static_cast<uint8_t>(filter[ky * PMB_IMGF_MAX_FILTER_DIM + kx]))
+                                << (8 * b);
+                }
+                p.pat[ky][k][w] = word;
+            }
+    int64_t total = 0;
+    int m = 0;
+    for (int i = 0; i < n; ++i) {
+        const pmb_imgf_item& it = items[i];
+        if (it.r0 == it.r1 || it.c0 == it.c1) continue;
+        const int txs = (it.c1 - it.c0 + kTW - 1) / kTW;
+        const int tys = (it.r1 - it.r0 + kTH - 1) / kTH;
+        p.items[m] = it;
+        p.tiles_x[m] = txs;
+        p.tile_start[m] = static_cast<int>(total);
+        total += static_cast<int64_t>(txs) * tys;
+        ++m;
+    }
+    if (m == 0) return PMB_SUCCESS;
+    if (total > 0x7fffffffLL) return pmb::fail(PMB_BEYOND_LIMITS, "too many tiles: %lld", (long long)total);
+    p.n_items = m;
+    p.tile_start[m] = static_cast<int>(total);
+    imgf_kernel<R, MODE, MAXI><<<static_cast<unsigned>(total), kThreads, 0, s>>>(p);
+    PMB_CUDA_TRY(cudaGetLastError());
+    return PMB_SUCCESS;
+}
+
+template <int R, int MAXI>
+int launch_mode(const pmb_imgf_item* items, int n, const int8_t* filter, int mode, cudaStream_t s) {
+    return mode == PMB_IMGF_WRAP ? launch_t<R, PMB_IMGF_WRAP, MAXI>(items, n, filter, s)
+                                 : launch_t<R, PMB_IMGF_CLAMP, MAXI>(items, n, filter, s);
+}
+
+template <int MAXI>
+int launch_radius(const pmb_imgf_item* items, int n, const int8_t* filter, int R, int mode,
+                  cudaStream_t s) {
+    switch (R) {
+#define PMB_IMGF_CASE(r) \
+    case r: return launch_mode<r, MAXI>(items, n, filter, mode, s);
+        PMB_IMGF_CASE(1) PMB_IMGF_CASE(2) PMB_IMGF_CASE(3) PMB_IMGF_CASE(4) PMB_IMGF_CASE(5)
+        PMB_IMGF_CASE(6) PMB_IMGF_CASE(7) PMB_IMGF_CASE(8) PMB_IMGF_CASE(9) PMB_IMGF_CASE(10)
+        PMB_IMGF_CASE(11) PMB_IMGF_CASE(12) PMB_IMGF_CASE(13) PMB_IMGF_CASE(14) PMB_IMGF_CASE(15)
+#undef PMB_IMGF_CASE
+        default: return pmb::fail(PMB_INVALID_INDEX, "filter radius %d outside [1,%d]", R, PMB_IMGF_MAX_RADIUS);
+    }
+}
+
+}  // namespace
+
+extern "C" int pmb_image_filter(const pmb_imgf_item* items, int n_items, const int8_t* filter,
+                                int radius, int mode, void* stream) {
+    PMB_CHECK_ARG(items && filter, "null items/filter");
+    PMB_CHECK_ARG(n_items >= 1 && n_items <= PMB_IMGF_MAX_ITEMS, "n_items %d outside [1,%d]",
+                  n_items, PMB_IMGF_MAX_ITEMS);
+    PMB_CHECK_ARG(radius >= 1 && radius <= PMB_IMGF_MAX_RADIUS, "filter radius %d outside [1,%d]",
+                  radius, PMB_IMGF_MAX_RADIUS);
+    PMB_CHECK_ARG(mode == PMB_IMGF_WRAP || mode == PMB_IMGF_CLAMP, "bad mode %d", mode);
+    for (int i = 0; i < n_items; ++i) {
+        const int st = validate_item(items[i], radius, i);
+        if (st != PMB_SUCCESS) return st;
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    return n_items <= 8 ? launch_radius<8>(items, n_items, filter, radius, mode, s)
+                        : launch_radius<PMB_IMGF_MAX_ITEMS>(items, n_items, filter, radius, mode, s);
+}
+
+extern "C" int pmb_image_filter_full(const uint8_t* d_in, uint8_t* d_out, int width, int height,
+                                     const int8_t* filter, int radius, int mode, void* stream) {
+    pmb_imgf_item it;
+    it.in = d_in;
+    it.out = d_out;
+    it.in_pitch = it.out_pitch = 3LL * width;
+    it.width = width;
+    it.height = height;
+    it.in_row0 = it.in_col0 = it.out_row0 = it.out_col0 = 0;
+    it.r0 = 0;
+    it.r1 = height;
+    it.c0 = 0;
+    it.c1 = width;
+    return pmb_image_filter(&it, 1, filter, radius, mode, stream);
+}
+
+extern "C" int pmb_image_filter_plain(const uint8_t* d_in, uint8_t* d_out, int width, int height,
+                                      const int8_t* filter, int radius, int mode, void* stream) {
+    PMB_CHECK_ARG(d_in && d_out && filter, "null pointer");
+    PMB_CHECK_ARG(width > 0 && height > 0, "bad image size");
+    PMB_CHECK_ARG(radius >= 1 && radius <= PMB_IMGF_MAX_RADIUS, "bad radius %d", radius);
+    PMB_CHECK_ARG(mode == PMB_IMGF_WRAP || mode == PMB_IMGF_CLAMP, "bad mode %d", mode);
+    PlainFilter pf;
+    for (int i = 0; i < PMB_IMGF_MAX_FILTER_DIM * PMB_IMGF_MAX_FILTER_DIM; ++i)
+        pf.f[i / PMB_IMGF_MAX_FILTER_DIM][i % PMB_IMGF_MAX_FILTER_DIM] = filter[i];
+    dim3 block(32, 8);
+    dim3 grid((width + 31) / 32, (height + 7) / 8);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (mode == PMB_IMGF_WRAP)
+        imgf_plain_kernel<PMB_IMGF_WRAP><<<grid, block, 0, s>>>(d_in, d_out, width, height, radius, pf);
+    else
+        imgf_plain_kernel<PMB_IMGF_CLAMP><<<grid, block, 0, s>>>(d_in, d_out, width, height, radius, pf);
+    PMB_CUDA_TRY(cudaGetLastError());
+    return PMB_SUCCESS;
+}

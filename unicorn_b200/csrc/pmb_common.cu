@@ -1,0 +1,41 @@
+// Library-wide C ABI entry points (version, last error, device check) and the
+// error plumbing behind them.
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+#include "pmb_common.cuh"
+
+namespace pmb {
+
+static thread_local char t_last_error[1024] = {0};
+
+int fail(int status, const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(t_last_error, sizeof(t_last_error), fmt, ap);
+    va_end(ap);
+    return status;
+}
+
+int cuda_fail(cudaError_t err, const char* what) {
+    return fail(PMB_GRAPHICS_CARD_ERROR, "%s failed: %s (%d)", what, cudaGetErrorString(err),
+                static_cast<int>(err));
+}
+
+void clear_error() { t_last_error[0] = 0; }
+
+}  // namespace pmb
+
+extern "C" const char* pmb_last_error(void) { return pmb::t_last_error; }
+
+extern "C" const char* pmb_version(void) { return "1_0_0"; }
+
+extern "C" int pmb_device_supported(int dev) {
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return prop.major == 10 && prop.minor == 0 ? 1 : 0;
+}
