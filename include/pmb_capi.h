@@ -97,7 +97,7 @@ int pmb_image_filter(const pmb_imgf_item* items, int n_items,
                      const int8_t* filter, int radius, int mode, void* stream);
 
 /* Whole-image convenience form: one item covering the full image with
- * NATURAL views (in_pitch = out_pitch = 3W); needs no scratch. */
+ * NATURAL views (in_pitch = out_pitch = 3W). */
 int pmb_image_filter_full(const uint8_t* d_in, uint8_t* d_out, int width, int height,
                           const int8_t* filter, int radius, int mode, void* stream);
 
@@ -106,6 +106,47 @@ int pmb_image_filter_full(const uint8_t* d_in, uint8_t* d_out, int width, int he
  * one-task-at-a-time baseline the stencil kernel is compared with. */
 int pmb_image_filter_plain(const uint8_t* d_in, uint8_t* d_out, int width, int height,
                            const int8_t* filter, int radius, int mode, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* prefixSum: inclusive scan                                                */
+/* ------------------------------------------------------------------------ */
+
+/* Bytes of device scratch pmb_inclusive_scan_u32_u64 needs for n elements
+ * (a 256-byte header plus 8 bytes per 4096-element tile). */
+size_t pmb_scan_scratch_bytes(size_t n);
+
+/* out[i] = in[0] + ... + in[i] with 64-bit sums, n <= 2^30, one launch on
+ * `stream` (plus a memset of the scratch).  d_in, d_out and d_scratch are
+ * device pointers, 16-byte aligned.  Replaces prefixSum_cudaLaunchFunc /
+ * prefixSum_cuda / elemAdd_cuda and the host scan of subtask totals
+ * (testSuite/prefixSum/source/code/src/prefixSumCUDA.cu:68-267,
+ * prefixSum.cpp:189-294); result equals serialPrefixSum (prefixSum.cpp:47-53)
+ * widened to uint64. */
+int pmb_inclusive_scan_u32_u64(const uint32_t* d_in, uint64_t* d_out, size_t n, void* d_scratch,
+                               size_t scratch_bytes, void* stream);
+
+/* Copy the error word of a scan/sort scratch buffer to the host (synchronous).
+ * 0 = clean; 1 = a look-back wait hit its poll limit (the result is then
+ * not trustworthy).  Replaces nothing in the reference (its kernels never wait
+ * on one another). */
+int pmb_scratch_error(const void* d_scratch, uint32_t* error_out);
+
+/* ------------------------------------------------------------------------ */
+/* radixSort: stable LSD sort of uint32 keys                                */
+/* ------------------------------------------------------------------------ */
+
+/* Bytes of device scratch pmb_radix_sort_u32 needs (digits of 4 or 8 bits). */
+size_t pmb_radix_sort_scratch_bytes(size_t n, int bits_per_pass);
+
+/* Stable sort of d_keys[0..n) on bits [begin_bit, end_bit) (a multiple of
+ * bits_per_pass, which is 4 or 8), result left in d_keys; d_alt is a second
+ * device buffer of n keys.  n < 2^30; keys and scratch 16-byte aligned.  Each
+ * pass is one stable counting-sort round: one round of radixSort_cpu +
+ * radixSortDataRedistribution over all subtasks
+ * (testSuite/radixSort/source/code/src/radixSort.cpp:55-69, :136-162;
+ * the reference's GPU callback radixSort.cu:39-42 is an empty stub). */
+int pmb_radix_sort_u32(uint32_t* d_keys, uint32_t* d_alt, size_t n, int begin_bit, int end_bit,
+                       int bits_per_pass, void* d_scratch, size_t scratch_bytes, void* stream);
 
 #ifdef __cplusplus
 }

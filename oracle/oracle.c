@@ -98,3 +98,48 @@ void orc_image_filter(const uint8_t* in, uint8_t* out, int W, int H, int R, cons
     struct imgf_args a = {in, out, W, H, R, filter, mode, r0, c0, c1};
     orc_parallel_for(r1 - r0, imgf_rows, &a);
 }
+
+/*
+ * Inclusive prefix sum, uint32 in -> uint64 out.  Follows serialPrefixSum,
+ * testSuite/prefixSum/source/code/src/prefixSum.cpp:47-53 (out[0] = in[0];
+ * out[i] = in[i] + out[i-1]) with the sum widened to 64 bits.
+ */
+void orc_prefix_sum_u32_u64(const uint32_t* in, uint64_t* out, size_t n) {
+    if (n == 0) return;
+    out[0] = in[0];
+    for (size_t i = 1; i < n; ++i) out[i] = (uint64_t)in[i] + out[i - 1];
+}
+
+/*
+ * One stable counting-sort round on the digit (key >> shift) & (2^bits - 1).
+ * Follows serialRadixSortRound, testSuite/radixSort/source/code/src/
+ * radixSort.cpp:55-69: count the bins, turn counts into inclusive positions,
+ * then place keys walking the input backwards (which keeps equal digits in
+ * input order).  `bins_out` (may be NULL) receives the per-digit counts, as the
+ * reference hands them to its redistribution callback.
+ */
+void orc_radix_round_u32(const uint32_t* in, uint32_t* out, size_t n, int shift, int bits, uint32_t* bins_out) {
+    const uint32_t nb = 1u << bits, mask = nb - 1;
+    size_t* bins = (size_t*)calloc(nb, sizeof(size_t));
+    for (size_t i = 0; i < n; ++i) ++bins[(in[i] >> shift) & mask];
+    if (bins_out)
+        for (uint32_t k = 0; k < nb; ++k) bins_out[k] = (uint32_t)bins[k];
+    for (uint32_t k = 1; k < nb; ++k) bins[k] += bins[k - 1];
+    for (size_t j = n; j-- > 0;) out[--bins[(in[j] >> shift) & mask]] = in[j];
+    free(bins);
+}
+
+/*
+ * Full LSD sort: rounds over digits [begin_bit, end_bit) of width `bits`,
+ * ping-ponging through `tmp` (serialLsbRadixSort, radixSort.cpp:71-114).
+ * The result is left in `keys`.
+ */
+void orc_radix_sort_u32(uint32_t* keys, uint32_t* tmp, size_t n, int begin_bit, int end_bit, int bits) {
+    uint32_t* a = keys;
+    uint32_t* b = tmp;
+    for (int s = begin_bit; s < end_bit; s += bits) {
+        orc_radix_round_u32(a, b, n, s, bits, NULL);
+        uint32_t* t = a; a = b; b = t;
+    }
+    if (a != keys) memcpy(keys, a, n * sizeof(uint32_t));
+}

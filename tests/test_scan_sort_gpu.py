@@ -1,0 +1,113 @@
+"""GPU parity tests of the single-pass scan and the onesweep radix sort.
+
+Integer results must be bit-exact against the oracles (restatements of the
+reference's serialPrefixSum / serialRadixSortRound); every run also checks
+that no look-back wait gave up (scratch error word 0).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from test_scan_sort_oracle import orc_round, orc_scan
+
+pytestmark = pytest.mark.gpu
+
+
+def keys(n, seed, kind="uniform"):
+    rng = np.random.default_rng(seed)
+    if kind == "uniform":
+        return rng.integers(0, 2**32, size=n, dtype=np.uint64).astype(np.uint32)
+    if kind == "equal":
+        return np.full(n, 0xDEADBEEF, np.uint32)
+    if kind == "sorted":
+        return np.sort(keys(n, seed))
+    if kind == "reverse":
+        return np.sort(keys(n, seed))[::-1].copy()
+    if kind == "few":
+        return rng.integers(0, 3, size=n, dtype=np.uint32) << np.uint32(24)
+    raise ValueError(kind)
+
+
+def to_dev(cuda, x):
+    return cuda.from_numpy(x.view(np.int32)).cuda()
+
+
+@pytest.mark.parametrize("n", [1, 3, 4, 5, 4095, 4096, 4097, 8192 + 17, 1 << 20, (1 << 22) + 3])
+def test_scan_matches_oracle(cuda, oracle, n):
+    from unicorn_b200 import ops
+
+    x = keys(n, n)
+    out, scratch = ops.inclusive_scan_u32_u64(to_dev(cuda, x))
+    cuda.cuda.synchronize()
+    got = out.cpu().numpy().view(np.uint64)
+    assert np.array_equal(got, orc_scan(oracle, x))
+    assert ops.scratch_error(scratch) == 0
+
+
+def test_scan_repeated_calls_reuse_scratch(cuda):
+    from unicorn_b200 import ops
+
+    x = keys(100003, 1)
+    d = to_dev(cuda, x)
+    out, scratch = ops.inclusive_scan_u32_u64(d)
+    for _ in range(3):
+        out2, scratch = ops.inclusive_scan_u32_u64(d, scratch=scratch)
+    cuda.cuda.synchronize()
+    assert np.array_equal(out2.cpu().numpy().view(np.uint64), np.cumsum(x.astype(np.uint64)))
+
+
+@pytest.mark.parametrize("bits", [8, 4])
+@pytest.mark.parametrize("n", [1, 7, 4096, 4097, 100000, (1 << 21) + 5])
+def test_radix_sort_full(cuda, bits, n):
+    from unicorn_b200 import ops
+
+    x = keys(n, n + bits)
+    d = to_dev(cuda, x)
+    _, scratch = ops.radix_sort_u32(d, 0, 32, bits)
+    cuda.cuda.synchronize()
+    assert np.array_equal(d.cpu().numpy().view(np.uint32), np.sort(x))
+    assert ops.scratch_error(scratch) == 0
+
+
+@pytest.mark.parametrize("kind", ["equal", "sorted", "reverse", "few"])
+def test_radix_sort_edge_distributions(cuda, kind):
+    from unicorn_b200 import ops
+
+    x = keys(300001, 5, kind)
+    d = to_dev(cuda, x)
+    ops.radix_sort_u32(d)
+    cuda.cuda.synchronize()
+    assert np.array_equal(d.cpu().numpy().view(np.uint32), np.sort(x))
+
+
+@pytest.mark.parametrize("bits", [4, 8])
+def test_single_round_matches_reference_round(cuda, oracle, bits):
+    """One pass == one reference round (per-subtask counting sort + ordered
+    redistribution), including the stable order of equal digits."""
+    from unicorn_b200 import ops
+
+    x = keys(123457, 77)
+    for shift in range(0, 32, bits):
+        d = to_dev(cuda, x)
+        ops.radix_sort_u32(d, shift, shift + bits, bits)
+        cuda.cuda.synchronize()
+        expect, _ = orc_round(oracle, x, shift, bits)
+        assert np.array_equal(d.cpu().numpy().view(np.uint32), expect), shift
+
+
+def test_sort_then_scan_full_configuration(cuda):
+    """2^28 uint32 keys (seed 2): 8-bit LSD sort, then inclusive uint64 scan."""
+    from unicorn_b200 import ops
+
+    n = 1 << 28
+    x = keys(n, 2)
+    d = to_dev(cuda, x)
+    _, s1 = ops.radix_sort_u32(d)
+    out, s2 = ops.inclusive_scan_u32_u64(d)
+    cuda.cuda.synchronize()
+    ref_sorted = np.sort(x)
+    assert np.array_equal(d.cpu().numpy().view(np.uint32), ref_sorted)
+    del x
+    assert np.array_equal(out.cpu().numpy().view(np.uint64), np.cumsum(ref_sorted, dtype=np.uint64))
+    assert ops.scratch_error(s1) == 0 and ops.scratch_error(s2) == 0

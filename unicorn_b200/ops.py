@@ -71,3 +71,49 @@ def image_filter_plain(d_in, d_out, width: int, height: int, filt: np.ndarray,
     capi.check(capi.lib().pmb_image_filter_plain(_dev_ptr(d_in), _dev_ptr(d_out), width, height,
                                                  f.ctypes.data_as(ctypes.c_void_p), R, mode,
                                                  _stream_ptr(stream)))
+
+
+def _scratch(nbytes: int):
+    import torch
+
+    return torch.empty(max(int(nbytes), 16), dtype=torch.uint8, device="cuda")
+
+
+def scratch_error(scratch) -> int:
+    err = ctypes.c_uint32(0)
+    capi.check(capi.lib().pmb_scratch_error(_dev_ptr(scratch), ctypes.byref(err)))
+    return int(err.value)
+
+
+def inclusive_scan_u32_u64(d_in, d_out=None, scratch=None, stream=None):
+    """Inclusive 64-bit prefix sum of a uint32 CUDA tensor (int32/uint32 storage).
+
+    Returns (d_out, scratch); d_out holds the 64-bit sums in int64 storage.
+    """
+    import torch
+
+    n = d_in.numel()
+    if d_out is None:
+        d_out = torch.empty(n, dtype=torch.int64, device=d_in.device)
+    need = capi.lib().pmb_scan_scratch_bytes(n)
+    if scratch is None or scratch.numel() < need:
+        scratch = _scratch(need)
+    capi.check(capi.lib().pmb_inclusive_scan_u32_u64(_dev_ptr(d_in), _dev_ptr(d_out), n, _dev_ptr(scratch),
+                                                     scratch.numel(), _stream_ptr(stream)))
+    return d_out, scratch
+
+
+def radix_sort_u32(d_keys, begin_bit: int = 0, end_bit: int = 32, bits: int = 8, d_alt=None, scratch=None,
+                   stream=None):
+    """Stable in-place LSD sort of a uint32 CUDA tensor (int32/uint32 storage)."""
+    import torch
+
+    n = d_keys.numel()
+    if d_alt is None:
+        d_alt = torch.empty_like(d_keys)
+    need = capi.lib().pmb_radix_sort_scratch_bytes(n, bits)
+    if scratch is None or scratch.numel() < need:
+        scratch = _scratch(need)
+    capi.check(capi.lib().pmb_radix_sort_u32(_dev_ptr(d_keys), _dev_ptr(d_alt), n, begin_bit, end_bit, bits,
+                                             _dev_ptr(scratch), scratch.numel(), _stream_ptr(stream)))
+    return d_keys, scratch
