@@ -148,6 +148,105 @@ size_t pmb_radix_sort_scratch_bytes(size_t n, int bits_per_pass);
 int pmb_radix_sort_u32(uint32_t* d_keys, uint32_t* d_alt, size_t n, int begin_bit, int end_bit,
                        int bits_per_pass, void* d_scratch, size_t scratch_bytes, void* stream);
 
+/* Stable key-value variant of pmb_radix_sort_u32: d_vals[] (n uint32 values)
+ * moves with its key; d_vals_alt is the values' second buffer. */
+int pmb_radix_sort_pairs_u32(uint32_t* d_keys, uint32_t* d_alt, uint32_t* d_vals, uint32_t* d_vals_alt,
+                             size_t n, int begin_bit, int end_bit, int bits_per_pass, void* d_scratch,
+                             size_t scratch_bytes, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* pageRank: pull over CSR in-edges                                         */
+/* ------------------------------------------------------------------------ */
+
+/* Seeded R-MAT edge list (Chakrabarti et al., SDM 2004): n_edges edges over
+ * 2^scale vertices, quadrant probabilities a, b, c (d = 1-a-b-c); duplicates
+ * and self-loops kept; edge i depends only on (seed, i).  Stands in for the
+ * reference's web-dump input, which is generated offline
+ * (testSuite/pageRank/scripts/webGenerator.pl) and not shipped. */
+int pmb_rmat_edges(uint64_t seed, int scale, uint64_t n_edges, double a, double b, double c,
+                   uint32_t* d_src, uint32_t* d_dst, void* stream);
+
+/* CSR by destination: row_ptr[N+1], col[E] = source of each in-edge (edges
+ * of one destination keep their input order), out_degree[N].  Scratch:
+ * pmb_csr_scratch_bytes; edges naming a vertex >= n_vertices are dropped and
+ * set bit 2 of the scratch error word (pmb_scratch_error).  Replaces the padded fixed-stride out-link lists the
+ * reference reads (pageRank.cpp:53-143). */
+size_t pmb_csr_scratch_bytes(uint32_t n_vertices, uint64_t n_edges);
+int pmb_csr_by_destination(const uint32_t* d_src, const uint32_t* d_dst, uint32_t n_vertices, uint64_t n_edges,
+                           uint32_t* d_row_ptr, uint32_t* d_col, uint32_t* d_out_degree, void* d_scratch,
+                           size_t scratch_bytes, void* stream);
+
+/* Edge-slice partition of a CSR graph (once per graph). */
+size_t pmb_pagerank_plan_bytes(uint32_t n_vertices, uint64_t n_edges);
+int pmb_pagerank_plan(const uint32_t* d_row_ptr, uint32_t n_vertices, uint64_t n_edges, void* d_plan,
+                      size_t plan_bytes, void* stream);
+
+/* `iterations` PageRank steps r'[v] = sum_{u->v} damping*r[u]/outdeg(u) (no
+ * teleport), fp32, starting from d_rank_in, final ranks in d_rank_out.
+ * d_work: pmb_pagerank_work_bytes.  Replaces pageRank_cudaLaunchFunc /
+ * pageRank_cuda / zeroInit (testSuite/pageRank/source/code/src/
+ * pageRankCUDA.cu:46-164) plus the host REDUCE_ADD of the subtasks' rank
+ * arrays (pageRank.cpp:554-555); equals pageRank_cpu (:336-378) up to fp32
+ * summation order.  Each rank has a single writer: results are deterministic. */
+size_t pmb_pagerank_work_bytes(uint32_t n_vertices, uint64_t n_edges);
+int pmb_pagerank(const uint32_t* d_row_ptr, const uint32_t* d_col, const uint32_t* d_out_degree, uint32_t n_vertices,
+                 uint64_t n_edges, const void* d_plan, float damping, int iterations, const float* d_rank_in,
+                 float* d_rank_out, void* d_work, size_t work_bytes, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* matrixMultiply / luDecomposition: fp32 GEMM on tcgen05 tensor cores       */
+/* ------------------------------------------------------------------------ */
+
+/* Device workspace (256-byte aligned) pmb_sgemm_bf16x3 needs for M x N x K. */
+size_t pmb_gemm_workspace_bytes(int M, int N, int K);
+
+/* Row-major C = alpha*A*B + beta*C with fp32 operands (A: M x K, lda; B:
+ * K x N, ldb; C: M x N, ldc; all device pointers), computed as a BF16x3
+ * split product (A = Ahi + Alo, B = Bhi + Blo; Ahi*Bhi + Ahi*Blo + Alo*Bhi)
+ * with FP32 accumulation in tensor memory.  One split launch pair and one
+ * GEMM launch on `stream`.  Word 1 of the workspace is an error word
+ * (pmb_scratch_error): value 4 = a pipeline wait expired.  Replaces the
+ * cublasSgemm calls of matrixMultiply_cudaLaunchFunc
+ * (testSuite/matrixMultiplyBlas/source/code/src/matrixMultiplyBlasCUDA.cu:54-77)
+ * and diagComp_cudaLaunchFunc (luDecompositionCUDA.cu:153-193); for column-
+ * major data call it with the operands swapped (C^T = B^T A^T). */
+int pmb_sgemm_bf16x3(int M, int N, int K, float alpha, const float* A, int64_t lda, const float* B, int64_t ldb,
+                     float beta, float* C, int64_t ldc, void* workspace, size_t ws_bytes, void* stream);
+
+/* Plain GPU form of the same product: FP32 SIMT, 64 x 64 shared-memory
+ * tiles, no tensor cores (the one-task-at-a-time FP32 baseline). */
+int pmb_sgemm_plain(int M, int N, int K, float alpha, const float* A, int64_t lda, const float* B, int64_t ldb,
+                    float beta, float* C, int64_t ldc, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* luDecomposition: blocked unpivoted LU (Crout form), column-major          */
+/* ------------------------------------------------------------------------ */
+
+/* Device workspace (256-byte aligned) for an n x n LU with block size nb. */
+size_t pmb_lu_workspace_bytes(int n, int nb);
+
+/* In-place LU of the column-major n x n fp32 matrix d_A (lda >= n) in the
+ * reference's form: L lower triangular WITH the pivots on its diagonal, U unit
+ * upper triangular, A = L*U, no row exchanges
+ * (testSuite/luDecomposition/source/code/src/luDecomposition.cpp:116-125).
+ * Block size nb in [1,128].  Replaces the three task stages
+ * luDecomposition_cudaLaunchFunc / horizVertComp_cudaLaunchFunc /
+ * diagComp_cudaLaunchFunc (luDecompositionCUDA.cu:66-193): the nb x nb
+ * diagonal blocks are factored (and inverted) in FP64, panels and trailing
+ * updates run as BF16x3 tensor-core GEMMs.  Word 1 of the workspace gets flags
+ * (pmb_scratch_error): 1 = partial pivoting (FP64 comparison) would have
+ * exchanged rows in some column, 2 = a zero pivot. */
+int pmb_lu_decompose(float* d_A, int n, int64_t lda, int nb, void* d_workspace, size_t ws_bytes, void* stream);
+
+/* Same factorization with FP32 SIMT GEMMs (the plain one-task-at-a-time form). */
+int pmb_lu_decompose_plain(float* d_A, int n, int64_t lda, int nb, void* d_workspace, size_t ws_bytes,
+                           void* stream);
+
+/* FP64 residual: d_sums[0] = ||A0 - L*U||_F^2, d_sums[1] = ||A0||_F^2 (two
+ * device doubles), L and U read from the packed factorization d_LU. */
+int pmb_lu_residual_f64(const float* d_A0, int64_t lda0, const float* d_LU, int64_t ldlu, int n, double* d_sums,
+                        void* stream);
+
 #ifdef __cplusplus
 }
 #endif

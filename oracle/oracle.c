@@ -143,3 +143,82 @@ void orc_radix_sort_u32(uint32_t* keys, uint32_t* tmp, size_t n, int begin_bit, 
     }
     if (a != keys) memcpy(keys, a, n * sizeof(uint32_t));
 }
+
+/*
+ * PageRank, FP64, pulled over CSR in-edges (row_ptr[N+1], col[E] = sources).
+ * The formula of serialPageRank / pageRank_cpu (testSuite/pageRank/source/
+ * code/src/pageRank.cpp:237-276, :336-378): r'[v] = sum over u->v of
+ * d * r[u] / outdeg(u), no teleport term, pages without out-links give
+ * nothing.  Everything is carried in double; `rank_init` is the fp32 initial
+ * vector, `out` receives the ranks after `iters` iterations.
+ */
+struct pr_args {
+    const uint32_t* row_ptr; const uint32_t* col; const double* contrib; double* next; long n;
+};
+static void pr_rows(long lo, long hi, void* p) {
+    const struct pr_args* a = (const struct pr_args*)p;
+    for (long v = lo; v < hi; ++v) {
+        double s = 0.0;
+        for (uint32_t e = a->row_ptr[v]; e < a->row_ptr[v + 1]; ++e) s += a->contrib[a->col[e]];
+        a->next[v] = s;
+    }
+}
+void orc_pagerank_f64(const uint32_t* row_ptr, const uint32_t* col, const uint32_t* outdeg, uint32_t n, int iters,
+                      double damping, const float* rank_init, double* out) {
+    double* r = (double*)malloc(sizeof(double) * n);
+    double* c = (double*)malloc(sizeof(double) * n);
+    for (uint32_t v = 0; v < n; ++v) r[v] = rank_init[v];
+    for (int it = 0; it < iters; ++it) {
+        for (uint32_t v = 0; v < n; ++v) c[v] = outdeg[v] ? damping * r[v] / (double)outdeg[v] : 0.0;
+        struct pr_args a = {row_ptr, col, c, r, (long)n};
+        orc_parallel_for(n, pr_rows, &a);
+    }
+    memcpy(out, r, sizeof(double) * n);
+    free(r);
+    free(c);
+}
+
+/*
+ * PageRank in fp32 with the reference's push order: for each source page in
+ * ascending order, incr = (0.85f * r[u]) / (float)outdeg(u) is added to every
+ * target in edge order (pageRank.cpp:262-274 / :359-372).  `edge_src` must be
+ * sorted by source (stable in generation order within a source).
+ */
+void orc_pagerank_push_f32(const uint32_t* edge_src, const uint32_t* edge_dst, uint64_t n_edges, uint32_t n,
+                           const uint32_t* outdeg, int iters, float damping, const float* rank_init, float* out) {
+    float* r = (float*)malloc(sizeof(float) * n);
+    float* g = (float*)malloc(sizeof(float) * n);
+    memcpy(r, rank_init, sizeof(float) * n);
+    for (int it = 0; it < iters; ++it) {
+        memset(g, 0, sizeof(float) * n);
+        for (uint64_t e = 0; e < n_edges; ++e) {
+            const uint32_t u = edge_src[e];
+            const float incr = (float)(damping * r[u]) / (float)outdeg[u];
+            g[edge_dst[e]] += incr;
+        }
+        float* t = r; r = g; g = t;
+    }
+    memcpy(out, r, sizeof(float) * n);
+    free(r);
+    free(g);
+}
+
+/*
+ * Unpivoted Crout LU, column-major, in FP64.  Follows serialLUDecomposition,
+ * testSuite/luDecomposition/source/code/src/luDecomposition.cpp:116-125: for
+ * column i, the row to the right of the diagonal is scaled by 1/a_ii (cblas
+ * scal with stride ld) and the trailing block gets the rank-1 update
+ * a_rc -= a_ri * a_ic (cblas ger).  `a` (n x n, ld) is factored in place.
+ */
+void orc_lu_crout_f64(double* a, int n, long ld) {
+    for (int i = 0; i < n - 1; ++i) {
+        const double inv = 1.0 / a[i + (long)i * ld];
+        for (int c = i + 1; c < n; ++c) a[i + (long)c * ld] *= inv;
+        for (int c = i + 1; c < n; ++c) {
+            const double u = a[i + (long)c * ld];
+            double* col = a + (long)c * ld;
+            const double* li = a + (long)i * ld;
+            for (int r = i + 1; r < n; ++r) col[r] -= li[r] * u;
+        }
+    }
+}

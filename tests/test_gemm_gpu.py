@@ -1,0 +1,105 @@
+"""GPU tests of the tcgen05 BF16x3 GEMM and the plain FP32 SIMT GEMM.
+
+The FP64 oracle is numpy float64 matmul of the same fp32 inputs.  Bars:
+normwise ||C - C64||_F / ||C64||_F <= 1e-5 (the configuration's accuracy
+target) and elementwise |dC_ij| <= 2^-15 (|A||B|)_ij; the workspace error word
+must stay 0.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+NORM_TOL = 1e-5
+ELEM_TOL = 2.0 ** -15
+
+
+def mats(M, N, K, seed):
+    rng = np.random.default_rng(seed)
+    A = rng.uniform(-1, 1, (M, K)).astype(np.float32)
+    B = rng.uniform(-1, 1, (K, N)).astype(np.float32)
+    return A, B
+
+
+def errors(got, A, B, C0=None, alpha=1.0, beta=0.0):
+    ref = alpha * (A.astype(np.float64) @ B.astype(np.float64))
+    if C0 is not None and beta != 0.0:
+        ref += beta * C0.astype(np.float64)
+    scale = np.abs(A).astype(np.float64) @ np.abs(B).astype(np.float64)
+    norm = np.linalg.norm(got - ref) / max(np.linalg.norm(ref), 1e-300)
+    elem = np.max(np.abs(got - ref) / np.maximum(abs(alpha) * scale, 1e-30))
+    return norm, elem
+
+
+def run(cuda, A, B, C0=None, alpha=1.0, beta=0.0, plain=False):
+    from unicorn_b200 import ops
+
+    dA, dB = cuda.from_numpy(A).cuda(), cuda.from_numpy(B).cuda()
+    dC = cuda.from_numpy(C0).cuda() if C0 is not None else None
+    C, ws = ops.sgemm(dA, dB, dC, alpha, beta, plain=plain)
+    cuda.cuda.synchronize()
+    if ws is not None:
+        assert ops.scratch_error(ws) == 0
+    return C.cpu().numpy()
+
+
+@pytest.mark.parametrize("M,N,K", [(128, 256, 32), (256, 256, 1024), (1, 1, 1), (100, 300, 77), (129, 257, 33),
+                                   (300, 520, 640), (1024, 1024, 1024)])
+def test_bf16x3_matches_fp64(cuda, M, N, K):
+    A, B = mats(M, N, K, M + N + K)
+    norm, elem = errors(run(cuda, A, B), A, B)
+    assert norm <= NORM_TOL and elem <= ELEM_TOL, (norm, elem)
+
+
+def test_bf16x3_long_k(cuda):
+    A, B = mats(256, 512, 8192, 5)
+    norm, elem = errors(run(cuda, A, B), A, B)
+    assert norm <= NORM_TOL and elem <= ELEM_TOL, (norm, elem)
+
+
+@pytest.mark.parametrize("alpha,beta", [(-1.0, 1.0), (0.5, -2.0), (2.0, 0.0)])
+def test_alpha_beta_epilogue(cuda, alpha, beta):
+    M, N, K = 384, 512, 256
+    A, B = mats(M, N, K, 9)
+    C0 = np.random.default_rng(1).uniform(-1, 1, (M, N)).astype(np.float32)
+    norm, elem = errors(run(cuda, A, B, C0, alpha, beta), A, B, C0, alpha, beta)
+    assert norm <= NORM_TOL, norm
+
+
+def test_submatrix_views_with_leading_dimensions(cuda):
+    """A row block of A and a column block of B inside larger matrices (the
+    NATURAL view of a matrixMultiply subtask: lda = ldb = ldc = n)."""
+    from unicorn_b200 import ops
+
+    n, blk = 1024, 256
+    A, B = mats(n, n, n, 3)
+    dA, dB = cuda.from_numpy(A).cuda(), cuda.from_numpy(B).cuda()
+    dC = cuda.zeros(n, n, device="cuda")
+    for row in range(n // blk):
+        for col in range(n // blk):
+            ops.sgemm(dA[row * blk:(row + 1) * blk], dB[:, col * blk:(col + 1) * blk],
+                      dC[row * blk:(row + 1) * blk, col * blk:(col + 1) * blk])
+    cuda.cuda.synchronize()
+    norm, elem = errors(dC.cpu().numpy(), A, B)
+    assert norm <= NORM_TOL and elem <= ELEM_TOL, (norm, elem)
+
+
+@pytest.mark.parametrize("M,N,K", [(64, 64, 64), (100, 300, 77), (512, 512, 512)])
+def test_plain_sgemm(cuda, M, N, K):
+    A, B = mats(M, N, K, 2)
+    norm, _ = errors(run(cuda, A, B, plain=True), A, B)
+    assert norm <= NORM_TOL, norm
+
+
+def test_k_zero_scales_c(cuda):
+    from unicorn_b200 import ops
+
+    C0 = np.ones((4, 5), np.float32)
+    dA = cuda.zeros(4, 0, device="cuda")
+    dB = cuda.zeros(0, 5, device="cuda")
+    dC = cuda.from_numpy(C0).cuda()
+    ops.sgemm(dA, dB, dC, 1.0, 3.0)
+    cuda.cuda.synchronize()
+    assert np.allclose(dC.cpu().numpy(), 3.0)

@@ -1,0 +1,97 @@
+"""LU tests.  CPU: the FP64 Crout oracle (restating serialLUDecomposition)
+reconstructs A.  GPU: the blocked tensor-core LU and the plain FP32 form
+against that oracle (elementwise) and by FP64 residual ||A - LU||/||A||."""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import ptr
+
+
+def dd_matrix(n, seed):
+    """Diagonally dominant test matrix: U[-1,1] plus n on the diagonal."""
+    rng = np.random.default_rng(seed)
+    a = rng.uniform(-1, 1, (n, n)).astype(np.float32)
+    a[np.arange(n), np.arange(n)] += n
+    return a  # interpreted column-major: element (r, c) at a.T[r, c]
+
+
+def crout_f64(oracle, a_cm):
+    """a_cm: (n, n) array holding the column-major matrix (row index = column)."""
+    n = a_cm.shape[0]
+    x = np.ascontiguousarray(a_cm, dtype=np.float64)
+    oracle.orc_lu_crout_f64(ptr(x), n, ctypes.c_long(n))
+    return x
+
+
+def reconstruct(lu_cm):
+    lu = lu_cm.T.astype(np.float64)  # (row, col)
+    L = np.tril(lu)
+    U = np.triu(lu, 1) + np.eye(lu.shape[0])
+    return L @ U
+
+
+@pytest.mark.parametrize("n", [1, 2, 7, 64, 150])
+def test_oracle_reconstructs(oracle, n):
+    a = dd_matrix(n, n)
+    lu = crout_f64(oracle, a)
+    A = a.T.astype(np.float64)
+    assert np.linalg.norm(reconstruct(lu) - A) / np.linalg.norm(A) < 1e-13
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,nb", [(1, 128), (5, 4), (64, 32), (100, 64), (128, 128), (129, 128), (300, 64),
+                                  (512, 128), (1000, 96)])
+def test_gpu_lu_matches_oracle(cuda, oracle, n, nb):
+    from unicorn_b200 import ops
+
+    a = dd_matrix(n, 10 + n)
+    d = cuda.from_numpy(a.copy()).cuda()
+    d0 = cuda.from_numpy(a.copy()).cuda()
+    _, ws, flags = ops.lu_decompose(d, nb)
+    assert flags == 0
+    got = d.cpu().numpy()
+    ref = crout_f64(oracle, a)
+    assert np.allclose(got, ref, rtol=1e-4, atol=1e-5)
+    assert ops.lu_residual(d0, d) <= 1e-5
+
+
+@pytest.mark.gpu
+def test_gpu_lu_plain_form(cuda, oracle):
+    from unicorn_b200 import ops
+
+    n = 700
+    a = dd_matrix(n, 4)
+    d = cuda.from_numpy(a.copy()).cuda()
+    d0 = cuda.from_numpy(a.copy()).cuda()
+    ops.lu_decompose(d, 128, plain=True)
+    assert ops.lu_residual(d0, d) <= 1e-5
+    assert np.allclose(d.cpu().numpy(), crout_f64(oracle, a), rtol=1e-4, atol=1e-5)
+
+
+@pytest.mark.gpu
+def test_pivot_check_flags_non_dominant_matrix(cuda):
+    from unicorn_b200 import ops
+
+    rng = np.random.default_rng(0)
+    a = rng.uniform(-1, 1, (200, 200)).astype(np.float32)
+    a[np.arange(200), np.arange(200)] += 3.0  # not dominant enough: partial pivoting would swap
+    d = cuda.from_numpy(a).cuda()
+    _, _, flags = ops.lu_decompose(d, 64)
+    assert flags & 1
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [2048, 4096])
+def test_gpu_lu_large_residual(cuda, n):
+    from unicorn_b200 import ops
+
+    a = dd_matrix(n, n)
+    d = cuda.from_numpy(a.copy()).cuda()
+    d0 = cuda.from_numpy(a).cuda()
+    _, _, flags = ops.lu_decompose(d, 128)
+    assert flags == 0
+    assert ops.lu_residual(d0, d) <= 1e-5

@@ -66,6 +66,27 @@ _SIGS = {
     "pmb_scratch_error": (c_int, [c_void_p, ctypes.POINTER(ctypes.c_uint32)]),
     "pmb_radix_sort_scratch_bytes": (c_size_t, [c_size_t, c_int]),
     "pmb_radix_sort_u32": (c_int, [c_void_p, c_void_p, c_size_t, c_int, c_int, c_int, c_void_p, c_size_t, c_void_p]),
+    "pmb_radix_sort_pairs_u32": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_int, c_int, c_int,
+                                         c_void_p, c_size_t, c_void_p]),
+    "pmb_rmat_edges": (c_int, [ctypes.c_uint64, c_int, ctypes.c_uint64, ctypes.c_double, ctypes.c_double,
+                               ctypes.c_double, c_void_p, c_void_p, c_void_p]),
+    "pmb_csr_scratch_bytes": (c_size_t, [ctypes.c_uint32, ctypes.c_uint64]),
+    "pmb_csr_by_destination": (c_int, [c_void_p, c_void_p, ctypes.c_uint32, ctypes.c_uint64, c_void_p, c_void_p,
+                                       c_void_p, c_void_p, c_size_t, c_void_p]),
+    "pmb_pagerank_plan_bytes": (c_size_t, [ctypes.c_uint32, ctypes.c_uint64]),
+    "pmb_pagerank_plan": (c_int, [c_void_p, ctypes.c_uint32, ctypes.c_uint64, c_void_p, c_size_t, c_void_p]),
+    "pmb_pagerank_work_bytes": (c_size_t, [ctypes.c_uint32, ctypes.c_uint64]),
+    "pmb_gemm_workspace_bytes": (c_size_t, [c_int, c_int, c_int]),
+    "pmb_sgemm_bf16x3": (c_int, [c_int, c_int, c_int, ctypes.c_float, c_void_p, c_int64, c_void_p, c_int64,
+                                 ctypes.c_float, c_void_p, c_int64, c_void_p, c_size_t, c_void_p]),
+    "pmb_sgemm_plain": (c_int, [c_int, c_int, c_int, ctypes.c_float, c_void_p, c_int64, c_void_p, c_int64,
+                                ctypes.c_float, c_void_p, c_int64, c_void_p]),
+    "pmb_lu_workspace_bytes": (c_size_t, [c_int, c_int]),
+    "pmb_lu_decompose": (c_int, [c_void_p, c_int, c_int64, c_int, c_void_p, c_size_t, c_void_p]),
+    "pmb_lu_decompose_plain": (c_int, [c_void_p, c_int, c_int64, c_int, c_void_p, c_size_t, c_void_p]),
+    "pmb_lu_residual_f64": (c_int, [c_void_p, c_int64, c_void_p, c_int64, c_int, c_void_p, c_void_p]),
+    "pmb_pagerank": (c_int, [c_void_p, c_void_p, c_void_p, ctypes.c_uint32, ctypes.c_uint64, c_void_p,
+                             ctypes.c_float, c_int, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
 }
 
 _lib = None

@@ -1,0 +1,454 @@
+// matrixMultiply / luDecomposition GEMM for sm_100a: fp32 in, fp32 out,
+// computed as a BF16x3 split-precision product on the 5th-generation tensor
+// cores (tcgen05) with FP32 accumulation in tensor memory.
+//
+// Semantics (row-major): C = alpha * A * B + beta * C, A: M x K (lda),
+// B: K x N (ldb), C: M x N (ldc).  The reference reaches this through
+// cublasSgemm (testSuite/matrixMultiplyBlas/source/code/src/
+// matrixMultiplyBlasCUDA.cu:54-77, luDecompositionCUDA.cu:153-193) and
+// cblas_sgemm on the CPU (matrixMultiplyBlas.cpp:62-65).
+//
+// Split precision: x = hi + lo with hi = bf16(x) and lo = bf16(x - hi), so
+// A*B ~= Ahi*Bhi + Ahi*Blo + Alo*Bhi (the Alo*Blo term, ~2^-18 relative, is
+// dropped).  All three products accumulate into the same FP32 TMEM tile.
+//
+// Design: a split pass writes Ahi/Alo (M x Kp) and the transposed Bhi/Blo
+// (N x Kp) as K-major bf16.  The GEMM kernel owns a 128 x 256 output tile per
+// CTA and runs three warp roles:
+//   warp 0    TMA producer: one thread streams 32-deep K slices of the four
+//             operand tiles into a 4-stage shared-memory ring (SWIZZLE_64B),
+//             arming each stage's mbarrier with the expected byte count;
+//   warp 1    allocates 256 TMEM columns, then one thread issues the
+//             tcgen05.mma instructions (M=128, N=256, K=16, 3 per K step) and
+//             frees each stage back to the producer with tcgen05.commit;
+//   warps 2-5 epilogue: tcgen05.ld the accumulator (one row per thread),
+//             apply alpha/beta and store to C.
+// Every mbarrier wait is bounded: on expiry the kernel records an error in the
+// workspace header, skips the remaining work, waits (bounded) for its own
+// in-flight tensor-core work and frees its TMEM before returning.
+#include <cuda.h>
+#include <cuda_bf16.h>
+
+#include <mutex>
+
+#include "pmb_common.cuh"
+
+namespace {
+
+constexpr int BM = 128, BN = 256, BK = 32;  // BK in bf16 elements (64 bytes: one SWIZZLE_64B row)
+constexpr int kStages = 4;
+constexpr int kThreads = 192;
+constexpr int kTileA = BM * BK * 2;   // 8 KB
+constexpr int kTileB = BN * BK * 2;   // 16 KB
+constexpr int kStageBytes = 2 * kTileA + 2 * kTileB;  // 48 KB
+constexpr int kSmemBytes = kStages * kStageBytes + 1024 /*align slack*/ + 256 /*barriers*/;
+constexpr uint32_t kTmemCols = 256;
+constexpr uint32_t kWaitLimit = 1u << 21;   // try_wait polls (each suspends <= ~1 us)
+constexpr uint32_t kErrTimeout = 4;         // workspace error bit
+
+// Instruction descriptor, kind::f16: F32 accumulator, BF16 A and B, both
+// K-major, N = 256, M = 128.
+constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) | ((uint32_t)(BM >> 4) << 24);
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory matrix descriptor for a K-major SWIZZLE_64B tile: rows of 64
+// bytes, 8-row core groups 512 bytes apart.
+__device__ __forceinline__ uint64_t umma_desc_sw64(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= static_cast<uint64_t>((saddr >> 4) & 0x3FFF);
+    d |= static_cast<uint64_t>(1) << 16;                 // leading byte offset (unused for swizzled K-major)
+    d |= static_cast<uint64_t>(512 >> 4) << 32;          // stride byte offset: 8 rows x 64 B
+    d |= static_cast<uint64_t>(1) << 46;                 // descriptor version (sm_100)
+    d |= static_cast<uint64_t>(4) << 61;                 // SWIZZLE_64B
+    return d;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+// Bounded wait for the phase with the given parity; false on expiry.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (uint32_t i = 0; i < kWaitLimit; ++i) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, 1000;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+struct GemmMaps {
+    CUtensorMap ah, al, bh, bl;
+};
+
+__global__ void __launch_bounds__(kThreads, 1)
+gemm_bf16x3_kernel(const __grid_constant__ GemmMaps maps, int M, int N, int KT, float alpha, float beta,
+                   float* __restrict__ C, int64_t ldc, uint32_t* __restrict__ err) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
+    // bars[0..S): full, bars[S..2S): empty, bars[2S]: accumulator ready, bars[2S+1]: teardown
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 2);
+    __shared__ volatile int s_fail;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int n0 = blockIdx.x * BN, m0 = blockIdx.y * BM;
+
+    if (threadIdx.x == 0) {
+        s_fail = 0;
+        for (int s = 0; s < kStages; ++s) {
+            mbar_init(smem_u32(&bars[s]), 1);
+            mbar_init(smem_u32(&bars[kStages + s]), 1);
+        }
+        mbar_init(smem_u32(&bars[2 * kStages]), 1);
+        mbar_init(smem_u32(&bars[2 * kStages + 1]), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // ---- producer ----
+        for (int kt = 0; kt < KT; ++kt) {
+            const int s = kt % kStages;
+            if (kt >= kStages && !mbar_wait(smem_u32(&bars[kStages + s]), ((kt / kStages) + 1) & 1)) {
+                s_fail = 1;
+                atomicOr(err, kErrTimeout);
+                break;
+            }
+            if (s_fail) break;
+            uint8_t* st = smem + s * kStageBytes;
+            const uint32_t full = smem_u32(&bars[s]);
+            mbar_expect_tx(full, kStageBytes);
+            const int k = kt * BK;
+            tma_load_2d(smem_u32(st), &maps.ah, k, m0, full);
+            tma_load_2d(smem_u32(st + kTileA), &maps.al, k, m0, full);
+            tma_load_2d(smem_u32(st + 2 * kTileA), &maps.bh, k, n0, full);
+            tma_load_2d(smem_u32(st + 2 * kTileA + kTileB), &maps.bl, k, n0, full);
+        }
+    } else if (warp == 1 && lane == 0) {
+        // ---- MMA issuer ----
+        int issued = 0;
+        for (int kt = 0; kt < KT; ++kt) {
+            const int s = kt % kStages;
+            if (!mbar_wait(smem_u32(&bars[s]), (kt / kStages) & 1)) {
+                s_fail = 1;
+                atomicOr(err, kErrTimeout);
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t st = smem_u32(smem + s * kStageBytes);
+            const uint32_t a_hi = st, a_lo = st + kTileA, b_hi = st + 2 * kTileA, b_lo = st + 2 * kTileA + kTileB;
+#pragma unroll
+            for (int k16 = 0; k16 < BK / 16; ++k16) {
+                const uint32_t off = k16 * 32;  // 16 bf16 = 32 bytes along the swizzled row
+                umma_bf16(tmem, umma_desc_sw64(a_hi + off), umma_desc_sw64(b_hi + off), (kt | k16) != 0);
+                umma_bf16(tmem, umma_desc_sw64(a_hi + off), umma_desc_sw64(b_lo + off), 1u);
+                umma_bf16(tmem, umma_desc_sw64(a_lo + off), umma_desc_sw64(b_hi + off), 1u);
+            }
+            umma_commit(smem_u32(&bars[kStages + s]));
+            ++issued;
+        }
+        // Accumulator ready (or, after a failure, everything issued has retired).
+        umma_commit(smem_u32(&bars[2 * kStages]));
+        (void)issued;
+    } else if (warp >= 2) {
+        // ---- epilogue ----
+        const bool ok = mbar_wait(smem_u32(&bars[2 * kStages]), 0);
+        if (!ok) {
+            s_fail = 1;
+            atomicOr(err, kErrTimeout);
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const int q = warp & 3;  // TMEM lane quarter this warp may access
+        const int row = m0 + 32 * q + lane;
+        const bool write = ok && !s_fail && KT > 0;
+#pragma unroll 1
+        for (int c = 0; c < BN / 16; ++c) {
+            uint32_t r[16];
+            tmem_ld16(tmem + (static_cast<uint32_t>(32 * q) << 16) + 16 * c, r);
+            const int col = n0 + 16 * c;
+            if (!write || row >= M || col >= N) continue;
+            float* crow = C + static_cast<int64_t>(row) * ldc + col;
+            const bool vec = col + 16 <= N && ((reinterpret_cast<uintptr_t>(crow) & 15) == 0);
+            if (vec) {
+#pragma unroll
+                for (int j = 0; j < 16; j += 4) {
+                    float4 o;
+                    o.x = alpha * __uint_as_float(r[j]);
+                    o.y = alpha * __uint_as_float(r[j + 1]);
+                    o.z = alpha * __uint_as_float(r[j + 2]);
+                    o.w = alpha * __uint_as_float(r[j + 3]);
+                    if (beta != 0.0f) {
+                        const float4 old = *reinterpret_cast<const float4*>(crow + j);
+                        o.x += beta * old.x;
+                        o.y += beta * old.y;
+                        o.z += beta * old.z;
+                        o.w += beta * old.w;
+                    }
+                    *reinterpret_cast<float4*>(crow + j) = o;
+                }
+            } else {
+                for (int j = 0; j < 16 && col + j < N; ++j) {
+                    float o = alpha * __uint_as_float(r[j]);
+                    if (beta != 0.0f) o += beta * crow[j];
+                    crow[j] = o;
+                }
+            }
+        }
+    }
+
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 1) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (s_fail && lane == 0) {
+            // Make sure every MMA this CTA issued has retired before freeing TMEM.
+            umma_commit(smem_u32(&bars[2 * kStages + 1]));
+            mbar_wait(smem_u32(&bars[2 * kStages + 1]), 0);
+        }
+        __syncwarp();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+    }
+}
+
+// ---- split passes -----------------------------------------------------------
+// rows of X (R x K, ldx) -> hi/lo (R x Kp) bf16, zero padded to Kp.
+__global__ void split_rows_kernel(const float* __restrict__ X, int64_t ldx, int R, int K, int Kp,
+                                  __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo) {
+    const int64_t total = static_cast<int64_t>(R) * Kp;
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t r = i / Kp;
+        const int k = static_cast<int>(i - r * Kp);
+        const float x = k < K ? X[r * ldx + k] : 0.0f;
+        const __nv_bfloat16 h = __float2bfloat16_rn(x);
+        hi[i] = h;
+        lo[i] = __float2bfloat16_rn(x - __bfloat162float(h));
+    }
+}
+
+// X (K x N, ldx) -> transposed hi/lo (N x Kp), 32 x 32 tiles through shared memory.
+__global__ void split_transpose_kernel(const float* __restrict__ X, int64_t ldx, int K, int N, int Kp,
+                                       __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo) {
+    __shared__ float t[32][33];
+    const int k0 = blockIdx.y * 32, n0 = blockIdx.x * 32;
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int k = k0 + j, n = n0 + threadIdx.x;
+        t[j][threadIdx.x] = (k < K && n < N) ? X[static_cast<int64_t>(k) * ldx + n] : 0.0f;
+    }
+    __syncthreads();
+    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+        const int n = n0 + j, k = k0 + threadIdx.x;
+        if (n < N && k < Kp) {
+            const float x = t[threadIdx.x][j];
+            const __nv_bfloat16 h = __float2bfloat16_rn(x);
+            hi[static_cast<int64_t>(n) * Kp + k] = h;
+            lo[static_cast<int64_t>(n) * Kp + k] = __float2bfloat16_rn(x - __bfloat162float(h));
+        }
+    }
+}
+
+__global__ void scale_kernel(float* C, int64_t ldc, int M, int N, float beta) {
+    const int64_t total = static_cast<int64_t>(M) * N;
+    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
+        const int64_t r = i / N, c = i - r * N;
+        float* p = C + r * ldc + c;
+        *p = beta == 0.0f ? 0.0f : beta * *p;
+    }
+}
+
+// ---- plain GPU form: FP32 SIMT GEMM, 64x64 tiles, 4x4 outputs per thread ------
+__global__ void __launch_bounds__(256) sgemm_plain_kernel(int M, int N, int K, float alpha, const float* __restrict__ A,
+                                                          int64_t lda, const float* __restrict__ B, int64_t ldb,
+                                                          float beta, float* __restrict__ C, int64_t ldc) {
+    __shared__ float As[16][64 + 1];
+    __shared__ float Bs[16][64 + 1];
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    const int m0 = blockIdx.y * 64, n0 = blockIdx.x * 64;
+    float acc[4][4] = {};
+    for (int k0 = 0; k0 < K; k0 += 16) {
+        for (int i = threadIdx.x; i < 16 * 64; i += 256) {
+            const int kk = i / 64, mm = i % 64;
+            As[kk][mm] = (m0 + mm < M && k0 + kk < K) ? A[static_cast<int64_t>(m0 + mm) * lda + k0 + kk] : 0.0f;
+            Bs[kk][mm] = (n0 + mm < N && k0 + kk < K) ? B[static_cast<int64_t>(k0 + kk) * ldb + n0 + mm] : 0.0f;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < 16; ++kk) {
+            float a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = As[kk][ty * 4 + i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx * 4 + j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int m = m0 + ty * 4 + i, n = n0 + tx * 4 + j;
+            if (m < M && n < N) {
+                float* p = C + static_cast<int64_t>(m) * ldc + n;
+                *p = alpha * acc[i][j] + (beta != 0.0f ? beta * *p : 0.0f);
+            }
+        }
+}
+
+// ---- host side ----------------------------------------------------------------
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    return fn;
+}
+
+int make_map(CUtensorMap* map, const void* base, int rows, int kp, int box_rows) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return pmb::fail(PMB_GRAPHICS_CARD_ERROR, "cuTensorMapEncodeTiled unavailable");
+    const cuuint64_t dims[2] = {static_cast<cuuint64_t>(kp), static_cast<cuuint64_t>(rows)};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(kp) * 2};
+    const cuuint32_t box[2] = {BK, static_cast<cuuint32_t>(box_rows)};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return pmb::fail(PMB_GRAPHICS_CARD_ERROR, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return PMB_SUCCESS;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
+int padded_k(int K) { return (K + BK - 1) / BK * BK; }
+
+}  // namespace
+
+extern "C" size_t pmb_gemm_workspace_bytes(int M, int N, int K) {
+    if (M <= 0 || N <= 0 || K <= 0) return 256;
+    const size_t kp = padded_k(K);
+    return 256 + 2 * align256(static_cast<size_t>(M) * kp * 2) + 2 * align256(static_cast<size_t>(N) * kp * 2);
+}
+
+extern "C" int pmb_sgemm_bf16x3(int M, int N, int K, float alpha, const float* A, int64_t lda, const float* B,
+                                int64_t ldb, float beta, float* C, int64_t ldc, void* workspace, size_t ws_bytes,
+                                void* stream) {
+    PMB_CHECK_ARG(M >= 0 && N >= 0 && K >= 0, "negative GEMM size");
+    if (M == 0 || N == 0) return PMB_SUCCESS;
+    PMB_CHECK_ARG(C && workspace && (K == 0 || (A && B)), "null pointer");
+    PMB_CHECK_ARG(ldc >= N && (K == 0 || (lda >= K && ldb >= N)), "leading dimension too small");
+    PMB_CHECK_ARG((reinterpret_cast<uintptr_t>(workspace) & 255) == 0, "workspace must be 256-byte aligned");
+    PMB_CHECK_ARG(ws_bytes >= pmb_gemm_workspace_bytes(M, N, K), "GEMM workspace %zu bytes, need %zu", ws_bytes,
+                  pmb_gemm_workspace_bytes(M, N, K));
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    if (K == 0) {
+        scale_kernel<<<256, 256, 0, s>>>(C, ldc, M, N, beta);
+        PMB_CUDA_TRY(cudaGetLastError());
+        return PMB_SUCCESS;
+    }
+    const int kp = padded_k(K);
+    char* ws = static_cast<char*>(workspace);
+    uint32_t* err = reinterpret_cast<uint32_t*>(ws) + 1;
+    __nv_bfloat16* ah = reinterpret_cast<__nv_bfloat16*>(ws + 256);
+    __nv_bfloat16* al = reinterpret_cast<__nv_bfloat16*>(ws + 256 + align256(static_cast<size_t>(M) * kp * 2));
+    __nv_bfloat16* bh = reinterpret_cast<__nv_bfloat16*>(reinterpret_cast<char*>(al) + align256(static_cast<size_t>(M) * kp * 2));
+    __nv_bfloat16* bl = reinterpret_cast<__nv_bfloat16*>(reinterpret_cast<char*>(bh) + align256(static_cast<size_t>(N) * kp * 2));
+
+    PMB_CUDA_TRY(cudaMemsetAsync(ws, 0, 256, s));
+    split_rows_kernel<<<1184, 256, 0, s>>>(A, lda, M, K, kp, ah, al);
+    PMB_CUDA_TRY(cudaGetLastError());
+    split_transpose_kernel<<<dim3((N + 31) / 32, (kp + 31) / 32), dim3(32, 8), 0, s>>>(B, ldb, K, N, kp, bh, bl);
+    PMB_CUDA_TRY(cudaGetLastError());
+
+    GemmMaps maps;
+    int st;
+    if ((st = make_map(&maps.ah, ah, M, kp, BM)) != PMB_SUCCESS) return st;
+    if ((st = make_map(&maps.al, al, M, kp, BM)) != PMB_SUCCESS) return st;
+    if ((st = make_map(&maps.bh, bh, N, kp, BN)) != PMB_SUCCESS) return st;
+    if ((st = make_map(&maps.bl, bl, N, kp, BN)) != PMB_SUCCESS) return st;
+
+    static std::once_flag attr_once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(attr_once, [] {
+        attr_err = cudaFuncSetAttribute(gemm_bf16x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+    });
+    PMB_CUDA_TRY(attr_err);
+    const dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
+    gemm_bf16x3_kernel<<<grid, kThreads, kSmemBytes, s>>>(maps, M, N, kp / BK, alpha, beta, C, ldc, err);
+    PMB_CUDA_TRY(cudaGetLastError());
+    return PMB_SUCCESS;
+}
+
+extern "C" int pmb_sgemm_plain(int M, int N, int K, float alpha, const float* A, int64_t lda, const float* B,
+                               int64_t ldb, float beta, float* C, int64_t ldc, void* stream) {
+    PMB_CHECK_ARG(M >= 0 && N >= 0 && K >= 0, "negative GEMM size");
+    if (M == 0 || N == 0) return PMB_SUCCESS;
+    PMB_CHECK_ARG(C && (K == 0 || (A && B)), "null pointer");
+    sgemm_plain_kernel<<<dim3((N + 63) / 64, (M + 63) / 64), 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
+    PMB_CUDA_TRY(cudaGetLastError());
+    return PMB_SUCCESS;
+}

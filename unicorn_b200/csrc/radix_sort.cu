@@ -82,15 +82,16 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t* s
     return r;
 }
 
-template <int BITS>
+template <int BITS, bool VALUES>
 __global__ void __launch_bounds__(kThreads)
-onesweep_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, size_t n, int shift,
-                const uint32_t* __restrict__ hist_pass, uint32_t* __restrict__ tile_counter,
-                uint32_t* __restrict__ err, uint32_t* __restrict__ status) {
+onesweep_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, const uint32_t* __restrict__ vin,
+                uint32_t* __restrict__ vout, size_t n, int shift, const uint32_t* __restrict__ hist_pass,
+                uint32_t* __restrict__ tile_counter, uint32_t* __restrict__ err, uint32_t* __restrict__ status) {
     constexpr int RADIX = 1 << BITS;
     constexpr uint32_t MASK = RADIX - 1;
     static_assert(RADIX <= kThreads, "one digit per thread");
     __shared__ uint32_t s_keys[kTile];
+    __shared__ uint32_t s_vals[VALUES ? kTile : 1];
     __shared__ uint32_t s_whist[kWarps][RADIX];
     __shared__ uint32_t s_tile_start[RADIX];
     __shared__ uint32_t s_goff[RADIX];
@@ -175,7 +176,9 @@ onesweep_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, siz
     for (int i = 0; i < kItems; ++i) {
         if (wbase + i * 32 + lane < n) {
             const uint32_t d = (key[i] >> shift) & MASK;
-            s_keys[s_tile_start[d] + s_whist[warp][d] + rank[i]] = key[i];
+            const uint32_t pos = s_tile_start[d] + s_whist[warp][d] + rank[i];
+            s_keys[pos] = key[i];
+            if constexpr (VALUES) s_vals[pos] = vin[wbase + i * 32 + lane];
         }
     }
     __syncthreads();
@@ -184,7 +187,9 @@ onesweep_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, siz
     for (int p = tid; p < tile_n; p += kThreads) {
         const uint32_t k = s_keys[p];
         const uint32_t d = (k >> shift) & MASK;
-        out[s_goff[d] + (p - s_tile_start[d])] = k;
+        const uint32_t g = s_goff[d] + (p - s_tile_start[d]);
+        out[g] = k;
+        if constexpr (VALUES) vout[g] = s_vals[p];
     }
 }
 
@@ -195,7 +200,8 @@ size_t scratch_bytes_for(size_t n, int bits) {
 }
 
 template <int BITS>
-int sort_t(uint32_t* keys, uint32_t* alt, size_t n, int begin_bit, int passes, void* scratch, cudaStream_t s) {
+int sort_t(uint32_t* keys, uint32_t* alt, uint32_t* vals, uint32_t* valt, size_t n, int begin_bit, int passes,
+           void* scratch, cudaStream_t s) {
     constexpr int RADIX = 1 << BITS;
     char* base = static_cast<char*>(scratch);
     uint32_t* hdr = reinterpret_cast<uint32_t*>(base);
@@ -212,23 +218,39 @@ int sort_t(uint32_t* keys, uint32_t* alt, size_t n, int begin_bit, int passes, v
     PMB_CUDA_TRY(cudaGetLastError());
     const uint32_t* src = keys;
     uint32_t* dst = alt;
+    const uint32_t* vsrc = vals;
+    uint32_t* vdst = valt;
     for (int p = 0; p < passes; ++p) {
         PMB_CUDA_TRY(cudaMemsetAsync(status, 0, 4 * tiles * RADIX, s));
-        onesweep_kernel<BITS><<<static_cast<unsigned>(tiles), kThreads, 0, s>>>(
-            src, dst, n, begin_bit + p * BITS, hist + p * RADIX, &hdr[2 + p], &hdr[1], status);
+        if (vals)
+            onesweep_kernel<BITS, true><<<static_cast<unsigned>(tiles), kThreads, 0, s>>>(
+                src, dst, vsrc, vdst, n, begin_bit + p * BITS, hist + p * RADIX, &hdr[2 + p], &hdr[1], status);
+        else
+            onesweep_kernel<BITS, false><<<static_cast<unsigned>(tiles), kThreads, 0, s>>>(
+                src, dst, nullptr, nullptr, n, begin_bit + p * BITS, hist + p * RADIX, &hdr[2 + p], &hdr[1], status);
         PMB_CUDA_TRY(cudaGetLastError());
         src = dst;
         dst = (dst == alt) ? keys : alt;
+        if (vals) {
+            vsrc = vdst;
+            vdst = (vdst == valt) ? vals : valt;
+        }
     }
-    if (src != keys) PMB_CUDA_TRY(cudaMemcpyAsync(keys, src, 4 * n, cudaMemcpyDeviceToDevice, s));
+    if (src != keys) {
+        PMB_CUDA_TRY(cudaMemcpyAsync(keys, src, 4 * n, cudaMemcpyDeviceToDevice, s));
+        if (vals) PMB_CUDA_TRY(cudaMemcpyAsync(vals, vsrc, 4 * n, cudaMemcpyDeviceToDevice, s));
+    }
     return PMB_SUCCESS;
 }
 
-int sort_checked(uint32_t* keys, uint32_t* alt, size_t n, int begin_bit, int end_bit, int bits, void* scratch,
-                 size_t scratch_bytes, cudaStream_t s) {
+int sort_checked(uint32_t* keys, uint32_t* alt, uint32_t* vals, uint32_t* valt, size_t n, int begin_bit, int end_bit,
+                 int bits, void* scratch, size_t scratch_bytes, cudaStream_t s) {
     if (n == 0) return PMB_SUCCESS;
     PMB_CHECK_ARG(keys && alt && scratch, "null pointer");
     PMB_CHECK_ARG(keys != alt, "keys and alternate buffer must differ");
+    PMB_CHECK_ARG((vals == nullptr) == (valt == nullptr), "values need both buffers");
+    PMB_CHECK_ARG(vals == nullptr || (vals != valt && vals != keys && vals != alt && valt != keys && valt != alt),
+                  "value buffers must be distinct from each other and from the key buffers");
     PMB_CHECK_ARG(bits == 4 || bits == 8, "digit width %d not 4 or 8", bits);
     PMB_CHECK_ARG(0 <= begin_bit && begin_bit < end_bit && end_bit <= 32 && (end_bit - begin_bit) % bits == 0,
                   "bit range [%d,%d) not a multiple of %d-bit digits", begin_bit, end_bit, bits);
@@ -239,8 +261,8 @@ int sort_checked(uint32_t* keys, uint32_t* alt, size_t n, int begin_bit, int end
     if (scratch_bytes < need)
         return pmb::fail(PMB_BEYOND_LIMITS, "radix scratch %zu bytes, need %zu", scratch_bytes, need);
     const int passes = (end_bit - begin_bit) / bits;
-    return bits == 8 ? sort_t<8>(keys, alt, n, begin_bit, passes, scratch, s)
-                     : sort_t<4>(keys, alt, n, begin_bit, passes, scratch, s);
+    return bits == 8 ? sort_t<8>(keys, alt, vals, valt, n, begin_bit, passes, scratch, s)
+                     : sort_t<4>(keys, alt, vals, valt, n, begin_bit, passes, scratch, s);
 }
 
 }  // namespace
@@ -251,6 +273,14 @@ extern "C" size_t pmb_radix_sort_scratch_bytes(size_t n, int bits_per_pass) {
 
 extern "C" int pmb_radix_sort_u32(uint32_t* d_keys, uint32_t* d_alt, size_t n, int begin_bit, int end_bit,
                                   int bits_per_pass, void* d_scratch, size_t scratch_bytes, void* stream) {
-    return sort_checked(d_keys, d_alt, n, begin_bit, end_bit, bits_per_pass, d_scratch, scratch_bytes,
-                        static_cast<cudaStream_t>(stream));
+    return sort_checked(d_keys, d_alt, nullptr, nullptr, n, begin_bit, end_bit, bits_per_pass, d_scratch,
+                        scratch_bytes, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int pmb_radix_sort_pairs_u32(uint32_t* d_keys, uint32_t* d_alt, uint32_t* d_vals, uint32_t* d_vals_alt,
+                                        size_t n, int begin_bit, int end_bit, int bits_per_pass, void* d_scratch,
+                                        size_t scratch_bytes, void* stream) {
+    PMB_CHECK_ARG(d_vals && d_vals_alt, "null value buffer");
+    return sort_checked(d_keys, d_alt, d_vals, d_vals_alt, n, begin_bit, end_bit, bits_per_pass, d_scratch,
+                        scratch_bytes, static_cast<cudaStream_t>(stream));
 }

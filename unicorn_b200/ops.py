@@ -117,3 +117,125 @@ def radix_sort_u32(d_keys, begin_bit: int = 0, end_bit: int = 32, bits: int = 8,
     capi.check(capi.lib().pmb_radix_sort_u32(_dev_ptr(d_keys), _dev_ptr(d_alt), n, begin_bit, end_bit, bits,
                                              _dev_ptr(scratch), scratch.numel(), _stream_ptr(stream)))
     return d_keys, scratch
+
+
+def radix_sort_pairs_u32(d_keys, d_vals, begin_bit: int = 0, end_bit: int = 32, bits: int = 8, stream=None):
+    """Stable in-place key-value sort (uint32 keys and values, int32 storage)."""
+    import torch
+
+    n = d_keys.numel()
+    k_alt, v_alt = torch.empty_like(d_keys), torch.empty_like(d_vals)
+    scratch = _scratch(capi.lib().pmb_radix_sort_scratch_bytes(n, bits))
+    capi.check(capi.lib().pmb_radix_sort_pairs_u32(_dev_ptr(d_keys), _dev_ptr(k_alt), _dev_ptr(d_vals),
+                                                   _dev_ptr(v_alt), n, begin_bit, end_bit, bits, _dev_ptr(scratch),
+                                                   scratch.numel(), _stream_ptr(stream)))
+    return d_keys, d_vals
+
+
+def rmat_edges(seed: int, scale: int, n_edges: int, a=0.57, b=0.19, c=0.19, stream=None):
+    import torch
+
+    src = torch.empty(max(n_edges, 1), dtype=torch.int32, device="cuda")
+    dst = torch.empty(max(n_edges, 1), dtype=torch.int32, device="cuda")
+    capi.check(capi.lib().pmb_rmat_edges(seed, scale, n_edges, a, b, c, _dev_ptr(src), _dev_ptr(dst),
+                                         _stream_ptr(stream)))
+    return src[:n_edges], dst[:n_edges]
+
+
+class CsrGraph:
+    """Device CSR by destination plus the PageRank slice plan."""
+
+    def __init__(self, d_src, d_dst, n_vertices: int, stream=None):
+        import torch
+
+        L = capi.lib()
+        E = d_src.numel()
+        self.n, self.e = n_vertices, E
+        self.row_ptr = torch.empty(n_vertices + 1, dtype=torch.int32, device="cuda")
+        self.col = torch.empty(max(E, 1), dtype=torch.int32, device="cuda")
+        self.outdeg = torch.empty(n_vertices, dtype=torch.int32, device="cuda")
+        scratch = self.csr_scratch = _scratch(L.pmb_csr_scratch_bytes(n_vertices, E))
+        src = d_src if E else torch.zeros(1, dtype=torch.int32, device="cuda")
+        dst = d_dst if E else torch.zeros(1, dtype=torch.int32, device="cuda")
+        capi.check(L.pmb_csr_by_destination(_dev_ptr(src), _dev_ptr(dst), n_vertices, E, _dev_ptr(self.row_ptr),
+                                            _dev_ptr(self.col), _dev_ptr(self.outdeg), _dev_ptr(scratch),
+                                            scratch.numel(), _stream_ptr(stream)))
+        self.plan = _scratch(L.pmb_pagerank_plan_bytes(n_vertices, E))
+        capi.check(L.pmb_pagerank_plan(_dev_ptr(self.row_ptr), n_vertices, E, _dev_ptr(self.plan), self.plan.numel(),
+                                       _stream_ptr(stream)))
+        self.work = _scratch(L.pmb_pagerank_work_bytes(n_vertices, E))
+
+    def build_error(self) -> int:
+        """Error word of the CSR build (bit 2: an edge named a vertex >= n)."""
+        return scratch_error(self.csr_scratch)
+
+    def pagerank(self, rank_in, iterations: int, damping: float = 0.85, rank_out=None, stream=None):
+        import torch
+
+        if rank_out is None:
+            rank_out = torch.empty_like(rank_in)
+        capi.check(capi.lib().pmb_pagerank(_dev_ptr(self.row_ptr), _dev_ptr(self.col), _dev_ptr(self.outdeg), self.n,
+                                           self.e, _dev_ptr(self.plan), damping, iterations, _dev_ptr(rank_in),
+                                           _dev_ptr(rank_out), _dev_ptr(self.work), self.work.numel(),
+                                           _stream_ptr(stream)))
+        return rank_out
+
+
+def sgemm(A, B, C=None, alpha: float = 1.0, beta: float = 0.0, plain: bool = False, workspace=None, stream=None):
+    """Row-major fp32 C = alpha*A@B + beta*C on CUDA tensors (2-D, unit inner stride).
+
+    plain=False: BF16x3 tcgen05 kernel; plain=True: FP32 SIMT kernel.
+    Returns (C, workspace).
+    """
+    import torch
+
+    M, K = A.shape
+    K2, N = B.shape
+    if K != K2:
+        raise ValueError("inner dimensions differ")
+    if C is None:
+        C = torch.zeros(M, N, dtype=torch.float32, device=A.device)
+    for t in (A, B, C):
+        if t.dtype != torch.float32 or not t.is_cuda or t.stride(1) != 1:
+            raise ValueError("fp32 CUDA matrices with unit column stride expected")
+    L = capi.lib()
+    if plain:
+        capi.check(L.pmb_sgemm_plain(M, N, K, alpha, A.data_ptr(), A.stride(0), B.data_ptr(), B.stride(0), beta,
+                                     C.data_ptr(), C.stride(0), _stream_ptr(stream)))
+        return C, None
+    need = L.pmb_gemm_workspace_bytes(M, N, K)
+    if workspace is None or workspace.numel() < need:
+        workspace = _scratch(need)
+    capi.check(L.pmb_sgemm_bf16x3(M, N, K, alpha, A.data_ptr(), A.stride(0), B.data_ptr(), B.stride(0), beta,
+                                  C.data_ptr(), C.stride(0), workspace.data_ptr(), workspace.numel(),
+                                  _stream_ptr(stream)))
+    return C, workspace
+
+
+def lu_decompose(d_A, nb: int = 128, plain: bool = False, workspace=None, stream=None):
+    """In-place Crout LU of a square fp32 CUDA matrix stored column-major.
+
+    d_A is a 2-D tensor whose memory holds the column-major matrix (i.e. the
+    row-major transpose view).  Returns (d_A, workspace, flags) -- flags is the
+    workspace flag word (1: pivoting would swap rows, 2: zero pivot).
+    """
+    n = d_A.shape[0]
+    L = capi.lib()
+    need = L.pmb_lu_workspace_bytes(n, nb)
+    if workspace is None or workspace.numel() < need:
+        workspace = _scratch(need)
+    fn = L.pmb_lu_decompose_plain if plain else L.pmb_lu_decompose
+    capi.check(fn(_dev_ptr(d_A), n, d_A.stride(0), nb, _dev_ptr(workspace), workspace.numel(), _stream_ptr(stream)))
+    return d_A, workspace, scratch_error(workspace)
+
+
+def lu_residual(d_A0, d_LU, stream=None) -> float:
+    """||A0 - L*U||_F / ||A0||_F in FP64 (column-major storage for both)."""
+    import torch
+
+    n = d_A0.shape[0]
+    sums = torch.zeros(2, dtype=torch.float64, device="cuda")
+    capi.check(capi.lib().pmb_lu_residual_f64(_dev_ptr(d_A0), d_A0.stride(0), _dev_ptr(d_LU), d_LU.stride(0), n,
+                                              _dev_ptr(sums), _stream_ptr(stream)))
+    s = sums.cpu().numpy()
+    return float(np.sqrt(s[0] / s[1])) if s[1] > 0 else 0.0
