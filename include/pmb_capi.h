@@ -45,6 +45,53 @@ const char* pmb_version(void);
 int pmb_device_supported(int dev);
 
 /* ------------------------------------------------------------------------ */
+/* Device layer: what the pm:: runtime (libpmlib.so) uses instead of calling  */
+/* the CUDA runtime itself (replaces pmCudaInterface's dlsym'd calls,        */
+/* source/code/src/pmCudaInterface.cu:69-173, :336-339, :474-550).           */
+/* ------------------------------------------------------------------------ */
+
+/* Copy directions for pmb_memcpy_async / pmb_memcpy2d_async. */
+#define PMB_H2D 0
+#define PMB_D2H 1
+#define PMB_D2D 2
+#define PMB_COPY_DEFAULT 3
+
+int pmb_device_count(int* count);
+int pmb_set_device(int dev);
+int pmb_device_properties(int dev, char* name, size_t name_len, int* sm_count, int* cc_major, int* cc_minor);
+int pmb_mem_get_info(size_t* free_bytes, size_t* total_bytes);
+int pmb_malloc(void** p, size_t bytes);
+int pmb_free(void* p);
+int pmb_malloc_async(void** p, size_t bytes, void* stream);
+int pmb_free_async(void* p, void* stream);
+int pmb_host_alloc(void** p, size_t bytes); /* pinned, portable */
+int pmb_host_free(void* p);
+int pmb_stream_create(void** stream);        /* non-blocking stream */
+int pmb_stream_destroy(void* stream);
+int pmb_stream_synchronize(void* stream);
+int pmb_event_create(void** event, int timing);
+int pmb_event_destroy(void* event);
+int pmb_event_record(void* event, void* stream);
+int pmb_event_query(void* event);            /* PMB_SUCCESS done, PMB_STATUS_UNAVAILABLE pending */
+int pmb_event_synchronize(void* event);
+int pmb_event_elapsed_ms(void* start, void* end, float* ms);
+int pmb_stream_wait_event(void* stream, void* event);
+int pmb_memcpy_async(void* dst, const void* src, size_t bytes, int kind, void* stream);
+int pmb_memcpy2d_async(void* dst, size_t dpitch, const void* src, size_t spitch, size_t width, size_t height,
+                       int kind, void* stream);
+int pmb_memset_async(void* p, int value, size_t bytes, void* stream);
+/* cudaLaunchKernel of a __global__ function pointer (an app's
+ * subtask_gpu_cuda kernel) with the argument array `args`. */
+int pmb_launch_kernel(const void* fn, unsigned gx, unsigned gy, unsigned gz, unsigned bx, unsigned by, unsigned bz,
+                      unsigned smem, void** args, void* stream);
+int pmb_device_synchronize(void);
+/* Stream capture into an instantiated CUDA graph, and its launch. */
+int pmb_graph_begin_capture(void* stream);
+int pmb_graph_end_capture(void* stream, void** graph_exec);
+int pmb_graph_launch(void* graph_exec, void* stream);
+int pmb_graph_destroy(void* graph_exec);
+
+/* ------------------------------------------------------------------------ */
 /* imageFiltering: 2-D (2r+1)^2 RGB stencil                                  */
 /* ------------------------------------------------------------------------ */
 

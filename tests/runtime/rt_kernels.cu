@@ -1,0 +1,36 @@
+// App-style subtask_gpu_cuda kernel used by the runtime self-test: the
+// runtime launches it with (pmTaskInfo, pmDeviceInfo*, pmSubtaskInfo,
+// pmStatus*) by value, exactly as an unchanged app kernel is launched.
+#include "pmPublicDefinitions.h"
+
+using namespace pm;
+
+struct RtConf {
+    int add;     // constant added to every element
+    int ld;      // row pitch of the whole matrix, in ints (NATURAL views)
+};
+
+// Per-subtask scratch (PRE_SUBTASK_TO_SUBTASK): {extra, rows, cols}.
+// out[r][c] = in[r][c] + add + extra, staged through reserved device memory.
+__global__ void rt_add_kernel(pmTaskInfo ti, pmDeviceInfo* di, pmSubtaskInfo si, pmStatus* st) {
+    const RtConf* conf = static_cast<const RtConf*>(ti.taskConf);
+    const int* in = static_cast<const int*>(si.memInfo[0].ptr);
+    int* out = static_cast<int*>(si.memInfo[1].ptr);
+    const int* scratch = static_cast<const int*>(si.gpuContext.scratchBuffer);
+    const int extra = scratch[0], rows = scratch[1], cols = scratch[2];
+    const int in_ld = si.memInfo[0].visibilityType == SUBSCRIPTION_NATURAL ? conf->ld : cols;
+    const int out_ld = si.memInfo[1].visibilityType == SUBSCRIPTION_NATURAL ? conf->ld : cols;
+    int* reserved = static_cast<int*>(si.gpuContext.reservedGlobalMem);
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < rows * cols; e += gridDim.x * blockDim.x) {
+        const int r = e / cols, c = e % cols;
+        int v = in[r * in_ld + c] + conf->add + extra;
+        if (reserved) {
+            reserved[e] = v;
+            v = reserved[e];
+        }
+        out[r * out_ld + c] = v;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && di->deviceType != GPU_CUDA) *st = pmFatalError;
+}
+
+extern "C" void* rt_add_kernel_ptr() { return reinterpret_cast<void*>(&rt_add_kernel); }

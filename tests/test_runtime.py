@@ -1,0 +1,78 @@
+"""pm:: runtime tests (libpmlib.so) through its public C++ API.
+
+* tests/runtime/rt_selftest: our own driver of the API -- scattered
+  subscriptions, NATURAL and COMPACT views, scratch buffers, launch
+  configuration and reserved memory for an app-style subtask_gpu_cuda kernel,
+  chained tasks that stay device-resident, write-through with the CUDA cache
+  disabled, many tasks in flight vs alone, error returns and timeouts.
+* oracle/_ref/imageFiltering_b200.exe: the reference's own imageFiltering app
+  and harness (imageFiltering.cpp + commonAPI.cpp, unchanged) linked against
+  this runtime and the B200 GPU callbacks; it checks itself against its serial
+  CPU implementation and prints "Serial Comparison Test Passed".
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+
+import pytest
+
+from conftest import ROOT
+
+SELFTEST = os.path.join(ROOT, "tests", "runtime", "_build", "rt_selftest")
+APP = os.path.join(ROOT, "oracle", "_ref", "imageFiltering_b200.exe")
+
+
+@pytest.fixture(scope="module")
+def selftest():
+    subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "tests", "runtime")], check=True)
+    return SELFTEST
+
+
+def run(cmd, timeout=300):
+    p = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+    return p.returncode, p.stdout + p.stderr
+
+
+@pytest.mark.parametrize("name", ["views_cpu", "views_cpu_compact", "errors", "timeout"])
+def test_runtime_cpu(selftest, name):
+    rc, out = run([selftest, name])
+    assert rc == 0 and f"PASS {name}" in out, out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["views_gpu", "views_gpu_compact", "chain", "write_through", "mix"])
+def test_runtime_gpu(selftest, name):
+    rc, out = run([selftest, name])
+    assert rc == 0 and f"PASS {name}" in out, out
+
+
+def app_or_skip():
+    if not os.path.exists(APP):
+        pytest.skip("reference app not built (oracle/ref/Makefile needs the reference tree)")
+    return APP
+
+
+def test_reference_app_cpu_mode_on_b200_runtime():
+    """Parallel mode 1 (local CPU): subscriptions and views of the runtime
+    drive the reference's own CPU callback across 3 chained tasks."""
+    rc, out = run([app_or_skip(), "1", "1", "0", "2", "1", "4100", "2100", "3"])
+    assert rc == 0 and "Serial Comparison Test Passed" in out and "Failed" not in out, out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("args", [["2", "0", "4100", "2100", "3"], ["1", "1", "8192", "8192", "2"],
+                                  ["3", "2", "777", "513", "2"]])
+def test_reference_app_gpu_mode(args):
+    """Parallel mode 2 (local GPU): the unchanged app runs its subtasks on the
+    B200 stencil through the runtime (batched into one launch per task) and
+    compares with its serial CPU run."""
+    rc, out = run([app_or_skip(), "1", "2", "0"] + args, timeout=600)
+    assert rc == 0 and "Serial Comparison Test Passed" in out and "Failed" not in out, out
+
+
+@pytest.mark.gpu
+def test_reference_app_single_gpu_mode():
+    """Run mode 4: the app's single-GPU path (singleGpuImageFilter) vs serial."""
+    rc, out = run([app_or_skip(), "4", "2", "0", "2", "0", "3000", "1000", "1"])
+    assert rc == 0 and "Single GPU Task's Sequential Comparison Test Passed" in out, out

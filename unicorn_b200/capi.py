@@ -58,6 +58,37 @@ _SIGS = {
     "pmb_last_error": (ctypes.c_char_p, []),
     "pmb_version": (ctypes.c_char_p, []),
     "pmb_device_supported": (c_int, [c_int]),
+    "pmb_device_count": (c_int, [ctypes.POINTER(c_int)]),
+    "pmb_set_device": (c_int, [c_int]),
+    "pmb_device_properties": (c_int, [c_int, ctypes.c_char_p, c_size_t, ctypes.POINTER(c_int), ctypes.POINTER(c_int),
+                                      ctypes.POINTER(c_int)]),
+    "pmb_mem_get_info": (c_int, [ctypes.POINTER(c_size_t), ctypes.POINTER(c_size_t)]),
+    "pmb_malloc": (c_int, [ctypes.POINTER(c_void_p), c_size_t]),
+    "pmb_free": (c_int, [c_void_p]),
+    "pmb_malloc_async": (c_int, [ctypes.POINTER(c_void_p), c_size_t, c_void_p]),
+    "pmb_free_async": (c_int, [c_void_p, c_void_p]),
+    "pmb_host_alloc": (c_int, [ctypes.POINTER(c_void_p), c_size_t]),
+    "pmb_host_free": (c_int, [c_void_p]),
+    "pmb_stream_create": (c_int, [ctypes.POINTER(c_void_p)]),
+    "pmb_stream_destroy": (c_int, [c_void_p]),
+    "pmb_stream_synchronize": (c_int, [c_void_p]),
+    "pmb_event_create": (c_int, [ctypes.POINTER(c_void_p), c_int]),
+    "pmb_event_destroy": (c_int, [c_void_p]),
+    "pmb_event_record": (c_int, [c_void_p, c_void_p]),
+    "pmb_event_query": (c_int, [c_void_p]),
+    "pmb_event_synchronize": (c_int, [c_void_p]),
+    "pmb_event_elapsed_ms": (c_int, [c_void_p, c_void_p, ctypes.POINTER(ctypes.c_float)]),
+    "pmb_stream_wait_event": (c_int, [c_void_p, c_void_p]),
+    "pmb_memcpy_async": (c_int, [c_void_p, c_void_p, c_size_t, c_int, c_void_p]),
+    "pmb_memcpy2d_async": (c_int, [c_void_p, c_size_t, c_void_p, c_size_t, c_size_t, c_size_t, c_int, c_void_p]),
+    "pmb_memset_async": (c_int, [c_void_p, c_int, c_size_t, c_void_p]),
+    "pmb_launch_kernel": (c_int, [c_void_p, ctypes.c_uint, ctypes.c_uint, ctypes.c_uint, ctypes.c_uint, ctypes.c_uint,
+                                  ctypes.c_uint, ctypes.c_uint, ctypes.POINTER(c_void_p), c_void_p]),
+    "pmb_device_synchronize": (c_int, []),
+    "pmb_graph_begin_capture": (c_int, [c_void_p]),
+    "pmb_graph_end_capture": (c_int, [c_void_p, ctypes.POINTER(c_void_p)]),
+    "pmb_graph_launch": (c_int, [c_void_p, c_void_p]),
+    "pmb_graph_destroy": (c_int, [c_void_p]),
     "pmb_image_filter": (c_int, [ctypes.POINTER(ImgfItem), c_int, c_void_p, c_int, c_int, c_void_p]),
     "pmb_image_filter_full": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_int, c_int, c_void_p]),
     "pmb_image_filter_plain": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_int, c_int, c_void_p]),

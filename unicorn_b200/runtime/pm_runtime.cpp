@@ -1,0 +1,1336 @@
+// pm:: runtime of the B200 subtask path (libpmlib.so).
+//
+// Implements the public API of pmPublicDefinitions.h / pmPublicUtilities.h for
+// one process and one CUDA device.  The reference spreads this over pmController,
+// pmTask*, pmScheduler, pmSubscriptionManager, pmExecutionStub and
+// pmCudaInterface (source/code/src/); here it is one in-process controller
+// with two worker threads:
+//
+//  * the CUDA execution stub (replaces pmStubCUDA::Execute and its helpers,
+//    pmExecutionStub.cpp:2980-4042): runs each task's data-distribution
+//    callback for every subtask, turns the recorded subscriptions into device
+//    views, stages the missing bytes into a device-resident mirror of every
+//    address space (one 2-D copy per scattered subscription, on a dedicated
+//    copy stream), launches each subtask's GPU callback on one of four compute
+//    streams, and keeps results on the device.  Tasks are issued back to back:
+//    dependencies between tasks that share address spaces are CUDA events,
+//    never host waits, so consecutive tasks overlap on the device;
+//  * the completion thread: waits for each task's completion event, finishes
+//    bookkeeping, runs the completion callback and wakes waiters.
+//
+// Address spaces keep a pinned host copy and, once a GPU task has used them,
+// a full device mirror.  Coherence is tracked per byte range: dev_valid (the
+// device copy is current) and host_stale (the device is newer than the host,
+// written back by pmFetchMemory).  This is the analogue of the reference's
+// CUDA cache (pmCache, pmExecutionStub.cpp:3022-3070) at address-space
+// granularity; with the cache disabled (pmTaskDetails::cudaCacheEnabled or
+// PMLIB_DISABLE_CUDA_CACHE) writes go back to the host at task end and the
+// device copy is dropped.
+//
+// All CUDA work goes through the C ABI of libpmb.so (pmb_capi.h).
+#include "pm_runtime.h"
+
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <set>
+
+#include "pmb_capi.h"
+
+namespace pmr {
+
+// ---------------------------------------------------------------------------
+// errors
+
+static thread_local std::string t_last_error;
+
+static pmStatus fail(pmStatus st, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    t_last_error = buf;
+    return st;
+}
+
+// Map a non-zero libpmb status to pmStatus (same numbering) and keep its message.
+static pmStatus dev_fail(int st, const char* what) {
+    return fail(static_cast<pmStatus>(st), "%s: %s", what, pmb_last_error());
+}
+
+#define PMR_DEV(call)                                            \
+    do {                                                         \
+        const int pmr_st_ = (call);                              \
+        if (pmr_st_ != PMB_SUCCESS) return dev_fail(pmr_st_, #call); \
+    } while (0)
+
+static double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+static bool env_flag(const char* name) {
+    const char* v = getenv(name);
+    return v && atoi(v) != 0;
+}
+
+// ---------------------------------------------------------------------------
+// RangeSet
+
+void RangeSet::add(size_t lo, size_t hi) {
+    if (lo >= hi) return;
+    auto it = m_.upper_bound(lo);
+    if (it != m_.begin()) {
+        auto prev = std::prev(it);
+        if (prev->second >= lo) {
+            lo = prev->first;
+            hi = std::max(hi, prev->second);
+            it = m_.erase(prev);
+        }
+    }
+    while (it != m_.end() && it->first <= hi) {
+        hi = std::max(hi, it->second);
+        it = m_.erase(it);
+    }
+    m_[lo] = hi;
+}
+
+void RangeSet::remove(size_t lo, size_t hi) {
+    if (lo >= hi) return;
+    auto it = m_.upper_bound(lo);
+    if (it != m_.begin()) --it;
+    std::vector<std::pair<size_t, size_t>> keep;
+    while (it != m_.end() && it->first < hi) {
+        if (it->second <= lo) {
+            ++it;
+            continue;
+        }
+        if (it->first < lo) keep.emplace_back(it->first, lo);
+        if (it->second > hi) keep.emplace_back(hi, it->second);
+        it = m_.erase(it);
+    }
+    for (auto& k : keep) m_[k.first] = k.second;
+}
+
+bool RangeSet::covers(size_t lo, size_t hi) const {
+    if (lo >= hi) return true;
+    auto it = m_.upper_bound(lo);
+    if (it == m_.begin()) return false;
+    --it;
+    return it->first <= lo && it->second >= hi;
+}
+
+void RangeSet::missing(size_t lo, size_t hi, std::vector<std::pair<size_t, size_t>>& out) const {
+    size_t cur = lo;
+    auto it = m_.upper_bound(lo);
+    if (it != m_.begin()) --it;
+    for (; it != m_.end() && it->first < hi; ++it) {
+        if (it->second <= cur) continue;
+        if (it->first > cur) out.emplace_back(cur, std::min(it->first, hi));
+        cur = std::max(cur, it->second);
+        if (cur >= hi) break;
+    }
+    if (cur < hi) out.emplace_back(cur, hi);
+}
+
+void RangeSet::present(size_t lo, size_t hi, std::vector<std::pair<size_t, size_t>>& out) const {
+    auto it = m_.upper_bound(lo);
+    if (it != m_.begin()) --it;
+    for (; it != m_.end() && it->first < hi; ++it) {
+        const size_t a = std::max(lo, it->first), b = std::min(hi, it->second);
+        if (a < b) out.emplace_back(a, b);
+    }
+}
+
+size_t RangeSet::bytes() const {
+    size_t b = 0;
+    for (auto& kv : m_) b += kv.second - kv.first;
+    return b;
+}
+
+// ---------------------------------------------------------------------------
+// controller state
+
+struct Stats {
+    std::atomic<unsigned long long> h2d{0}, d2h{0}, gpu_subtasks{0}, batched{0};
+};
+
+struct Controller {
+    std::mutex mu;  // registries
+    bool initialized = false;
+    bool has_gpu = false;
+    int device = 0;
+    pmDeviceInfo gpu_info, cpu_info;
+    void* dev_device_info = nullptr;
+    void* dev_status = nullptr;
+    std::vector<std::unique_ptr<CallbackSet>> callbacks;
+    std::set<AddressSpace*> spaces;
+    std::set<Task*> tasks;
+    std::map<void*, BatchFn> batch;
+    // stub
+    std::thread stub, completer;
+    std::mutex qmu;
+    std::condition_variable qcv;
+    std::deque<Task*> queue;
+    std::deque<Task*> inflight;
+    std::condition_variable icv;
+    bool stopping = false;
+    void* copy_stream = nullptr;
+    std::vector<void*> streams;
+    void* join_stream = nullptr;
+    void* fetch_stream = nullptr;
+    size_t reserve_bytes = 0;
+    std::atomic<uint64_t> lru{0};
+    Stats stats;
+    // memory-mapped files
+    std::map<std::string, std::pair<void*, size_t>> files;
+};
+
+static Controller& ctl() {
+    static Controller c;
+    return c;
+}
+
+void register_batch(pmSubtaskCallback_GPU_Custom callback, BatchFn batch) {
+    std::lock_guard<std::mutex> g(ctl().mu);
+    ctl().batch[reinterpret_cast<void*>(callback)] = batch;
+}
+
+// Data-distribution context of the calling thread.
+struct DdContext {
+    Task* task = nullptr;
+};
+static thread_local DdContext t_dd;
+
+static Task* task_of(pmTaskHandle h) {
+    Controller& c = ctl();
+    std::lock_guard<std::mutex> g(c.mu);
+    Task* t = static_cast<Task*>(h);
+    return c.tasks.count(t) ? t : nullptr;
+}
+
+static AddressSpace* space_of(pmMemHandle h) {
+    Controller& c = ctl();
+    std::lock_guard<std::mutex> g(c.mu);
+    AddressSpace* a = static_cast<AddressSpace*>(h);
+    return c.spaces.count(a) && !a->released ? a : nullptr;
+}
+
+static void free_space(AddressSpace* a) {
+    if (a->dev) pmb_free(a->dev);
+    if (a->host) {
+        if (ctl().has_gpu) pmb_host_free(a->host);
+        else free(a->host);
+    }
+    if (a->last_write) pmb_event_destroy(a->last_write);
+    if (a->last_access) pmb_event_destroy(a->last_access);
+    delete a;
+}
+
+// ---------------------------------------------------------------------------
+// subscriptions -> views
+
+static void consolidated(const std::vector<Record>& rs, size_t& lo, size_t& hi) {
+    lo = SIZE_MAX;
+    hi = 0;
+    for (const Record& r : rs) {
+        if (!r.count || !r.size) continue;
+        lo = std::min(lo, r.lo());
+        hi = std::max(hi, r.hi());
+    }
+    if (lo > hi) lo = hi = 0;
+}
+
+static void add_record(RangeSet& s, const Record& r) {
+    if (r.contiguous()) {
+        s.add(r.offset, r.hi());
+        return;
+    }
+    for (size_t k = 0; k < r.count; ++k) s.add(r.offset + k * r.step, r.offset + k * r.step + r.size);
+}
+
+// Compact layout of one address space for one subtask: the union of its read
+// and write ranges, packed back to back in offset order
+// (pmSubscriptionManager::GetCompactedSubscription, pmSubscriptionManager.cpp:1978-2030).
+struct Compact {
+    RangeSet uni;
+    std::vector<std::pair<size_t, size_t>> pieces;  // (space offset, length) in packed order
+    size_t length = 0;
+    size_t offset_of(size_t space_off) const {  // packed offset of a byte inside the union
+        size_t covered = 0;
+        for (auto& p : pieces) {
+            if (space_off >= p.first && space_off < p.first + p.second) return covered + space_off - p.first;
+            covered += p.second;
+        }
+        return covered;
+    }
+};
+
+static Compact compact_of(const SubtaskMem& m) {
+    Compact c;
+    for (const Record& r : m.reads) add_record(c.uni, r);
+    for (const Record& r : m.writes) add_record(c.uni, r);
+    for (auto& kv : c.uni.map()) {
+        c.pieces.emplace_back(kv.first, kv.second - kv.first);
+        c.length += kv.second - kv.first;
+    }
+    return c;
+}
+
+// ---------------------------------------------------------------------------
+// device staging helpers (copy stream unless noted)
+
+// Upload the rows of record `r` that are not yet valid on the device.
+static pmStatus upload_record(AddressSpace* a, const Record& r, void* stream) {
+    if (!r.count || !r.size) return pmSuccess;
+    Controller& c = ctl();
+    if (a->dev_valid.covers(r.lo(), r.hi())) return pmSuccess;
+    if (r.contiguous()) {
+        std::vector<std::pair<size_t, size_t>> miss;
+        a->dev_valid.missing(r.lo(), r.hi(), miss);
+        for (auto& m : miss) {
+            PMR_DEV(pmb_memcpy_async(a->dev + m.first, a->host + m.first, m.second - m.first, PMB_H2D, stream));
+            c.stats.h2d += m.second - m.first;
+        }
+        a->dev_valid.add(r.lo(), r.hi());
+        return pmSuccess;
+    }
+    // Scattered: 2-D copies over runs of consecutive rows that miss bytes.
+    size_t k = 0;
+    while (k < r.count) {
+        while (k < r.count && a->dev_valid.covers(r.offset + k * r.step, r.offset + k * r.step + r.size)) ++k;
+        size_t e = k;
+        while (e < r.count && !a->dev_valid.covers(r.offset + e * r.step, r.offset + e * r.step + r.size)) ++e;
+        if (e > k) {
+            const size_t off = r.offset + k * r.step;
+            PMR_DEV(pmb_memcpy2d_async(a->dev + off, r.step, a->host + off, r.step, r.size, e - k, PMB_H2D, stream));
+            c.stats.h2d += r.size * (e - k);
+        }
+        k = e;
+    }
+    add_record(a->dev_valid, r);
+    return pmSuccess;
+}
+
+// Copy a record between the mirror and a packed buffer (D2D).
+static pmStatus pack_record(AddressSpace* a, const Record& r, const Compact& cp, char* packed, bool to_packed,
+                            void* stream) {
+    if (!r.count || !r.size) return pmSuccess;
+    const size_t poff = cp.offset_of(r.offset);
+    if (r.contiguous()) {
+        const size_t n = r.hi() - r.lo();
+        return to_packed ? (pmb_memcpy_async(packed + poff, a->dev + r.offset, n, PMB_D2D, stream) == PMB_SUCCESS
+                                ? pmSuccess
+                                : dev_fail(PMB_GRAPHICS_CARD_ERROR, "pack"))
+                         : (pmb_memcpy_async(a->dev + r.offset, packed + poff, n, PMB_D2D, stream) == PMB_SUCCESS
+                                ? pmSuccess
+                                : dev_fail(PMB_GRAPHICS_CARD_ERROR, "unpack"));
+    }
+    // One 2-D copy when the record's rows sit at a uniform pitch in the packed
+    // view (the usual case: rows do not interleave with other records);
+    // otherwise one copy per row.
+    const size_t ppitch = r.count > 1 ? cp.offset_of(r.offset + r.step) - poff : r.size;
+    bool uniform = ppitch >= r.size;
+    for (size_t k = 2; uniform && k < r.count; ++k) uniform = cp.offset_of(r.offset + k * r.step) == poff + k * ppitch;
+    if (uniform) {
+        const int st = to_packed ? pmb_memcpy2d_async(packed + poff, ppitch, a->dev + r.offset, r.step, r.size, r.count,
+                                                      PMB_D2D, stream)
+                                 : pmb_memcpy2d_async(a->dev + r.offset, r.step, packed + poff, ppitch, r.size, r.count,
+                                                      PMB_D2D, stream);
+        return st == PMB_SUCCESS ? pmSuccess : dev_fail(st, "compact copy");
+    }
+    for (size_t k = 0; k < r.count; ++k) {
+        const size_t off = r.offset + k * r.step, po = cp.offset_of(off);
+        const int st = to_packed ? pmb_memcpy_async(packed + po, a->dev + off, r.size, PMB_D2D, stream)
+                                 : pmb_memcpy_async(a->dev + off, packed + po, r.size, PMB_D2D, stream);
+        if (st != PMB_SUCCESS) return dev_fail(st, "compact row copy");
+    }
+    return pmSuccess;
+}
+
+// Write the host-stale bytes of [lo, hi) back to the host (synchronous).
+static pmStatus fetch_range(AddressSpace* a, size_t lo, size_t hi) {
+    Controller& c = ctl();
+    std::vector<std::pair<size_t, size_t>> st;
+    a->host_stale.present(lo, hi, st);
+    if (st.empty()) return pmSuccess;
+    if (a->last_write) PMR_DEV(pmb_event_synchronize(a->last_write));
+    for (auto& r : st) {
+        PMR_DEV(pmb_memcpy_async(a->host + r.first, a->dev + r.first, r.second - r.first, PMB_D2H, c.fetch_stream));
+        c.stats.d2h += r.second - r.first;
+    }
+    PMR_DEV(pmb_stream_synchronize(c.fetch_stream));
+    for (auto& r : st) a->host_stale.remove(r.first, r.second);
+    return pmSuccess;
+}
+
+// Free device mirrors of idle address spaces (least recently used first)
+// until `need` bytes are free beyond the reserve.
+static bool make_room(size_t need, const std::vector<AddressSpace*>& keep) {
+    Controller& c = ctl();
+    for (;;) {
+        size_t fr = 0, tot = 0;
+        if (pmb_mem_get_info(&fr, &tot) != PMB_SUCCESS) return false;
+        if (fr >= need + c.reserve_bytes) return true;
+        AddressSpace* victim = nullptr;
+        {
+            std::lock_guard<std::mutex> g(c.mu);
+            for (AddressSpace* a : c.spaces) {
+                if (!a->dev || a->users > 0) continue;
+                if (std::find(keep.begin(), keep.end(), a) != keep.end()) continue;
+                if (!victim || a->lru < victim->lru) victim = a;
+            }
+        }
+        if (!victim) return false;
+        std::lock_guard<std::mutex> g(victim->mu);
+        fetch_range(victim, 0, victim->length);
+        pmb_free(victim->dev);
+        victim->dev = nullptr;
+        victim->dev_valid.clear();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// task execution: CUDA stub
+
+static pmStatus run_dd(Task* t, const pmDeviceInfo& dev) {
+    const pmDataDistributionCallback dd = t->callbacks->cb.dataDistribution;
+    t_dd.task = t;
+    for (Subtask& s : t->subtasks) {
+        if (!dd) continue;
+        pmSubtaskInfo si;
+        si.subtaskId = s.id;
+        si.memCount = static_cast<uint>(t->spaces.size());
+        const pmStatus st = dd(t->info, dev, si);
+        if (st != pmSuccess) {
+            t_dd.task = nullptr;
+            return fail(st, "data distribution callback of subtask %lu returned %d", s.id, static_cast<int>(st));
+        }
+    }
+    t_dd.task = nullptr;
+    return pmSuccess;
+}
+
+static pmStatus stage_and_launch_gpu(Task* t) {
+    Controller& c = ctl();
+    const pmCallbacks& cb = t->callbacks->cb;
+    const size_t ns = t->spaces.size();
+    const bool write_through = !t->details.cudaCacheEnabled || env_flag("PMLIB_DISABLE_CUDA_CACHE");
+
+    // Views: OPTIMAL is NATURAL here -- every address space has a resident
+    // mirror, so natural views need no packing copies.
+    t->views.resize(ns);
+    for (size_t i = 0; i < ns; ++i)
+        t->views[i] = t->mem[i].subscriptionVisibilityType == SUBSCRIPTION_COMPACT ? SUBSCRIPTION_COMPACT
+                                                                                  : SUBSCRIPTION_NATURAL;
+
+    // Device mirrors (admission by free device memory).
+    size_t need = 0;
+    for (AddressSpace* a : t->spaces)
+        if (!a->dev) need += a->length;
+    for (Subtask& s : t->subtasks) need += s.reserved;
+    if (need && !make_room(need, t->spaces))
+        return fail(pmMemoryError, "task needs %zu bytes of device memory; not available", need);
+    for (AddressSpace* a : t->spaces) {
+        std::lock_guard<std::mutex> g(a->mu);
+        if (!a->dev) {
+            void* p = nullptr;
+            PMR_DEV(pmb_malloc(&p, a->length));
+            a->dev = static_cast<char*>(p);
+        }
+        a->lru = ++c.lru;
+    }
+
+    // Dependencies on earlier tasks: read-after-write, write-after-access.
+    for (size_t i = 0; i < ns; ++i) {
+        AddressSpace* a = t->spaces[i];
+        const bool writes = t->mem[i].memType != READ_ONLY && t->mem[i].memType != READ_ONLY_LAZY;
+        void* ev = writes ? a->last_access : a->last_write;
+        if (ev) PMR_DEV(pmb_stream_wait_event(c.copy_stream, ev));
+    }
+
+    // Task configuration on the device for subtask_gpu_cuda kernels.
+    t->dev_info = t->info;
+    if (cb.subtask_gpu_cuda && !t->conf.empty()) {
+        PMR_DEV(pmb_malloc_async(&t->dev_conf, t->conf.size(), c.copy_stream));
+        PMR_DEV(pmb_memcpy_async(t->dev_conf, t->conf.data(), t->conf.size(), PMB_H2D, c.copy_stream));
+        t->dev_info.taskConf = t->dev_conf;
+    }
+
+    BatchFn batch = nullptr;
+    if (cb.subtask_gpu_custom) {
+        std::lock_guard<std::mutex> g(c.mu);
+        auto it = c.batch.find(reinterpret_cast<void*>(cb.subtask_gpu_custom));
+        if (it != c.batch.end()) batch = it->second;
+        for (size_t i = 0; i < ns && batch; ++i)
+            if (t->views[i] != SUBSCRIPTION_NATURAL) batch = nullptr;
+        for (Subtask& s : t->subtasks)
+            if (s.reserved || !s.scratch.empty()) batch = nullptr;
+    }
+
+    std::vector<void*> events;
+    auto new_event = [&]() -> void* {
+        void* e = nullptr;
+        if (pmb_event_create(&e, 0) != PMB_SUCCESS) return nullptr;
+        events.push_back(e);
+        return e;
+    };
+
+    std::vector<pmSubtaskInfo> infos(t->subtasks.size());
+    std::vector<bool> used_stream(c.streams.size(), false);
+    for (size_t si = 0; si < t->subtasks.size(); ++si) {
+        Subtask& s = t->subtasks[si];
+        pmSubtaskInfo& info = infos[si];
+        info.subtaskId = s.id;
+        info.memCount = static_cast<uint>(ns);
+        s.dev_compact.assign(ns, nullptr);
+        std::vector<Compact> compacts(ns);
+        // ---- stage (copy stream) ----
+        for (size_t i = 0; i < ns; ++i) {
+            AddressSpace* a = t->spaces[i];
+            const SubtaskMem& m = s.mem[i];
+            std::lock_guard<std::mutex> g(a->mu);
+            for (const Record& r : m.reads) {
+                const pmStatus st = upload_record(a, r, c.copy_stream);
+                if (st != pmSuccess) return st;
+            }
+            pmMemInfo mi;
+            mi.visibilityType = t->views[i];
+            size_t rlo, rhi, wlo, whi;
+            consolidated(m.reads, rlo, rhi);
+            consolidated(m.writes, wlo, whi);
+            const bool has_r = rhi > rlo, has_w = whi > wlo;
+            if (!has_r && !has_w) {
+                info.memInfo[i] = mi;
+                continue;
+            }
+            if (t->views[i] == SUBSCRIPTION_NATURAL) {
+                const size_t lo = has_r && has_w ? std::min(rlo, wlo) : (has_r ? rlo : wlo);
+                const size_t hi = has_r && has_w ? std::max(rhi, whi) : (has_r ? rhi : whi);
+                mi.ptr = a->dev + lo;
+                mi.readPtr = has_r ? a->dev + rlo : nullptr;
+                mi.writePtr = has_w ? a->dev + wlo : nullptr;
+                mi.length = hi - lo;
+            } else {
+                compacts[i] = compact_of(m);
+                PMR_DEV(pmb_malloc_async(&s.dev_compact[i], compacts[i].length, c.copy_stream));
+                char* packed = static_cast<char*>(s.dev_compact[i]);
+                for (const Record& r : m.reads) {
+                    const pmStatus st = pack_record(a, r, compacts[i], packed, true, c.copy_stream);
+                    if (st != pmSuccess) return st;
+                }
+                mi.ptr = packed;
+                mi.readPtr = has_r ? packed + compacts[i].offset_of(m.reads.front().offset) : nullptr;
+                mi.writePtr = has_w ? packed + compacts[i].offset_of(m.writes.front().offset) : nullptr;
+                mi.length = compacts[i].length;
+            }
+            info.memInfo[i] = mi;
+        }
+        void* staged = new_event();
+        if (!staged) return fail(pmGraphicsCardError, "event creation failed: %s", pmb_last_error());
+        PMR_DEV(pmb_event_record(staged, c.copy_stream));
+        if (batch) continue;  // launched once for the whole task below
+
+        // ---- launch (compute stream) ----
+        const size_t sidx = si % c.streams.size();
+        void* stream = c.streams[sidx];
+        used_stream[sidx] = true;
+        PMR_DEV(pmb_stream_wait_event(stream, staged));
+        if (s.reserved) {
+            PMR_DEV(pmb_malloc_async(&s.dev_reserved, s.reserved, stream));
+            info.gpuContext.reservedGlobalMem = s.dev_reserved;
+        }
+        auto sc = s.scratch.find(PRE_SUBTASK_TO_SUBTASK);
+        if (sc == s.scratch.end()) sc = s.scratch.find(PRE_SUBTASK_TO_POST_SUBTASK);
+        if (sc == s.scratch.end()) sc = s.scratch.find(SUBTASK_TO_POST_SUBTASK);
+        if (sc != s.scratch.end() && !sc->second.empty()) {
+            PMR_DEV(pmb_malloc_async(&s.dev_scratch, sc->second.size(), stream));
+            if (sc->first != SUBTASK_TO_POST_SUBTASK)
+                PMR_DEV(pmb_memcpy_async(s.dev_scratch, sc->second.data(), sc->second.size(), PMB_H2D, stream));
+            info.gpuContext.scratchBuffer = s.dev_scratch;
+        }
+        s.info = info;
+        pmStatus st = pmSuccess;
+        if (cb.subtask_gpu_custom) {
+            st = cb.subtask_gpu_custom(t->info, c.gpu_info, info, stream);
+        } else {
+            const pmCudaLaunchConf lc = s.has_conf ? s.conf : pmCudaLaunchConf();
+            pmTaskInfo ti = t->dev_info;
+            void* dinfo = c.dev_device_info;
+            pmSubtaskInfo sinfo = info;
+            void* dstat = c.dev_status;
+            void* args[4] = {&ti, &dinfo, &sinfo, &dstat};
+            const int ls = pmb_launch_kernel(reinterpret_cast<const void*>(cb.subtask_gpu_cuda), lc.blocksX, lc.blocksY,
+                                             lc.blocksZ, lc.threadsX, lc.threadsY, lc.threadsZ, lc.sharedMem, args,
+                                             stream);
+            if (ls != PMB_SUCCESS) return dev_fail(ls, "subtask kernel launch");
+        }
+        if (st != pmSuccess) return fail(st, "GPU callback of subtask %lu returned %d", s.id, static_cast<int>(st));
+        c.stats.gpu_subtasks++;
+        // ---- results (compute stream) ----
+        for (size_t i = 0; i < ns; ++i) {
+            AddressSpace* a = t->spaces[i];
+            const SubtaskMem& m = s.mem[i];
+            if (m.writes.empty()) continue;
+            std::lock_guard<std::mutex> g(a->mu);
+            if (t->views[i] == SUBSCRIPTION_COMPACT) {
+                for (const Record& r : m.writes) {
+                    const pmStatus ps = pack_record(a, r, compacts[i], static_cast<char*>(s.dev_compact[i]), false, stream);
+                    if (ps != pmSuccess) return ps;
+                }
+            }
+            for (const Record& r : m.writes) {
+                add_record(a->dev_valid, r);
+                add_record(a->host_stale, r);
+            }
+        }
+        if (s.dev_scratch && (sc->first == SUBTASK_TO_POST_SUBTASK || sc->first == PRE_SUBTASK_TO_POST_SUBTASK))
+            PMR_DEV(pmb_memcpy_async(sc->second.data(), s.dev_scratch, sc->second.size(), PMB_D2H, stream));
+        for (size_t i = 0; i < ns; ++i)
+            if (s.dev_compact[i]) PMR_DEV(pmb_free_async(s.dev_compact[i], stream));
+        if (s.dev_reserved) PMR_DEV(pmb_free_async(s.dev_reserved, stream));
+        if (s.dev_scratch) PMR_DEV(pmb_free_async(s.dev_scratch, stream));
+    }
+
+    if (batch) {
+        void* stream = c.streams[0];
+        used_stream[0] = true;
+        PMR_DEV(pmb_stream_wait_event(stream, events.back()));  // copy stream is ordered: all staged
+        const pmStatus st = batch(&t->info, &c.gpu_info, infos.data(), infos.size(), stream);
+        if (st != pmSuccess) return fail(st, "batched GPU callback returned %d", static_cast<int>(st));
+        c.stats.batched++;
+        c.stats.gpu_subtasks += infos.size();
+        for (size_t si = 0; si < t->subtasks.size(); ++si) {
+            t->subtasks[si].info = infos[si];
+            for (size_t i = 0; i < ns; ++i) {
+                AddressSpace* a = t->spaces[i];
+                std::lock_guard<std::mutex> g(a->mu);
+                for (const Record& r : t->subtasks[si].mem[i].writes) {
+                    add_record(a->dev_valid, r);
+                    add_record(a->host_stale, r);
+                }
+            }
+        }
+    }
+
+    // ---- join all streams into the task's completion event ----
+    {
+        void* e = new_event();
+        if (!e) return fail(pmGraphicsCardError, "event creation failed");
+        PMR_DEV(pmb_event_record(e, c.copy_stream));
+        PMR_DEV(pmb_stream_wait_event(c.join_stream, e));
+    }
+    for (size_t k = 0; k < c.streams.size(); ++k) {
+        if (!used_stream[k]) continue;
+        void* e = new_event();
+        if (!e) return fail(pmGraphicsCardError, "event creation failed");
+        PMR_DEV(pmb_event_record(e, c.streams[k]));
+        PMR_DEV(pmb_stream_wait_event(c.join_stream, e));
+    }
+    if (write_through) {
+        for (size_t i = 0; i < ns; ++i) {
+            AddressSpace* a = t->spaces[i];
+            std::lock_guard<std::mutex> g(a->mu);
+            std::vector<std::pair<size_t, size_t>> st;
+            a->host_stale.present(0, a->length, st);
+            for (auto& r : st) {
+                PMR_DEV(pmb_memcpy_async(a->host + r.first, a->dev + r.first, r.second - r.first, PMB_D2H, c.join_stream));
+                c.stats.d2h += r.second - r.first;
+            }
+            a->host_stale.clear();
+        }
+    }
+    if (t->dev_conf) PMR_DEV(pmb_free_async(t->dev_conf, c.join_stream));
+    t->dev_conf = nullptr;
+    PMR_DEV(pmb_event_record(t->done_event, c.join_stream));
+    for (size_t i = 0; i < ns; ++i) {
+        AddressSpace* a = t->spaces[i];
+        std::lock_guard<std::mutex> g(a->mu);
+        if (!a->last_access) PMR_DEV(pmb_event_create(&a->last_access, 0));
+        PMR_DEV(pmb_event_record(a->last_access, c.join_stream));
+        const bool writes = t->mem[i].memType != READ_ONLY && t->mem[i].memType != READ_ONLY_LAZY;
+        if (writes) {
+            if (!a->last_write) PMR_DEV(pmb_event_create(&a->last_write, 0));
+            PMR_DEV(pmb_event_record(a->last_write, c.join_stream));
+        }
+        if (write_through) a->dev_valid.clear();
+    }
+    // Events may be destroyed once recorded: CUDA keeps recorded work alive.
+    for (void* e : events) pmb_event_destroy(e);
+    return pmSuccess;
+}
+
+// CPU execution (tasks whose callbacks have no GPU subtask function): NATURAL
+// views of the host copies, subtasks spread over the host cores.
+static pmStatus run_cpu_task(Task* t) {
+    const size_t ns = t->spaces.size();
+    if (!t->callbacks->cb.subtask_cpu) return pmSuccess;  // placement-only task
+    for (size_t i = 0; i < ns; ++i) {
+        AddressSpace* a = t->spaces[i];
+        std::lock_guard<std::mutex> g(a->mu);
+        const pmStatus st = fetch_range(a, 0, a->length);
+        if (st != pmSuccess) return st;
+    }
+    const unsigned nthreads = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(),
+                                                              static_cast<unsigned>(t->subtasks.size())));
+    std::atomic<size_t> next(0);
+    std::atomic<int> err(pmSuccess);
+    auto worker = [&]() {
+        for (;;) {
+            const size_t k = next.fetch_add(1);
+            if (k >= t->subtasks.size() || err.load() != pmSuccess) break;
+            if (t->deadline > 0 && now_s() > t->deadline) {
+                err.store(pmStatusUnavailable);
+                break;
+            }
+            Subtask& s = t->subtasks[k];
+            pmSubtaskInfo info;
+            info.subtaskId = s.id;
+            info.memCount = static_cast<uint>(ns);
+            std::vector<std::vector<char>> packed(ns);
+            std::vector<Compact> compacts(ns);
+            for (size_t i = 0; i < ns; ++i) {
+                AddressSpace* a = t->spaces[i];
+                const SubtaskMem& m = s.mem[i];
+                size_t rlo, rhi, wlo, whi;
+                consolidated(m.reads, rlo, rhi);
+                consolidated(m.writes, wlo, whi);
+                const bool has_r = rhi > rlo, has_w = whi > wlo;
+                pmMemInfo mi;
+                mi.visibilityType = t->mem[i].subscriptionVisibilityType == SUBSCRIPTION_COMPACT ? SUBSCRIPTION_COMPACT
+                                                                                               : SUBSCRIPTION_NATURAL;
+                if (has_r || has_w) {
+                    if (mi.visibilityType == SUBSCRIPTION_NATURAL) {
+                        const size_t lo = has_r && has_w ? std::min(rlo, wlo) : (has_r ? rlo : wlo);
+                        const size_t hi = has_r && has_w ? std::max(rhi, whi) : (has_r ? rhi : whi);
+                        mi.ptr = a->host + lo;
+                        mi.readPtr = has_r ? a->host + rlo : nullptr;
+                        mi.writePtr = has_w ? a->host + wlo : nullptr;
+                        mi.length = hi - lo;
+                    } else {
+                        compacts[i] = compact_of(m);
+                        packed[i].assign(compacts[i].length, 0);
+                        for (auto& pc : compacts[i].pieces)
+                            memcpy(packed[i].data() + compacts[i].offset_of(pc.first), a->host + pc.first, pc.second);
+                        mi.ptr = packed[i].data();
+                        mi.readPtr = has_r ? packed[i].data() + compacts[i].offset_of(m.reads.front().offset) : nullptr;
+                        mi.writePtr = has_w ? packed[i].data() + compacts[i].offset_of(m.writes.front().offset) : nullptr;
+                        mi.length = compacts[i].length;
+                    }
+                }
+                info.memInfo[i] = mi;
+            }
+            const pmStatus st = t->callbacks->cb.subtask_cpu(t->info, ctl().cpu_info, info);
+            if (st != pmSuccess) {
+                err.store(st);
+                break;
+            }
+            for (size_t i = 0; i < ns; ++i) {
+                if (!packed[i].empty())
+                    for (const Record& r : s.mem[i].writes)
+                        for (size_t q = 0; q < std::max<size_t>(r.count, 1); ++q) {
+                            const size_t off = r.offset + q * r.step;
+                            memcpy(t->spaces[i]->host + off, packed[i].data() + compacts[i].offset_of(off), r.size);
+                        }
+            }
+        }
+    };
+    std::vector<std::thread> pool;
+    for (unsigned k = 1; k < nthreads; ++k) pool.emplace_back(worker);
+    worker();
+    for (auto& th : pool) th.join();
+    for (size_t i = 0; i < ns; ++i) {
+        AddressSpace* a = t->spaces[i];
+        std::lock_guard<std::mutex> g(a->mu);
+        for (Subtask& s : t->subtasks)
+            for (const Record& r : s.mem[i].writes) {
+                for (size_t q = 0; q < std::max<size_t>(r.count, 1); ++q)
+                    a->dev_valid.remove(r.offset + q * r.step, r.offset + q * r.step + r.size);
+            }
+    }
+    if (err.load() == pmStatusUnavailable) return fail(pmStatusUnavailable, "task timed out");
+    if (err.load() != pmSuccess) return fail(static_cast<pmStatus>(err.load()), "CPU subtask callback failed");
+    return pmSuccess;
+}
+
+static void finish_task(Task* t, pmStatus st, const std::string& msg) {
+    Controller& c = ctl();
+    for (AddressSpace* a : t->spaces) {
+        bool free_now = false;
+        {
+            std::lock_guard<std::mutex> g(c.mu);
+            a->users--;
+            free_now = a->released && a->users == 0;
+            if (free_now) c.spaces.erase(a);
+        }
+        if (free_now) free_space(a);
+    }
+    if (st == pmSuccess && t->callbacks->cb.taskCompletionCallback) st = t->callbacks->cb.taskCompletionCallback(t->info);
+    {
+        std::lock_guard<std::mutex> g(t->mu);
+        if (t->status == pmSuccess) t->status = st;
+        if (!msg.empty() && t->error.empty()) t->error = msg;
+        t->t_end = now_s();
+        t->state = 2;
+    }
+    t->cv.notify_all();
+}
+
+static void stub_main() {
+    Controller& c = ctl();
+    if (c.has_gpu) pmb_set_device(c.device);
+    for (;;) {
+        Task* t = nullptr;
+        {
+            std::unique_lock<std::mutex> lk(c.qmu);
+            c.qcv.wait(lk, [&] { return c.stopping || !c.queue.empty(); });
+            if (c.queue.empty()) return;
+            t = c.queue.front();
+            c.queue.pop_front();
+        }
+        t->t_start = now_s();
+        t->state = 1;
+        if (t->deadline > 0 && now_s() > t->deadline) {
+            finish_task(t, pmStatusUnavailable, "task timed out before it started");
+            continue;
+        }
+        pmStatus st = run_dd(t, t->on_gpu ? c.gpu_info : c.cpu_info);
+        if (st == pmSuccess) {
+            if (t->on_gpu) {
+                st = stage_and_launch_gpu(t);
+                if (st == pmSuccess) {
+                    std::lock_guard<std::mutex> lk(c.qmu);
+                    c.inflight.push_back(t);
+                    c.icv.notify_all();
+                    continue;
+                }
+                // Work already enqueued must drain before the task is reported.
+                pmb_device_synchronize();
+            } else {
+                st = run_cpu_task(t);
+            }
+        }
+        finish_task(t, st, st == pmSuccess ? "" : t_last_error);
+    }
+}
+
+static void completer_main() {
+    Controller& c = ctl();
+    if (c.has_gpu) pmb_set_device(c.device);
+    for (;;) {
+        Task* t = nullptr;
+        {
+            std::unique_lock<std::mutex> lk(c.qmu);
+            c.icv.wait(lk, [&] { return c.stopping || !c.inflight.empty(); });
+            if (c.inflight.empty()) return;
+            t = c.inflight.front();
+        }
+        int st;
+        while ((st = pmb_event_query(t->done_event)) == PMB_STATUS_UNAVAILABLE)
+            std::this_thread::sleep_for(std::chrono::microseconds(20));
+        {
+            std::lock_guard<std::mutex> lk(c.qmu);
+            c.inflight.pop_front();
+        }
+        finish_task(t, st == PMB_SUCCESS ? pmSuccess : pmGraphicsCardError,
+                    st == PMB_SUCCESS ? "" : std::string(pmb_last_error()));
+    }
+}
+
+static pmStatus ensure_init() {
+    return ctl().initialized ? pmSuccess : fail(pmInitializationFailure, "pmInitialize has not been called");
+}
+
+}  // namespace pmr
+
+// ===========================================================================
+// public API
+// ===========================================================================
+namespace pm {
+
+using namespace pmr;
+
+const char* pmGetLibVersion() { return "pmlib-b200 1_0_0"; }
+
+const char* pmGetLastError() { return t_last_error.c_str(); }
+
+pmStatus pmInitialize() {
+    Controller& c = ctl();
+    std::lock_guard<std::mutex> g(c.mu);
+    if (c.initialized) return pmSuccess;
+    int n = 0;
+    pmb_device_count(&n);
+    const char* dv = getenv("PMB_DEVICE");
+    c.device = dv ? atoi(dv) : 0;
+    c.has_gpu = n > c.device && pmb_device_supported(c.device);
+    std::memset(c.cpu_info.name, 0, sizeof(c.cpu_info.name));
+    std::snprintf(c.cpu_info.name, MAX_NAME_STR_LEN, "host CPU");
+    std::snprintf(c.cpu_info.description, MAX_DESC_STR_LEN, "%u hardware threads", std::thread::hardware_concurrency());
+    c.cpu_info.deviceHandle = &c.cpu_info;
+    c.cpu_info.deviceType = CPU;
+    c.cpu_info.host = 0;
+    c.cpu_info.deviceIdOnHost = 0;
+    c.cpu_info.deviceIdInCluster = 0;
+    if (c.has_gpu) {
+        if (pmb_set_device(c.device) != PMB_SUCCESS) return dev_fail(PMB_GRAPHICS_CARD_ERROR, "device selection");
+        int sms = 0, ma = 0, mi = 0;
+        pmb_device_properties(c.device, c.gpu_info.name, MAX_NAME_STR_LEN, &sms, &ma, &mi);
+        std::snprintf(c.gpu_info.description, MAX_DESC_STR_LEN, "sm_%d%d, %d SMs", ma, mi, sms);
+        c.gpu_info.deviceHandle = &c.gpu_info;
+        c.gpu_info.deviceType = GPU_CUDA;
+        c.gpu_info.host = 0;
+        c.gpu_info.deviceIdOnHost = static_cast<uint>(c.device);
+        c.gpu_info.deviceIdInCluster = 1;
+        PMR_DEV(pmb_stream_create(&c.copy_stream));
+        PMR_DEV(pmb_stream_create(&c.join_stream));
+        PMR_DEV(pmb_stream_create(&c.fetch_stream));
+        c.streams.resize(4);
+        for (auto& s : c.streams) PMR_DEV(pmb_stream_create(&s));
+        PMR_DEV(pmb_malloc(&c.dev_device_info, sizeof(pmDeviceInfo)));
+        PMR_DEV(pmb_memcpy_async(c.dev_device_info, &c.gpu_info, sizeof(pmDeviceInfo), PMB_H2D, c.copy_stream));
+        PMR_DEV(pmb_malloc(&c.dev_status, sizeof(pmStatus)));
+        PMR_DEV(pmb_stream_synchronize(c.copy_stream));
+        const char* rv = getenv("PMLIB_CUDA_MEM_PER_CARD_RESERVED_FOR_EXTERNAL_USE");
+        c.reserve_bytes = rv ? static_cast<size_t>(atoll(rv)) : (size_t(512) << 20);
+    }
+    c.stopping = false;
+    c.stub = std::thread(stub_main);
+    c.completer = std::thread(completer_main);
+    c.initialized = true;
+    return pmSuccess;
+}
+
+pmStatus pmFinalize() {
+    Controller& c = ctl();
+    if (!c.initialized) return pmSuccess;
+    {
+        std::lock_guard<std::mutex> lk(c.qmu);
+        c.stopping = true;
+    }
+    c.qcv.notify_all();
+    c.icv.notify_all();
+    if (c.stub.joinable()) c.stub.join();
+    if (c.completer.joinable()) c.completer.join();
+    std::lock_guard<std::mutex> g(c.mu);
+    if (c.has_gpu) {
+        pmb_device_synchronize();
+        for (void* s : c.streams) pmb_stream_destroy(s);
+        c.streams.clear();
+        pmb_stream_destroy(c.copy_stream);
+        pmb_stream_destroy(c.join_stream);
+        pmb_stream_destroy(c.fetch_stream);
+        pmb_free(c.dev_device_info);
+        pmb_free(c.dev_status);
+    }
+    for (AddressSpace* a : c.spaces) free_space(a);
+    c.spaces.clear();
+    for (auto& kv : c.files) munmap(kv.second.first, kv.second.second);
+    c.files.clear();
+    c.callbacks.clear();
+    c.initialized = false;
+    return pmSuccess;
+}
+
+uint pmGetHostId() { return 0; }
+uint pmGetHostCount() { return 1; }
+
+pmStatus pmRegisterCallbacks(const char* pKey, pmCallbacks pCallbacks, pmCallbackHandle* pCallbackHandle) {
+    if (ensure_init() != pmSuccess) return pmInitializationFailure;
+    if (!pKey || !pCallbackHandle) return fail(pmInvalidKey, "null key or handle");
+    if (strlen(pKey) >= MAX_CB_KEY_LEN) return fail(pmMaxKeyLengthExceeded, "callback key longer than %zu", MAX_CB_KEY_LEN - 1);
+    if (pCallbacks.subtask_gpu_cuda && pCallbacks.subtask_gpu_custom)
+        return fail(pmInvalidCallbacks, "subtask_gpu_cuda and subtask_gpu_custom are both set");
+    Controller& c = ctl();
+    std::lock_guard<std::mutex> g(c.mu);
+    for (auto& cs : c.callbacks)
+        if (cs->key == pKey) return fail(pmInvalidKey, "callback key '%s' already registered", pKey);
+    c.callbacks.emplace_back(new CallbackSet{pKey, pCallbacks});
+    *pCallbackHandle = c.callbacks.back().get();
+    return pmSuccess;
+}
+
+pmStatus pmReleaseCallbacks(pmCallbackHandle pCallbackHandle) {
+    Controller& c = ctl();
+    std::lock_guard<std::mutex> g(c.mu);
+    for (auto it = c.callbacks.begin(); it != c.callbacks.end(); ++it)
+        if (it->get() == pCallbackHandle) {
+            c.callbacks.erase(it);
+            return pmSuccess;
+        }
+    return fail(pmInvalidKey, "unknown callback handle");
+}
+
+pmStatus pmCreateMemory(size_t pLength, pmMemHandle* pMemHandle) {
+    if (ensure_init() != pmSuccess) return pmInitializationFailure;
+    if (!pMemHandle) return fail(pmInvalidIndex, "null handle");
+    Controller& c = ctl();
+    std::unique_ptr<AddressSpace> a(new AddressSpace);
+    a->length = pLength;
+    void* p = nullptr;
+    if (c.has_gpu) {
+        if (pmb_host_alloc(&p, pLength ? pLength : 1) != PMB_SUCCESS) return dev_fail(PMB_MEMORY_ERROR, "pinned host allocation");
+    } else {
+        p = malloc(pLength ? pLength : 1);
+        if (!p) return fail(pmMemoryError, "host allocation of %zu bytes failed", pLength);
+    }
+    a->host = static_cast<char*>(p);
+    std::lock_guard<std::mutex> g(c.mu);
+    c.spaces.insert(a.get());
+    *pMemHandle = a.release();
+    return pmSuccess;
+}
+
+pmStatus pmCreateMemory2D(size_t pRows, size_t pCols, pmMemHandle* pMemHandle) {
+    const pmStatus st = pmCreateMemory(pRows * pCols, pMemHandle);
+    if (st == pmSuccess) {
+        AddressSpace* a = static_cast<AddressSpace*>(*pMemHandle);
+        a->rows = pRows;
+        a->cols = pCols;
+    }
+    return st;
+}
+
+pmStatus pmReleaseMemory(pmMemHandle pMemHandle) {
+    Controller& c = ctl();
+    AddressSpace* a = space_of(pMemHandle);
+    if (!a) return fail(pmUnrecognizedMemory, "unknown memory handle");
+    bool free_now;
+    {
+        std::lock_guard<std::mutex> g(c.mu);
+        a->released = true;
+        free_now = a->users == 0;
+        if (free_now) c.spaces.erase(a);
+    }
+    if (free_now) {
+        if (a->last_access) pmb_event_synchronize(a->last_access);
+        free_space(a);
+    }
+    return pmSuccess;
+}
+
+pmStatus pmFetchMemory(pmMemHandle pMemHandle) {
+    AddressSpace* a = space_of(pMemHandle);
+    if (!a) return fail(pmUnrecognizedMemory, "unknown memory handle");
+    if (ctl().has_gpu) pmb_set_device(ctl().device);
+    std::lock_guard<std::mutex> g(a->mu);
+    return fetch_range(a, 0, a->length);
+}
+
+pmStatus pmFetchMemoryRange(pmMemHandle pMemHandle, size_t pOffset, size_t pLength) {
+    AddressSpace* a = space_of(pMemHandle);
+    if (!a) return fail(pmUnrecognizedMemory, "unknown memory handle");
+    if (pOffset + pLength > a->length) return fail(pmInvalidOffset, "range beyond the address space");
+    if (ctl().has_gpu) pmb_set_device(ctl().device);
+    std::lock_guard<std::mutex> g(a->mu);
+    return fetch_range(a, pOffset, pOffset + pLength);
+}
+
+pmStatus pmGetRawMemPtr(pmMemHandle pMemHandle, pmRawMemPtr* pPtr) {
+    AddressSpace* a = space_of(pMemHandle);
+    if (!a || !pPtr) return fail(pmUnrecognizedMemory, "unknown memory handle");
+    std::lock_guard<std::mutex> g(a->mu);
+    // The caller may now write the host copy: device bytes that are not newer
+    // than the host are no longer trusted (they are re-staged on next use).
+    RangeSet keep;
+    for (auto& kv : a->host_stale.map()) keep.add(kv.first, kv.second);
+    a->dev_valid = keep;
+    *pPtr = a->host;
+    return pmSuccess;
+}
+
+static pmStatus subscribe(pmTaskHandle pTaskHandle, ulong pSubtaskId, uint pMemIndex, pmSubscriptionType pType,
+                          const Record& r) {
+    Task* t = static_cast<Task*>(pTaskHandle);
+    if (!t || t_dd.task != t) return fail(pmInvalidCommand, "pmSubscribeToMemory outside a data-distribution callback");
+    if (pSubtaskId >= t->subtasks.size()) return fail(pmInvalidIndex, "subtask %lu out of range", pSubtaskId);
+    if (pMemIndex >= t->spaces.size()) return fail(pmInvalidIndex, "memory index %u out of range", pMemIndex);
+    AddressSpace* a = t->spaces[pMemIndex];
+    if (r.count && r.size && (r.hi() > a->length || (r.count > 1 && r.step < r.size)))
+        return fail(pmInvalidOffset, "subscription [%zu, %zu) outside the %zu-byte address space or overlapping",
+                    r.lo(), r.hi(), a->length);
+    const pmMemType mt = t->mem[pMemIndex].memType;
+    if (pType != READ_SUBSCRIPTION && (mt == READ_ONLY || mt == READ_ONLY_LAZY))
+        return fail(pmInvalidCommand, "write subscription on a read-only address space");
+    if (pType != WRITE_SUBSCRIPTION && (mt == WRITE_ONLY || mt == WRITE_ONLY_LAZY))
+        return fail(pmInvalidCommand, "read subscription on a write-only address space");
+    SubtaskMem& m = t->subtasks[pSubtaskId].mem[pMemIndex];
+    if (pType != WRITE_SUBSCRIPTION) m.reads.push_back(r);
+    if (pType != READ_SUBSCRIPTION) m.writes.push_back(r);
+    return pmSuccess;
+}
+
+pmStatus pmSubscribeToMemory(pmTaskHandle pTaskHandle, pmDeviceHandle, ulong pSubtaskId, pmSplitInfo&, uint pMemIndex,
+                             pmSubscriptionType pSubscriptionType, const pmSubscriptionInfo& pSubscriptionInfo) {
+    Record r;
+    r.offset = pSubscriptionInfo.offset;
+    r.size = pSubscriptionInfo.length;
+    r.step = pSubscriptionInfo.length;
+    r.count = pSubscriptionInfo.length ? 1 : 0;
+    return subscribe(pTaskHandle, pSubtaskId, pMemIndex, pSubscriptionType, r);
+}
+
+pmStatus pmSubscribeToMemory(pmTaskHandle pTaskHandle, pmDeviceHandle, ulong pSubtaskId, pmSplitInfo&, uint pMemIndex,
+                             pmSubscriptionType pSubscriptionType, const pmScatteredSubscriptionInfo& pInfo) {
+    Record r;
+    r.offset = pInfo.offset;
+    r.size = pInfo.size;
+    r.step = pInfo.step;
+    r.count = pInfo.count;
+    return subscribe(pTaskHandle, pSubtaskId, pMemIndex, pSubscriptionType, r);
+}
+
+pmStatus pmRedistributeData(pmTaskHandle, pmDeviceHandle, ulong, pmSplitInfo&, uint, size_t, size_t, uint) {
+    return fail(pmStatusUnavailable, "data redistribution is not supported by the B200 runtime");
+}
+
+pmStatus pmSetCudaLaunchConf(pmTaskHandle pTaskHandle, pmDeviceHandle, ulong pSubtaskId, pmSplitInfo&,
+                             pmCudaLaunchConf& pCudaLaunchConf) {
+    Task* t = static_cast<Task*>(pTaskHandle);
+    if (!t || t_dd.task != t) return fail(pmInvalidCommand, "pmSetCudaLaunchConf outside a data-distribution callback");
+    if (pSubtaskId >= t->subtasks.size()) return fail(pmInvalidIndex, "subtask %lu out of range", pSubtaskId);
+    t->subtasks[pSubtaskId].conf = pCudaLaunchConf;
+    t->subtasks[pSubtaskId].has_conf = true;
+    return pmSuccess;
+}
+
+pmStatus pmReserveCudaGlobalMem(pmTaskHandle pTaskHandle, pmDeviceHandle, ulong pSubtaskId, pmSplitInfo&, size_t pSize) {
+    Task* t = static_cast<Task*>(pTaskHandle);
+    if (!t || t_dd.task != t) return fail(pmInvalidCommand, "pmReserveCudaGlobalMem outside a data-distribution callback");
+    if (pSubtaskId >= t->subtasks.size()) return fail(pmInvalidIndex, "subtask %lu out of range", pSubtaskId);
+    t->subtasks[pSubtaskId].reserved = pSize;
+    return pmSuccess;
+}
+
+pmStatus pmSubmitTask(pmTaskDetails pTaskDetails, pmTaskHandle* pTaskHandle) {
+    if (ensure_init() != pmSuccess) return pmInitializationFailure;
+    Controller& c = ctl();
+    if (!pTaskHandle) return fail(pmInvalidIndex, "null task handle");
+    if (pTaskDetails.taskMemCount > MAX_MEM_SECTIONS_PER_TASK)
+        return fail(pmInvalidIndex, "%u address spaces (maximum %zu)", pTaskDetails.taskMemCount, MAX_MEM_SECTIONS_PER_TASK);
+    if (pTaskDetails.taskMemCount && !pTaskDetails.taskMem) return fail(pmInvalidIndex, "null taskMem");
+    std::unique_ptr<Task> t(new Task);
+    {
+        std::lock_guard<std::mutex> g(c.mu);
+        for (auto& cs : c.callbacks)
+            if (cs.get() == pTaskDetails.callbackHandle) t->callbacks = cs.get();
+    }
+    if (!t->callbacks) return fail(pmInvalidCallbacks, "unknown callback handle");
+    const pmCallbacks& cb = t->callbacks->cb;
+    t->details = pTaskDetails;
+    if (pTaskDetails.taskConf && pTaskDetails.taskConfLength)
+        t->conf.assign(static_cast<char*>(pTaskDetails.taskConf),
+                       static_cast<char*>(pTaskDetails.taskConf) + pTaskDetails.taskConfLength);
+    for (uint i = 0; i < pTaskDetails.taskMemCount; ++i) {
+        AddressSpace* a = space_of(pTaskDetails.taskMem[i].memHandle);
+        if (!a) return fail(pmUnrecognizedMemory, "taskMem[%u] is not a live address space", i);
+        if (pTaskDetails.taskMem[i].memType >= MAX_MEM_TYPE) return fail(pmInvalidIndex, "taskMem[%u] has no memType", i);
+        t->mem.push_back(pTaskDetails.taskMem[i]);
+        t->spaces.push_back(a);
+    }
+    t->subtasks.resize(pTaskDetails.subtaskCount);
+    for (ulong i = 0; i < pTaskDetails.subtaskCount; ++i) {
+        t->subtasks[i].id = i;
+        t->subtasks[i].mem.resize(t->spaces.size());
+    }
+    t->info.taskHandle = t.get();
+    t->info.taskConf = t->conf.empty() ? nullptr : t->conf.data();
+    t->info.taskConfLength = static_cast<uint>(t->conf.size());
+    t->info.taskId = pTaskDetails.taskId;
+    t->info.subtaskCount = pTaskDetails.subtaskCount;
+    t->info.priority = pTaskDetails.priority;
+    t->info.originatingHost = 0;
+    const bool gpu_cb = cb.subtask_gpu_cuda || cb.subtask_gpu_custom;
+    bool gpu_ok = gpu_cb && c.has_gpu;
+    if (gpu_ok && cb.deviceSelection) gpu_ok = cb.deviceSelection(t->info, c.gpu_info);
+    if (gpu_ok) {
+        t->on_gpu = true;
+        if (pmb_event_create(&t->done_event, 0) != PMB_SUCCESS) return dev_fail(PMB_GRAPHICS_CARD_ERROR, "event");
+    } else if (cb.subtask_cpu && (!cb.deviceSelection || cb.deviceSelection(t->info, c.cpu_info))) {
+        t->on_gpu = false;
+    } else if (!gpu_cb && !cb.subtask_cpu) {
+        t->on_gpu = false;  // placement-only task: data distribution runs, nothing executes
+    } else {
+        return fail(pmNoCompatibleDevice, gpu_cb ? "no supported CUDA device for this task" : "task has no usable subtask callback");
+    }
+    t->t_submit = now_s();
+    if (pTaskDetails.timeOutInSecs > 0 && pTaskDetails.timeOutInSecs < INT32_MAX)
+        t->deadline = t->t_submit + pTaskDetails.timeOutInSecs;
+    Task* raw = t.release();
+    {
+        std::lock_guard<std::mutex> g(c.mu);
+        c.tasks.insert(raw);
+        for (AddressSpace* a : raw->spaces) a->users++;
+    }
+    {
+        std::lock_guard<std::mutex> lk(c.qmu);
+        c.queue.push_back(raw);
+    }
+    c.qcv.notify_all();
+    *pTaskHandle = raw;
+    return pmSuccess;
+}
+
+pmStatus pmWaitForTaskCompletion(pmTaskHandle pTaskHandle) {
+    Task* t = task_of(pTaskHandle);
+    if (!t) return fail(pmInvalidIndex, "unknown task handle");
+    std::unique_lock<std::mutex> lk(t->mu);
+    if (t->deadline > 0) {
+        const auto dl = std::chrono::steady_clock::time_point(std::chrono::duration_cast<std::chrono::steady_clock::duration>(
+            std::chrono::duration<double>(t->deadline)));
+        if (!t->cv.wait_until(lk, dl, [&] { return t->state.load() == 2; }))
+            return fail(pmStatusUnavailable, "task timed out after %d s", t->details.timeOutInSecs);
+    } else {
+        t->cv.wait(lk, [&] { return t->state.load() == 2; });
+    }
+    if (t->status != pmSuccess) t_last_error = t->error;
+    return t->status;
+}
+
+pmStatus pmGetTaskExecutionTimeInSecs(pmTaskHandle pTaskHandle, double* pTime) {
+    const pmStatus st = pmWaitForTaskCompletion(pTaskHandle);
+    Task* t = task_of(pTaskHandle);
+    if (!t || !pTime) return fail(pmInvalidIndex, "unknown task handle");
+    *pTime = t->t_end - t->t_start;
+    return st;
+}
+
+pmStatus pmReleaseTask(pmTaskHandle pTaskHandle) {
+    Task* t = task_of(pTaskHandle);
+    if (!t) return fail(pmInvalidIndex, "unknown task handle");
+    {
+        std::unique_lock<std::mutex> lk(t->mu);
+        t->cv.wait(lk, [&] { return t->state.load() == 2; });  // even after a timeout: resources are in use
+    }
+    const pmStatus st = t->status;
+    {
+        std::lock_guard<std::mutex> g(ctl().mu);
+        ctl().tasks.erase(t);
+    }
+    if (t->done_event) pmb_event_destroy(t->done_event);
+    delete t;
+    return st;
+}
+
+pmStatus pmReleaseTaskAndResources(pmTaskDetails pTaskDetails, pmTaskHandle pTaskHandle) {
+    const pmStatus st = pmReleaseTask(pTaskHandle);
+    pmReleaseCallbacks(pTaskDetails.callbackHandle);
+    for (uint i = 0; i < pTaskDetails.taskMemCount; ++i) pmReleaseMemory(pTaskDetails.taskMem[i].memHandle);
+    return st;
+}
+
+void* pmGetScratchBufferHostFunc(pmTaskHandle pTaskHandle, pmDeviceHandle, ulong pSubtaskId, pmSplitInfo&,
+                                 pmScratchBufferType pScratchBufferType, size_t pBufferSize) {
+    Task* t = static_cast<Task*>(pTaskHandle);
+    if (!t || pSubtaskId >= t->subtasks.size()) return nullptr;
+    auto& m = t->subtasks[pSubtaskId].scratch;
+    auto it = m.find(pScratchBufferType);
+    if (it == m.end()) {
+        if (!pBufferSize) return nullptr;
+        it = m.emplace(pScratchBufferType, std::vector<char>(pBufferSize, 0)).first;
+    }
+    return it->second.data();
+}
+
+pmStatus pmReleaseScratchBuffer(pmTaskHandle pTaskHandle, pmDeviceHandle, ulong pSubtaskId, pmSplitInfo&,
+                                pmScratchBufferType pScratchBufferType) {
+    Task* t = static_cast<Task*>(pTaskHandle);
+    if (!t || pSubtaskId >= t->subtasks.size()) return fail(pmInvalidIndex, "unknown subtask");
+    t->subtasks[pSubtaskId].scratch.erase(pScratchBufferType);
+    return pmSuccess;
+}
+
+void* pmGetLastReductionScratchBuffer(pmTaskHandle) { return nullptr; }
+
+pmRedistributionMetadata* pmGetRedistributionMetadata(pmTaskHandle, uint, ulong* pCount) {
+    if (pCount) *pCount = 0;
+    return nullptr;
+}
+
+pmDataReductionCallback pmGetSubtaskReductionCallbackImpl(pmReductionOpType, pmReductionDataType) { return nullptr; }
+
+pmStatus pmReduceSubtasks(pmTaskHandle, pmDeviceHandle, unsigned long, pmSplitInfo&, pmDeviceHandle, unsigned long,
+                          pmSplitInfo&, pmReductionOpType, pmReductionDataType) {
+    return fail(pmStatusUnavailable, "subtask reduction is not supported by the B200 runtime");
+}
+
+void* pmGetMappedFile(const char* pPath) {
+    if (!pPath) return nullptr;
+    std::lock_guard<std::mutex> g(ctl().mu);
+    auto it = ctl().files.find(pPath);
+    return it == ctl().files.end() ? nullptr : it->second.first;
+}
+
+pmStatus pmMapFile(const char* pPath) {
+    if (!pPath || strlen(pPath) >= MAX_FILE_SIZE_LEN) return fail(pmInvalidKey, "bad path");
+    const int fd = open(pPath, O_RDONLY);
+    if (fd < 0) return fail(pmConfFileNotFound, "cannot open %s", pPath);
+    struct stat sb;
+    if (fstat(fd, &sb) != 0) {
+        close(fd);
+        return fail(pmConfFileNotFound, "cannot stat %s", pPath);
+    }
+    void* p = mmap(nullptr, sb.st_size ? sb.st_size : 1, PROT_READ, MAP_PRIVATE, fd, 0);
+    close(fd);
+    if (p == MAP_FAILED) return fail(pmMemoryError, "mmap of %s failed", pPath);
+    std::lock_guard<std::mutex> g(ctl().mu);
+    ctl().files[pPath] = {p, static_cast<size_t>(sb.st_size ? sb.st_size : 1)};
+    return pmSuccess;
+}
+
+pmStatus pmUnmapFile(const char* pPath) {
+    std::lock_guard<std::mutex> g(ctl().mu);
+    auto it = pPath ? ctl().files.find(pPath) : ctl().files.end();
+    if (it == ctl().files.end()) return fail(pmInvalidKey, "file not mapped");
+    munmap(it->second.first, it->second.second);
+    ctl().files.erase(it);
+    return pmSuccess;
+}
+
+pmStatus pmMapFiles(const char* const* pPaths, uint pFileCount) {
+    for (uint i = 0; i < pFileCount; ++i) {
+        const pmStatus st = pmMapFile(pPaths[i]);
+        if (st != pmSuccess) return st;
+    }
+    return pmSuccess;
+}
+
+pmStatus pmUnmapFiles(const char* const* pPaths, uint pFileCount) {
+    for (uint i = 0; i < pFileCount; ++i) {
+        const pmStatus st = pmUnmapFile(pPaths[i]);
+        if (st != pmSuccess) return st;
+    }
+    return pmSuccess;
+}
+
+}  // namespace pm
+
+extern "C" int pmb_runtime_register_batch(void* subtask_gpu_custom, void* batch_fn) {
+    if (!subtask_gpu_custom || !batch_fn) return pm::pmInvalidIndex;
+    pmr::register_batch(reinterpret_cast<pm::pmSubtaskCallback_GPU_Custom>(subtask_gpu_custom),
+                        reinterpret_cast<pmr::BatchFn>(batch_fn));
+    return pm::pmSuccess;
+}
+
+extern "C" void pmb_runtime_stats(unsigned long long* h2d, unsigned long long* d2h, unsigned long long* gpu_subtasks,
+                                  unsigned long long* batched) {
+    pmr::Controller& c = pmr::ctl();
+    if (h2d) *h2d = c.stats.h2d;
+    if (d2h) *d2h = c.stats.d2h;
+    if (gpu_subtasks) *gpu_subtasks = c.stats.gpu_subtasks;
+    if (batched) *batched = c.stats.batched;
+}
+
+extern "C" void pmb_runtime_reset_stats(void) {
+    pmr::Controller& c = pmr::ctl();
+    c.stats.h2d = 0;
+    c.stats.d2h = 0;
+    c.stats.gpu_subtasks = 0;
+    c.stats.batched = 0;
+}

@@ -1,0 +1,131 @@
+// Internal declarations of the pm:: runtime (libpmlib.so).  Not installed:
+// apps include pmPublicDefinitions.h / pmPublicUtilities.h only.
+#pragma once
+
+#include <atomic>
+#include <condition_variable>
+#include <cstddef>
+#include <cstdint>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "pmPublicDefinitions.h"
+#include "pmPublicUtilities.h"
+
+namespace pmr {
+
+using namespace pm;
+
+// Sorted, disjoint, non-adjacent set of byte ranges [lo, hi).
+class RangeSet {
+public:
+    void add(size_t lo, size_t hi);
+    void remove(size_t lo, size_t hi);
+    bool covers(size_t lo, size_t hi) const;
+    // Parts of [lo, hi) not in the set, appended to `out`.
+    void missing(size_t lo, size_t hi, std::vector<std::pair<size_t, size_t>>& out) const;
+    // Parts of [lo, hi) in the set, appended to `out`.
+    void present(size_t lo, size_t hi, std::vector<std::pair<size_t, size_t>>& out) const;
+    bool empty() const { return m_.empty(); }
+    void clear() { m_.clear(); }
+    size_t bytes() const;
+    const std::map<size_t, size_t>& map() const { return m_; }
+
+private:
+    std::map<size_t, size_t> m_;  // lo -> hi
+};
+
+// `count` pieces of `size` bytes, `step` apart, the first at `offset`.
+struct Record {
+    size_t offset = 0, size = 0, step = 0, count = 0;
+    size_t lo() const { return offset; }
+    size_t hi() const { return count ? offset + (count - 1) * step + size : offset; }
+    bool contiguous() const { return count <= 1 || step == size; }
+};
+
+struct AddressSpace {
+    size_t length = 0;
+    size_t rows = 0, cols = 0;  // pmCreateMemory2D layout (informational)
+    char* host = nullptr;       // pinned host copy
+    char* dev = nullptr;        // device mirror, allocated on first GPU use
+    RangeSet dev_valid;         // bytes whose device copy is current
+    RangeSet host_stale;        // bytes the device has newer than the host
+    void* last_write = nullptr; // event after the last device write (owned)
+    void* last_access = nullptr;// event after the last device read or write (owned)
+    int users = 0;              // tasks submitted and not yet finished
+    bool released = false;
+    uint64_t lru = 0;
+    std::mutex mu;
+};
+
+struct SubtaskMem {
+    std::vector<Record> reads, writes;
+};
+
+struct Subtask {
+    ulong id = 0;
+    std::vector<SubtaskMem> mem;  // per task address space
+    bool has_conf = false;
+    pmCudaLaunchConf conf;
+    size_t reserved = 0;
+    std::map<int, std::vector<char>> scratch;  // pmScratchBufferType -> host buffer
+    void* dev_scratch = nullptr;
+    void* dev_reserved = nullptr;
+    std::vector<void*> dev_compact;  // per address space
+    pmSubtaskInfo info;              // device view handed to the GPU callback
+    pmStatus status = pmSuccess;
+};
+
+struct CallbackSet {
+    std::string key;
+    pmCallbacks cb;
+};
+
+struct Task;
+
+using BatchFn = pmStatus (*)(const pmTaskInfo* task, const pmDeviceInfo* device, const pmSubtaskInfo* subtasks,
+                             unsigned long count, void* stream);
+
+struct Task {
+    pmTaskDetails details;
+    std::vector<char> conf;      // host copy of taskConf
+    void* dev_conf = nullptr;    // device copy (subtask_gpu_cuda kernels dereference it)
+    std::vector<pmTaskMem> mem;
+    std::vector<AddressSpace*> spaces;
+    std::vector<pmSubscriptionVisibilityType> views;  // resolved per address space
+    CallbackSet* callbacks = nullptr;
+    std::vector<Subtask> subtasks;
+    pmTaskInfo info;             // host task info (taskConf = host copy)
+    pmTaskInfo dev_info;         // taskConf = device copy
+    bool on_gpu = false;
+    void* done_event = nullptr;
+    double t_submit = 0, t_start = 0, t_end = 0;
+    double deadline = 0;         // 0: none
+    std::atomic<int> state{0};   // 0 queued, 1 running, 2 done
+    pmStatus status = pmSuccess;
+    std::string error;
+    std::mutex mu;
+    std::condition_variable cv;
+};
+
+// Registers a whole-task GPU implementation for a subtask_gpu_custom callback:
+// when every subtask of a task uses that callback with NATURAL views, the
+// CUDA stub calls `batch` once for all of them instead of once per subtask.
+void register_batch(pmSubtaskCallback_GPU_Custom callback, BatchFn batch);
+
+}  // namespace pmr
+
+extern "C" {
+// C entry for apps libraries (see register_batch).
+int pmb_runtime_register_batch(void* subtask_gpu_custom, void* batch_fn);
+// Runtime statistics: bytes moved host->device / device->host, GPU callback
+// invocations, batched launches; for tests and benchmarks.
+void pmb_runtime_stats(unsigned long long* h2d_bytes, unsigned long long* d2h_bytes,
+                       unsigned long long* gpu_subtasks, unsigned long long* batched_launches);
+void pmb_runtime_reset_stats(void);
+}
