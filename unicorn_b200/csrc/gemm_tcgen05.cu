@@ -12,17 +12,26 @@
 // A*B ~= Ahi*Bhi + Ahi*Blo + Alo*Bhi (the Alo*Blo term, ~2^-18 relative, is
 // dropped).  All three products accumulate into the same FP32 TMEM tile.
 //
+// Accumulation: the tensor core's FP32 accumulate is not round-to-nearest, so
+// its error grows with the number of MMA results added into one accumulator
+// (measured: ~2.8e-5 normwise at K = 8192 in a single accumulator).  The K
+// loop is therefore cut into segments of 1024: each segment accumulates into
+// one of two 256-column TMEM buffers, and the epilogue warps drain a finished
+// buffer into C in IEEE FP32 (C = alpha*P + beta*C for the first segment,
+// C += alpha*P after) while the MMAs continue in the other buffer.
+//
 // Design: a split pass writes Ahi/Alo (M x Kp) and the transposed Bhi/Blo
 // (N x Kp) as K-major bf16.  The GEMM kernel owns a 128 x 256 output tile per
 // CTA and runs three warp roles:
 //   warp 0    TMA producer: one thread streams 32-deep K slices of the four
 //             operand tiles into a 4-stage shared-memory ring (SWIZZLE_64B),
 //             arming each stage's mbarrier with the expected byte count;
-//   warp 1    allocates 256 TMEM columns, then one thread issues the
-//             tcgen05.mma instructions (M=128, N=256, K=16, 3 per K step) and
-//             frees each stage back to the producer with tcgen05.commit;
-//   warps 2-5 epilogue: tcgen05.ld the accumulator (one row per thread),
-//             apply alpha/beta and store to C.
+//   warp 1    allocates 512 TMEM columns, then one thread issues the
+//             tcgen05.mma instructions (M=128, N=256, K=16, 3 per K step),
+//             frees each stage back to the producer with tcgen05.commit and
+//             signals each finished accumulator segment;
+//   warps 2-5 epilogue: tcgen05.ld each segment (one row per thread), apply
+//             alpha/beta and accumulate into C, then hand the buffer back.
 // Every mbarrier wait is bounded: on expiry the kernel records an error in the
 // workspace header, skips the remaining work, waits (bounded) for its own
 // in-flight tensor-core work and frees its TMEM before returning.
@@ -42,7 +51,8 @@ constexpr int kTileA = BM * BK * 2;   // 8 KB
 constexpr int kTileB = BN * BK * 2;   // 16 KB
 constexpr int kStageBytes = 2 * kTileA + 2 * kTileB;  // 48 KB
 constexpr int kSmemBytes = kStages * kStageBytes + 1024 /*align slack*/ + 256 /*barriers*/;
-constexpr uint32_t kTmemCols = 256;
+constexpr uint32_t kTmemCols = 512;         // two 256-column accumulators
+constexpr int kFlushStages = 32;            // K = 1024 per accumulator segment
 constexpr uint32_t kWaitLimit = 1u << 21;   // try_wait polls (each suspends <= ~1 us)
 constexpr uint32_t kErrTimeout = 4;         // workspace error bit
 
@@ -127,8 +137,12 @@ gemm_bf16x3_kernel(const __grid_constant__ GemmMaps maps, int M, int N, int KT, 
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
-    // bars[0..S): full, bars[S..2S): empty, bars[2S]: accumulator ready, bars[2S+1]: teardown
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 2);
+    // bars[0..S): stage full, [S..2S): stage empty, [2S, 2S+2): accumulator b
+    // full, [2S+2, 2S+4): accumulator b drained, [2S+4]: teardown
+    uint64_t* acc_full = bars + 2 * kStages;
+    uint64_t* acc_empty = bars + 2 * kStages + 2;
+    uint64_t* teardown = bars + 2 * kStages + 4;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages + 5);
     __shared__ volatile int s_fail;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -140,8 +154,11 @@ gemm_bf16x3_kernel(const __grid_constant__ GemmMaps maps, int M, int N, int KT, 
             mbar_init(smem_u32(&bars[s]), 1);
             mbar_init(smem_u32(&bars[kStages + s]), 1);
         }
-        mbar_init(smem_u32(&bars[2 * kStages]), 1);
-        mbar_init(smem_u32(&bars[2 * kStages + 1]), 1);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(smem_u32(&acc_full[b]), 1);
+            mbar_init(smem_u32(&acc_empty[b]), 4);  // one arrival per epilogue warp
+        }
+        mbar_init(smem_u32(teardown), 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
@@ -177,73 +194,85 @@ gemm_bf16x3_kernel(const __grid_constant__ GemmMaps maps, int M, int N, int KT, 
         }
     } else if (warp == 1 && lane == 0) {
         // ---- MMA issuer ----
-        int issued = 0;
         for (int kt = 0; kt < KT; ++kt) {
             const int s = kt % kStages;
+            const int seg = kt / kFlushStages, seg_k = kt % kFlushStages, b = seg & 1;
+            if (seg_k == 0 && seg >= 2 && !mbar_wait(smem_u32(&acc_empty[b]), ((seg >> 1) - 1) & 1)) {
+                s_fail = 1;
+                atomicOr(err, kErrTimeout);
+                break;
+            }
             if (!mbar_wait(smem_u32(&bars[s]), (kt / kStages) & 1)) {
                 s_fail = 1;
                 atomicOr(err, kErrTimeout);
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t acc = tmem + 256u * b;
             const uint32_t st = smem_u32(smem + s * kStageBytes);
             const uint32_t a_hi = st, a_lo = st + kTileA, b_hi = st + 2 * kTileA, b_lo = st + 2 * kTileA + kTileB;
 #pragma unroll
             for (int k16 = 0; k16 < BK / 16; ++k16) {
                 const uint32_t off = k16 * 32;  // 16 bf16 = 32 bytes along the swizzled row
-                umma_bf16(tmem, umma_desc_sw64(a_hi + off), umma_desc_sw64(b_hi + off), (kt | k16) != 0);
-                umma_bf16(tmem, umma_desc_sw64(a_hi + off), umma_desc_sw64(b_lo + off), 1u);
-                umma_bf16(tmem, umma_desc_sw64(a_lo + off), umma_desc_sw64(b_hi + off), 1u);
+                umma_bf16(acc, umma_desc_sw64(a_hi + off), umma_desc_sw64(b_hi + off), (seg_k | k16) != 0);
+                umma_bf16(acc, umma_desc_sw64(a_hi + off), umma_desc_sw64(b_lo + off), 1u);
+                umma_bf16(acc, umma_desc_sw64(a_lo + off), umma_desc_sw64(b_hi + off), 1u);
             }
             umma_commit(smem_u32(&bars[kStages + s]));
-            ++issued;
+            if (seg_k == kFlushStages - 1 || kt == KT - 1) umma_commit(smem_u32(&acc_full[b]));
         }
-        // Accumulator ready (or, after a failure, everything issued has retired).
-        umma_commit(smem_u32(&bars[2 * kStages]));
-        (void)issued;
     } else if (warp >= 2) {
-        // ---- epilogue ----
-        const bool ok = mbar_wait(smem_u32(&bars[2 * kStages]), 0);
-        if (!ok) {
-            s_fail = 1;
-            atomicOr(err, kErrTimeout);
-        }
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        // ---- epilogue: drain each accumulator segment into C ----
         const int q = warp & 3;  // TMEM lane quarter this warp may access
         const int row = m0 + 32 * q + lane;
-        const bool write = ok && !s_fail && KT > 0;
+        const int nseg = (KT + kFlushStages - 1) / kFlushStages;
+        for (int seg = 0; seg < nseg; ++seg) {
+            const int b = seg & 1;
+            if (!mbar_wait(smem_u32(&acc_full[b]), (seg >> 1) & 1)) {
+                s_fail = 1;
+                atomicOr(err, kErrTimeout);
+                break;
+            }
+            if (s_fail) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const float bscale = seg == 0 ? beta : 1.0f;
 #pragma unroll 1
-        for (int c = 0; c < BN / 16; ++c) {
-            uint32_t r[16];
-            tmem_ld16(tmem + (static_cast<uint32_t>(32 * q) << 16) + 16 * c, r);
-            const int col = n0 + 16 * c;
-            if (!write || row >= M || col >= N) continue;
-            float* crow = C + static_cast<int64_t>(row) * ldc + col;
-            const bool vec = col + 16 <= N && ((reinterpret_cast<uintptr_t>(crow) & 15) == 0);
-            if (vec) {
+            for (int c = 0; c < BN / 16; ++c) {
+                uint32_t r[16];
+                tmem_ld16(tmem + 256u * b + (static_cast<uint32_t>(32 * q) << 16) + 16 * c, r);
+                const int col = n0 + 16 * c;
+                if (row >= M || col >= N) continue;
+                float* crow = C + static_cast<int64_t>(row) * ldc + col;
+                const bool vec = col + 16 <= N && ((reinterpret_cast<uintptr_t>(crow) & 15) == 0);
+                if (vec) {
 #pragma unroll
-                for (int j = 0; j < 16; j += 4) {
-                    float4 o;
-                    o.x = alpha * __uint_as_float(r[j]);
-                    o.y = alpha * __uint_as_float(r[j + 1]);
-                    o.z = alpha * __uint_as_float(r[j + 2]);
-                    o.w = alpha * __uint_as_float(r[j + 3]);
-                    if (beta != 0.0f) {
-                        const float4 old = *reinterpret_cast<const float4*>(crow + j);
-                        o.x += beta * old.x;
-                        o.y += beta * old.y;
-                        o.z += beta * old.z;
-                        o.w += beta * old.w;
+                    for (int j = 0; j < 16; j += 4) {
+                        float4 o;
+                        o.x = alpha * __uint_as_float(r[j]);
+                        o.y = alpha * __uint_as_float(r[j + 1]);
+                        o.z = alpha * __uint_as_float(r[j + 2]);
+                        o.w = alpha * __uint_as_float(r[j + 3]);
+                        if (bscale != 0.0f) {
+                            const float4 old = *reinterpret_cast<const float4*>(crow + j);
+                            o.x += bscale * old.x;
+                            o.y += bscale * old.y;
+                            o.z += bscale * old.z;
+                            o.w += bscale * old.w;
+                        }
+                        *reinterpret_cast<float4*>(crow + j) = o;
                     }
-                    *reinterpret_cast<float4*>(crow + j) = o;
-                }
-            } else {
-                for (int j = 0; j < 16 && col + j < N; ++j) {
-                    float o = alpha * __uint_as_float(r[j]);
-                    if (beta != 0.0f) o += beta * crow[j];
-                    crow[j] = o;
+                } else {
+                    for (int j = 0; j < 16 && col + j < N; ++j) {
+                        float o = alpha * __uint_as_float(r[j]);
+                        if (bscale != 0.0f) o += bscale * crow[j];
+                        crow[j] = o;
+                    }
                 }
             }
+            // Buffer b is drained: its tcgen05.ld have completed (tmem_ld16 waits).
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acc_empty[b])) : "memory");
         }
     }
 
@@ -253,8 +282,8 @@ gemm_bf16x3_kernel(const __grid_constant__ GemmMaps maps, int M, int N, int KT, 
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         if (s_fail && lane == 0) {
             // Make sure every MMA this CTA issued has retired before freeing TMEM.
-            umma_commit(smem_u32(&bars[2 * kStages + 1]));
-            mbar_wait(smem_u32(&bars[2 * kStages + 1]), 0);
+            umma_commit(smem_u32(teardown));
+            mbar_wait(smem_u32(teardown), 0);
         }
         __syncwarp();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
