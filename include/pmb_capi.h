@@ -148,6 +148,17 @@ int pmb_image_filter(const pmb_imgf_item* items, int n_items,
 int pmb_image_filter_full(const uint8_t* d_in, uint8_t* d_out, int width, int height,
                           const int8_t* filter, int radius, int mode, void* stream);
 
+/* Host-to-host form: h_in / h_out are host images (pinned memory overlaps the
+ * copies), d_in / d_out device buffers of the same size (3*W*H bytes).  The
+ * image is processed in `bands` row bands (1..256) pipelined over three
+ * streams: band k+1 uploads while band k is filtered and band k-1 downloads.
+ * `stream` is the caller's stream; the call's work is complete when work
+ * enqueued on `stream` after it starts.  Replaces the staging of
+ * pmStubCUDA (source/code/src/pmExecutionStub.cpp:3655-3847) for a whole
+ * imageFiltering task whose address spaces live in host memory. */
+int pmb_image_filter_host(const uint8_t* h_in, uint8_t* h_out, uint8_t* d_in, uint8_t* d_out, int width, int height,
+                          const int8_t* filter, int radius, int mode, int bands, void* stream);
+
 /* Plain GPU form: one thread per output pixel, 3*(2r+1)^2 byte loads from
  * global memory and scalar multiply-adds; NATURAL views only.  The
  * one-task-at-a-time baseline the stencil kernel is compared with. */

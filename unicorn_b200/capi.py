@@ -93,6 +93,8 @@ _SIGS = {
     "pmb_image_filter_full": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_int, c_int, c_void_p]),
     "pmb_image_filter_plain": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_int, c_int, c_void_p]),
     "pmb_scan_scratch_bytes": (c_size_t, [c_size_t]),
+    "pmb_image_filter_host": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p, c_int, c_int,
+                                      c_int, c_void_p]),
     "pmb_inclusive_scan_u32_u64": (c_int, [c_void_p, c_void_p, c_size_t, c_void_p, c_size_t, c_void_p]),
     "pmb_scratch_error": (c_int, [c_void_p, ctypes.POINTER(ctypes.c_uint32)]),
     "pmb_radix_sort_scratch_bytes": (c_size_t, [c_size_t, c_int]),

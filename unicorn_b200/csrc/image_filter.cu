@@ -27,6 +27,7 @@
 // algorithmic 2 x 3WH bytes per pass.  The batch of subtasks (items) of one or
 // several tasks runs in ONE launch: blockIdx.x is mapped to (item, tile).
 #include <algorithm>
+#include <mutex>
 
 #include "pmb_common.cuh"
 
@@ -704,5 +705,100 @@ extern "C" int pmb_image_filter_plain(const uint8_t* d_in, uint8_t* d_out, int w
     else
         imgf_plain_kernel<PMB_IMGF_CLAMP><<<grid, block, 0, s>>>(d_in, d_out, width, height, radius, pf);
     PMB_CUDA_TRY(cudaGetLastError());
+    return PMB_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// Host-to-host form: the whole image comes from and returns to host memory.
+// Row bands are pipelined over three streams -- band k+1 uploads while band k
+// is filtered and band k-1 downloads -- so the PCIe transfers in both
+// directions overlap each other and the stencil.  Only the rows a band adds
+// (its new rows plus halo not yet uploaded) cross PCIe.
+namespace {
+
+struct PipeStreams {
+    cudaStream_t up = nullptr, down = nullptr;
+};
+
+int pipe_streams(PipeStreams& ps) {
+    static std::mutex mu;
+    static PipeStreams per_dev[64];
+    int dev = 0;
+    PMB_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return pmb::fail(PMB_BEYOND_LIMITS, "device ordinal %d", dev);
+    std::lock_guard<std::mutex> g(mu);
+    if (!per_dev[dev].up) {
+        PMB_CUDA_TRY(cudaStreamCreateWithFlags(&per_dev[dev].up, cudaStreamNonBlocking));
+        PMB_CUDA_TRY(cudaStreamCreateWithFlags(&per_dev[dev].down, cudaStreamNonBlocking));
+    }
+    ps = per_dev[dev];
+    return PMB_SUCCESS;
+}
+
+}  // namespace
+
+extern "C" int pmb_image_filter_host(const uint8_t* h_in, uint8_t* h_out, uint8_t* d_in, uint8_t* d_out, int width,
+                                     int height, const int8_t* filter, int radius, int mode, int bands, void* stream) {
+    PMB_CHECK_ARG(h_in && h_out && d_in && d_out && filter, "null pointer");
+    PMB_CHECK_ARG(width > 0 && height > 0, "bad image size");
+    PMB_CHECK_ARG(radius >= 1 && radius <= PMB_IMGF_MAX_RADIUS, "filter radius %d outside [1,%d]", radius,
+                  PMB_IMGF_MAX_RADIUS);
+    PMB_CHECK_ARG(bands >= 1 && bands <= 256, "bands %d outside [1,256]", bands);
+    if (bands > height) bands = height;
+    PipeStreams ps;
+    int st = pipe_streams(ps);
+    if (st != PMB_SUCCESS) return st;
+    cudaStream_t comp = static_cast<cudaStream_t>(stream);
+    const int64_t pitch = 3LL * width;
+    const int R = radius;
+    // Events are created per call (cheap); recorded ones may be destroyed at once.
+    cudaEvent_t start, ev_up[256], ev_k[256], done;
+    PMB_CUDA_TRY(cudaEventCreateWithFlags(&start, cudaEventDisableTiming));
+    PMB_CUDA_TRY(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+    PMB_CUDA_TRY(cudaEventRecord(start, comp));
+    PMB_CUDA_TRY(cudaStreamWaitEvent(ps.up, start, 0));
+    PMB_CUDA_TRY(cudaStreamWaitEvent(ps.down, start, 0));
+    int uploaded_hi = 0;  // image rows [0, uploaded_hi) are on the device
+    for (int b = 0; b < bands; ++b) {
+        const int r0 = static_cast<int>(static_cast<int64_t>(height) * b / bands);
+        const int r1 = static_cast<int>(static_cast<int64_t>(height) * (b + 1) / bands);
+        const int need_hi = r1 + R < height ? r1 + R : height;
+        if (need_hi > uploaded_hi) {
+            // image rows [uploaded_hi, need_hi) = buffer rows [H - need_hi, H - uploaded_hi)
+            const int64_t off = static_cast<int64_t>(height - need_hi) * pitch;
+            const size_t bytes = static_cast<size_t>(need_hi - uploaded_hi) * pitch;
+            PMB_CUDA_TRY(cudaMemcpyAsync(d_in + off, h_in + off, bytes, cudaMemcpyHostToDevice, ps.up));
+            uploaded_hi = need_hi;
+        }
+        PMB_CUDA_TRY(cudaEventCreateWithFlags(&ev_up[b], cudaEventDisableTiming));
+        PMB_CUDA_TRY(cudaEventRecord(ev_up[b], ps.up));
+        PMB_CUDA_TRY(cudaStreamWaitEvent(comp, ev_up[b], 0));
+        pmb_imgf_item it;
+        it.in = d_in;
+        it.out = d_out;
+        it.in_pitch = it.out_pitch = pitch;
+        it.width = width;
+        it.height = height;
+        it.in_row0 = it.in_col0 = it.out_row0 = it.out_col0 = 0;
+        it.r0 = r0;
+        it.r1 = r1;
+        it.c0 = 0;
+        it.c1 = width;
+        st = pmb_image_filter(&it, 1, filter, radius, mode, comp);
+        if (st != PMB_SUCCESS) return st;
+        PMB_CUDA_TRY(cudaEventCreateWithFlags(&ev_k[b], cudaEventDisableTiming));
+        PMB_CUDA_TRY(cudaEventRecord(ev_k[b], comp));
+        PMB_CUDA_TRY(cudaStreamWaitEvent(ps.down, ev_k[b], 0));
+        PMB_CUDA_TRY(cudaMemcpyAsync(h_out + static_cast<int64_t>(r0) * pitch, d_out + static_cast<int64_t>(r0) * pitch,
+                                     static_cast<size_t>(r1 - r0) * pitch, cudaMemcpyDeviceToHost, ps.down));
+    }
+    PMB_CUDA_TRY(cudaEventRecord(done, ps.down));
+    PMB_CUDA_TRY(cudaStreamWaitEvent(comp, done, 0));
+    for (int b = 0; b < bands; ++b) {
+        cudaEventDestroy(ev_up[b]);
+        cudaEventDestroy(ev_k[b]);
+    }
+    cudaEventDestroy(start);
+    cudaEventDestroy(done);
     return PMB_SUCCESS;
 }
