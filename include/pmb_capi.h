@@ -183,6 +183,23 @@ size_t pmb_scan_scratch_bytes(size_t n);
 int pmb_inclusive_scan_u32_u64(const uint32_t* d_in, uint64_t* d_out, size_t n, void* d_scratch,
                                size_t scratch_bytes, void* stream);
 
+/* Allocation-free form of pmb_inclusive_scan_u32_u64, with no counterpart in
+ * the reference.  It is for callers that must not allocate device memory: a
+ * pm:: subtask_gpu_custom callback may only enqueue work on the stream it is
+ * handed (cudaMalloc/cudaFree synchronise the device and would stall every
+ * subtask in flight), and a service that fixes its memory budget up front
+ * cannot let a library grow it.  The look-back scratch is a fixed 1 MiB
+ * device array inside libpmb.so, held by every GPU that loads the library
+ * until the process exits; the call allocates nothing, which limits n to
+ * PMB_SCAN_NOALLOC_MAX_ELEMS (longer inputs return PMB_BEYOND_LIMITS).  The
+ * first call on a device looks up the array's device address with that
+ * device current; make that first call before any stream capture.  All calls
+ * share the one array (each clears the part it uses before its kernel runs),
+ * so calls whose work overlaps on the GPU -- on different streams, or from
+ * different threads -- race and must be serialised by the caller. */
+#define PMB_SCAN_NOALLOC_MAX_ELEMS 536739840ull /* (1 MiB - 256 B) / 8 B per 4096-element tile */
+int pmb_inclusive_scan_u32_u64_noalloc(const uint32_t* d_in, uint64_t* d_out, size_t n, void* stream);
+
 /* Copy the error word of a scan/sort scratch buffer to the host (synchronous).
  * 0 = clean; 1 = a look-back wait hit its poll limit (the result is then
  * not trustworthy).  Replaces nothing in the reference (its kernels never wait

@@ -14,6 +14,8 @@
 // prefix.  Status words pack {flag:2, value:62}, so a relaxed 64-bit load sees
 // flag and value together.  Every input byte is read once and every output
 // byte written once: 12 bytes of HBM traffic per element.
+#include <mutex>
+
 #include "lookback.cuh"
 #include "pmb_common.cuh"
 
@@ -164,4 +166,57 @@ extern "C" int pmb_scratch_error(const void* d_scratch, uint32_t* error_out) {
     PMB_CUDA_TRY(cudaMemcpy(error_out, static_cast<const uint32_t*>(d_scratch) + 1, sizeof(uint32_t),
                             cudaMemcpyDeviceToHost));
     return PMB_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant.  Some callers may not allocate device memory at
+// all: a pm:: subtask_gpu_custom callback must only enqueue work on the stream
+// it is given (cudaMalloc and cudaFree synchronise the device and would stall
+// the stub's pipeline of in-flight subtasks), and services that fix their
+// memory budget up front cannot let a library grow it behind their back.  For
+// them the scan's look-back scratch lives in a fixed device array that every
+// GPU loading this library holds until the process exits.
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(1) << 20;  // 1 MiB per device
+__device__ __align__(256) unsigned char g_noalloc_scan_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kMaxDevices] = {};
+
+// Device address of g_noalloc_scan_scratch on the current device, looked up
+// once per device (the host-side name of the array is not a device address).
+int noalloc_scratch(void** out) {
+    int dev = 0;
+    PMB_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kMaxDevices) return pmb::fail(PMB_BEYOND_LIMITS, "device %d beyond %d", dev, kMaxDevices);
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+        void* p = nullptr;
+        PMB_CUDA_TRY(cudaGetSymbolAddress(&p, g_noalloc_scan_scratch));
+        g_noalloc_addr[dev] = p;
+    }
+    *out = g_noalloc_addr[dev];
+    return PMB_SUCCESS;
+}
+
+}  // namespace
+
+static_assert(PMB_SCAN_NOALLOC_MAX_ELEMS == (kNoAllocScratchBytes - kHeaderBytes) / 8 * kTile,
+              "header limit must match the scratch array");
+
+extern "C" int pmb_inclusive_scan_u32_u64_noalloc(const uint32_t* d_in, uint64_t* d_out, size_t n, void* stream) {
+    if (n == 0) return PMB_SUCCESS;
+    if (n > PMB_SCAN_NOALLOC_MAX_ELEMS)
+        return pmb::fail(PMB_BEYOND_LIMITS,
+                         "pmb_inclusive_scan_u32_u64_noalloc: %zu elements exceed the fixed scratch limit of %llu; "
+                         "use pmb_inclusive_scan_u32_u64 with caller-provided scratch",
+                         n, static_cast<unsigned long long>(PMB_SCAN_NOALLOC_MAX_ELEMS));
+    void* scratch = nullptr;
+    const int st = noalloc_scratch(&scratch);
+    if (st != PMB_SUCCESS) return st;
+    // The shared array keeps the previous call's contents: scan_launch clears
+    // the header and the status words this call uses before the kernel runs.
+    return pmb::scan_launch(d_in, d_out, n, scratch, kNoAllocScratchBytes, static_cast<cudaStream_t>(stream), true);
 }
