@@ -249,91 +249,74 @@ __device__ __forceinline__ void deinterleave4(uint32_t w0, uint32_t w1, uint32_t
     o2 = __byte_perm(__byte_perm(w0, w1, 0x0630), w2, 0x5210);
 }
 
-// Per-tile geometry shared by the prefetch and compute phases.
-struct TileGeo {
-    const uint8_t* in;
-    uint8_t* out;
-    int64_t ip, op;
-    int H, in_row0, in_col0, out_row0, out_col0, r1, c1;
-    int tile_r0, tile_c0, mlo, mhi, clo, chi;
-    bool al16, al4;
-};
-
-template <int R, int MAXI>
-__device__ __forceinline__ TileGeo tile_geo(const ImgfParamsF<R, MAXI>& p, int t) {
-    int lo = 0, hi = p.n_items - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (p.tile_start[mid] <= t) lo = mid; else hi = mid - 1;
-    }
-    const pmb_imgf_item& it = p.items[lo];
-    TileGeo g;
-    g.in = it.in;
-    g.out = it.out;
-    g.ip = it.in_pitch;
-    g.op = it.out_pitch;
-    g.H = it.height;
-    g.in_row0 = it.in_row0;
-    g.in_col0 = it.in_col0;
-    g.out_row0 = it.out_row0;
-    g.out_col0 = it.out_col0;
-    g.r1 = it.r1;
-    g.c1 = it.c1;
-    const int local = t - p.tile_start[lo];
-    const int txs = p.tiles_x[lo];
-    const int ty = local / txs, tx = local - ty * txs;
-    g.tile_c0 = it.c0 + tx * kTW;
-    g.tile_r0 = it.r0 + ty * kTH;
-    g.mlo = max(0, it.r0 - R);
-    g.mhi = min(it.height - 1, it.r1 - 1 + R);
-    g.clo = max(0, it.c0 - R);
-    g.chi = min(it.width - 1, it.c1 - 1 + R);
-    g.al16 = ((reinterpret_cast<uintptr_t>(it.in) | static_cast<uintptr_t>(it.in_pitch)) & 15) == 0;
-    g.al4 = ((reinterpret_cast<uintptr_t>(it.in) | static_cast<uintptr_t>(it.in_pitch)) & 3) == 0;
-    return g;
-}
-
-// Can the 16-pixel group starting at pixel n0 of row `m` be copied verbatim
-// (no column clamping, 16-byte aligned source)?
-__device__ __forceinline__ bool group_direct(const TileGeo& g, int n0) {
-    return g.al16 && n0 >= g.clo && n0 + 15 <= g.chi && ((n0 - g.in_col0) & 15) == 0;
-}
-
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-    const uint32_t sa = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
-
-constexpr int kRawRow = 3 * kPWF;  // 288 bytes: the raw RGB bytes of one staged row
-
-// Issue the asynchronous copies of every directly copyable group of a tile.
-template <int R>
-__device__ __forceinline__ void prefetch_tile(const TileGeo& g, uint8_t (*raw)[kRawRow]) {
-    using G = GeoF<R>;
-    constexpr int kG16 = kPWF / 16;
-    for (int c = threadIdx.x; c < G::PH * kG16 * 3; c += kThreads) {
-        const int yy = c / (kG16 * 3);
-        const int rem = c - yy * (kG16 * 3);
-        const int xg = rem / 3, part = rem - xg * 3;
-        const int n0 = g.tile_c0 - kPadF + 16 * xg;
-        if (!group_direct(g, n0)) continue;
-        const int m = pmb::clampi(g.tile_r0 - R + yy, g.mlo, g.mhi);
-        const uint8_t* src = g.in + static_cast<int64_t>(g.H - 1 - m - g.in_row0) * g.ip + 3 * (n0 - g.in_col0) + 16 * part;
-        cp_async16(&raw[yy][48 * xg + 16 * part], src);
-    }
-}
-
+// One CTA per 64 x 32 tile; blockIdx.y selects the item (subtask), blockIdx.x
+// the tile inside it (CTAs past the item's tile count exit at once).
 template <int R, int MODE, int MAXI, int CB>
 __global__ void __launch_bounds__(kThreads, 4)
-imgf_fast_kernel(const __grid_constant__ ImgfParamsF<R, MAXI> p, int total_tiles) {
+imgf_fast_kernel(const __grid_constant__ ImgfParamsF<R, MAXI> p) {
     using G = GeoF<R>;
-    constexpr int kG16 = kPWF / 16;
-    __shared__ __align__(16) uint8_t raw[2][G::PH][kRawRow];
     __shared__ __align__(16) uint8_t planes[3][G::PH][kPWF];
 
-    // Filter pattern words stay in registers for the CTA's lifetime.
+    const int item = blockIdx.y;
+    const int txs = p.tiles_x[item];
+    const int local = blockIdx.x;
+    if (local >= p.tile_start[item + 1] - p.tile_start[item]) return;
+    const uint8_t* const in = p.items[item].in;
+    uint8_t* const out = p.items[item].out;
+    const int64_t ip = p.items[item].in_pitch, op = p.items[item].out_pitch;
+    const int H = p.items[item].height, Wd = p.items[item].width;
+    const int in_row0 = p.items[item].in_row0, in_col0 = p.items[item].in_col0;
+    const int out_row0 = p.items[item].out_row0, out_col0 = p.items[item].out_col0;
+    const int r0 = p.items[item].r0, r1 = p.items[item].r1, c0 = p.items[item].c0, c1 = p.items[item].c1;
+    const int ty = local / txs, tx = local - ty * txs;
+    const int tile_c0 = c0 + tx * kTW, tile_r0 = r0 + ty * kTH;
+    const int mlo = max(0, r0 - R), mhi = min(H - 1, r1 - 1 + R);
+    const int clo = max(0, c0 - R), chi = min(Wd - 1, c1 - 1 + R);
+    const bool al16 = ((reinterpret_cast<uintptr_t>(in) | static_cast<uintptr_t>(ip)) & 15) == 0;
+    const bool al4 = ((reinterpret_cast<uintptr_t>(in) | static_cast<uintptr_t>(ip)) & 3) == 0;
+
+    // ---- staging: 16-pixel groups, 6 per plane row, straight from HBM -------
+    constexpr int kG16 = kPWF / 16;
+    for (int g = threadIdx.x; g < G::PH * kG16; g += kThreads) {
+        const int yy = g / kG16;
+        const int xg = g - yy * kG16;
+        const int m = pmb::clampi(tile_r0 - R + yy, mlo, mhi);
+        const uint8_t* rowp = in + static_cast<int64_t>(H - 1 - m - in_row0) * ip;
+        const int n0 = tile_c0 - kPadF + 16 * xg;
+        uint32_t o[3][4];
+        if (al16 && n0 >= clo && n0 + 15 <= chi && ((n0 - in_col0) & 15) == 0) {
+            const uint4* sp = reinterpret_cast<const uint4*>(rowp + 3 * (n0 - in_col0));
+            const uint4 a = __ldg(sp), b = __ldg(sp + 1), c = __ldg(sp + 2);
+            deinterleave4(a.x, a.y, a.z, o[0][0], o[1][0], o[2][0]);
+            deinterleave4(a.w, b.x, b.y, o[0][1], o[1][1], o[2][1]);
+            deinterleave4(b.z, b.w, c.x, o[0][2], o[1][2], o[2][2]);
+            deinterleave4(c.y, c.z, c.w, o[0][3], o[1][3], o[2][3]);
+        } else {
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int nq = n0 + 4 * q;
+                if (al4 && nq >= clo && nq + 3 <= chi && ((nq - in_col0) & 3) == 0) {
+                    const uint32_t* s4 = reinterpret_cast<const uint32_t*>(rowp + 3 * (nq - in_col0));
+                    deinterleave4(__ldg(s4), __ldg(s4 + 1), __ldg(s4 + 2), o[0][q], o[1][q], o[2][q]);
+                } else {
+                    o[0][q] = o[1][q] = o[2][q] = 0;
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        const int n = pmb::clampi(nq + e, clo, chi);
+                        const uint8_t* px = rowp + 3 * (n - in_col0);
+                        o[0][q] |= static_cast<uint32_t>(__ldg(px + 2)) << (8 * e);
+                        o[1][q] |= static_cast<uint32_t>(__ldg(px + 1)) << (8 * e);
+                        o[2][q] |= static_cast<uint32_t>(__ldg(px + 0)) << (8 * e);
+                    }
+                }
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            *reinterpret_cast<uint4*>(&planes[c][yy][16 * xg]) = make_uint4(o[c][0], o[c][1], o[c][2], o[c][3]);
+    }
+
+    // ---- filter patterns into registers --------------------------------------
     uint32_t pat[G::KD][4][G::NW];
 #pragma unroll
     for (int ky = 0; ky < G::KD; ++ky)
@@ -341,140 +324,83 @@ imgf_fast_kernel(const __grid_constant__ ImgfParamsF<R, MAXI> p, int total_tiles
         for (int k = 0; k < 4; ++k)
 #pragma unroll
             for (int w = 0; w < G::NW; ++w) pat[ky][k][w] = tap_word_used_f<R>(k, w) ? p.pat[ky][k][w] : 0u;
+    __syncthreads();
 
     const int gx = threadIdx.x % kGX;
     const int gy = threadIdx.x / kGX;
-    int buf = 0;
-    if (static_cast<int>(blockIdx.x) < total_tiles) prefetch_tile<R>(tile_geo<R, MAXI>(p, blockIdx.x), raw[0]);
-    cp_async_commit();
-
-    for (int t = blockIdx.x; t < total_tiles; t += gridDim.x, buf ^= 1) {
-        const int tn = t + gridDim.x;
-        if (tn < total_tiles) prefetch_tile<R>(tile_geo<R, MAXI>(p, tn), raw[buf ^ 1]);
-        cp_async_commit();
-        cp_async_wait_1();
-        __syncthreads();
-
-        const TileGeo g = tile_geo<R, MAXI>(p, t);
-        // ---- de-interleave the staged rows into the three planes -----------
-        for (int q = threadIdx.x; q < G::PH * kG16; q += kThreads) {
-            const int yy = q / kG16;
-            const int xg = q - yy * kG16;
-            const int n0 = g.tile_c0 - kPadF + 16 * xg;
-            uint32_t o[3][4];
-            if (group_direct(g, n0)) {
-                const uint4* sp = reinterpret_cast<const uint4*>(&raw[buf][yy][48 * xg]);
-                const uint4 a = sp[0], b = sp[1], c = sp[2];
-                deinterleave4(a.x, a.y, a.z, o[0][0], o[1][0], o[2][0]);
-                deinterleave4(a.w, b.x, b.y, o[0][1], o[1][1], o[2][1]);
-                deinterleave4(b.z, b.w, c.x, o[0][2], o[1][2], o[2][2]);
-                deinterleave4(c.y, c.z, c.w, o[0][3], o[1][3], o[2][3]);
-            } else {
-                const int m = pmb::clampi(g.tile_r0 - R + yy, g.mlo, g.mhi);
-                const uint8_t* rowp = g.in + static_cast<int64_t>(g.H - 1 - m - g.in_row0) * g.ip;
+    uint32_t res[kV][4];
 #pragma unroll
-                for (int k4 = 0; k4 < 4; ++k4) {
-                    const int nq = n0 + 4 * k4;
-                    if (g.al4 && nq >= g.clo && nq + 3 <= g.chi && ((nq - g.in_col0) & 3) == 0) {
-                        const uint32_t* s4 = reinterpret_cast<const uint32_t*>(rowp + 3 * (nq - g.in_col0));
-                        deinterleave4(__ldg(s4), __ldg(s4 + 1), __ldg(s4 + 2), o[0][k4], o[1][k4], o[2][k4]);
-                    } else {
-                        o[0][k4] = o[1][k4] = o[2][k4] = 0;
+    for (int v = 0; v < kV; ++v)
 #pragma unroll
-                        for (int e = 0; e < 4; ++e) {
-                            const int n = pmb::clampi(nq + e, g.clo, g.chi);
-                            const uint8_t* px = rowp + 3 * (n - g.in_col0);
-                            o[0][k4] |= static_cast<uint32_t>(__ldg(px + 2)) << (8 * e);
-                            o[1][k4] |= static_cast<uint32_t>(__ldg(px + 1)) << (8 * e);
-                            o[2][k4] |= static_cast<uint32_t>(__ldg(px + 0)) << (8 * e);
-                        }
-                    }
-                }
+        for (int k = 0; k < 4; ++k) res[v][k] = 0;
+
+#pragma unroll
+    for (int cb = 0; cb < 3; cb += CB) {
+        int acc[CB][kV][4];
+#pragma unroll
+        for (int c = 0; c < CB; ++c)
+#pragma unroll
+            for (int v = 0; v < kV; ++v)
+#pragma unroll
+                for (int k = 0; k < 4; ++k) acc[c][v][k] = 0;
+#pragma unroll
+        for (int yy = 0; yy < kV + 2 * R; ++yy) {
+            uint32_t win[CB][G::NW];
+#pragma unroll
+            for (int c = 0; c < CB; ++c) {
+                const uint32_t* rp = reinterpret_cast<const uint32_t*>(&planes[cb + c][gy * kV + yy][0]) + gx + G::WS;
+#pragma unroll
+                for (int w = 0; w < G::NW; ++w) win[c][w] = rp[w];
             }
-#pragma unroll
-            for (int c = 0; c < 3; ++c)
-                *reinterpret_cast<uint4*>(&planes[c][yy][16 * xg]) = make_uint4(o[c][0], o[c][1], o[c][2], o[c][3]);
-        }
-        __syncthreads();
-
-        // ---- 4 pixels x kV rows per thread ---------------------------------
-        uint32_t res[kV][4];
-#pragma unroll
-        for (int v = 0; v < kV; ++v)
-#pragma unroll
-            for (int k = 0; k < 4; ++k) res[v][k] = 0;
-#pragma unroll
-        for (int cb = 0; cb < 3; cb += CB) {
-            int acc[CB][kV][4];
-#pragma unroll
-            for (int c = 0; c < CB; ++c)
-#pragma unroll
-                for (int v = 0; v < kV; ++v)
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) acc[c][v][k] = 0;
-#pragma unroll
-            for (int yy = 0; yy < kV + 2 * R; ++yy) {
-                uint32_t win[CB][G::NW];
-#pragma unroll
-                for (int c = 0; c < CB; ++c) {
-                    const uint32_t* rp =
-                        reinterpret_cast<const uint32_t*>(&planes[cb + c][gy * kV + yy][0]) + gx + G::WS;
-#pragma unroll
-                    for (int w = 0; w < G::NW; ++w) win[c][w] = rp[w];
-                }
-#pragma unroll
-                for (int v = 0; v < kV; ++v) {
-                    const int ky = yy - v;
-                    if (ky < 0 || ky >= G::KD) continue;
-#pragma unroll
-                    for (int c = 0; c < CB; ++c)
-#pragma unroll
-                        for (int k = 0; k < 4; ++k)
-#pragma unroll
-                            for (int w = 0; w < G::NW; ++w)
-                                if (tap_word_used_f<R>(k, w))
-                                    acc[c][v][k] = dp4a_us(win[c][w], pat[ky][k][w], acc[c][v][k]);
-                }
-            }
-#pragma unroll
-            for (int c = 0; c < CB; ++c)
-#pragma unroll
-                for (int v = 0; v < kV; ++v)
-#pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        int a = acc[c][v][k];
-                        if (MODE == PMB_IMGF_CLAMP) a = min(max(a, 0), 255);
-                        constexpr uint32_t kSel[3] = {0x3214u, 0x3240u, 0x3410u};
-                        res[v][k] = __byte_perm(res[v][k], static_cast<uint32_t>(a), kSel[cb + c]);
-                    }
-        }
-
-        const int j0 = g.tile_c0 + 4 * gx;
-        if (j0 < g.c1) {
 #pragma unroll
             for (int v = 0; v < kV; ++v) {
-                const int i = g.tile_r0 + gy * kV + v;
-                if (i >= g.r1) break;
-                uint8_t* dst = g.out + static_cast<int64_t>(i - g.out_row0) * g.op + 3 * (j0 - g.out_col0);
-                if (j0 + 3 < g.c1 && (reinterpret_cast<uintptr_t>(dst) & 3) == 0) {
-                    uint32_t* d = reinterpret_cast<uint32_t*>(dst);
-                    d[0] = __byte_perm(res[v][0], res[v][1], 0x4210);
-                    d[1] = __byte_perm(res[v][1], res[v][2], 0x5421);
-                    d[2] = __byte_perm(res[v][2], res[v][3], 0x6542);
-                } else {
+                const int ky = yy - v;
+                if (ky < 0 || ky >= G::KD) continue;
 #pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        if (j0 + k >= g.c1) break;
-                        dst[3 * k + 0] = static_cast<uint8_t>(res[v][k]);
-                        dst[3 * k + 1] = static_cast<uint8_t>(res[v][k] >> 8);
-                        dst[3 * k + 2] = static_cast<uint8_t>(res[v][k] >> 16);
-                    }
+                for (int c = 0; c < CB; ++c)
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+#pragma unroll
+                        for (int w = 0; w < G::NW; ++w)
+                            if (tap_word_used_f<R>(k, w)) acc[c][v][k] = dp4a_us(win[c][w], pat[ky][k][w], acc[c][v][k]);
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < CB; ++c)
+#pragma unroll
+            for (int v = 0; v < kV; ++v)
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    int a = acc[c][v][k];
+                    if (MODE == PMB_IMGF_CLAMP) a = min(max(a, 0), 255);
+                    // byte 0 of `a` into byte (cb + c) of res
+                    constexpr uint32_t kSel[3] = {0x3214u, 0x3240u, 0x3410u};
+                    res[v][k] = __byte_perm(res[v][k], static_cast<uint32_t>(a), kSel[cb + c]);
                 }
+    }
+
+    const int j0 = tile_c0 + 4 * gx;
+    if (j0 >= c1) return;
+#pragma unroll
+    for (int v = 0; v < kV; ++v) {
+        const int i = tile_r0 + gy * kV + v;
+        if (i >= r1) break;
+        uint8_t* dst = out + static_cast<int64_t>(i - out_row0) * op + 3 * (j0 - out_col0);
+        if (j0 + 3 < c1 && (reinterpret_cast<uintptr_t>(dst) & 3) == 0) {
+            uint32_t* d = reinterpret_cast<uint32_t*>(dst);
+            d[0] = __byte_perm(res[v][0], res[v][1], 0x4210);
+            d[1] = __byte_perm(res[v][1], res[v][2], 0x5421);
+            d[2] = __byte_perm(res[v][2], res[v][3], 0x6542);
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                if (j0 + k >= c1) break;
+                dst[3 * k + 0] = static_cast<uint8_t>(res[v][k]);
+                dst[3 * k + 1] = static_cast<uint8_t>(res[v][k] >> 8);
+                dst[3 * k + 2] = static_cast<uint8_t>(res[v][k] >> 16);
             }
         }
     }
-    // Drain the (empty) last group before exit.
-    asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
 // ---------------------------------------------------------------------------
@@ -613,17 +539,9 @@ int launch_fast(const pmb_imgf_item* items, int n, const int8_t* filter, cudaStr
     p.n_items = m;
     p.tile_start[m] = static_cast<int>(total);
     constexpr int CB = R <= 2 ? 3 : 1;
-    static int s_ctas = 0;  // resident CTAs on the whole device for this instantiation
-    if (s_ctas == 0) {
-        int dev = 0, sms = 0, per_sm = 0;
-        PMB_CUDA_TRY(cudaGetDevice(&dev));
-        PMB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-        PMB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, imgf_fast_kernel<R, MODE, MAXI, CB>,
-                                                                   kThreads, 0));
-        s_ctas = sms * (per_sm > 0 ? per_sm : 1);
-    }
-    const int grid = static_cast<int>(total < s_ctas ? total : s_ctas);
-    imgf_fast_kernel<R, MODE, MAXI, CB><<<grid, kThreads, 0, s>>>(p, static_cast<int>(total));
+    int max_tiles = 0;
+    for (int i = 0; i < m; ++i) max_tiles = std::max(max_tiles, p.tile_start[i + 1] - p.tile_start[i]);
+    imgf_fast_kernel<R, MODE, MAXI, CB><<<dim3(static_cast<unsigned>(max_tiles), static_cast<unsigned>(m)), kThreads, 0, s>>>(p);
     PMB_CUDA_TRY(cudaGetLastError());
     return PMB_SUCCESS;
 }
