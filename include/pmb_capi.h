@@ -85,6 +85,13 @@ int pmb_memset_async(void* p, int value, size_t bytes, void* stream);
 int pmb_launch_kernel(const void* fn, unsigned gx, unsigned gy, unsigned gz, unsigned bx, unsigned by, unsigned bz,
                       unsigned smem, void** args, void* stream);
 int pmb_device_synchronize(void);
+/* Keep blocks freed with pmb_free_async in the device's default pool for
+ * reuse (release threshold = unlimited). */
+int pmb_mempool_retain(int dev);
+/* Return idle pool memory beyond keep_bytes to the device. */
+int pmb_mempool_trim(int dev, size_t keep_bytes);
+/* Free device memory plus memory the default pool holds but does not use. */
+int pmb_mem_available(int dev, size_t* available);
 /* Stream capture into an instantiated CUDA graph, and its launch. */
 int pmb_graph_begin_capture(void* stream);
 int pmb_graph_end_capture(void* stream, void** graph_exec);

@@ -87,6 +87,9 @@ _SIGS = {
     "pmb_launch_kernel": (c_int, [c_void_p, ctypes.c_uint, ctypes.c_uint, ctypes.c_uint, ctypes.c_uint, ctypes.c_uint,
                                   ctypes.c_uint, ctypes.c_uint, ctypes.POINTER(c_void_p), c_void_p]),
     "pmb_device_synchronize": (c_int, []),
+    "pmb_mempool_retain": (c_int, [c_int]),
+    "pmb_mempool_trim": (c_int, [c_int, c_size_t]),
+    "pmb_mem_available": (c_int, [c_int, ctypes.POINTER(c_size_t)]),
     "pmb_graph_begin_capture": (c_int, [c_void_p]),
     "pmb_graph_end_capture": (c_int, [c_void_p, ctypes.POINTER(c_void_p)]),
     "pmb_graph_launch": (c_int, [c_void_p, c_void_p]),

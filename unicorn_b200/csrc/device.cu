@@ -225,3 +225,31 @@ extern "C" int pmb_graph_destroy(void* exec) {
     if (exec) PMB_CUDA_TRY(cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(exec)));
     return PMB_SUCCESS;
 }
+
+extern "C" int pmb_mempool_retain(int dev) {
+    cudaMemPool_t pool;
+    PMB_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, dev));
+    uint64_t threshold = UINT64_MAX;  // keep freed blocks for reuse instead of returning them
+    PMB_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &threshold));
+    return PMB_SUCCESS;
+}
+
+extern "C" int pmb_mempool_trim(int dev, size_t keep_bytes) {
+    cudaMemPool_t pool;
+    PMB_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, dev));
+    PMB_CUDA_TRY(cudaMemPoolTrimTo(pool, keep_bytes));
+    return PMB_SUCCESS;
+}
+
+extern "C" int pmb_mem_available(int dev, size_t* available) {
+    PMB_CHECK_ARG(available, "null pointer");
+    size_t fr = 0, tot = 0;
+    PMB_CUDA_TRY(cudaMemGetInfo(&fr, &tot));
+    cudaMemPool_t pool;
+    PMB_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, dev));
+    uint64_t reserved = 0, used = 0;
+    PMB_CUDA_TRY(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved));
+    PMB_CUDA_TRY(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used));
+    *available = fr + (reserved > used ? static_cast<size_t>(reserved - used) : 0);
+    return PMB_SUCCESS;
+}

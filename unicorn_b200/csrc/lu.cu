@@ -12,8 +12,8 @@
 // :99-151), update the trailing matrix (cublasSgemm, :153-193).
 //
 // B200 design, per nb-step:
-//  1. one CTA factors the nb x nb diagonal block in FP64 in shared memory
-//     (two barriers per column) and, in the same launch, inverts both
+//  1. one CTA factors the nb x nb diagonal block in FP64, held in registers
+//     (one barrier per column) and, in the same launch, inverts both
 //     triangles in FP64 (W = L11^-1, V = U11^-1), written as fp32;
 //  2. U12 = W * A12 and L21 = A21 * V run as tensor-core GEMMs (BF16x3);
 //  3. A22 -= L21 * U12 runs as a tensor-core GEMM with alpha=-1, beta=1.
@@ -37,74 +37,171 @@ constexpr int kMaxNb = 128;
 constexpr uint32_t kFlagPivot = 1;      // partial pivoting would have swapped rows
 constexpr uint32_t kFlagZeroPivot = 2;  // a pivot was exactly zero
 
-// Factor the kb x kb diagonal block at A (lda) and write W = L^-1, V = U^-1
-// (kb x kb, column-major, ld = kb).  Dynamic shared memory: kb*kb doubles plus
-// 2*kb doubles of scratch.
-__global__ void __launch_bounds__(kDiagThreads)
+// Factor the kb x kb diagonal block at A (lda) in FP64 and write W = L^-1,
+// V = U^-1 (kb x kb, column-major, ld = kb).
+//
+// The block lives in registers for the whole kernel: thread (tx = lane,
+// ty = warp) owns rows tx + 32*ii (ii < 4) of columns ty + 16*jj (jj < 8),
+// a cyclic layout that keeps every thread busy as the active part shrinks.
+// Blocks smaller than 128 are padded with the identity, which neither step
+// changes.  Each elimination step publishes one column and one row through a
+// double-buffered shared vector, so a step costs one barrier:
+//  - factorization (Crout): step i scales row i by 1/a_ii and applies the
+//    rank-1 update a_rc -= a_ri * u_ic to the trailing block;
+//  - inverses, both triangles in the same steps: W by right-looking forward
+//    substitution (row k of W final at step k, X_rj -= L_rk W_kj below it) and
+//    V by right-looking back substitution from the last row (Y_rj -= U_rq V_qj
+//    above row q).  The entries of L (U) consumed at a step are dead after it,
+//    so W (V) overwrites the lower (strict upper) triangle in place.
+// Element (ii, js) / (is, jj) of a register tile with a run-time index on one
+// side, by a select chain (indexing the array at run time would move it to
+// local memory).
+template <int R, int C>
+__device__ __forceinline__ double pick_in_row(const double (&a)[R][C], int ii, int js) {
+    double v = a[ii][0];
+#pragma unroll
+    for (int jj = 1; jj < C; ++jj) v = jj == js ? a[ii][jj] : v;
+    return v;
+}
+template <int R, int C>
+__device__ __forceinline__ double pick_in_col(const double (&a)[R][C], int is, int jj) {
+    double v = a[0][jj];
+#pragma unroll
+    for (int ii = 1; ii < R; ++ii) v = ii == is ? a[ii][jj] : v;
+    return v;
+}
+
+__global__ void __launch_bounds__(kDiagThreads, 1)
 lu_diag_kernel(float* __restrict__ A, int64_t lda, int kb, float* __restrict__ W, float* __restrict__ V,
                uint32_t* __restrict__ flags) {
-    extern __shared__ double s[];
-    double* a = s;                 // a[c * kb + r]
-    double* xl = s + kb * kb;      // scratch column for the L inverse
-    double* xu = xl + kb;          // scratch column for the U inverse
-    const int tid = threadIdx.x;
-    for (int e = tid; e < kb * kb; e += kDiagThreads) {
-        const int c = e / kb, r = e - c * kb;
-        a[e] = A[static_cast<int64_t>(c) * lda + r];
+    constexpr int RI = kMaxNb / 32, CJ = kMaxNb / 16;
+    __shared__ double s_col[2][kMaxNb];
+    __shared__ double s_row[2][kMaxNb];
+    __shared__ double s_ucol[2][kMaxNb];
+    __shared__ double s_vrow[2][kMaxNb];
+    __shared__ double s_piv[2];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    double a[RI][CJ];
+#pragma unroll
+    for (int jj = 0; jj < CJ; ++jj) {
+        const int c = ty + 16 * jj;
+#pragma unroll
+        for (int ii = 0; ii < RI; ++ii) {
+            const int r = tx + 32 * ii;
+            a[ii][jj] = (r < kb && c < kb) ? static_cast<double>(A[static_cast<int64_t>(c) * lda + r])
+                                           : (r == c ? 1.0 : 0.0);
+        }
     }
-    __syncthreads();
 
     // ---- Crout LU: L keeps the pivots, U is unit upper ----------------------
     for (int i = 0; i < kb; ++i) {
-        const double piv = a[i * kb + i];
-        if (tid == 0 && piv == 0.0) atomicOr(flags, kFlagZeroPivot);
+        const int buf = i & 1;
+        if (ty == (i & 15)) {
+#pragma unroll
+            for (int ii = 0; ii < RI; ++ii) s_col[buf][tx + 32 * ii] = pick_in_row(a, ii, i >> 4);
+        }
+        if (tx == (i & 31)) {
+#pragma unroll
+            for (int jj = 0; jj < CJ; ++jj) s_row[buf][ty + 16 * jj] = pick_in_col(a, i >> 5, jj);
+        }
+        __syncthreads();
+        const double piv = s_col[buf][i];
+        if (threadIdx.x == 0 && piv == 0.0) atomicOr(flags, kFlagZeroPivot);
         const double inv = piv != 0.0 ? 1.0 / piv : 0.0;
-        for (int c = i + 1 + tid; c < kb; c += kDiagThreads) a[c * kb + i] *= inv;
-        __syncthreads();
-        const int m = kb - i - 1;
-        for (int e = tid; e < m * m; e += kDiagThreads) {
-            const int c = i + 1 + e / m, r = i + 1 + e % m;
-            a[c * kb + r] -= a[i * kb + r] * a[c * kb + i];
+#pragma unroll
+        for (int jj = 0; jj < CJ; ++jj) {
+            const int c = ty + 16 * jj;
+            if (c <= i) continue;
+            const double u = s_row[buf][c] * inv;
+#pragma unroll
+            for (int ii = 0; ii < RI; ++ii) {
+                const int r = tx + 32 * ii;
+                if (r == i) a[ii][jj] = u;
+                else if (r > i) a[ii][jj] = fma(-s_col[buf][r], u, a[ii][jj]);
+            }
         }
-        __syncthreads();
     }
-    for (int e = tid; e < kb * kb; e += kDiagThreads) {
-        const int c = e / kb, r = e - c * kb;
-        A[static_cast<int64_t>(c) * lda + r] = static_cast<float>(a[e]);
+#pragma unroll
+    for (int jj = 0; jj < CJ; ++jj) {
+        const int c = ty + 16 * jj;
+#pragma unroll
+        for (int ii = 0; ii < RI; ++ii) {
+            const int r = tx + 32 * ii;
+            if (r < kb && c < kb) A[static_cast<int64_t>(c) * lda + r] = static_cast<float>(a[ii][jj]);
+        }
     }
-    __syncthreads();
 
-    // ---- in-place triangular inverses (FP64) --------------------------------
-    // Lower (with diagonal): columns from the right; unit upper: from the left.
-    for (int step = 0; step < kb; ++step) {
-        const int jl = kb - 1 - step, ju = step;
-        // stage the columns to transform
-        for (int r = tid; r < kb; r += kDiagThreads) {
-            xl[r] = r > jl ? a[jl * kb + r] : 0.0;
-            xu[r] = r < ju ? a[ju * kb + r] : 0.0;
+    // ---- triangular inverses (FP64), W from the top, V from the bottom -------
+    for (int st = 0; st < kb; ++st) {
+        const int buf = st & 1;
+        const int k = st, q = kb - 1 - st;
+        if (tx == (k & 31)) {  // row k: X_kj (j < k), 1 at j = k; and the pivot L_kk
+#pragma unroll
+            for (int jj = 0; jj < CJ; ++jj) {
+                const int c = ty + 16 * jj;
+                const double x = pick_in_col(a, k >> 5, jj);
+                s_row[buf][c] = c < k ? x : (c == k ? 1.0 : 0.0);
+                if (c == k) s_piv[buf] = x;
+            }
+        }
+        if (ty == (k & 15)) {  // column k of L below the diagonal
+#pragma unroll
+            for (int ii = 0; ii < RI; ++ii) {
+                const int r = tx + 32 * ii;
+                s_col[buf][r] = r > k ? pick_in_row(a, ii, k >> 4) : 0.0;
+            }
+        }
+        if (tx == (q & 31)) {  // row q: Y_qj (j > q), 1 at j = q
+#pragma unroll
+            for (int jj = 0; jj < CJ; ++jj) {
+                const int c = ty + 16 * jj;
+                s_vrow[buf][c] = c > q ? pick_in_col(a, q >> 5, jj) : (c == q ? 1.0 : 0.0);
+            }
+        }
+        if (ty == (q & 15)) {  // column q of U above the diagonal
+#pragma unroll
+            for (int ii = 0; ii < RI; ++ii) {
+                const int r = tx + 32 * ii;
+                s_ucol[buf][r] = r < q ? pick_in_row(a, ii, q >> 4) : 0.0;
+            }
         }
         __syncthreads();
-        const double dl = a[jl * kb + jl] != 0.0 ? 1.0 / a[jl * kb + jl] : 0.0;
-        // L: y = Linv[jl+1:, jl+1:] * x (trailing part already inverted)
-        for (int r = jl + 1 + tid; r < kb; r += kDiagThreads) {
-            double y = 0.0;
-            for (int p = jl + 1; p <= r; ++p) y += a[p * kb + r] * xl[p];
-            a[jl * kb + r] = -dl * y;
+        const double d = s_piv[buf];
+        const double dinv = d != 0.0 ? 1.0 / d : 0.0;
+#pragma unroll
+        for (int jj = 0; jj < CJ; ++jj) {
+            const int c = ty + 16 * jj;
+            if (c <= k) {
+                const double w = s_row[buf][c] * dinv;  // W_kc
+#pragma unroll
+                for (int ii = 0; ii < RI; ++ii) {
+                    const int r = tx + 32 * ii;
+                    if (r == k) a[ii][jj] = w;
+                    else if (r > k) a[ii][jj] = fma(-s_col[buf][r], w, c == k ? 0.0 : a[ii][jj]);
+                }
+            }
+            if (c >= q) {
+                const double v = s_vrow[buf][c];  // V_qc
+#pragma unroll
+                for (int ii = 0; ii < RI; ++ii) {
+                    const int r = tx + 32 * ii;
+                    if (r < q) a[ii][jj] = fma(-s_ucol[buf][r], v, c == q ? 0.0 : a[ii][jj]);
+                }
+            }
         }
-        // U (unit): y = Uinv[0:ju, 0:ju] * x (leading part already inverted)
-        for (int r = tid - 256; r >= 0 && r < ju; r += kDiagThreads - 256) {
-            double y = xu[r];
-            for (int p = r + 1; p < ju; ++p) y += a[p * kb + r] * xu[p];
-            a[ju * kb + r] = -y;
-        }
-        __syncthreads();
-        if (tid == 0) a[jl * kb + jl] = dl;
-        __syncthreads();
     }
-    for (int e = tid; e < kb * kb; e += kDiagThreads) {
-        const int c = e / kb, r = e - c * kb;
-        W[e] = r >= c ? static_cast<float>(a[e]) : 0.0f;
-        V[e] = r < c ? static_cast<float>(a[e]) : (r == c ? 1.0f : 0.0f);
+#pragma unroll
+    for (int jj = 0; jj < CJ; ++jj) {
+        const int c = ty + 16 * jj;
+#pragma unroll
+        for (int ii = 0; ii < RI; ++ii) {
+            const int r = tx + 32 * ii;
+            if (r < kb && c < kb) {
+                const int64_t e = static_cast<int64_t>(c) * kb + r;
+                W[e] = r >= c ? static_cast<float>(a[ii][jj]) : 0.0f;
+                V[e] = r < c ? static_cast<float>(a[ii][jj]) : (r == c ? 1.0f : 0.0f);
+            }
+        }
     }
 }
 
@@ -224,18 +321,11 @@ static int lu_impl(float* A, int n, int64_t lda, int nb, void* workspace, size_t
     PMB_CHECK_ARG(ws_bytes >= pmb_lu_workspace_bytes(n, nb), "LU workspace too small");
     LuWs w = carve(workspace, n, nb);
     PMB_CUDA_TRY(cudaMemsetAsync(workspace, 0, 256, s));
-    static bool attr_done = false;
-    if (!attr_done) {
-        PMB_CUDA_TRY(cudaFuncSetAttribute(lu_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          static_cast<int>((kMaxNb * kMaxNb + 2 * kMaxNb) * sizeof(double))));
-        attr_done = true;
-    }
     for (int k0 = 0; k0 < n; k0 += nb) {
         const int kb = n - k0 < nb ? n - k0 : nb;
         const int rest = n - k0 - kb;
         float* A11 = A + static_cast<int64_t>(k0) * lda + k0;
-        const size_t smem = (static_cast<size_t>(kb) * kb + 2 * kb) * sizeof(double);
-        lu_diag_kernel<<<1, kDiagThreads, smem, s>>>(A11, lda, kb, w.W, w.V, &w.flags[1]);
+        lu_diag_kernel<<<1, kDiagThreads, 0, s>>>(A11, lda, kb, w.W, w.V, &w.flags[1]);
         PMB_CUDA_TRY(cudaGetLastError());
         if (rest > 0) {
             float* A12 = A + static_cast<int64_t>(k0 + kb) * lda + k0;  // kb x rest

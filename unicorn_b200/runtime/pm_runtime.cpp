@@ -11,12 +11,16 @@
 //    callback for every subtask, turns the recorded subscriptions into device
 //    views, stages the missing bytes into a device-resident mirror of every
 //    address space (one 2-D copy per scattered subscription, on a dedicated
-//    copy stream), launches each subtask's GPU callback on one of four compute
-//    streams, and keeps results on the device.  Tasks are issued back to back:
-//    dependencies between tasks that share address spaces are CUDA events,
-//    never host waits, so consecutive tasks overlap on the device;
-//  * the completion thread: waits for each task's completion event, finishes
-//    bookkeeping, runs the completion callback and wakes waiters.
+//    copy stream), launches each subtask's GPU callback on the next of
+//    PMB_STREAMS (default 8) compute streams, round robin across tasks, and
+//    keeps results on the device.  Tasks are issued back to back: dependencies
+//    between tasks that share address spaces are CUDA events, never host
+//    waits, so independent tasks overlap on the device.  A task is admitted
+//    when one of PMB_MAX_INFLIGHT (default 64) slots is free and its device
+//    memory fits; otherwise the stub waits for in-flight tasks to finish;
+//  * the completion thread: polls the in-flight tasks' completion events,
+//    finishes each task as soon as its own work is done (out of issue order),
+//    runs the completion callback and wakes waiters.
 //
 // Address spaces keep a pinned host copy and, once a GPU task has used them,
 // a full device mirror.  Coherence is tracked per byte range: dev_valid (the
@@ -184,9 +188,14 @@ struct Controller {
     bool stopping = false;
     void* copy_stream = nullptr;
     std::vector<void*> streams;
-    void* join_stream = nullptr;
+    std::atomic<uint64_t> next_stream{0};  // compute streams are handed out round robin
     void* fetch_stream = nullptr;
     size_t reserve_bytes = 0;
+    size_t max_inflight = 64;              // GPU tasks on the device at once (admission slots)
+    // pinned host buffers of released address spaces, kept for reuse
+    std::mutex pin_mu;
+    std::multimap<size_t, char*> pin_free;
+    size_t pin_cached = 0, pin_limit = 0;
     std::atomic<uint64_t> lru{0};
     Stats stats;
     // memory-mapped files
@@ -223,12 +232,64 @@ static AddressSpace* space_of(pmMemHandle h) {
     return c.spaces.count(a) && !a->released ? a : nullptr;
 }
 
-static void free_space(AddressSpace* a) {
-    if (a->dev) pmb_free(a->dev);
-    if (a->host) {
-        if (ctl().has_gpu) pmb_host_free(a->host);
-        else free(a->host);
+// Host copies are allocated on first host use (pmGetRawMemPtr, a fetch, a CPU
+// task, a write-back): an address space only the GPU ever touches never costs
+// a pinned allocation.  Called with a->mu held (or before the space is shared).
+//
+// Pinned allocations are expensive (page locking, and freeing one synchronises
+// the device), so buffers of released address spaces are cached, up to
+// PMB_PINNED_CACHE_BYTES (default 8 GiB), and handed to new address spaces of
+// up to 1.5x smaller size.
+static pmStatus ensure_host(AddressSpace* a) {
+    if (a->host) return pmSuccess;
+    Controller& c = ctl();
+    const size_t len = a->length ? a->length : 1;
+    void* p = nullptr;
+    size_t cap = len;
+    if (c.has_gpu) {
+        {
+            std::lock_guard<std::mutex> g(c.pin_mu);
+            auto it = c.pin_free.lower_bound(len);
+            if (it != c.pin_free.end() && it->first <= len + len / 2) {
+                p = it->second;
+                cap = it->first;
+                c.pin_cached -= cap;
+                c.pin_free.erase(it);
+            }
+        }
+        if (!p && pmb_host_alloc(&p, len) != PMB_SUCCESS) return dev_fail(PMB_MEMORY_ERROR, "pinned host allocation");
+    } else {
+        p = malloc(len);
+        if (!p) return fail(pmMemoryError, "host allocation of %zu bytes failed", a->length);
     }
+    a->host = static_cast<char*>(p);
+    a->host_cap = cap;
+    return pmSuccess;
+}
+
+static void release_host(char* host, size_t cap) {
+    Controller& c = ctl();
+    if (!c.has_gpu) {
+        free(host);
+        return;
+    }
+    {
+        std::lock_guard<std::mutex> g(c.pin_mu);
+        if (c.pin_cached + cap <= c.pin_limit) {
+            c.pin_free.emplace(cap, host);
+            c.pin_cached += cap;
+            return;
+        }
+    }
+    pmb_host_free(host);
+}
+
+static void free_space(AddressSpace* a) {
+    if (a->dev) {
+        if (a->last_access) pmb_stream_wait_event(ctl().fetch_stream, a->last_access);
+        pmb_free_async(a->dev, ctl().fetch_stream);
+    }
+    if (a->host) release_host(a->host, a->host_cap);
     if (a->last_write) pmb_event_destroy(a->last_write);
     if (a->last_access) pmb_event_destroy(a->last_access);
     delete a;
@@ -292,6 +353,10 @@ static pmStatus upload_record(AddressSpace* a, const Record& r, void* stream) {
     if (!r.count || !r.size) return pmSuccess;
     Controller& c = ctl();
     if (a->dev_valid.covers(r.lo(), r.hi())) return pmSuccess;
+    if (!a->host) {  // never written by the host: contents are undefined either way
+        add_record(a->dev_valid, r);
+        return pmSuccess;
+    }
     if (r.contiguous()) {
         std::vector<std::pair<size_t, size_t>> miss;
         a->dev_valid.missing(r.lo(), r.hi(), miss);
@@ -361,6 +426,8 @@ static pmStatus fetch_range(AddressSpace* a, size_t lo, size_t hi) {
     std::vector<std::pair<size_t, size_t>> st;
     a->host_stale.present(lo, hi, st);
     if (st.empty()) return pmSuccess;
+    const pmStatus hs = ensure_host(a);
+    if (hs != pmSuccess) return hs;
     if (a->last_write) PMR_DEV(pmb_event_synchronize(a->last_write));
     for (auto& r : st) {
         PMR_DEV(pmb_memcpy_async(a->host + r.first, a->dev + r.first, r.second - r.first, PMB_D2H, c.fetch_stream));
@@ -372,13 +439,23 @@ static pmStatus fetch_range(AddressSpace* a, size_t lo, size_t hi) {
 }
 
 // Free device mirrors of idle address spaces (least recently used first)
-// until `need` bytes are free beyond the reserve.
+// until `need` bytes are available beyond the reserve.  Mirrors come from the
+// device's stream-ordered pool, which keeps freed blocks for reuse; those count
+// as available, but the reserve (memory left to the app's own allocations) must
+// be physically free, so idle pool memory beyond `need` is trimmed when it eats
+// into it.
 static bool make_room(size_t need, const std::vector<AddressSpace*>& keep) {
     Controller& c = ctl();
     for (;;) {
-        size_t fr = 0, tot = 0;
-        if (pmb_mem_get_info(&fr, &tot) != PMB_SUCCESS) return false;
-        if (fr >= need + c.reserve_bytes) return true;
+        size_t avail = 0, fr = 0, tot = 0;
+        if (pmb_mem_available(c.device, &avail) != PMB_SUCCESS) return false;
+        if (avail >= need + c.reserve_bytes) {
+            if (pmb_mem_get_info(&fr, &tot) == PMB_SUCCESS && fr < c.reserve_bytes) {
+                pmb_stream_synchronize(c.copy_stream);
+                pmb_mempool_trim(c.device, need);
+            }
+            return true;
+        }
         AddressSpace* victim = nullptr;
         {
             std::lock_guard<std::mutex> g(c.mu);
@@ -391,7 +468,9 @@ static bool make_room(size_t need, const std::vector<AddressSpace*>& keep) {
         if (!victim) return false;
         std::lock_guard<std::mutex> g(victim->mu);
         fetch_range(victim, 0, victim->length);
-        pmb_free(victim->dev);
+        if (victim->last_access) pmb_event_synchronize(victim->last_access);
+        pmb_free_async(victim->dev, c.fetch_stream);
+        pmb_stream_synchronize(c.fetch_stream);
         victim->dev = nullptr;
         victim->dev_valid.clear();
     }
@@ -418,6 +497,17 @@ static pmStatus run_dd(Task* t, const pmDeviceInfo& dev) {
     return pmSuccess;
 }
 
+// Admission by free device memory: the task's missing mirrors and reserved
+// subtask memory must fit beside the reserve, after idle mirrors are evicted.
+static bool admit(Task* t, size_t* need_out) {
+    size_t need = 0;
+    for (AddressSpace* a : t->spaces)
+        if (!a->dev) need += a->length;
+    for (Subtask& s : t->subtasks) need += s.reserved;
+    *need_out = need;
+    return need == 0 || make_room(need, t->spaces);
+}
+
 static pmStatus stage_and_launch_gpu(Task* t) {
     Controller& c = ctl();
     const pmCallbacks& cb = t->callbacks->cb;
@@ -431,18 +521,12 @@ static pmStatus stage_and_launch_gpu(Task* t) {
         t->views[i] = t->mem[i].subscriptionVisibilityType == SUBSCRIPTION_COMPACT ? SUBSCRIPTION_COMPACT
                                                                                   : SUBSCRIPTION_NATURAL;
 
-    // Device mirrors (admission by free device memory).
-    size_t need = 0;
-    for (AddressSpace* a : t->spaces)
-        if (!a->dev) need += a->length;
-    for (Subtask& s : t->subtasks) need += s.reserved;
-    if (need && !make_room(need, t->spaces))
-        return fail(pmMemoryError, "task needs %zu bytes of device memory; not available", need);
+    // Device mirrors (admission by free device memory happened in admit()).
     for (AddressSpace* a : t->spaces) {
         std::lock_guard<std::mutex> g(a->mu);
         if (!a->dev) {
-            void* p = nullptr;
-            PMR_DEV(pmb_malloc(&p, a->length));
+            void* p = nullptr;  // stream-ordered: no device-wide synchronisation
+            PMR_DEV(pmb_malloc_async(&p, a->length ? a->length : 1, c.copy_stream));
             a->dev = static_cast<char*>(p);
         }
         a->lru = ++c.lru;
@@ -539,7 +623,7 @@ static pmStatus stage_and_launch_gpu(Task* t) {
         if (batch) continue;  // launched once for the whole task below
 
         // ---- launch (compute stream) ----
-        const size_t sidx = si % c.streams.size();
+        const size_t sidx = c.next_stream++ % c.streams.size();
         void* stream = c.streams[sidx];
         used_stream[sidx] = true;
         PMR_DEV(pmb_stream_wait_event(stream, staged));
@@ -600,8 +684,9 @@ static pmStatus stage_and_launch_gpu(Task* t) {
     }
 
     if (batch) {
-        void* stream = c.streams[0];
-        used_stream[0] = true;
+        const size_t sidx = c.next_stream++ % c.streams.size();
+        void* stream = c.streams[sidx];
+        used_stream[sidx] = true;
         PMR_DEV(pmb_stream_wait_event(stream, events.back()));  // copy stream is ordered: all staged
         const pmStatus st = batch(&t->info, &c.gpu_info, infos.data(), infos.size(), stream);
         if (st != pmSuccess) return fail(st, "batched GPU callback returned %d", static_cast<int>(st));
@@ -620,19 +705,26 @@ static pmStatus stage_and_launch_gpu(Task* t) {
         }
     }
 
-    // ---- join all streams into the task's completion event ----
+    // ---- join the task's streams into its completion event ----
+    // The join point is the last compute stream the task used (the copy stream
+    // for a task without launches), so a task's completion waits only for its
+    // own work, never for unrelated tasks on other streams.
+    void* join = c.copy_stream;
+    for (size_t k = 0; k < c.streams.size(); ++k)
+        if (used_stream[k]) join = c.streams[k];
+    auto join_on = [&](void* from) -> pmStatus {
+        if (from == join) return pmSuccess;
+        void* e = new_event();
+        if (!e) return fail(pmGraphicsCardError, "event creation failed");
+        PMR_DEV(pmb_event_record(e, from));
+        PMR_DEV(pmb_stream_wait_event(join, e));
+        return pmSuccess;
+    };
     {
-        void* e = new_event();
-        if (!e) return fail(pmGraphicsCardError, "event creation failed");
-        PMR_DEV(pmb_event_record(e, c.copy_stream));
-        PMR_DEV(pmb_stream_wait_event(c.join_stream, e));
-    }
-    for (size_t k = 0; k < c.streams.size(); ++k) {
-        if (!used_stream[k]) continue;
-        void* e = new_event();
-        if (!e) return fail(pmGraphicsCardError, "event creation failed");
-        PMR_DEV(pmb_event_record(e, c.streams[k]));
-        PMR_DEV(pmb_stream_wait_event(c.join_stream, e));
+        pmStatus js = join_on(c.copy_stream);
+        for (size_t k = 0; k < c.streams.size() && js == pmSuccess; ++k)
+            if (used_stream[k]) js = join_on(c.streams[k]);
+        if (js != pmSuccess) return js;
     }
     if (write_through) {
         for (size_t i = 0; i < ns; ++i) {
@@ -640,25 +732,29 @@ static pmStatus stage_and_launch_gpu(Task* t) {
             std::lock_guard<std::mutex> g(a->mu);
             std::vector<std::pair<size_t, size_t>> st;
             a->host_stale.present(0, a->length, st);
+            if (!st.empty()) {
+                const pmStatus hs = ensure_host(a);
+                if (hs != pmSuccess) return hs;
+            }
             for (auto& r : st) {
-                PMR_DEV(pmb_memcpy_async(a->host + r.first, a->dev + r.first, r.second - r.first, PMB_D2H, c.join_stream));
+                PMR_DEV(pmb_memcpy_async(a->host + r.first, a->dev + r.first, r.second - r.first, PMB_D2H, join));
                 c.stats.d2h += r.second - r.first;
             }
             a->host_stale.clear();
         }
     }
-    if (t->dev_conf) PMR_DEV(pmb_free_async(t->dev_conf, c.join_stream));
+    if (t->dev_conf) PMR_DEV(pmb_free_async(t->dev_conf, join));
     t->dev_conf = nullptr;
-    PMR_DEV(pmb_event_record(t->done_event, c.join_stream));
+    PMR_DEV(pmb_event_record(t->done_event, join));
     for (size_t i = 0; i < ns; ++i) {
         AddressSpace* a = t->spaces[i];
         std::lock_guard<std::mutex> g(a->mu);
         if (!a->last_access) PMR_DEV(pmb_event_create(&a->last_access, 0));
-        PMR_DEV(pmb_event_record(a->last_access, c.join_stream));
+        PMR_DEV(pmb_event_record(a->last_access, join));
         const bool writes = t->mem[i].memType != READ_ONLY && t->mem[i].memType != READ_ONLY_LAZY;
         if (writes) {
             if (!a->last_write) PMR_DEV(pmb_event_create(&a->last_write, 0));
-            PMR_DEV(pmb_event_record(a->last_write, c.join_stream));
+            PMR_DEV(pmb_event_record(a->last_write, join));
         }
         if (write_through) a->dev_valid.clear();
     }
@@ -675,7 +771,9 @@ static pmStatus run_cpu_task(Task* t) {
     for (size_t i = 0; i < ns; ++i) {
         AddressSpace* a = t->spaces[i];
         std::lock_guard<std::mutex> g(a->mu);
-        const pmStatus st = fetch_range(a, 0, a->length);
+        pmStatus st = ensure_host(a);
+        if (st != pmSuccess) return st;
+        st = fetch_range(a, 0, a->length);
         if (st != pmSuccess) return st;
     }
     const unsigned nthreads = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(),
@@ -804,7 +902,23 @@ static void stub_main() {
         pmStatus st = run_dd(t, t->on_gpu ? c.gpu_info : c.cpu_info);
         if (st == pmSuccess) {
             if (t->on_gpu) {
-                st = stage_and_launch_gpu(t);
+                // Admission: a free slot, then device memory.  While tasks are in
+                // flight their completion frees both, so wait for one and retry;
+                // with nothing in flight a task that still does not fit fails.
+                {
+                    std::unique_lock<std::mutex> lk(c.qmu);
+                    c.icv.wait(lk, [&] { return c.inflight.size() < c.max_inflight; });
+                }
+                size_t need = 0;
+                for (;;) {
+                    if (admit(t, &need)) break;
+                    std::unique_lock<std::mutex> lk(c.qmu);
+                    if (c.inflight.empty()) break;
+                    const size_t before = c.inflight.size();
+                    c.icv.wait_for(lk, std::chrono::milliseconds(50), [&] { return c.inflight.size() < before; });
+                }
+                st = admit(t, &need) ? stage_and_launch_gpu(t)
+                                     : fail(pmMemoryError, "task needs %zu bytes of device memory; not available", need);
                 if (st == pmSuccess) {
                     std::lock_guard<std::mutex> lk(c.qmu);
                     c.inflight.push_back(t);
@@ -824,23 +938,30 @@ static void stub_main() {
 static void completer_main() {
     Controller& c = ctl();
     if (c.has_gpu) pmb_set_device(c.device);
+    // Tasks finish in the order the device completes them, not the order they
+    // were issued: a small task is not held behind a large one.
+    std::vector<Task*> polled;
     for (;;) {
-        Task* t = nullptr;
         {
             std::unique_lock<std::mutex> lk(c.qmu);
             c.icv.wait(lk, [&] { return c.stopping || !c.inflight.empty(); });
             if (c.inflight.empty()) return;
-            t = c.inflight.front();
+            polled.assign(c.inflight.begin(), c.inflight.end());
         }
-        int st;
-        while ((st = pmb_event_query(t->done_event)) == PMB_STATUS_UNAVAILABLE)
-            std::this_thread::sleep_for(std::chrono::microseconds(20));
-        {
-            std::lock_guard<std::mutex> lk(c.qmu);
-            c.inflight.pop_front();
+        bool any = false;
+        for (Task* t : polled) {
+            const int st = pmb_event_query(t->done_event);
+            if (st == PMB_STATUS_UNAVAILABLE) continue;
+            any = true;
+            {
+                std::lock_guard<std::mutex> lk(c.qmu);
+                c.inflight.erase(std::find(c.inflight.begin(), c.inflight.end(), t));
+            }
+            c.icv.notify_all();
+            finish_task(t, st == PMB_SUCCESS ? pmSuccess : pmGraphicsCardError,
+                        st == PMB_SUCCESS ? "" : std::string(pmb_last_error()));
         }
-        finish_task(t, st == PMB_SUCCESS ? pmSuccess : pmGraphicsCardError,
-                    st == PMB_SUCCESS ? "" : std::string(pmb_last_error()));
+        if (!any) std::this_thread::sleep_for(std::chrono::microseconds(20));
     }
 }
 
@@ -889,16 +1010,21 @@ pmStatus pmInitialize() {
         c.gpu_info.deviceIdOnHost = static_cast<uint>(c.device);
         c.gpu_info.deviceIdInCluster = 1;
         PMR_DEV(pmb_stream_create(&c.copy_stream));
-        PMR_DEV(pmb_stream_create(&c.join_stream));
         PMR_DEV(pmb_stream_create(&c.fetch_stream));
-        c.streams.resize(4);
+        const char* ns = getenv("PMB_STREAMS");
+        c.streams.resize(ns && atoi(ns) > 0 ? static_cast<size_t>(atoi(ns)) : 8);
         for (auto& s : c.streams) PMR_DEV(pmb_stream_create(&s));
+        PMR_DEV(pmb_mempool_retain(c.device));
         PMR_DEV(pmb_malloc(&c.dev_device_info, sizeof(pmDeviceInfo)));
         PMR_DEV(pmb_memcpy_async(c.dev_device_info, &c.gpu_info, sizeof(pmDeviceInfo), PMB_H2D, c.copy_stream));
         PMR_DEV(pmb_malloc(&c.dev_status, sizeof(pmStatus)));
         PMR_DEV(pmb_stream_synchronize(c.copy_stream));
         const char* rv = getenv("PMLIB_CUDA_MEM_PER_CARD_RESERVED_FOR_EXTERNAL_USE");
         c.reserve_bytes = rv ? static_cast<size_t>(atoll(rv)) : (size_t(512) << 20);
+        const char* pv = getenv("PMB_PINNED_CACHE_BYTES");
+        c.pin_limit = pv ? static_cast<size_t>(atoll(pv)) : (size_t(8) << 30);
+        const char* mv = getenv("PMB_MAX_INFLIGHT");
+        c.max_inflight = mv && atoi(mv) > 0 ? static_cast<size_t>(atoi(mv)) : 64;
     }
     c.stopping = false;
     c.stub = std::thread(stub_main);
@@ -919,18 +1045,22 @@ pmStatus pmFinalize() {
     if (c.stub.joinable()) c.stub.join();
     if (c.completer.joinable()) c.completer.join();
     std::lock_guard<std::mutex> g(c.mu);
+    if (c.has_gpu) pmb_device_synchronize();
+    // Address spaces first: freeing a device mirror is ordered on the fetch stream.
+    for (AddressSpace* a : c.spaces) free_space(a);
+    c.spaces.clear();
     if (c.has_gpu) {
-        pmb_device_synchronize();
+        pmb_stream_synchronize(c.fetch_stream);
         for (void* s : c.streams) pmb_stream_destroy(s);
         c.streams.clear();
         pmb_stream_destroy(c.copy_stream);
-        pmb_stream_destroy(c.join_stream);
         pmb_stream_destroy(c.fetch_stream);
         pmb_free(c.dev_device_info);
         pmb_free(c.dev_status);
     }
-    for (AddressSpace* a : c.spaces) free_space(a);
-    c.spaces.clear();
+    for (auto& kv : c.pin_free) pmb_host_free(kv.second);
+    c.pin_free.clear();
+    c.pin_cached = 0;
     for (auto& kv : c.files) munmap(kv.second.first, kv.second.second);
     c.files.clear();
     c.callbacks.clear();
@@ -972,15 +1102,7 @@ pmStatus pmCreateMemory(size_t pLength, pmMemHandle* pMemHandle) {
     if (!pMemHandle) return fail(pmInvalidIndex, "null handle");
     Controller& c = ctl();
     std::unique_ptr<AddressSpace> a(new AddressSpace);
-    a->length = pLength;
-    void* p = nullptr;
-    if (c.has_gpu) {
-        if (pmb_host_alloc(&p, pLength ? pLength : 1) != PMB_SUCCESS) return dev_fail(PMB_MEMORY_ERROR, "pinned host allocation");
-    } else {
-        p = malloc(pLength ? pLength : 1);
-        if (!p) return fail(pmMemoryError, "host allocation of %zu bytes failed", pLength);
-    }
-    a->host = static_cast<char*>(p);
+    a->length = pLength;  // host and device copies are allocated on first use
     std::lock_guard<std::mutex> g(c.mu);
     c.spaces.insert(a.get());
     *pMemHandle = a.release();
@@ -1036,6 +1158,8 @@ pmStatus pmGetRawMemPtr(pmMemHandle pMemHandle, pmRawMemPtr* pPtr) {
     AddressSpace* a = space_of(pMemHandle);
     if (!a || !pPtr) return fail(pmUnrecognizedMemory, "unknown memory handle");
     std::lock_guard<std::mutex> g(a->mu);
+    const pmStatus hs = ensure_host(a);
+    if (hs != pmSuccess) return hs;
     // The caller may now write the host copy: device bytes that are not newer
     // than the host are no longer trusted (they are re-staged on next use).
     RangeSet keep;

@@ -51,7 +51,8 @@ struct Record {
 struct AddressSpace {
     size_t length = 0;
     size_t rows = 0, cols = 0;  // pmCreateMemory2D layout (informational)
-    char* host = nullptr;       // pinned host copy
+    char* host = nullptr;       // pinned host copy, allocated on first host use
+    size_t host_cap = 0;        // bytes of the host allocation (>= length when reused)
     char* dev = nullptr;        // device mirror, allocated on first GPU use
     RangeSet dev_valid;         // bytes whose device copy is current
     RangeSet host_stale;        // bytes the device has newer than the host
