@@ -56,6 +56,7 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-apps", action="store_true", help="skip the per-app roofline measurements")
+    ap.add_argument("--no-served", action="store_true", help="skip the served mixed-size task stream")
     return ap.parse_args()
 
 
@@ -296,16 +297,16 @@ def app_measurements(torch, L, stream):
                 "plain_fp32_simt_tflops": round(fl / tp / 1e9, 2),
                 "cublas_sgemm_fp32_tflops": round(fl / tc / 1e9, 2)}
             del A, B, C, ws
-        # LU: n = 4096, diagonally dominant, nb = 128
+        # LU: n = 4096, diagonally dominant, nb = 64
         nl = 4096
         A0 = torch.rand(nl, nl, device="cuda", generator=g) * 2 - 1
         A0 += torch.eye(nl, device="cuda") * nl
         Aw = A0.clone()
-        lws = ops._scratch(L.pmb_lu_workspace_bytes(nl, 128))
+        lws = ops._scratch(L.pmb_lu_workspace_bytes(nl, 64))
 
         def lu_once():
             Aw.copy_(A0)
-            capi.check(L.pmb_lu_decompose(Aw.data_ptr(), nl, nl, 128, lws.data_ptr(), lws.numel(), sp))
+            capi.check(L.pmb_lu_decompose(Aw.data_ptr(), nl, nl, 64, lws.data_ptr(), lws.numel(), sp))
 
         cp_ms = _timed(torch, stream, lambda: Aw.copy_(A0), 5)
         lu_ms = _timed(torch, stream, lu_once, 5) - cp_ms
@@ -314,6 +315,45 @@ def app_measurements(torch, L, stream):
         res["lu_4096"] = {"gflops": round((2.0 / 3.0) * nl ** 3 / lu_ms / 1e6, 1), "ms": round(lu_ms, 3),
                           "residual_fro": resid}
     return res
+
+
+SERVED_BIN = os.path.join(ROOT, "unicorn_b200", "serve", "_build", "served_mix")
+SERVED_TASKS = 2000
+
+
+def _served_run(args):
+    p = subprocess.run([SERVED_BIN, *map(str, args)], capture_output=True, text=True, timeout=1200)
+    lines = p.stdout.strip().splitlines()
+    if p.returncode != 0 or not lines:
+        return {"error": f"served_mix exited {p.returncode}: {(p.stderr or p.stdout)[-300:]}"}
+    return json.loads(lines[-1])
+
+
+def served_measurement():
+    """Served mixed-size stream (2,000 GEMM/LU tasks over the pm:: API) against
+    the plain FP32 one-task-at-a-time form: first with arrivals faster than
+    either form can serve (throughput), then at 75 % of the served capacity
+    (latency under load; the plain form is overloaded at that rate)."""
+    if not os.path.exists(SERVED_BIN):
+        return {"error": "served_mix not built (make -C unicorn_b200/serve)"}
+    keep = ("tasks_per_s", "completed", "span_s", "p50_ms", "p99_ms", "gemm_p50_ms", "gemm_p99_ms", "lu_p50_ms",
+            "lu_p99_ms", "max_gemm_rel_err", "max_lu_residual", "error")
+    sat = _served_run(["--tasks", SERVED_TASKS, "--rate", 20000])
+    if "error" in sat:
+        return sat
+    out = {"workload": sat["workload"], "gemm_gflop": sat["gemm_gflop"], "lu_gflop": sat["lu_gflop"],
+           "result_bytes": sat["result_bytes"], "plain_form": sat["plain_gemm"] + " GEMM, FP32 SIMT blocked LU, "
+           "one task at a time",
+           "saturated": {"rate_per_s": sat["rate_per_s"], "served": {k: sat["served"][k] for k in keep},
+                         "plain": {k: sat["plain"][k] for k in keep},
+                         "served_over_plain_tasks_per_s": sat.get("served_over_plain"),
+                         "alone_vs_mix": sat["served_alone_vs_mix"]}}
+    rate = round(0.75 * sat["served"]["tasks_per_s"], 1)
+    ld = _served_run(["--tasks", SERVED_TASKS, "--rate", rate, "--check", 4])
+    if "error" not in ld:
+        out["at_load"] = {"rate_per_s": rate, "served": {k: ld["served"][k] for k in keep},
+                          "plain": {k: ld["plain"][k] for k in keep}}
+    return out
 
 
 def _hbm_entry(nbytes: int, ms: float, hbm: float):
@@ -437,6 +477,8 @@ def main():
     }
     if apps is not None:
         line["apps"] = apps
+    if rank == 0 and world == 1 and not args.no_served:
+        line["served_mix"] = served_measurement()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(img, f, os.cpu_count() or 1)
     if dist is not None:

@@ -38,7 +38,10 @@
 #include <cuda.h>
 #include <cuda_bf16.h>
 
+#include <algorithm>
+#include <cstdlib>
 #include <mutex>
+#include <string>
 
 #include "pmb_common.cuh"
 
@@ -290,39 +293,314 @@ gemm_bf16x3_kernel(const __grid_constant__ GemmMaps maps, int M, int N, int KT, 
     }
 }
 
-// ---- split passes -----------------------------------------------------------
-// rows of X (R x K, ldx) -> hi/lo (R x Kp) bf16, zero padded to Kp.
-__global__ void split_rows_kernel(const float* __restrict__ X, int64_t ldx, int R, int K, int Kp,
-                                  __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo) {
-    const int64_t total = static_cast<int64_t>(R) * Kp;
-    for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
-         i += static_cast<int64_t>(gridDim.x) * blockDim.x) {
-        const int64_t r = i / Kp;
-        const int k = static_cast<int>(i - r * Kp);
-        const float x = k < K ? X[r * ldx + k] : 0.0f;
-        const __nv_bfloat16 h = __float2bfloat16_rn(x);
-        hi[i] = h;
-        lo[i] = __float2bfloat16_rn(x - __bfloat162float(h));
+// ---- 2-SM kernel: one 256 x 256 output tile per CTA pair ----------------------
+// A cluster of two CTAs on two SMs issues tcgen05.mma.cta_group::2 with M = 256,
+// N = 256: each CTA stages its own 128 rows of A and its own 128 rows of B^T
+// (non-multicast TMA), the leader CTA's single MMA thread reads both CTAs'
+// shared memory, and each CTA's tensor memory receives its 128 rows of the
+// tile.  Per CTA and K-slice that is 64 KB of operands for the work the 1-SM
+// kernel needs 96 KB for, and the 128-byte K slices (SWIZZLE_128B) halve the
+// number of TMA requests; three stages fill the shared memory.
+//   full[s]     leader only: one arrive.expect_tx from each CTA's producer plus
+//               both CTAs' TMA bytes (the peer's loads signal it remotely);
+//   empty[s]    both CTAs: multicast tcgen05.commit from the leader;
+//   acc_full[b] both CTAs: multicast commit after a 1024-deep K segment;
+//   acc_empty[b] leader only: one remote arrive per epilogue warp of each CTA.
+// The epilogue stages each 32 x 16 chunk through shared memory so that global
+// reads and writes of C are whole 64-byte row pieces.
+constexpr int BK2 = 64;                                   // 128-byte rows
+constexpr int kStages2 = 3;
+constexpr int kHalf2 = 128 * BK2 * 2;                     // 16 KB: 128 rows of one operand
+constexpr int kStage2Bytes = 4 * kHalf2;                  // A hi, A lo, B hi, B lo halves
+constexpr int kStageOutFloats = 4 * 32 * 20;              // per-warp 32 x 16 staging, row stride 20
+constexpr int kSmem2Bytes = kStages2 * kStage2Bytes + kStageOutFloats * 4 + 1024 + 256;
+constexpr int kFlush2 = 16;                               // K = 1024 per accumulator segment
+constexpr int kGroupRows = 8;                             // tile rows per raster group
+constexpr uint32_t kIdesc2 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(256 >> 3) << 17) |
+                             ((uint32_t)(256 >> 4) << 24);
+
+// K-major SWIZZLE_128B tile: rows of 128 bytes, 8-row core groups 1024 bytes apart.
+__device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= static_cast<uint64_t>((saddr >> 4) & 0x3FFF);
+    d |= static_cast<uint64_t>(1) << 16;
+    d |= static_cast<uint64_t>(1024 >> 4) << 32;
+    d |= static_cast<uint64_t>(1) << 46;
+    d |= static_cast<uint64_t>(2) << 61;  // SWIZZLE_128B
+    return d;
+}
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+// shared::cluster address of the same shared variable in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t cluster_addr(uint32_t saddr, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(saddr), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ void cluster_sync_all() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx_cluster(uint32_t cbar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.release.cluster.shared::cluster.b64 _, [%0], %1;" ::"r"(cbar), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t cbar) {
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cbar) : "memory");
+}
+// TMA load into this CTA's shared memory, completion on an mbarrier of either CTA of the pair.
+__device__ __forceinline__ void tma_load_2d_pair(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t cbar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes.cta_group::2 [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(cbar)
+        : "memory");
+}
+__device__ __forceinline__ void umma_bf16_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(kIdesc2), "r"(accumulate)
+        : "memory");
+}
+// Arrive once on the mbarrier at this shared offset in both CTAs of the pair.
+__device__ __forceinline__ void umma_commit_pair(uint32_t bar) {
+    asm volatile(
+        "tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;" ::"r"(bar),
+        "h"(static_cast<uint16_t>(3))
+        : "memory");
+}
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
+gemm_bf16x3_2sm_kernel(const __grid_constant__ GemmMaps maps, int M, int N, int KT, float alpha, float beta,
+                       float* __restrict__ C, int64_t ldc, uint32_t* __restrict__ err) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    float* stage_out = reinterpret_cast<float*>(smem + kStages2 * kStage2Bytes);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kStages2 * kStage2Bytes + kStageOutFloats * 4);
+    uint64_t* full = bars;                          // [kStages2]
+    uint64_t* empty = bars + kStages2;              // [kStages2]
+    uint64_t* acc_full = bars + 2 * kStages2;       // [2]
+    uint64_t* acc_empty = bars + 2 * kStages2 + 2;  // [2]
+    uint64_t* teardown = bars + 2 * kStages2 + 4;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 2 * kStages2 + 5);
+    __shared__ volatile int s_fail;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_rank();
+    // Grouped tile order: consecutive pairs sweep the columns of a band of
+    // kGroupRows tile rows, so the pairs resident at one time share A and B
+    // panels (read once from HBM, then from L2) instead of each wave reading
+    // every row panel of A.
+    int pm, pn;
+    {
+        const int num_pm = (M + 255) / 256, num_pn = (N + 255) / 256;
+        const int pid = static_cast<int>(blockIdx.x >> 1);
+        const int per_group = kGroupRows * num_pn;
+        const int first = (pid / per_group) * kGroupRows;
+        const int rows = min(num_pm - first, kGroupRows);
+        const int in_group = pid % per_group;
+        pm = first + in_group % rows;
+        pn = in_group / rows;
+    }
+    const int m0 = pm * 256 + 128 * static_cast<int>(rank);  // this CTA's rows of A and C
+    const int n0 = pn * 256;                                 // the pair's columns
+    const int nb0 = n0 + 128 * static_cast<int>(rank);       // this CTA's rows of B^T
+
+    if (threadIdx.x == 0) {
+        s_fail = 0;
+        for (int s = 0; s < kStages2; ++s) {
+            mbar_init(smem_u32(&full[s]), 2);
+            mbar_init(smem_u32(&empty[s]), 1);
+        }
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(smem_u32(&acc_full[b]), 1);
+            mbar_init(smem_u32(&acc_empty[b]), 8);  // 4 epilogue warps in each CTA
+        }
+        mbar_init(smem_u32(teardown), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    cluster_sync_all();  // the peer's barriers exist before anyone signals them
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // ---- producer (both CTAs) ----
+        for (int kt = 0; kt < KT; ++kt) {
+            const int s = kt % kStages2;
+            if (kt >= kStages2 && !mbar_wait(smem_u32(&empty[s]), ((kt / kStages2) + 1) & 1)) {
+                s_fail = 1;
+                atomicOr(err, kErrTimeout);
+                break;
+            }
+            if (s_fail) break;
+            uint8_t* st = smem + s * kStage2Bytes;
+            const uint32_t fbar = cluster_addr(smem_u32(&full[s]), 0);
+            mbar_arrive_expect_tx_cluster(fbar, kStage2Bytes);
+            const int k = kt * BK2;
+            tma_load_2d_pair(smem_u32(st), &maps.ah, k, m0, fbar);
+            tma_load_2d_pair(smem_u32(st + kHalf2), &maps.al, k, m0, fbar);
+            tma_load_2d_pair(smem_u32(st + 2 * kHalf2), &maps.bh, k, nb0, fbar);
+            tma_load_2d_pair(smem_u32(st + 3 * kHalf2), &maps.bl, k, nb0, fbar);
+        }
+    } else if (warp == 1 && lane == 0 && rank == 0) {
+        // ---- MMA issuer (leader CTA) ----
+        for (int kt = 0; kt < KT; ++kt) {
+            const int s = kt % kStages2;
+            const int seg = kt / kFlush2, seg_k = kt % kFlush2, b = seg & 1;
+            if (seg_k == 0 && seg >= 2 && !mbar_wait(smem_u32(&acc_empty[b]), ((seg >> 1) - 1) & 1)) {
+                s_fail = 1;
+                atomicOr(err, kErrTimeout);
+                break;
+            }
+            if (!mbar_wait(smem_u32(&full[s]), (kt / kStages2) & 1)) {
+                s_fail = 1;
+                atomicOr(err, kErrTimeout);
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t acc = tmem + 256u * b;
+            const uint32_t st = smem_u32(smem + s * kStage2Bytes);
+            const uint32_t a_hi = st, a_lo = st + kHalf2, b_hi = st + 2 * kHalf2, b_lo = st + 3 * kHalf2;
+#pragma unroll
+            for (int k16 = 0; k16 < BK2 / 16; ++k16) {
+                const uint32_t off = k16 * 32;  // 16 bf16 = 32 bytes along the swizzled row
+                umma_bf16_pair(acc, umma_desc_sw128(a_hi + off), umma_desc_sw128(b_hi + off), (seg_k | k16) != 0);
+                umma_bf16_pair(acc, umma_desc_sw128(a_hi + off), umma_desc_sw128(b_lo + off), 1u);
+                umma_bf16_pair(acc, umma_desc_sw128(a_lo + off), umma_desc_sw128(b_hi + off), 1u);
+            }
+            umma_commit_pair(smem_u32(&empty[s]));
+            if (seg_k == kFlush2 - 1 || kt == KT - 1) umma_commit_pair(smem_u32(&acc_full[b]));
+        }
+    } else if (warp >= 2) {
+        // ---- epilogue (both CTAs): drain each segment of this CTA's 128 rows ----
+        const int q = warp & 3;
+        float* stg = stage_out + q * 32 * 20;
+        const int nseg = (KT + kFlush2 - 1) / kFlush2;
+        const bool vec_ok = (ldc & 3) == 0 && (reinterpret_cast<uintptr_t>(C) & 15) == 0;
+        for (int seg = 0; seg < nseg; ++seg) {
+            const int b = seg & 1;
+            if (!mbar_wait(smem_u32(&acc_full[b]), (seg >> 1) & 1)) {
+                s_fail = 1;
+                atomicOr(err, kErrTimeout);
+                break;
+            }
+            if (s_fail) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const float bscale = seg == 0 ? beta : 1.0f;
+#pragma unroll 1
+            for (int c = 0; c < 256 / 16; ++c) {
+                uint32_t r[16];
+                tmem_ld16(tmem + 256u * b + (static_cast<uint32_t>(32 * q) << 16) + 16 * c, r);
+                float4* mine = reinterpret_cast<float4*>(stg + lane * 20);
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                    mine[j] = make_float4(__uint_as_float(r[4 * j]), __uint_as_float(r[4 * j + 1]),
+                                          __uint_as_float(r[4 * j + 2]), __uint_as_float(r[4 * j + 3]));
+                __syncwarp();
+#pragma unroll
+                for (int i = 0; i < 4; ++i) {
+                    const int rl = i * 8 + (lane >> 2), c4 = (lane & 3) * 4;
+                    const int grow = m0 + 32 * q + rl, gcol = n0 + 16 * c + c4;
+                    if (grow >= M || gcol >= N) continue;
+                    float4 v = *reinterpret_cast<const float4*>(stg + rl * 20 + c4);
+                    float* cp = C + static_cast<int64_t>(grow) * ldc + gcol;
+                    if (vec_ok && gcol + 4 <= N) {
+                        float4 o = make_float4(alpha * v.x, alpha * v.y, alpha * v.z, alpha * v.w);
+                        if (bscale != 0.0f) {
+                            const float4 old = *reinterpret_cast<const float4*>(cp);
+                            o.x += bscale * old.x;
+                            o.y += bscale * old.y;
+                            o.z += bscale * old.z;
+                            o.w += bscale * old.w;
+                        }
+                        *reinterpret_cast<float4*>(cp) = o;
+                    } else {
+                        const float vv[4] = {v.x, v.y, v.z, v.w};
+                        for (int j = 0; j < 4 && gcol + j < N; ++j) {
+                            float o = alpha * vv[j];
+                            if (bscale != 0.0f) o += bscale * cp[j];
+                            cp[j] = o;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive_cluster(cluster_addr(smem_u32(&acc_empty[b]), 0));
+        }
+    }
+
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 1 && rank == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (s_fail && lane == 0) {
+            // Every MMA this pair issued must retire before the tensor memory is freed.
+            umma_commit_pair(smem_u32(teardown));
+            mbar_wait(smem_u32(teardown), 0);
+        }
+        __syncwarp();
+    }
+    // Neither CTA leaves (or frees its tensor memory) while the other may still
+    // read its shared memory or write its tensor memory.
+    cluster_sync_all();
+    if (warp == 1) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
     }
 }
 
-// X (K x N, ldx) -> transposed hi/lo (N x Kp), 32 x 32 tiles through shared memory.
-__global__ void split_transpose_kernel(const float* __restrict__ X, int64_t ldx, int K, int N, int Kp,
-                                       __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo) {
+// ---- split passes -----------------------------------------------------------
+// Both splits in one launch: blocks [0, row_blocks) split the rows of A
+// (M x K) as split_rows_kernel does, the others take one 32 x 32 tile of B
+// (K x N) each as split_transpose_kernel does.  256 threads per block.
+__global__ void __launch_bounds__(256)
+split_both_kernel(const float* __restrict__ A, int64_t lda, int M, const float* __restrict__ B, int64_t ldb, int N,
+                  int K, int Kp, int row_blocks, __nv_bfloat16* __restrict__ ah, __nv_bfloat16* __restrict__ al,
+                  __nv_bfloat16* __restrict__ bh, __nv_bfloat16* __restrict__ bl) {
     __shared__ float t[32][33];
-    const int k0 = blockIdx.y * 32, n0 = blockIdx.x * 32;
-    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
-        const int k = k0 + j, n = n0 + threadIdx.x;
-        t[j][threadIdx.x] = (k < K && n < N) ? X[static_cast<int64_t>(k) * ldx + n] : 0.0f;
+    if (static_cast<int>(blockIdx.x) < row_blocks) {
+        const int64_t total = static_cast<int64_t>(M) * Kp;
+        for (int64_t i = blockIdx.x * static_cast<int64_t>(blockDim.x) + threadIdx.x; i < total;
+             i += static_cast<int64_t>(row_blocks) * blockDim.x) {
+            const int64_t r = i / Kp;
+            const int k = static_cast<int>(i - r * Kp);
+            const float x = k < K ? A[r * lda + k] : 0.0f;
+            const __nv_bfloat16 h = __float2bfloat16_rn(x);
+            ah[i] = h;
+            al[i] = __float2bfloat16_rn(x - __bfloat162float(h));
+        }
+        return;
+    }
+    const int tile = blockIdx.x - row_blocks;
+    const int tiles_n = (N + 31) / 32;
+    const int k0 = (tile / tiles_n) * 32, n0 = (tile % tiles_n) * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    for (int j = ty; j < 32; j += 8) {
+        const int k = k0 + j, n = n0 + tx;
+        t[j][tx] = (k < K && n < N) ? B[static_cast<int64_t>(k) * ldb + n] : 0.0f;
     }
     __syncthreads();
-    for (int j = threadIdx.y; j < 32; j += blockDim.y) {
-        const int n = n0 + j, k = k0 + threadIdx.x;
+    for (int j = ty; j < 32; j += 8) {
+        const int n = n0 + j, k = k0 + tx;
         if (n < N && k < Kp) {
-            const float x = t[threadIdx.x][j];
+            const float x = t[tx][j];
             const __nv_bfloat16 h = __float2bfloat16_rn(x);
-            hi[static_cast<int64_t>(n) * Kp + k] = h;
-            lo[static_cast<int64_t>(n) * Kp + k] = __float2bfloat16_rn(x - __bfloat162float(h));
+            bh[static_cast<int64_t>(n) * Kp + k] = h;
+            bl[static_cast<int64_t>(n) * Kp + k] = __float2bfloat16_rn(x - __bfloat162float(h));
         }
     }
 }
@@ -397,16 +675,18 @@ EncodeTiledFn encode_fn() {
     return fn;
 }
 
-int make_map(CUtensorMap* map, const void* base, int rows, int kp, int box_rows) {
+// K-major bf16 operand [rows][kp]: boxes of box_k x box_rows, 64- or 128-byte swizzle.
+int make_map(CUtensorMap* map, const void* base, int rows, int kp, int box_rows, int box_k = BK) {
     EncodeTiledFn fn = encode_fn();
     if (!fn) return pmb::fail(PMB_GRAPHICS_CARD_ERROR, "cuTensorMapEncodeTiled unavailable");
     const cuuint64_t dims[2] = {static_cast<cuuint64_t>(kp), static_cast<cuuint64_t>(rows)};
     const cuuint64_t strides[1] = {static_cast<cuuint64_t>(kp) * 2};
-    const cuuint32_t box[2] = {BK, static_cast<cuuint32_t>(box_rows)};
+    const cuuint32_t box[2] = {static_cast<cuuint32_t>(box_k), static_cast<cuuint32_t>(box_rows)};
     const cuuint32_t estr[2] = {1, 1};
     const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
-                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
-                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+                          CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          box_k == 64 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return pmb::fail(PMB_GRAPHICS_CARD_ERROR, "cuTensorMapEncodeTiled failed (%d)", (int)r);
     return PMB_SUCCESS;
 }
@@ -422,9 +702,29 @@ extern "C" size_t pmb_gemm_workspace_bytes(int M, int N, int K) {
     return 256 + 2 * align256(static_cast<size_t>(M) * kp * 2) + 2 * align256(static_cast<size_t>(N) * kp * 2);
 }
 
+namespace pmb {
+
+// The GEMM behind pmb_sgemm_bf16x3.  A and B are copied into the split buffers
+// of the workspace before the product runs, so C may overlap A or B (the LU
+// panel solves write their result over their own operand).  clear_error=false
+// skips clearing the workspace's error word (a caller issuing many products on
+// one workspace clears it once).
+int sgemm_bf16x3_launch(int M, int N, int K, float alpha, const float* A, int64_t lda, const float* B, int64_t ldb,
+                        float beta, float* C, int64_t ldc, void* workspace, size_t ws_bytes, cudaStream_t s,
+                        bool clear_error);
+
+}  // namespace pmb
+
 extern "C" int pmb_sgemm_bf16x3(int M, int N, int K, float alpha, const float* A, int64_t lda, const float* B,
                                 int64_t ldb, float beta, float* C, int64_t ldc, void* workspace, size_t ws_bytes,
                                 void* stream) {
+    return pmb::sgemm_bf16x3_launch(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, workspace, ws_bytes,
+                                    static_cast<cudaStream_t>(stream), true);
+}
+
+int pmb::sgemm_bf16x3_launch(int M, int N, int K, float alpha, const float* A, int64_t lda, const float* B,
+                             int64_t ldb, float beta, float* C, int64_t ldc, void* workspace, size_t ws_bytes,
+                             cudaStream_t s, bool clear_error) {
     PMB_CHECK_ARG(M >= 0 && N >= 0 && K >= 0, "negative GEMM size");
     if (M == 0 || N == 0) return PMB_SUCCESS;
     PMB_CHECK_ARG(C && workspace && (K == 0 || (A && B)), "null pointer");
@@ -432,7 +732,6 @@ extern "C" int pmb_sgemm_bf16x3(int M, int N, int K, float alpha, const float* A
     PMB_CHECK_ARG((reinterpret_cast<uintptr_t>(workspace) & 255) == 0, "workspace must be 256-byte aligned");
     PMB_CHECK_ARG(ws_bytes >= pmb_gemm_workspace_bytes(M, N, K), "GEMM workspace %zu bytes, need %zu", ws_bytes,
                   pmb_gemm_workspace_bytes(M, N, K));
-    cudaStream_t s = static_cast<cudaStream_t>(stream);
     if (K == 0) {
         scale_kernel<<<256, 256, 0, s>>>(C, ldc, M, N, beta);
         PMB_CUDA_TRY(cudaGetLastError());
@@ -446,14 +745,40 @@ extern "C" int pmb_sgemm_bf16x3(int M, int N, int K, float alpha, const float* A
     __nv_bfloat16* bh = reinterpret_cast<__nv_bfloat16*>(reinterpret_cast<char*>(al) + align256(static_cast<size_t>(M) * kp * 2));
     __nv_bfloat16* bl = reinterpret_cast<__nv_bfloat16*>(reinterpret_cast<char*>(bh) + align256(static_cast<size_t>(N) * kp * 2));
 
-    PMB_CUDA_TRY(cudaMemsetAsync(ws, 0, 256, s));
-    split_rows_kernel<<<1184, 256, 0, s>>>(A, lda, M, K, kp, ah, al);
-    PMB_CUDA_TRY(cudaGetLastError());
-    split_transpose_kernel<<<dim3((N + 31) / 32, (kp + 31) / 32), dim3(32, 8), 0, s>>>(B, ldb, K, N, kp, bh, bl);
-    PMB_CUDA_TRY(cudaGetLastError());
+    if (clear_error) PMB_CUDA_TRY(cudaMemsetAsync(ws, 0, 256, s));
+    {
+        const int64_t row_elems = static_cast<int64_t>(M) * kp;
+        const int row_blocks = static_cast<int>(std::min<int64_t>(1184, (row_elems + 255) / 256));
+        const int tiles = ((N + 31) / 32) * ((kp + 31) / 32);
+        split_both_kernel<<<row_blocks + tiles, 256, 0, s>>>(A, lda, M, B, ldb, N, K, kp, row_blocks, ah, al, bh, bl);
+        PMB_CUDA_TRY(cudaGetLastError());
+    }
 
     GemmMaps maps;
     int st;
+    // Tiles of 256 rows per CTA pair for M > 128 (PMB_GEMM_KERNEL=1sm keeps the 1-SM kernel).
+    static const bool force_1sm = [] {
+        const char* v = getenv("PMB_GEMM_KERNEL");
+        return v && std::string(v) == "1sm";
+    }();
+    if (M > BM && !force_1sm) {
+        if ((st = make_map(&maps.ah, ah, M, kp, 128, BK2)) != PMB_SUCCESS) return st;
+        if ((st = make_map(&maps.al, al, M, kp, 128, BK2)) != PMB_SUCCESS) return st;
+        if ((st = make_map(&maps.bh, bh, N, kp, 128, BK2)) != PMB_SUCCESS) return st;
+        if ((st = make_map(&maps.bl, bl, N, kp, 128, BK2)) != PMB_SUCCESS) return st;
+        static std::once_flag attr2_once;
+        static cudaError_t attr2_err = cudaSuccess;
+        std::call_once(attr2_once, [] {
+            attr2_err =
+                cudaFuncSetAttribute(gemm_bf16x3_2sm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem2Bytes);
+        });
+        PMB_CUDA_TRY(attr2_err);
+        const dim3 grid2(2 * ((M + 255) / 256) * ((N + 255) / 256));
+        gemm_bf16x3_2sm_kernel<<<grid2, kThreads, kSmem2Bytes, s>>>(maps, M, N, (kp + BK2 - 1) / BK2, alpha, beta, C,
+                                                                     ldc, err);
+        PMB_CUDA_TRY(cudaGetLastError());
+        return PMB_SUCCESS;
+    }
     if ((st = make_map(&maps.ah, ah, M, kp, BM)) != PMB_SUCCESS) return st;
     if ((st = make_map(&maps.al, al, M, kp, BM)) != PMB_SUCCESS) return st;
     if ((st = make_map(&maps.bh, bh, N, kp, BN)) != PMB_SUCCESS) return st;

@@ -14,7 +14,9 @@
 // B200 design, per nb-step:
 //  1. one CTA factors the nb x nb diagonal block in FP64, held in registers
 //     (one barrier per column) and, in the same launch, inverts both
-//     triangles in FP64 (W = L11^-1, V = U11^-1), written as fp32;
+//     triangles in FP64 (W = L11^-1, V = U11^-1), written as fp32.  nb = 64
+//     (256 threads) is the default: the step chain is serial, so a smaller
+//     block halves its length and lets the CTA share an SM with GEMM tiles;
 //  2. U12 = W * A12 and L21 = A21 * V run as tensor-core GEMMs (BF16x3);
 //  3. A22 -= L21 * U12 runs as a tensor-core GEMM with alpha=-1, beta=1.
 // An FP64 scan of each finished L column checks that partial pivoting would
@@ -27,32 +29,20 @@ extern "C" size_t pmb_gemm_workspace_bytes(int M, int N, int K);
 extern "C" int pmb_sgemm_bf16x3(int M, int N, int K, float alpha, const float* A, int64_t lda, const float* B,
                                 int64_t ldb, float beta, float* C, int64_t ldc, void* workspace, size_t ws_bytes,
                                 void* stream);
+namespace pmb {
+int sgemm_bf16x3_launch(int M, int N, int K, float alpha, const float* A, int64_t lda, const float* B, int64_t ldb,
+                        float beta, float* C, int64_t ldc, void* workspace, size_t ws_bytes, cudaStream_t s,
+                        bool clear_error);
+}
 extern "C" int pmb_sgemm_plain(int M, int N, int K, float alpha, const float* A, int64_t lda, const float* B,
                                int64_t ldb, float beta, float* C, int64_t ldc, void* stream);
 
 namespace {
 
-constexpr int kDiagThreads = 512;
 constexpr int kMaxNb = 128;
 constexpr uint32_t kFlagPivot = 1;      // partial pivoting would have swapped rows
 constexpr uint32_t kFlagZeroPivot = 2;  // a pivot was exactly zero
 
-// Factor the kb x kb diagonal block at A (lda) in FP64 and write W = L^-1,
-// V = U^-1 (kb x kb, column-major, ld = kb).
-//
-// The block lives in registers for the whole kernel: thread (tx = lane,
-// ty = warp) owns rows tx + 32*ii (ii < 4) of columns ty + 16*jj (jj < 8),
-// a cyclic layout that keeps every thread busy as the active part shrinks.
-// Blocks smaller than 128 are padded with the identity, which neither step
-// changes.  Each elimination step publishes one column and one row through a
-// double-buffered shared vector, so a step costs one barrier:
-//  - factorization (Crout): step i scales row i by 1/a_ii and applies the
-//    rank-1 update a_rc -= a_ri * u_ic to the trailing block;
-//  - inverses, both triangles in the same steps: W by right-looking forward
-//    substitution (row k of W final at step k, X_rj -= L_rk W_kj below it) and
-//    V by right-looking back substitution from the last row (Y_rj -= U_rq V_qj
-//    above row q).  The entries of L (U) consumed at a step are dead after it,
-//    so W (V) overwrites the lower (strict upper) triangle in place.
 // Element (ii, js) / (is, jj) of a register tile with a run-time index on one
 // side, by a select chain (indexing the array at run time would move it to
 // local memory).
@@ -71,20 +61,46 @@ __device__ __forceinline__ double pick_in_col(const double (&a)[R][C], int is, i
     return v;
 }
 
-__global__ void __launch_bounds__(kDiagThreads, 1)
+// Factor the kb x kb diagonal block at A (lda) in FP64 and write W = L^-1,
+// V = U^-1 (kb x kb, column-major, ld = kb); kb <= NB.
+//
+// The block lives in registers for the whole kernel: thread (tx = lane,
+// ty = warp) owns rows tx + 32*ii of columns ty + WARPS*jj (16 elements for
+// NB = 64 on 256 threads, 32 for NB = 128 on 512), a cyclic layout that keeps
+// every thread busy as the active part shrinks.  Blocks smaller than NB are
+// padded with the identity, which neither phase changes.  Each elimination
+// step publishes one column and one row through double-buffered shared
+// vectors, so a step costs one barrier.  The published column is zero outside
+// the rows a step updates, so the update of every column a warp owns is one
+// unconditional FMA per element (the column-ownership test is warp-uniform);
+// only the one column a step retires takes per-lane selects.
+//  - factorization (Crout): step i publishes column i (zero at rows <= i) and
+//    the unscaled row i; the pivot's owner computes 1/a_ii once.  Trailing
+//    elements do a_rc -= a_ri * (a_ic / a_ii); row i itself is scaled by the
+//    stored reciprocals after the last step (U unit upper, L keeps pivots).
+//  - inverses, both triangles in the same steps: W by right-looking forward
+//    substitution (row k of W final at step k: its owner scales it while
+//    publishing; X_rj -= L_rk W_kj below it) and V by right-looking back
+//    substitution from the last row (Y_rj -= U_rq V_qj above row q).  The
+//    entries of L (U) consumed at a step are dead after it, so W (V)
+//    overwrites the lower (strict upper) triangle in place.
+template <int NB, int THREADS>
+__global__ void __launch_bounds__(THREADS, 1)
 lu_diag_kernel(float* __restrict__ A, int64_t lda, int kb, float* __restrict__ W, float* __restrict__ V,
                uint32_t* __restrict__ flags) {
-    constexpr int RI = kMaxNb / 32, CJ = kMaxNb / 16;
-    __shared__ double s_col[2][kMaxNb];
-    __shared__ double s_row[2][kMaxNb];
-    __shared__ double s_ucol[2][kMaxNb];
-    __shared__ double s_vrow[2][kMaxNb];
-    __shared__ double s_piv[2];
+    constexpr int WARPS = THREADS / 32;
+    constexpr int RI = NB / 32, CJ = NB / WARPS;
+    static_assert(RI * CJ * THREADS == NB * NB, "every element owned once");
+    __shared__ double s_col[2][NB];
+    __shared__ double s_row[2][NB];
+    __shared__ double s_ucol[2][NB];
+    __shared__ double s_vrow[2][NB];
+    __shared__ double s_inv[NB];  // 1 / pivot, by step
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     double a[RI][CJ];
 #pragma unroll
     for (int jj = 0; jj < CJ; ++jj) {
-        const int c = ty + 16 * jj;
+        const int c = ty + WARPS * jj;
 #pragma unroll
         for (int ii = 0; ii < RI; ++ii) {
             const int r = tx + 32 * ii;
@@ -93,37 +109,54 @@ lu_diag_kernel(float* __restrict__ A, int64_t lda, int kb, float* __restrict__ W
         }
     }
 
-    // ---- Crout LU: L keeps the pivots, U is unit upper ----------------------
+    // ---- Crout LU ------------------------------------------------------------
     for (int i = 0; i < kb; ++i) {
         const int buf = i & 1;
-        if (ty == (i & 15)) {
-#pragma unroll
-            for (int ii = 0; ii < RI; ++ii) s_col[buf][tx + 32 * ii] = pick_in_row(a, ii, i >> 4);
-        }
-        if (tx == (i & 31)) {
-#pragma unroll
-            for (int jj = 0; jj < CJ; ++jj) s_row[buf][ty + 16 * jj] = pick_in_col(a, i >> 5, jj);
-        }
-        __syncthreads();
-        const double piv = s_col[buf][i];
-        if (threadIdx.x == 0 && piv == 0.0) atomicOr(flags, kFlagZeroPivot);
-        const double inv = piv != 0.0 ? 1.0 / piv : 0.0;
-#pragma unroll
-        for (int jj = 0; jj < CJ; ++jj) {
-            const int c = ty + 16 * jj;
-            if (c <= i) continue;
-            const double u = s_row[buf][c] * inv;
+        if (ty == i % WARPS) {
 #pragma unroll
             for (int ii = 0; ii < RI; ++ii) {
                 const int r = tx + 32 * ii;
-                if (r == i) a[ii][jj] = u;
-                else if (r > i) a[ii][jj] = fma(-s_col[buf][r], u, a[ii][jj]);
+                const double v = pick_in_row(a, ii, i / WARPS);
+                s_col[buf][r] = r > i ? v : 0.0;
+                if (r == i) {
+                    if (v == 0.0) atomicOr(flags, kFlagZeroPivot);
+                    s_inv[i] = v != 0.0 ? 1.0 / v : 0.0;
+                }
             }
+        }
+        if (tx == (i & 31)) {
+#pragma unroll
+            for (int jj = 0; jj < CJ; ++jj) s_row[buf][ty + WARPS * jj] = pick_in_col(a, i >> 5, jj);
+        }
+        __syncthreads();
+        const double inv = s_inv[i];
+        double lc[RI];
+#pragma unroll
+        for (int ii = 0; ii < RI; ++ii) lc[ii] = s_col[buf][tx + 32 * ii];
+#pragma unroll
+        for (int jj = 0; jj < CJ; ++jj) {
+            const int c = ty + WARPS * jj;
+            if (c <= i) continue;
+            const double u = s_row[buf][c] * inv;  // same address across the warp: broadcast
+#pragma unroll
+            for (int ii = 0; ii < RI; ++ii) a[ii][jj] = fma(-lc[ii], u, a[ii][jj]);
+        }
+    }
+    __syncthreads();
+    // U = unit upper: scale each row of the strict upper triangle by its pivot's reciprocal.
+#pragma unroll
+    for (int ii = 0; ii < RI; ++ii) {
+        const int r = tx + 32 * ii;
+        const double sr = r < kb ? s_inv[r] : 1.0;
+#pragma unroll
+        for (int jj = 0; jj < CJ; ++jj) {
+            const int c = ty + WARPS * jj;
+            if (r < c) a[ii][jj] *= sr;
         }
     }
 #pragma unroll
     for (int jj = 0; jj < CJ; ++jj) {
-        const int c = ty + 16 * jj;
+        const int c = ty + WARPS * jj;
 #pragma unroll
         for (int ii = 0; ii < RI; ++ii) {
             const int r = tx + 32 * ii;
@@ -135,64 +168,79 @@ lu_diag_kernel(float* __restrict__ A, int64_t lda, int kb, float* __restrict__ W
     for (int st = 0; st < kb; ++st) {
         const int buf = st & 1;
         const int k = st, q = kb - 1 - st;
-        if (tx == (k & 31)) {  // row k: X_kj (j < k), 1 at j = k; and the pivot L_kk
+        const double dinv = s_inv[k];
+        if (tx == (k & 31)) {  // row k: publish X_kj (j < k) and scale it into W_kj in place
 #pragma unroll
             for (int jj = 0; jj < CJ; ++jj) {
-                const int c = ty + 16 * jj;
+                const int c = ty + WARPS * jj;
                 const double x = pick_in_col(a, k >> 5, jj);
-                s_row[buf][c] = c < k ? x : (c == k ? 1.0 : 0.0);
-                if (c == k) s_piv[buf] = x;
+                s_row[buf][c] = c < k ? x : 0.0;
+                const bool scale = c < k;
+#pragma unroll
+                for (int ii = 0; ii < RI; ++ii) a[ii][jj] = (scale && ii == (k >> 5)) ? x * dinv : a[ii][jj];
             }
         }
-        if (ty == (k & 15)) {  // column k of L below the diagonal
+        if (ty == k % WARPS) {  // column k of L below the diagonal (zero elsewhere)
 #pragma unroll
             for (int ii = 0; ii < RI; ++ii) {
                 const int r = tx + 32 * ii;
-                s_col[buf][r] = r > k ? pick_in_row(a, ii, k >> 4) : 0.0;
+                const double v = pick_in_row(a, ii, k / WARPS);
+                s_col[buf][r] = r > k ? v : 0.0;
             }
         }
-        if (tx == (q & 31)) {  // row q: Y_qj (j > q), 1 at j = q
+        if (tx == (q & 31)) {  // row q: Y_qj (j > q)
 #pragma unroll
             for (int jj = 0; jj < CJ; ++jj) {
-                const int c = ty + 16 * jj;
-                s_vrow[buf][c] = c > q ? pick_in_col(a, q >> 5, jj) : (c == q ? 1.0 : 0.0);
+                const int c = ty + WARPS * jj;
+                const double y = pick_in_col(a, q >> 5, jj);
+                s_vrow[buf][c] = c > q ? y : 0.0;
             }
         }
-        if (ty == (q & 15)) {  // column q of U above the diagonal
+        if (ty == q % WARPS) {  // column q of U above the diagonal (zero elsewhere)
 #pragma unroll
             for (int ii = 0; ii < RI; ++ii) {
                 const int r = tx + 32 * ii;
-                s_ucol[buf][r] = r < q ? pick_in_row(a, ii, q >> 4) : 0.0;
+                const double v = pick_in_row(a, ii, q / WARPS);
+                s_ucol[buf][r] = r < q ? v : 0.0;
             }
         }
         __syncthreads();
-        const double d = s_piv[buf];
-        const double dinv = d != 0.0 ? 1.0 / d : 0.0;
+        double lc[RI], uc[RI];
+#pragma unroll
+        for (int ii = 0; ii < RI; ++ii) {
+            lc[ii] = s_col[buf][tx + 32 * ii];
+            uc[ii] = s_ucol[buf][tx + 32 * ii];
+        }
 #pragma unroll
         for (int jj = 0; jj < CJ; ++jj) {
-            const int c = ty + 16 * jj;
-            if (c <= k) {
-                const double w = s_row[buf][c] * dinv;  // W_kc
+            const int c = ty + WARPS * jj;
+            if (c < k) {  // X_rc -= L_rk W_kc for rows below k
+                const double w = s_row[buf][c] * dinv;
+#pragma unroll
+                for (int ii = 0; ii < RI; ++ii) a[ii][jj] = fma(-lc[ii], w, a[ii][jj]);
+            } else if (c == k) {  // the retiring column: W_kk and -L_rk W_kk below it
 #pragma unroll
                 for (int ii = 0; ii < RI; ++ii) {
                     const int r = tx + 32 * ii;
-                    if (r == k) a[ii][jj] = w;
-                    else if (r > k) a[ii][jj] = fma(-s_col[buf][r], w, c == k ? 0.0 : a[ii][jj]);
+                    a[ii][jj] = r == k ? dinv : (r > k ? -lc[ii] * dinv : a[ii][jj]);
                 }
             }
-            if (c >= q) {
-                const double v = s_vrow[buf][c];  // V_qc
+            if (c > q) {  // Y_rc -= U_rq V_qc for rows above q
+                const double v = s_vrow[buf][c];
+#pragma unroll
+                for (int ii = 0; ii < RI; ++ii) a[ii][jj] = fma(-uc[ii], v, a[ii][jj]);
+            } else if (c == q) {  // the retiring column: -U_rq above the diagonal
 #pragma unroll
                 for (int ii = 0; ii < RI; ++ii) {
                     const int r = tx + 32 * ii;
-                    if (r < q) a[ii][jj] = fma(-s_ucol[buf][r], v, c == q ? 0.0 : a[ii][jj]);
+                    a[ii][jj] = r < q ? -uc[ii] : a[ii][jj];
                 }
             }
         }
     }
 #pragma unroll
     for (int jj = 0; jj < CJ; ++jj) {
-        const int c = ty + 16 * jj;
+        const int c = ty + WARPS * jj;
 #pragma unroll
         for (int ii = 0; ii < RI; ++ii) {
             const int r = tx + 32 * ii;
@@ -321,36 +369,47 @@ static int lu_impl(float* A, int n, int64_t lda, int nb, void* workspace, size_t
     PMB_CHECK_ARG(ws_bytes >= pmb_lu_workspace_bytes(n, nb), "LU workspace too small");
     LuWs w = carve(workspace, n, nb);
     PMB_CUDA_TRY(cudaMemsetAsync(workspace, 0, 256, s));
+    if (!plain) PMB_CUDA_TRY(cudaMemsetAsync(w.gemm, 0, 256, s));  // the products' error word, cleared once
     for (int k0 = 0; k0 < n; k0 += nb) {
         const int kb = n - k0 < nb ? n - k0 : nb;
         const int rest = n - k0 - kb;
         float* A11 = A + static_cast<int64_t>(k0) * lda + k0;
-        lu_diag_kernel<<<1, kDiagThreads, 0, s>>>(A11, lda, kb, w.W, w.V, &w.flags[1]);
+        if (nb <= 64) lu_diag_kernel<64, 256><<<1, 256, 0, s>>>(A11, lda, kb, w.W, w.V, &w.flags[1]);
+        else lu_diag_kernel<128, 512><<<1, 512, 0, s>>>(A11, lda, kb, w.W, w.V, &w.flags[1]);
         PMB_CUDA_TRY(cudaGetLastError());
         if (rest > 0) {
             float* A12 = A + static_cast<int64_t>(k0 + kb) * lda + k0;  // kb x rest
             float* A21 = A + static_cast<int64_t>(k0) * lda + k0 + kb;  // rest x kb
             float* A22 = A + static_cast<int64_t>(k0 + kb) * lda + k0 + kb;
             int st;
-            // U12 = W * A12 (column-major) == row-major (A12^T)(W^T): M = rest, N = kb, K = kb
-            st = plain ? pmb_sgemm_plain(rest, kb, kb, 1.0f, A12, lda, w.W, kb, 0.0f, w.panel, kb, s)
-                       : pmb_sgemm_bf16x3(rest, kb, kb, 1.0f, A12, lda, w.W, kb, 0.0f, w.panel, kb, w.gemm,
-                                          w.gemm_bytes, s);
-            if (st != PMB_SUCCESS) return st;
-            copy_block_kernel<<<296, 256, 0, s>>>(w.panel, kb, A12, lda, kb, rest);
-            PMB_CUDA_TRY(cudaGetLastError());
-            // L21 = A21 * V (column-major) == row-major (V^T)(A21^T): M = kb, N = rest, K = kb
-            st = plain ? pmb_sgemm_plain(kb, rest, kb, 1.0f, w.V, kb, A21, lda, 0.0f, w.panel, rest, s)
-                       : pmb_sgemm_bf16x3(kb, rest, kb, 1.0f, w.V, kb, A21, lda, 0.0f, w.panel, rest, w.gemm,
-                                          w.gemm_bytes, s);
-            if (st != PMB_SUCCESS) return st;
-            copy_block_kernel<<<296, 256, 0, s>>>(w.panel, rest, A21, lda, rest, kb);
-            PMB_CUDA_TRY(cudaGetLastError());
-            // A22 -= L21 * U12 (column-major) == row-major (U12^T)(L21^T): M = rest, N = rest, K = kb
-            st = plain ? pmb_sgemm_plain(rest, rest, kb, -1.0f, A12, lda, A21, lda, 1.0f, A22, lda, s)
-                       : pmb_sgemm_bf16x3(rest, rest, kb, -1.0f, A12, lda, A21, lda, 1.0f, A22, lda, w.gemm,
-                                          w.gemm_bytes, s);
-            if (st != PMB_SUCCESS) return st;
+            if (plain) {
+                // The SIMT kernel reads its operands in place: solve into the panel buffer, copy back.
+                st = pmb_sgemm_plain(rest, kb, kb, 1.0f, A12, lda, w.W, kb, 0.0f, w.panel, kb, s);
+                if (st != PMB_SUCCESS) return st;
+                copy_block_kernel<<<296, 256, 0, s>>>(w.panel, kb, A12, lda, kb, rest);
+                PMB_CUDA_TRY(cudaGetLastError());
+                st = pmb_sgemm_plain(kb, rest, kb, 1.0f, w.V, kb, A21, lda, 0.0f, w.panel, rest, s);
+                if (st != PMB_SUCCESS) return st;
+                copy_block_kernel<<<296, 256, 0, s>>>(w.panel, rest, A21, lda, rest, kb);
+                PMB_CUDA_TRY(cudaGetLastError());
+                st = pmb_sgemm_plain(rest, rest, kb, -1.0f, A12, lda, A21, lda, 1.0f, A22, lda, s);
+                if (st != PMB_SUCCESS) return st;
+            } else {
+                // The split pass copies the operands first, so each panel solve writes
+                // over its own operand: two launches per product, no copy back.
+                // U12 = W * A12 (column-major) == row-major (A12^T)(W^T): M = rest, N = kb, K = kb
+                st = pmb::sgemm_bf16x3_launch(rest, kb, kb, 1.0f, A12, lda, w.W, kb, 0.0f, A12, lda, w.gemm,
+                                              w.gemm_bytes, s, false);
+                if (st != PMB_SUCCESS) return st;
+                // L21 = A21 * V (column-major) == row-major (V^T)(A21^T): M = kb, N = rest, K = kb
+                st = pmb::sgemm_bf16x3_launch(kb, rest, kb, 1.0f, w.V, kb, A21, lda, 0.0f, A21, lda, w.gemm,
+                                              w.gemm_bytes, s, false);
+                if (st != PMB_SUCCESS) return st;
+                // A22 -= L21 * U12 (column-major) == row-major (U12^T)(L21^T): M = rest, N = rest, K = kb
+                st = pmb::sgemm_bf16x3_launch(rest, rest, kb, -1.0f, A12, lda, A21, lda, 1.0f, A22, lda, w.gemm,
+                                              w.gemm_bytes, s, false);
+                if (st != PMB_SUCCESS) return st;
+            }
         }
         lu_pivot_check_kernel<<<(kb + 7) / 8, 256, 0, s>>>(A, lda, n, k0, kb, &w.flags[1]);
         PMB_CUDA_TRY(cudaGetLastError());

@@ -212,7 +212,7 @@ def sgemm(A, B, C=None, alpha: float = 1.0, beta: float = 0.0, plain: bool = Fal
     return C, workspace
 
 
-def lu_decompose(d_A, nb: int = 128, plain: bool = False, workspace=None, stream=None):
+def lu_decompose(d_A, nb: int = 64, plain: bool = False, workspace=None, stream=None):
     """In-place Crout LU of a square fp32 CUDA matrix stored column-major.
 
     d_A is a 2-D tensor whose memory holds the column-major matrix (i.e. the

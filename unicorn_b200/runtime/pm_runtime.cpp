@@ -12,7 +12,7 @@
 //    views, stages the missing bytes into a device-resident mirror of every
 //    address space (one 2-D copy per scattered subscription, on a dedicated
 //    copy stream), launches each subtask's GPU callback on the next of
-//    PMB_STREAMS (default 8) compute streams, round robin across tasks, and
+//    PMB_STREAMS (default 16) compute streams, round robin across tasks, and
 //    keeps results on the device.  Tasks are issued back to back: dependencies
 //    between tasks that share address spaces are CUDA events, never host
 //    waits, so independent tasks overlap on the device.  A task is admitted
@@ -79,6 +79,8 @@ static pmStatus dev_fail(int st, const char* what) {
 static double now_s() {
     return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
+
+static unsigned long long ns_since(double t0) { return static_cast<unsigned long long>((now_s() - t0) * 1e9); }
 
 static bool env_flag(const char* name) {
     const char* v = getenv(name);
@@ -164,7 +166,11 @@ size_t RangeSet::bytes() const {
 
 struct Stats {
     std::atomic<unsigned long long> h2d{0}, d2h{0}, gpu_subtasks{0}, batched{0};
+    // nanoseconds: stub thread issuing tasks, stub waiting for admission, pinned allocation
+    std::atomic<unsigned long long> stub_ns{0}, admit_ns{0}, pin_ns{0}, pin_bytes{0};
 };
+
+static unsigned long long ns_since(double t0);
 
 struct Controller {
     std::mutex mu;  // registries
@@ -237,9 +243,19 @@ static AddressSpace* space_of(pmMemHandle h) {
 // a pinned allocation.  Called with a->mu held (or before the space is shared).
 //
 // Pinned allocations are expensive (page locking, and freeing one synchronises
-// the device), so buffers of released address spaces are cached, up to
-// PMB_PINNED_CACHE_BYTES (default 8 GiB), and handed to new address spaces of
-// up to 1.5x smaller size.
+// the device), so they come in size classes -- 64 KiB, then four classes per
+// power of two, at most 25 % above the request -- and buffers of released
+// address spaces are cached per class, up to PMB_PINNED_CACHE_BYTES (default
+// 16 GiB), for the next address space of the same class.
+static size_t pin_class(size_t len) {
+    if (len <= (size_t(64) << 10)) return size_t(64) << 10;
+    size_t p = 1;
+    while (p < len) p <<= 1;
+    size_t cls = p / 2;
+    while (cls < len) cls += p / 8;
+    return cls;
+}
+
 static pmStatus ensure_host(AddressSpace* a) {
     if (a->host) return pmSuccess;
     Controller& c = ctl();
@@ -247,17 +263,22 @@ static pmStatus ensure_host(AddressSpace* a) {
     void* p = nullptr;
     size_t cap = len;
     if (c.has_gpu) {
+        cap = pin_class(len);
         {
             std::lock_guard<std::mutex> g(c.pin_mu);
-            auto it = c.pin_free.lower_bound(len);
-            if (it != c.pin_free.end() && it->first <= len + len / 2) {
+            auto it = c.pin_free.find(cap);
+            if (it != c.pin_free.end()) {
                 p = it->second;
-                cap = it->first;
                 c.pin_cached -= cap;
                 c.pin_free.erase(it);
             }
         }
-        if (!p && pmb_host_alloc(&p, len) != PMB_SUCCESS) return dev_fail(PMB_MEMORY_ERROR, "pinned host allocation");
+        if (!p) {
+            const double t0 = now_s();
+            if (pmb_host_alloc(&p, cap) != PMB_SUCCESS) return dev_fail(PMB_MEMORY_ERROR, "pinned host allocation");
+            c.stats.pin_ns += ns_since(t0);
+            c.stats.pin_bytes += cap;
+        }
     } else {
         p = malloc(len);
         if (!p) return fail(pmMemoryError, "host allocation of %zu bytes failed", a->length);
@@ -905,6 +926,7 @@ static void stub_main() {
                 // Admission: a free slot, then device memory.  While tasks are in
                 // flight their completion frees both, so wait for one and retry;
                 // with nothing in flight a task that still does not fit fails.
+                const double ta = now_s();
                 {
                     std::unique_lock<std::mutex> lk(c.qmu);
                     c.icv.wait(lk, [&] { return c.inflight.size() < c.max_inflight; });
@@ -917,8 +939,12 @@ static void stub_main() {
                     const size_t before = c.inflight.size();
                     c.icv.wait_for(lk, std::chrono::milliseconds(50), [&] { return c.inflight.size() < before; });
                 }
-                st = admit(t, &need) ? stage_and_launch_gpu(t)
-                                     : fail(pmMemoryError, "task needs %zu bytes of device memory; not available", need);
+                const bool fits = admit(t, &need);
+                c.stats.admit_ns += ns_since(ta);
+                const double tl = now_s();
+                st = fits ? stage_and_launch_gpu(t)
+                          : fail(pmMemoryError, "task needs %zu bytes of device memory; not available", need);
+                c.stats.stub_ns += ns_since(tl);
                 if (st == pmSuccess) {
                     std::lock_guard<std::mutex> lk(c.qmu);
                     c.inflight.push_back(t);
@@ -1012,7 +1038,7 @@ pmStatus pmInitialize() {
         PMR_DEV(pmb_stream_create(&c.copy_stream));
         PMR_DEV(pmb_stream_create(&c.fetch_stream));
         const char* ns = getenv("PMB_STREAMS");
-        c.streams.resize(ns && atoi(ns) > 0 ? static_cast<size_t>(atoi(ns)) : 8);
+        c.streams.resize(ns && atoi(ns) > 0 ? static_cast<size_t>(atoi(ns)) : 16);
         for (auto& s : c.streams) PMR_DEV(pmb_stream_create(&s));
         PMR_DEV(pmb_mempool_retain(c.device));
         PMR_DEV(pmb_malloc(&c.dev_device_info, sizeof(pmDeviceInfo)));
@@ -1022,7 +1048,7 @@ pmStatus pmInitialize() {
         const char* rv = getenv("PMLIB_CUDA_MEM_PER_CARD_RESERVED_FOR_EXTERNAL_USE");
         c.reserve_bytes = rv ? static_cast<size_t>(atoll(rv)) : (size_t(512) << 20);
         const char* pv = getenv("PMB_PINNED_CACHE_BYTES");
-        c.pin_limit = pv ? static_cast<size_t>(atoll(pv)) : (size_t(8) << 30);
+        c.pin_limit = pv ? static_cast<size_t>(atoll(pv)) : (size_t(16) << 30);
         const char* mv = getenv("PMB_MAX_INFLIGHT");
         c.max_inflight = mv && atoi(mv) > 0 ? static_cast<size_t>(atoi(mv)) : 64;
     }
@@ -1451,8 +1477,21 @@ extern "C" void pmb_runtime_stats(unsigned long long* h2d, unsigned long long* d
     if (batched) *batched = c.stats.batched;
 }
 
+extern "C" void pmb_runtime_timers(double* stub_s, double* admit_wait_s, double* pinned_alloc_s,
+                                   unsigned long long* pinned_alloc_bytes) {
+    pmr::Controller& c = pmr::ctl();
+    if (stub_s) *stub_s = c.stats.stub_ns * 1e-9;
+    if (admit_wait_s) *admit_wait_s = c.stats.admit_ns * 1e-9;
+    if (pinned_alloc_s) *pinned_alloc_s = c.stats.pin_ns * 1e-9;
+    if (pinned_alloc_bytes) *pinned_alloc_bytes = c.stats.pin_bytes;
+}
+
 extern "C" void pmb_runtime_reset_stats(void) {
     pmr::Controller& c = pmr::ctl();
+    c.stats.stub_ns = 0;
+    c.stats.admit_ns = 0;
+    c.stats.pin_ns = 0;
+    c.stats.pin_bytes = 0;
     c.stats.h2d = 0;
     c.stats.d2h = 0;
     c.stats.gpu_subtasks = 0;

@@ -128,5 +128,10 @@ int pmb_runtime_register_batch(void* subtask_gpu_custom, void* batch_fn);
 // invocations, batched launches; for tests and benchmarks.
 void pmb_runtime_stats(unsigned long long* h2d_bytes, unsigned long long* d2h_bytes,
                        unsigned long long* gpu_subtasks, unsigned long long* batched_launches);
+// Seconds the CUDA stub spent issuing GPU tasks (staging and launching) and
+// waiting to admit them, and the pinned host allocations it made (seconds,
+// bytes); for benchmarks.
+void pmb_runtime_timers(double* stub_s, double* admit_wait_s, double* pinned_alloc_s,
+                        unsigned long long* pinned_alloc_bytes);
 void pmb_runtime_reset_stats(void);
 }

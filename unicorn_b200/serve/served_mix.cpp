@@ -59,6 +59,8 @@ using namespace pm;
 extern "C" void pmb_runtime_stats(unsigned long long* h2d_bytes, unsigned long long* d2h_bytes,
                                   unsigned long long* gpu_subtasks, unsigned long long* batched_launches);
 extern "C" void pmb_runtime_reset_stats(void);
+extern "C" void pmb_runtime_timers(double* stub_s, double* admit_wait_s, double* pinned_alloc_s,
+                                   unsigned long long* pinned_alloc_bytes);
 extern "C" int sm_prepare_lu(const float* pool, int64_t ldp, float* out, int n, float diag, void* stream);
 extern "C" double sm_gemm_rel_error(const float* dA, int64_t lda, const float* dB, int64_t ldb, const float* dC,
                                     int64_t ldc, int n);
@@ -67,7 +69,7 @@ namespace {
 
 constexpr int kGemmPool = 8192;
 constexpr int kLuPool = 4096;
-constexpr int kLuNb = 128;
+constexpr int kLuNb = 64;
 
 enum Kind { GEMM = 0, LU = 1 };
 enum Mode { SERVED = 0, PLAIN = 1 };
@@ -92,7 +94,7 @@ struct Options {
     uint64_t seed = 5;
     int gemm_min = 256, gemm_max = 8192, lu_min = 512, lu_max = 4096;
     double gemm_frac = 0.6;
-    int warmup = 48;
+    int warmup = 256;
     int check = 16;
     bool run_served = true, run_plain = true;
     int plain_gemm = PLAIN_CUBLAS;
@@ -223,6 +225,7 @@ struct Pools {
 
 struct Run {
     std::vector<double> done;      // completion (result on the host), seconds after start
+    double fetch_busy = 0;         // seconds the client spent in pmFetchMemory
     std::vector<int> sampled;      // task indices whose outputs are kept
     std::map<int, std::vector<float>> outputs;
     double wall = 0;
@@ -304,7 +307,9 @@ bool submit(const Spec& s, int mode, uint64_t id, Live& L) {
 
 // Fetch a finished task's result to the host, keep it if sampled, release.
 bool collect(Live& L, int idx, bool keep, Run& r, double t0) {
+    const double f0 = now_s();
     if (pmFetchMemory(L.out) != pmSuccess) return false;
+    r.fetch_busy += now_s() - f0;
     if (keep) {
         void* hp = nullptr;
         pmGetRawMemPtr(L.out, &hp);
@@ -476,10 +481,11 @@ std::string stream_json(const char* name, const std::vector<Spec>& specs, const 
     snprintf(buf, sizeof(buf),
              "\"%s\": {\"tasks_per_s\": %.2f, \"completed\": %zu, \"span_s\": %.4f, \"p50_ms\": %.3f, \"p99_ms\": %.3f, "
              "\"gemm_p50_ms\": %.3f, \"gemm_p99_ms\": %.3f, \"lu_p50_ms\": %.3f, \"lu_p99_ms\": %.3f, "
-             "\"max_gemm_rel_err\": %.3e, \"max_lu_residual\": %.3e, \"error\": \"%s\", \"checks\": [",
+             "\"max_gemm_rel_err\": %.3e, \"max_lu_residual\": %.3e, \"fetch_busy_s\": %.4f, \"error\": \"%s\", "
+             "\"checks\": [",
              name, *tasks_per_s, lat.size(), last, 1e3 * pct(lat, 50), 1e3 * pct(lat, 99), 1e3 * pct(lat_g, 50),
              1e3 * pct(lat_g, 99), 1e3 * pct(lat_l, 50), 1e3 * pct(lat_l, 99), *max_gemm_err, *max_lu_res,
-             esc(r.error).c_str());
+             r.fetch_busy, esc(r.error).c_str());
     return std::string(buf) + checks + "]}";
 }
 
@@ -604,8 +610,10 @@ int main(int argc, char** argv) {
         }
         pmb_runtime_reset_stats();
         const Run r = run_stream(specs, SERVED, sampled, true);
-        unsigned long long h2d = 0, d2h = 0, subs = 0, bat = 0;
+        unsigned long long h2d = 0, d2h = 0, subs = 0, bat = 0, pin_b = 0;
+        double stub_s = 0, admit_s = 0, pin_s = 0;
         pmb_runtime_stats(&h2d, &d2h, &subs, &bat);
+        pmb_runtime_timers(&stub_s, &admit_s, &pin_s, &pin_b);
         js += ", " + stream_json("served", specs, r, dp, &served_tps, &ge, &lr);
         // Alone vs. in the mix: recompute each sampled task by itself.
         int same = 0, compared = 0;
@@ -620,10 +628,12 @@ int main(int argc, char** argv) {
                 std::memcmp(jt->second.data(), it->second.data(), 4 * it->second.size()) == 0)
                 ++same;
         }
-        char b[256];
+        char b[512];
         snprintf(b, sizeof(b), ", \"served_alone_vs_mix\": {\"compared\": %d, \"bit_identical\": %d}, "
-                               "\"served_h2d_bytes\": %llu, \"served_d2h_bytes\": %llu",
-                 compared, same, h2d, d2h);
+                               "\"served_h2d_bytes\": %llu, \"served_d2h_bytes\": %llu, \"served_runtime\": "
+                               "{\"stub_issue_s\": %.4f, \"admission_wait_s\": %.4f, \"pinned_alloc_s\": %.4f, "
+                               "\"pinned_alloc_bytes\": %llu}",
+                 compared, same, h2d, d2h, stub_s, admit_s, pin_s, pin_b);
         js += b;
     }
     if (o.run_plain) {
