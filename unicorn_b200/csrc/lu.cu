@@ -253,6 +253,171 @@ lu_diag_kernel(float* __restrict__ A, int64_t lda, int kb, float* __restrict__ W
     }
 }
 
+// The 64 x 64 diagonal block with every step unrolled: the block is always
+// factored as 64 x 64 (a smaller block is padded with the identity, whose
+// factors and inverses are the identity, and only its kb x kb corner is
+// written), so every step's owner warp, owner lane and register index are
+// compile-time constants -- no select chains to reach a register, and only
+// warp-uniform tests besides the per-lane row ranges.  Same algorithm and
+// shared-memory protocol as lu_diag_kernel: 256 threads, thread (tx, ty) owns
+// rows tx, tx + 32 of columns ty + 8*jj.
+__global__ void __launch_bounds__(256, 1)
+lu_diag64_kernel(float* __restrict__ A, int64_t lda, int kb, float* __restrict__ W, float* __restrict__ V,
+                 uint32_t* __restrict__ flags) {
+    constexpr int NB = 64, WARPS = 8, RI = 2, CJ = 8;
+    __shared__ double s_col[2][NB];
+    __shared__ double s_row[2][NB];
+    __shared__ double s_ucol[2][NB];
+    __shared__ double s_vrow[2][NB];
+    __shared__ double s_inv[NB];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    double a[RI][CJ];
+#pragma unroll
+    for (int jj = 0; jj < CJ; ++jj) {
+        const int c = ty + WARPS * jj;
+#pragma unroll
+        for (int ii = 0; ii < RI; ++ii) {
+            const int r = tx + 32 * ii;
+            a[ii][jj] = (r < kb && c < kb) ? static_cast<double>(A[static_cast<int64_t>(c) * lda + r])
+                                           : (r == c ? 1.0 : 0.0);
+        }
+    }
+
+#pragma unroll
+    for (int i = 0; i < NB; ++i) {
+        const int buf = i & 1;
+        if (ty == i % WARPS) {
+#pragma unroll
+            for (int ii = 0; ii < RI; ++ii) {
+                const int r = tx + 32 * ii;
+                const double v = a[ii][i / WARPS];
+                s_col[buf][r] = r > i ? v : 0.0;
+                if (r == i) {
+                    if (v == 0.0) atomicOr(flags, kFlagZeroPivot);
+                    s_inv[i] = v != 0.0 ? 1.0 / v : 0.0;
+                }
+            }
+        }
+        if (tx == (i & 31)) {
+#pragma unroll
+            for (int jj = 0; jj < CJ; ++jj) s_row[buf][ty + WARPS * jj] = a[i >> 5][jj];
+        }
+        __syncthreads();
+        const double inv = s_inv[i];
+        double lc[RI];
+#pragma unroll
+        for (int ii = 0; ii < RI; ++ii) lc[ii] = s_col[buf][tx + 32 * ii];
+#pragma unroll
+        for (int jj = 0; jj < CJ; ++jj) {
+            if (ty + WARPS * jj <= i) continue;
+            const double u = s_row[buf][ty + WARPS * jj] * inv;
+#pragma unroll
+            for (int ii = 0; ii < RI; ++ii) a[ii][jj] = fma(-lc[ii], u, a[ii][jj]);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int ii = 0; ii < RI; ++ii) {
+        const int r = tx + 32 * ii;
+        const double sr = s_inv[r];
+#pragma unroll
+        for (int jj = 0; jj < CJ; ++jj)
+            if (r < ty + WARPS * jj) a[ii][jj] *= sr;
+    }
+#pragma unroll
+    for (int jj = 0; jj < CJ; ++jj) {
+        const int c = ty + WARPS * jj;
+#pragma unroll
+        for (int ii = 0; ii < RI; ++ii) {
+            const int r = tx + 32 * ii;
+            if (r < kb && c < kb) A[static_cast<int64_t>(c) * lda + r] = static_cast<float>(a[ii][jj]);
+        }
+    }
+
+#pragma unroll
+    for (int st = 0; st < NB; ++st) {
+        const int buf = st & 1;
+        const int k = st, q = NB - 1 - st;
+        const double dinv = s_inv[k];
+        if (tx == (k & 31)) {
+#pragma unroll
+            for (int jj = 0; jj < CJ; ++jj) {
+                const int c = ty + WARPS * jj;
+                const double x = a[k >> 5][jj];
+                s_row[buf][c] = c < k ? x : 0.0;
+                if (c < k) a[k >> 5][jj] = x * dinv;
+            }
+        }
+        if (ty == k % WARPS) {
+#pragma unroll
+            for (int ii = 0; ii < RI; ++ii) {
+                const int r = tx + 32 * ii;
+                s_col[buf][r] = r > k ? a[ii][k / WARPS] : 0.0;
+            }
+        }
+        if (tx == (q & 31)) {
+#pragma unroll
+            for (int jj = 0; jj < CJ; ++jj) {
+                const int c = ty + WARPS * jj;
+                s_vrow[buf][c] = c > q ? a[q >> 5][jj] : 0.0;
+            }
+        }
+        if (ty == q % WARPS) {
+#pragma unroll
+            for (int ii = 0; ii < RI; ++ii) {
+                const int r = tx + 32 * ii;
+                s_ucol[buf][r] = r < q ? a[ii][q / WARPS] : 0.0;
+            }
+        }
+        __syncthreads();
+        double lc[RI], uc[RI];
+#pragma unroll
+        for (int ii = 0; ii < RI; ++ii) {
+            lc[ii] = s_col[buf][tx + 32 * ii];
+            uc[ii] = s_ucol[buf][tx + 32 * ii];
+        }
+#pragma unroll
+        for (int jj = 0; jj < CJ; ++jj) {
+            const int c = ty + WARPS * jj;
+            if (c < k) {
+                const double w = s_row[buf][c] * dinv;
+#pragma unroll
+                for (int ii = 0; ii < RI; ++ii) a[ii][jj] = fma(-lc[ii], w, a[ii][jj]);
+            } else if (c == k) {
+#pragma unroll
+                for (int ii = 0; ii < RI; ++ii) {
+                    const int r = tx + 32 * ii;
+                    a[ii][jj] = r == k ? dinv : (r > k ? -lc[ii] * dinv : a[ii][jj]);
+                }
+            }
+            if (c > q) {
+                const double v = s_vrow[buf][c];
+#pragma unroll
+                for (int ii = 0; ii < RI; ++ii) a[ii][jj] = fma(-uc[ii], v, a[ii][jj]);
+            } else if (c == q) {
+#pragma unroll
+                for (int ii = 0; ii < RI; ++ii) {
+                    const int r = tx + 32 * ii;
+                    a[ii][jj] = r < q ? -uc[ii] : a[ii][jj];
+                }
+            }
+        }
+    }
+#pragma unroll
+    for (int jj = 0; jj < CJ; ++jj) {
+        const int c = ty + WARPS * jj;
+#pragma unroll
+        for (int ii = 0; ii < RI; ++ii) {
+            const int r = tx + 32 * ii;
+            if (r < kb && c < kb) {
+                const int64_t e = static_cast<int64_t>(c) * kb + r;
+                W[e] = r >= c ? static_cast<float>(a[ii][jj]) : 0.0f;
+                V[e] = r < c ? static_cast<float>(a[ii][jj]) : (r == c ? 1.0f : 0.0f);
+            }
+        }
+    }
+}
+
 // FP64 pivot check of finished L columns k0..k0+kb-1 (rows k0+i..n-1): would
 // partial pivoting keep the diagonal?  One warp per column.
 __global__ void lu_pivot_check_kernel(const float* __restrict__ A, int64_t lda, int n, int k0, int kb,
@@ -374,7 +539,7 @@ static int lu_impl(float* A, int n, int64_t lda, int nb, void* workspace, size_t
         const int kb = n - k0 < nb ? n - k0 : nb;
         const int rest = n - k0 - kb;
         float* A11 = A + static_cast<int64_t>(k0) * lda + k0;
-        if (nb <= 64) lu_diag_kernel<64, 256><<<1, 256, 0, s>>>(A11, lda, kb, w.W, w.V, &w.flags[1]);
+        if (nb <= 64) lu_diag64_kernel<<<1, 256, 0, s>>>(A11, lda, kb, w.W, w.V, &w.flags[1]);
         else lu_diag_kernel<128, 512><<<1, 512, 0, s>>>(A11, lda, kb, w.W, w.V, &w.flags[1]);
         PMB_CUDA_TRY(cudaGetLastError());
         if (rest > 0) {
