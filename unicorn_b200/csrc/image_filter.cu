@@ -209,12 +209,17 @@ imgf_kernel(const __grid_constant__ ImgfParams<R, MAXI> p) {
 // as imgf_kernel, with the per-instruction overhead removed:
 //  - the halo is staged 16 pixels (48 bytes, three 16-byte loads) at a time
 //    and de-interleaved with byte permutes into 16-byte plane stores;
-//  - the filter pattern words live in registers for the whole CTA lifetime;
+//  - the filter pattern words stay in the parameter space (constant bank);
 //  - for CB == 3 all three channels accumulate in the same pass over the
 //    staged rows (patterns are shared by the channels);
 //  - results are packed into the RGB byte stream with byte permutes.
 constexpr int kPadF = 16;                 // left halo of the fast planes (pixels)
-constexpr int kPWF = kTW + 2 * kPadF;     // 96-byte plane rows
+constexpr int kPWF = kTW + 2 * kPadF;     // 96 staged bytes per plane row
+// Row stride of the planes: a warp's two half-warps read rows kV apart, so the
+// stride is chosen to put those rows 16 banks apart (28 words * 4 rows = 112
+// words = 16 mod 32): conflict-free window loads.
+constexpr int kRowF = 112;
+static_assert((kRowF / 4 * kV) % 32 == 16 && kRowF % 16 == 0 && kRowF >= kPWF, "plane row stride");
 
 template <int R>
 struct GeoF {
@@ -240,6 +245,22 @@ struct ImgfParamsF {
     pmb_imgf_item items[MAXI];
 };
 
+// Four 32-bit sums into four bytes (sum k -> byte k): CLAMP saturates to
+// [0, 255] with cvt.pack.sat (two sums per instruction), WRAP keeps the low
+// byte of each sum.
+template <int MODE>
+__device__ __forceinline__ uint32_t pack4(const int (&a)[4]) {
+    if (MODE == PMB_IMGF_CLAMP) {
+        uint32_t hi, d;
+        asm("cvt.pack.sat.u8.s32.b32 %0, %1, %2, %3;" : "=r"(hi) : "r"(a[3]), "r"(a[2]), "r"(0));
+        asm("cvt.pack.sat.u8.s32.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(a[1]), "r"(a[0]), "r"(hi));
+        return d;
+    }
+    const uint32_t lo = __byte_perm(static_cast<uint32_t>(a[0]), static_cast<uint32_t>(a[1]), 0x0040);
+    const uint32_t hi = __byte_perm(static_cast<uint32_t>(a[2]), static_cast<uint32_t>(a[3]), 0x0040);
+    return __byte_perm(lo, hi, 0x5410);
+}
+
 // De-interleave a 12-byte RGB quad (pixels q0..q3) into the three plane words
 // (plane c holds input byte 2-c).
 __device__ __forceinline__ void deinterleave4(uint32_t w0, uint32_t w1, uint32_t w2, uint32_t& o0, uint32_t& o1,
@@ -255,7 +276,7 @@ template <int R, int MODE, int MAXI, int CB>
 __global__ void __launch_bounds__(kThreads, 4)
 imgf_fast_kernel(const __grid_constant__ ImgfParamsF<R, MAXI> p) {
     using G = GeoF<R>;
-    __shared__ __align__(16) uint8_t planes[3][G::PH][kPWF];
+    __shared__ __align__(16) uint8_t planes[3][G::PH][kRowF];
 
     const int item = blockIdx.y;
     const int txs = p.tiles_x[item];
@@ -316,23 +337,14 @@ imgf_fast_kernel(const __grid_constant__ ImgfParamsF<R, MAXI> p) {
             *reinterpret_cast<uint4*>(&planes[c][yy][16 * xg]) = make_uint4(o[c][0], o[c][1], o[c][2], o[c][3]);
     }
 
-    // ---- filter patterns into registers --------------------------------------
-    uint32_t pat[G::KD][4][G::NW];
-#pragma unroll
-    for (int ky = 0; ky < G::KD; ++ky)
-#pragma unroll
-        for (int k = 0; k < 4; ++k)
-#pragma unroll
-            for (int w = 0; w < G::NW; ++w) pat[ky][k][w] = tap_word_used_f<R>(k, w) ? p.pat[ky][k][w] : 0u;
+    // The filter pattern words stay in the kernel's parameter space: every
+    // index below is a compile-time constant, so each dp4a reads its pattern
+    // operand from the constant bank and no registers hold the filter.
     __syncthreads();
 
     const int gx = threadIdx.x % kGX;
     const int gy = threadIdx.x / kGX;
-    uint32_t res[kV][4];
-#pragma unroll
-    for (int v = 0; v < kV; ++v)
-#pragma unroll
-        for (int k = 0; k < 4; ++k) res[v][k] = 0;
+    uint32_t pl[kV][3];  // per output row and plane: the 4 pixels' bytes of that plane
 
 #pragma unroll
     for (int cb = 0; cb < 3; cb += CB) {
@@ -362,21 +374,14 @@ imgf_fast_kernel(const __grid_constant__ ImgfParamsF<R, MAXI> p) {
                     for (int k = 0; k < 4; ++k)
 #pragma unroll
                         for (int w = 0; w < G::NW; ++w)
-                            if (tap_word_used_f<R>(k, w)) acc[c][v][k] = dp4a_us(win[c][w], pat[ky][k][w], acc[c][v][k]);
+                            if (tap_word_used_f<R>(k, w))
+                                acc[c][v][k] = dp4a_us(win[c][w], p.pat[ky][k][w], acc[c][v][k]);
             }
         }
 #pragma unroll
         for (int c = 0; c < CB; ++c)
 #pragma unroll
-            for (int v = 0; v < kV; ++v)
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    int a = acc[c][v][k];
-                    if (MODE == PMB_IMGF_CLAMP) a = min(max(a, 0), 255);
-                    // byte 0 of `a` into byte (cb + c) of res
-                    constexpr uint32_t kSel[3] = {0x3214u, 0x3240u, 0x3410u};
-                    res[v][k] = __byte_perm(res[v][k], static_cast<uint32_t>(a), kSel[cb + c]);
-                }
+            for (int v = 0; v < kV; ++v) pl[v][cb + c] = pack4<MODE>(acc[c][v]);
     }
 
     const int j0 = tile_c0 + 4 * gx;
@@ -386,18 +391,21 @@ imgf_fast_kernel(const __grid_constant__ ImgfParamsF<R, MAXI> p) {
         const int i = tile_r0 + gy * kV + v;
         if (i >= r1) break;
         uint8_t* dst = out + static_cast<int64_t>(i - out_row0) * op + 3 * (j0 - out_col0);
+        // pixel k's bytes are (plane 0, plane 1, plane 2) byte k: with P2 = plane 0 and
+        // P0 = plane 2 the permutes below lay out P2.k P1.k P0.k for k = 0..3.
+        const uint32_t P0 = pl[v][2], P1 = pl[v][1], P2 = pl[v][0];
         if (j0 + 3 < c1 && (reinterpret_cast<uintptr_t>(dst) & 3) == 0) {
             uint32_t* d = reinterpret_cast<uint32_t*>(dst);
-            d[0] = __byte_perm(res[v][0], res[v][1], 0x4210);
-            d[1] = __byte_perm(res[v][1], res[v][2], 0x5421);
-            d[2] = __byte_perm(res[v][2], res[v][3], 0x6542);
+            d[0] = __byte_perm(__byte_perm(P2, P1, 0x5140), P0, 0x2410);  // P2.0 P1.0 P0.0 P2.1
+            d[1] = __byte_perm(__byte_perm(P1, P0, 0x6251), P2, 0x2610);  // P1.1 P0.1 P2.2 P1.2
+            d[2] = __byte_perm(P0, __byte_perm(P2, P1, 0x0073), 0x3542);  // P0.2 P2.3 P1.3 P0.3
         } else {
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
                 if (j0 + k >= c1) break;
-                dst[3 * k + 0] = static_cast<uint8_t>(res[v][k]);
-                dst[3 * k + 1] = static_cast<uint8_t>(res[v][k] >> 8);
-                dst[3 * k + 2] = static_cast<uint8_t>(res[v][k] >> 16);
+                dst[3 * k + 0] = static_cast<uint8_t>(P2 >> (8 * k));
+                dst[3 * k + 1] = static_cast<uint8_t>(P1 >> (8 * k));
+                dst[3 * k + 2] = static_cast<uint8_t>(P0 >> (8 * k));
             }
         }
     }

@@ -35,6 +35,7 @@ namespace {
 
 constexpr int kSlice = 2048;      // edges per warp
 constexpr int kWarpsPerCta = 8;
+constexpr int kChunks = 4;      // 32-edge chunks whose loads are in flight together
 constexpr int kCtaThreads = 32 * kWarpsPerCta;
 
 // ---------------------------------------------------------------------------
@@ -180,28 +181,40 @@ pull_kernel(const uint32_t* __restrict__ row_ptr, const uint32_t* __restrict__ c
         const int64_t last_lane = (end - vb) < 32 ? (end - vb - 1) : 31;
         const uint64_t g_hi = __shfl_sync(0xffffffffu, t, static_cast<int>(last_lane));
         float acc = 0.0f;
-        for (uint64_t cb = g_lo; cb < g_hi; cb += 32) {
-            const uint64_t e = cb + lane;
-            float val = 0.0f;
-            if (e < g_hi) {
-                const uint32_t u = __ldg(&col[e]);
-                val = u < n_vertices ? __ldg(&contrib[u]) : 0.0f;
-            }
-            // Segment heads: first edge of every owner whose run starts in this chunk.
-            const bool starts = have && s < t && s >= cb && s < cb + 32;
-            uint32_t heads = __reduce_or_sync(0xffffffffu, starts ? (1u << (s - cb)) : 0u) | 1u;
-            const int seg = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
+        // kChunks 32-edge chunks per round: all their index loads, then all their
+        // gathers, are issued before the first segmented scan, so each warp keeps
+        // kChunks dependent load pairs in flight instead of one.
+        for (uint64_t c0 = g_lo; c0 < g_hi; c0 += 32 * kChunks) {
+            uint32_t u[kChunks];
+            float vals[kChunks];
 #pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const float y = __shfl_up_sync(0xffffffffu, val, o);
-                if (lane - o >= seg) val += y;
+            for (int j = 0; j < kChunks; ++j) {
+                const uint64_t e = c0 + 32 * j + lane;
+                u[j] = e < g_hi ? __ldg(&col[e]) : n_vertices;
             }
-            // Owner lane pulls the total of its run's last edge in this chunk.
-            const bool mine = have && s < t && s < cb + 32 && t > cb;
-            const uint64_t last_e = (t < cb + 32 ? t : cb + 32) - 1;
-            const int src_lane = mine ? static_cast<int>(last_e - cb) : lane;
-            const float tot = __shfl_sync(0xffffffffu, val, src_lane);
-            if (mine) acc += tot;
+#pragma unroll
+            for (int j = 0; j < kChunks; ++j) vals[j] = u[j] < n_vertices ? __ldg(&contrib[u[j]]) : 0.0f;
+#pragma unroll
+            for (int j = 0; j < kChunks; ++j) {
+                const uint64_t cb = c0 + 32 * j;
+                if (cb >= g_hi) break;
+                float val = vals[j];
+                // Segment heads: first edge of every owner whose run starts in this chunk.
+                const bool starts = have && s < t && s >= cb && s < cb + 32;
+                uint32_t heads = __reduce_or_sync(0xffffffffu, starts ? (1u << (s - cb)) : 0u) | 1u;
+                const int seg = 31 - __clz(heads & (0xffffffffu >> (31 - lane)));
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const float y = __shfl_up_sync(0xffffffffu, val, o);
+                    if (lane - o >= seg) val += y;
+                }
+                // Owner lane pulls the total of its run's last edge in this chunk.
+                const bool mine = have && s < t && s < cb + 32 && t > cb;
+                const uint64_t last_e = (t < cb + 32 ? t : cb + 32) - 1;
+                const int src_lane = mine ? static_cast<int>(last_e - cb) : lane;
+                const float tot = __shfl_sync(0xffffffffu, val, src_lane);
+                if (mine) acc += tot;
+            }
         }
         if (have) {
             if (v == cv) {

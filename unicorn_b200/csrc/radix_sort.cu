@@ -12,7 +12,7 @@
 // Design (onesweep): one histogram kernel reads the keys once and counts the
 // digits of every pass.  Each pass is then a single launch: a 256-thread CTA
 // takes the next 4096-key tile from a global counter, ranks its keys stably
-// with warp-level match/popc (warp-striped order), publishes its per-digit
+// with warp-level ballots/popc (warp-striped order), publishes its per-digit
 // counts, and thread d looks back over predecessor tiles' status words for
 // digit d to get the tile's global offset for that digit.  Keys are reordered
 // by digit in shared memory, then written so that each digit run is a
@@ -93,6 +93,7 @@ onesweep_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, con
     __shared__ uint32_t s_keys[kTile];
     __shared__ uint32_t s_vals[VALUES ? kTile : 1];
     __shared__ uint32_t s_whist[kWarps][RADIX];
+    __shared__ uint32_t s_dummy[kWarps][32];
     __shared__ uint32_t s_tile_start[RADIX];
     __shared__ uint32_t s_goff[RADIX];
     __shared__ uint32_t s_tmp[kWarps];
@@ -106,25 +107,41 @@ onesweep_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, con
 
     uint32_t key[kItems];
     uint32_t rank[kItems];
+    // Every tile but the last is full: its loads, ranks, scatter and stores run
+    // without per-key bounds tests (branches are what limits this kernel).
+    const bool full = static_cast<size_t>(tile + 1) * kTile <= n;
+    if (full) {
 #pragma unroll
-    for (int i = 0; i < kItems; ++i) {
-        const size_t idx = wbase + i * 32 + lane;
-        key[i] = idx < n ? in[idx] : 0u;
+        for (int i = 0; i < kItems; ++i) key[i] = in[wbase + i * 32 + lane];
+    } else {
+#pragma unroll
+        for (int i = 0; i < kItems; ++i) {
+            const size_t idx = wbase + i * 32 + lane;
+            key[i] = idx < n ? in[idx] : 0u;
+        }
     }
-    // Stable warp-level ranking in (warp, item, lane) order.
+    // Stable warp-level ranking in (warp, item, lane) order.  Lanes holding the
+    // same digit are found with BITS ballots; the lowest of them (the leader)
+    // advances the warp's running count for that digit.  Every lane performs the
+    // same load and store -- the others on a private dummy slot -- so the update
+    // has no divergent branch.
 #pragma unroll
     for (int i = 0; i < kItems; ++i) {
-        const bool valid = wbase + i * 32 + lane < n;
-        const uint32_t d = valid ? (key[i] >> shift) & MASK : static_cast<uint32_t>(RADIX);
-        const uint32_t peers = __match_any_sync(0xffffffffu, d);
-        const int leader = __ffs(peers) - 1;
-        uint32_t cnt = 0;
-        if (lane == leader && valid) cnt = s_whist[warp][d];
-        cnt = __shfl_sync(0xffffffffu, cnt, leader);
-        rank[i] = cnt + __popc(peers & pmb::lanemask_lt());
+        const bool valid = full || wbase + i * 32 + lane < n;
+        const uint32_t d = (key[i] >> shift) & MASK;
+        uint32_t peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+        for (int b = 0; b < BITS; ++b) {
+            const bool bit = (d >> b) & 1u;
+            const uint32_t m = __ballot_sync(0xffffffffu, bit);
+            peers &= bit ? m : ~m;
+        }
+        const int leader = (__ffs(peers) - 1) & 31;
+        uint32_t* slot = (valid && lane == leader) ? &s_whist[warp][d] : &s_dummy[warp][lane];
+        const uint32_t cnt = *slot;
+        *slot = cnt + __popc(peers);
         __syncwarp();
-        if (lane == leader && valid) s_whist[warp][d] = cnt + __popc(peers);
-        __syncwarp();
+        rank[i] = __shfl_sync(0xffffffffu, cnt, leader) + __popc(peers & pmb::lanemask_lt());
     }
     __syncthreads();
 
@@ -174,7 +191,7 @@ onesweep_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, con
 
 #pragma unroll
     for (int i = 0; i < kItems; ++i) {
-        if (wbase + i * 32 + lane < n) {
+        if (full || wbase + i * 32 + lane < n) {
             const uint32_t d = (key[i] >> shift) & MASK;
             const uint32_t pos = s_tile_start[d] + s_whist[warp][d] + rank[i];
             s_keys[pos] = key[i];
@@ -183,13 +200,25 @@ onesweep_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, con
     }
     __syncthreads();
     const size_t tbase = static_cast<size_t>(tile) * kTile;
-    const int tile_n = n - tbase < static_cast<size_t>(kTile) ? static_cast<int>(n - tbase) : kTile;
-    for (int p = tid; p < tile_n; p += kThreads) {
-        const uint32_t k = s_keys[p];
-        const uint32_t d = (k >> shift) & MASK;
-        const uint32_t g = s_goff[d] + (p - s_tile_start[d]);
-        out[g] = k;
-        if constexpr (VALUES) vout[g] = s_vals[p];
+    if (full) {
+#pragma unroll
+        for (int j = 0; j < kItems; ++j) {
+            const int p = tid + j * kThreads;
+            const uint32_t k = s_keys[p];
+            const uint32_t d = (k >> shift) & MASK;
+            const uint32_t g = s_goff[d] + (p - s_tile_start[d]);
+            out[g] = k;
+            if constexpr (VALUES) vout[g] = s_vals[p];
+        }
+    } else {
+        const int tile_n = static_cast<int>(n - tbase);
+        for (int p = tid; p < tile_n; p += kThreads) {
+            const uint32_t k = s_keys[p];
+            const uint32_t d = (k >> shift) & MASK;
+            const uint32_t g = s_goff[d] + (p - s_tile_start[d]);
+            out[g] = k;
+            if constexpr (VALUES) vout[g] = s_vals[p];
+        }
     }
 }
 
