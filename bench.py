@@ -15,6 +15,12 @@ no flush is needed between steps.
   roofline: the stencil kernel against the measured HBM copy bandwidth.
   cpu_baseline: the reference's own imageFilter_cpu (oracle/_ref, compiled
             from the reference sources) on the host cores, one worker per core.
+  apps    : the other kernels of the path (radix sort, prefix sum, PageRank,
+            GEMM, LU) on their configurations against their rooflines, each
+            with a CPU figure (restated reference algorithm or BLAS-level
+            restatement) on the same host.
+  served_mix: the served mixed-size GEMM/LU stream over the pm:: API against
+            the plain FP32 one-task-at-a-time form (unicorn_b200/serve).
 
 `--impl reference` times that reference CPU implementation alone (the
 reference has no runnable GPU path for this app: its texture-reference kernel
@@ -317,6 +323,105 @@ def app_measurements(torch, L, stream):
     return res
 
 
+def _oracle_lib():
+    path = os.path.join(ROOT, "oracle", "liboracle.so")
+    return ctypes.CDLL(path) if os.path.exists(path) else None
+
+
+def _cpu_entry(value, unit, cores, kind, sample, seconds):
+    return {"value": round(value, 3), "unit": unit, "cores": cores, "kind": kind, "sample": sample,
+            "seconds": round(seconds, 3)}
+
+
+def app_cpu_baselines(torch, res):
+    """CPU figures next to each app kernel, on the box's host cores: the
+    restated reference algorithms of oracle/ (bounded samples of the same
+    workloads) and, for GEMM/LU, the reference's BLAS-level algorithm on the
+    CBLAS that numpy ships (the reference calls cblas_sgemm/strsm/sscal/sger)."""
+    from unicorn_b200 import ops
+
+    orc = _oracle_lib()
+    P = ctypes.c_void_p
+    cores = os.cpu_count() or 1
+    rng = np.random.default_rng(2)
+    if orc is not None:
+        n = 1 << 24
+        keys = rng.integers(0, 2**32, n, dtype=np.uint32)
+        tmp = np.empty_like(keys)
+        t0 = time.perf_counter()
+        orc.orc_radix_sort_u32(keys.ctypes.data_as(P), tmp.ctypes.data_as(P), ctypes.c_size_t(n), 0, 32, 8)
+        dt = time.perf_counter() - t0
+        res["radix_sort_2^28"]["cpu_baseline"] = _cpu_entry(
+            32.0 * n / dt / 1e9, "GB/s", 1, "port", "serialRadixSortRound restated (oracle/oracle.c), 8-bit digits, "
+            "2^24 keys, one thread (the reference's per-subtask CPU sort)", dt)
+        vals = rng.integers(0, 2**32, 1 << 26, dtype=np.uint32)
+        outv = np.empty(vals.size, np.uint64)
+        t0 = time.perf_counter()
+        orc.orc_prefix_sum_u32_u64(vals.ctypes.data_as(P), outv.ctypes.data_as(P), ctypes.c_size_t(vals.size))
+        dt = time.perf_counter() - t0
+        res["prefix_sum_2^28"]["cpu_baseline"] = _cpu_entry(
+            12.0 * vals.size / dt / 1e9, "GB/s", 1, "port", "serialPrefixSum restated (oracle/oracle.c), 2^26 "
+            "elements, one thread", dt)
+        del keys, tmp, vals, outv
+        nv, ne = 1 << 22, 1 << 26
+        s_, d_ = ops.rmat_edges(1, 22, ne)
+        src = s_.cpu().numpy().view(np.uint32)
+        dst = d_.cpu().numpy().view(np.uint32)
+        order = np.argsort(src, kind="stable")
+        src, dst = np.ascontiguousarray(src[order]), np.ascontiguousarray(dst[order])
+        outdeg = np.bincount(src, minlength=nv).astype(np.uint32)
+        outdeg[outdeg == 0] = 1
+        r0 = np.full(nv, 1.0 / nv, np.float32)
+        rout = np.empty_like(r0)
+        t0 = time.perf_counter()
+        orc.orc_pagerank_push_f32(src.ctypes.data_as(P), dst.ctypes.data_as(P), ctypes.c_uint64(ne), nv,
+                                  outdeg.ctypes.data_as(P), 1, ctypes.c_float(0.85), r0.ctypes.data_as(P),
+                                  rout.ctypes.data_as(P))
+        dt = time.perf_counter() - t0
+        res["pagerank_rmat22_per_iter"]["cpu_baseline"] = _cpu_entry(
+            (4 * (nv + 1) + 8 * ne + 8 * nv) / dt / 1e9, "GB/s", 1, "port",
+            "pageRank_cpu push arithmetic (oracle/oracle.c, bit-identical to the reference's), one iteration of "
+            "the full R-MAT 2^22/2^26 graph, one thread", dt)
+        del s_, d_, src, dst, order
+    # GEMM: the reference CPU callback is cblas_sgemm (matrixMultiplyBlas.cpp:62-65).
+    dim = 2048
+    A = rng.random((dim, dim), dtype=np.float32) * 2 - 1
+    B = rng.random((dim, dim), dtype=np.float32) * 2 - 1
+    A @ B
+    t0 = time.perf_counter()
+    reps = 40
+    for _ in range(reps):
+        A @ B
+    dt = (time.perf_counter() - t0) / reps
+    for key in ("gemm_bf16x3_1024", "gemm_bf16x3_8192"):
+        res[key]["cpu_baseline"] = _cpu_entry(2.0 * dim ** 3 / dt / 1e12, "TFLOP/s", cores, "port",
+                                              f"cblas_sgemm via numpy's OpenBLAS, {dim}^3 fp32, all cores", dt)
+    # LU: the reference's three stages per block (luDecomposition.cpp:116-125, 216-275, 301-347)
+    # -- unblocked Crout of the diagonal block, two triangular solves, trailing sgemm -- on BLAS.
+    import scipy.linalg as sla
+
+    nl, nb = 2048, 256
+    M = rng.random((nl, nl), dtype=np.float32) * 2 - 1 + nl * np.eye(nl, dtype=np.float32)
+    a = np.asfortranarray(M)
+    t0 = time.perf_counter()
+    for k0 in range(0, nl, nb):
+        k1 = min(nl, k0 + nb)
+        d = a[k0:k1, k0:k1]
+        for i in range(k1 - k0 - 1):
+            d[i, i + 1:] /= d[i, i]
+            d[i + 1:, i + 1:] -= np.outer(d[i + 1:, i], d[i, i + 1:])
+        if k1 < nl:
+            a[k0:k1, k1:] = sla.solve_triangular(np.tril(d), a[k0:k1, k1:], lower=True, check_finite=False)
+            a[k1:, k0:k1] = sla.solve_triangular(np.triu(d, 1) + np.eye(k1 - k0, dtype=np.float32),
+                                                 a[k1:, k0:k1].T, trans="T", lower=False, unit_diagonal=True,
+                                                 check_finite=False).T
+            a[k1:, k1:] -= a[k1:, k0:k1] @ a[k0:k1, k1:]
+    dt = time.perf_counter() - t0
+    res["lu_4096"]["cpu_baseline"] = _cpu_entry(
+        (2.0 / 3.0) * nl ** 3 / dt / 1e9, "GFLOP/s", cores, "port",
+        f"blocked Crout LU n={nl}, nb={nb}: the reference's 3 stages on numpy/scipy BLAS, all cores", dt)
+
+
 SERVED_BIN = os.path.join(ROOT, "unicorn_b200", "serve", "_build", "served_mix")
 SERVED_TASKS = 2000
 
@@ -476,6 +581,8 @@ def main():
         "clocks": clk.summary(),
     }
     if apps is not None:
+        if not args.no_cpu_baseline:
+            app_cpu_baselines(torch, apps)
         line["apps"] = apps
     if rank == 0 and world == 1 and not args.no_served:
         line["served_mix"] = served_measurement()

@@ -32,6 +32,7 @@ constexpr size_t kHistBytes = 4096;       // [passes][radix] u32, passes*radix <
 constexpr uint32_t kCountMask = (1u << 30) - 1;
 constexpr uint32_t kFlagAgg = 1u << 30;
 constexpr uint32_t kFlagInc = 2u << 30;
+constexpr int kLook = 4;                  // predecessor tiles read per look-back round
 
 template <int BITS>
 __global__ void __launch_bounds__(kThreads)
@@ -83,7 +84,7 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t* s
 }
 
 template <int BITS, bool VALUES>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 3)
 onesweep_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, const uint32_t* __restrict__ vin,
                 uint32_t* __restrict__ vout, size_t n, int shift, const uint32_t* __restrict__ hist_pass,
                 uint32_t* __restrict__ tile_counter, uint32_t* __restrict__ err, uint32_t* __restrict__ status) {
@@ -164,22 +165,40 @@ onesweep_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, con
         s_tile_start[tid] = tile_start;
         uint32_t excl = 0;
         if (tile > 0) {
+            // kLook predecessors per round, loaded together; only those nearer
+            // than the nearest inclusive count must be ready.
             bool gave_up = false;
-            for (long long t = static_cast<long long>(tile) - 1; t >= 0; --t) {
-                const uint32_t* sp = &status[static_cast<size_t>(t) * RADIX + tid];
-                uint32_t s = pmb::ld_relaxed_u32(sp);
+            for (long long t0 = static_cast<long long>(tile) - 1; t0 >= 0 && !gave_up; t0 -= kLook) {
+                uint32_t s[kLook];
+#pragma unroll
+                for (int j = 0; j < kLook; ++j)
+                    s[j] = t0 - j >= 0 ? pmb::ld_relaxed_u32(&status[static_cast<size_t>(t0 - j) * RADIX + tid])
+                                       : kFlagInc;
                 uint32_t polls = 0;
-                while ((s >> 30) == 0) {
+                int first;
+                for (;;) {
+                    first = kLook;
+#pragma unroll
+                    for (int j = kLook - 1; j >= 0; --j)
+                        if ((s[j] >> 30) == 2) first = j;
+                    bool pending = false;
+#pragma unroll
+                    for (int j = 0; j < kLook; ++j) pending |= j < first && (s[j] >> 30) == 0;
+                    if (!pending) break;
                     if (++polls > pmb::kSpinLimit) {
                         gave_up = true;
                         break;
                     }
-                    __nanosleep(100);
-                    s = pmb::ld_relaxed_u32(sp);
+                    __nanosleep(64);
+#pragma unroll
+                    for (int j = 0; j < kLook; ++j)
+                        if (j < first && (s[j] >> 30) == 0)
+                            s[j] = pmb::ld_relaxed_u32(&status[static_cast<size_t>(t0 - j) * RADIX + tid]);
                 }
-                if (gave_up) break;
-                excl += s & kCountMask;
-                if ((s >> 30) == 2) break;
+#pragma unroll
+                for (int j = 0; j < kLook; ++j)
+                    if (j <= first) excl += s[j] & kCountMask;
+                if (first < kLook) break;
             }
             if (gave_up) atomicOr(err, pmb::kErrLookbackTimeout);
             pmb::st_relaxed_u32(&status[static_cast<size_t>(tile) * RADIX + tid],

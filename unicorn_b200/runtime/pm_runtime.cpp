@@ -198,6 +198,7 @@ struct Controller {
     void* fetch_stream = nullptr;
     size_t reserve_bytes = 0;
     size_t max_inflight = 64;              // GPU tasks on the device at once (admission slots)
+    std::atomic<bool> eager_writeback{false};  // copy written bytes to the host at task end
     // pinned host buffers of released address spaces, kept for reuse
     std::mutex pin_mu;
     std::multimap<size_t, char*> pin_free;
@@ -286,6 +287,24 @@ static pmStatus ensure_host(AddressSpace* a) {
     a->host = static_cast<char*>(p);
     a->host_cap = cap;
     return pmSuccess;
+}
+
+// Host copy from the pinned cache only (no new allocation): false if none of
+// the right class is free.  Used where a pinned allocation would stall the
+// stub thread.
+static bool host_from_cache(AddressSpace* a) {
+    if (a->host) return true;
+    Controller& c = ctl();
+    if (!c.has_gpu) return false;
+    const size_t cap = pin_class(a->length ? a->length : 1);
+    std::lock_guard<std::mutex> g(c.pin_mu);
+    auto it = c.pin_free.find(cap);
+    if (it == c.pin_free.end()) return false;
+    a->host = it->second;
+    a->host_cap = cap;
+    c.pin_cached -= cap;
+    c.pin_free.erase(it);
+    return true;
 }
 
 static void release_host(char* host, size_t cap) {
@@ -747,15 +766,25 @@ static pmStatus stage_and_launch_gpu(Task* t) {
             if (used_stream[k]) js = join_on(c.streams[k]);
         if (js != pmSuccess) return js;
     }
-    if (write_through) {
+    // Write-back at task end: all stale bytes with the cache disabled (the
+    // mirrors are then dropped); with eager write-back (PMB_EAGER_WRITEBACK=1)
+    // the bytes of the address spaces this task writes, on the task's own
+    // stream so the copies overlap other tasks' kernels, keeping the mirrors.
+    if (write_through || c.eager_writeback) {
         for (size_t i = 0; i < ns; ++i) {
             AddressSpace* a = t->spaces[i];
+            const bool writes = t->mem[i].memType != READ_ONLY && t->mem[i].memType != READ_ONLY_LAZY;
+            if (!write_through && !writes) continue;
             std::lock_guard<std::mutex> g(a->mu);
             std::vector<std::pair<size_t, size_t>> st;
             a->host_stale.present(0, a->length, st);
             if (!st.empty()) {
-                const pmStatus hs = ensure_host(a);
-                if (hs != pmSuccess) return hs;
+                if (write_through) {
+                    const pmStatus hs = ensure_host(a);
+                    if (hs != pmSuccess) return hs;
+                } else if (!host_from_cache(a)) {
+                    continue;  // no pinned buffer at hand: pmFetchMemory copies it back later
+                }
             }
             for (auto& r : st) {
                 PMR_DEV(pmb_memcpy_async(a->host + r.first, a->dev + r.first, r.second - r.first, PMB_D2H, join));
@@ -1049,6 +1078,7 @@ pmStatus pmInitialize() {
         c.reserve_bytes = rv ? static_cast<size_t>(atoll(rv)) : (size_t(512) << 20);
         const char* pv = getenv("PMB_PINNED_CACHE_BYTES");
         c.pin_limit = pv ? static_cast<size_t>(atoll(pv)) : (size_t(16) << 30);
+        c.eager_writeback = env_flag("PMB_EAGER_WRITEBACK");
         const char* mv = getenv("PMB_MAX_INFLIGHT");
         c.max_inflight = mv && atoi(mv) > 0 ? static_cast<size_t>(atoi(mv)) : 64;
     }
@@ -1476,6 +1506,8 @@ extern "C" void pmb_runtime_stats(unsigned long long* h2d, unsigned long long* d
     if (gpu_subtasks) *gpu_subtasks = c.stats.gpu_subtasks;
     if (batched) *batched = c.stats.batched;
 }
+
+extern "C" void pmb_runtime_set_eager_writeback(int on) { pmr::ctl().eager_writeback = on != 0; }
 
 extern "C" void pmb_runtime_timers(double* stub_s, double* admit_wait_s, double* pinned_alloc_s,
                                    unsigned long long* pinned_alloc_bytes) {

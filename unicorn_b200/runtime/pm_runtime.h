@@ -128,6 +128,11 @@ int pmb_runtime_register_batch(void* subtask_gpu_custom, void* batch_fn);
 // invocations, batched launches; for tests and benchmarks.
 void pmb_runtime_stats(unsigned long long* h2d_bytes, unsigned long long* d2h_bytes,
                        unsigned long long* gpu_subtasks, unsigned long long* batched_launches);
+// Write back the bytes a GPU task writes at the end of the task, on the task's
+// own stream (1), or leave them on the device until pmFetchMemory (0, the
+// default; PMB_EAGER_WRITEBACK=1 sets 1 at pmInitialize).  Tasks issued after
+// the call follow the new setting.
+void pmb_runtime_set_eager_writeback(int on);
 // Seconds the CUDA stub spent issuing GPU tasks (staging and launching) and
 // waiting to admit them, and the pinned host allocations it made (seconds,
 // bytes); for benchmarks.

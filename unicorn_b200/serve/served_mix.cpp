@@ -11,7 +11,11 @@
 // uniform[-1,1] from fixed seeds; task i subscribes an n x n block at a random
 // 16-byte-aligned offset) and writes its own output address space, which the
 // client fetches to the host with pmFetchMemory; a task's latency runs from
-// its arrival time to the moment its result is in host memory.
+// its arrival time to the moment its result is in host memory.  Each form uses
+// the write-back policy that serves it best (measured): the served form leaves
+// results on the device until the fetch thread's pmFetchMemory (copies overlap
+// later tasks' kernels), the plain form has the runtime copy each result back
+// on the task's own stream at task end (pmb_runtime_set_eager_writeback).
 //
 // Two forms run the same task list:
 //  * served: tasks are submitted as they arrive and run concurrently -- the
@@ -59,6 +63,7 @@ using namespace pm;
 extern "C" void pmb_runtime_stats(unsigned long long* h2d_bytes, unsigned long long* d2h_bytes,
                                   unsigned long long* gpu_subtasks, unsigned long long* batched_launches);
 extern "C" void pmb_runtime_reset_stats(void);
+extern "C" void pmb_runtime_set_eager_writeback(int on);
 extern "C" void pmb_runtime_timers(double* stub_s, double* admit_wait_s, double* pinned_alloc_s,
                                    unsigned long long* pinned_alloc_bytes);
 extern "C" int sm_prepare_lu(const float* pool, int64_t ldp, float* out, int n, float diag, void* stream);
@@ -603,6 +608,7 @@ int main(int argc, char** argv) {
 
     double served_tps = 0, plain_tps = 0, ge, lr;
     if (o.run_served) {
+        pmb_runtime_set_eager_writeback(0);
         const Run w = run_stream(warm, SERVED, {}, false);
         if (!w.error.empty()) {
             printf("{\"error\": \"served warm-up: %s\"}\n", esc(w.error).c_str());
@@ -637,6 +643,7 @@ int main(int argc, char** argv) {
         js += b;
     }
     if (o.run_plain) {
+        pmb_runtime_set_eager_writeback(1);
         const Run w = run_stream(warm, PLAIN, {}, false);
         if (!w.error.empty()) {
             printf("{\"error\": \"plain warm-up: %s\"}\n", esc(w.error).c_str());
