@@ -12,9 +12,14 @@
 // writer: no atomics, no cross-subtask reduction, and the result is
 // deterministic run to run.
 //
-// Design.  The edge array is cut into fixed 2048-edge slices, one per warp, so
-// high in-degree vertices (R-MAT concentrates edges on low ids) cannot stall a
-// warp.  A warp walks its slice 32 edges at a time: coalesced col[] loads, one
+// Design.  The work is cut into slices of equal cost, one per warp: walking the
+// vertices in order, every in-edge costs 1 and every vertex kVertexCost (its
+// row bounds, segment bookkeeping and result), and each warp takes 2048 cost
+// units (a merge-path split of row_ptr against the edge array).  So neither a
+// high in-degree vertex (R-MAT concentrates edges on low ids) nor a long run
+// of vertices without in-edges (R-MAT leaves most high ids empty; a fixed
+// edge split once gave one warp 31k of them) can stall a warp.  A warp walks
+// the edges of its slice 32 at a time: coalesced col[] loads, one
 // gather of contrib[src] per edge, a segmented warp scan keyed by the owning
 // vertex, and a shuffle that hands each segment total to the lane that owns
 // the vertex.  A vertex whose in-edges cross slice boundaries leaves a partial
@@ -33,7 +38,8 @@ extern "C" size_t pmb_radix_sort_scratch_bytes(size_t n, int bits_per_pass);
 
 namespace {
 
-constexpr int kSlice = 2048;      // edges per warp
+constexpr int kSlice = 2048;      // cost units per warp
+constexpr int kVertexCost = 16;   // cost of a vertex in units of one edge
 constexpr int kWarpsPerCta = 8;
 constexpr int kChunks = 4;      // 32-edge chunks whose loads are in flight together
 constexpr int kCtaThreads = 32 * kWarpsPerCta;
@@ -104,34 +110,39 @@ __global__ void row_ptr_kernel(const uint32_t* __restrict__ sorted_dst, uint64_t
 }
 
 // ---------------------------------------------------------------------------
-// Plan: own_lo[w] = first vertex whose row_ptr >= w*kSlice (vertices are owned
-// by the slice their first edge position falls in); cont[w] = the vertex whose
-// in-edges started before slice w but continue into it, or -1.
+// Plan.  // Cost position of vertex v's first item: C(v) = row_ptr[v] + kVertexCost * v.
+// Vertex v occupies [C(v), C(v+1)): its in-edges, then kVertexCost units for
+// its result.  Slice w covers cost [w*kSlice, (w+1)*kSlice).
+//   e_start[w] : edges before the slice (its first edge; e_start[ns] = E);
+//   own_lo[w]  : first vertex whose range starts in slice w or later -- the
+//                slice owns (writes) the vertices [own_lo[w], own_lo[w+1]);
+//   cont[w]    : the vertex that started before the slice and still has
+//                in-edges in it (its sum there is carried), else -1.
 __global__ void plan_kernel(const uint32_t* __restrict__ row_ptr, uint32_t n_vertices, uint64_t n_edges,
-                            uint32_t n_slices, int32_t* __restrict__ own_lo, int32_t* __restrict__ cont) {
+                            uint32_t n_slices, int32_t* __restrict__ own_lo, int32_t* __restrict__ cont,
+                            uint32_t* __restrict__ e_start) {
     const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
     if (w > n_slices) return;
     if (w == n_slices) {
         own_lo[w] = static_cast<int32_t>(n_vertices);
+        e_start[w] = static_cast<uint32_t>(n_edges);
         return;
     }
     const uint64_t pos = static_cast<uint64_t>(w) * kSlice;
-    uint32_t lo = 0, hi = n_vertices;  // first v with row_ptr[v] >= pos (v in [0, N])
-    if (w == 0) {
-        hi = 0;
-    } else {
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if (row_ptr[mid] < pos) lo = mid + 1; else hi = mid;
-        }
+    // va = last vertex with C(va) <= pos (C(0) = 0 <= pos)
+    uint32_t lo = 0, hi = n_vertices - 1;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1) >> 1;
+        const uint64_t cm = static_cast<uint64_t>(row_ptr[mid]) + static_cast<uint64_t>(kVertexCost) * mid;
+        if (cm <= pos) lo = mid; else hi = mid - 1;
     }
-    own_lo[w] = static_cast<int32_t>(hi);
-    int32_t c = -1;
-    if (w > 0 && hi > 0 && row_ptr[hi - 1] < pos && row_ptr[hi] > pos) c = static_cast<int32_t>(hi - 1);
-    // hi == N: the vertex N-1 may still continue into this slice.
-    if (w > 0 && hi == n_vertices && n_vertices > 0 && row_ptr[n_vertices - 1] < pos && n_edges > pos)
-        c = static_cast<int32_t>(n_vertices - 1);
-    cont[w] = c;
+    const uint32_t va = lo;
+    const uint64_t ca = static_cast<uint64_t>(row_ptr[va]) + static_cast<uint64_t>(kVertexCost) * va;
+    const uint64_t indeg = row_ptr[va + 1] - row_ptr[va];
+    const uint64_t into = pos - ca;  // cost units of va before the slice
+    e_start[w] = static_cast<uint32_t>(row_ptr[va] + (into < indeg ? into : indeg));
+    own_lo[w] = static_cast<int32_t>(into == 0 ? va : va + 1);
+    cont[w] = (into > 0 && into < indeg) ? static_cast<int32_t>(va) : -1;
 }
 
 __global__ void init_contrib_kernel(const float* __restrict__ rank, const uint32_t* __restrict__ outdeg, float damping,
@@ -155,13 +166,13 @@ __device__ __forceinline__ float finish(float r, uint32_t v, const uint32_t* __r
 __global__ void __launch_bounds__(kCtaThreads)
 pull_kernel(const uint32_t* __restrict__ row_ptr, const uint32_t* __restrict__ col,
             const uint32_t* __restrict__ outdeg, const float* __restrict__ contrib, const int32_t* __restrict__ own_lo,
-            const int32_t* __restrict__ cont, uint32_t n_slices, uint64_t n_edges, uint32_t n_vertices,
-            float damping, int last, float* __restrict__ out, float* __restrict__ carry) {
+            const int32_t* __restrict__ cont, const uint32_t* __restrict__ e_start, uint32_t n_slices,
+            uint32_t n_vertices, float damping, int last, float* __restrict__ out, float* __restrict__ carry) {
     const uint32_t w = blockIdx.x * kWarpsPerCta + (threadIdx.x >> 5);
     if (w >= n_slices) return;
     const int lane = threadIdx.x & 31;
-    const uint64_t e_lo = static_cast<uint64_t>(w) * kSlice;
-    const uint64_t e_hi = e_lo + kSlice < n_edges ? e_lo + kSlice : n_edges;
+    const uint64_t e_lo = e_start[w];
+    const uint64_t e_hi = e_start[w + 1];
     const int32_t cv = cont[w];
     // Vertex list: [cv (if any), own_lo[w], ..., own_lo[w+1]-1]
     const int64_t first = cv >= 0 ? cv : own_lo[w];
@@ -240,7 +251,10 @@ __global__ void fixup_kernel(const int32_t* __restrict__ cont, uint32_t n_slices
     out[v] = finish(r, static_cast<uint32_t>(v), outdeg, damping, last != 0);
 }
 
-uint32_t slices_for(uint64_t n_edges) { return static_cast<uint32_t>((n_edges + kSlice - 1) / kSlice); }
+uint32_t slices_for(uint32_t n_vertices, uint64_t n_edges) {
+    const uint64_t cost = n_edges + static_cast<uint64_t>(kVertexCost) * n_vertices;
+    return static_cast<uint32_t>((cost + kSlice - 1) / kSlice);
+}
 
 unsigned grid_for(uint64_t n, int threads, unsigned cap) {
     const uint64_t g = (n + threads - 1) / threads;
@@ -305,25 +319,26 @@ extern "C" int pmb_csr_by_destination(const uint32_t* d_src, const uint32_t* d_d
 }
 
 extern "C" size_t pmb_pagerank_plan_bytes(uint32_t n_vertices, uint64_t n_edges) {
-    (void)n_vertices;
-    return 8ull * (slices_for(n_edges) + 1);
+    return 12ull * (slices_for(n_vertices, n_edges) + 1);
 }
 
 extern "C" int pmb_pagerank_plan(const uint32_t* d_row_ptr, uint32_t n_vertices, uint64_t n_edges, void* d_plan,
                                  size_t plan_bytes, void* stream) {
     PMB_CHECK_ARG(d_row_ptr && d_plan, "null pointer");
     PMB_CHECK_ARG(plan_bytes >= pmb_pagerank_plan_bytes(n_vertices, n_edges), "plan buffer too small");
-    const uint32_t ns = slices_for(n_edges);
+    PMB_CHECK_ARG(n_vertices >= 1, "no vertices");
+    const uint32_t ns = slices_for(n_vertices, n_edges);
     int32_t* own_lo = static_cast<int32_t*>(d_plan);
     int32_t* cont = own_lo + ns + 1;
+    uint32_t* e_start = reinterpret_cast<uint32_t*>(cont + ns + 1);
     plan_kernel<<<grid_for(ns + 1ull, 256, 0x7fffffffu), 256, 0, static_cast<cudaStream_t>(stream)>>>(
-        d_row_ptr, n_vertices, n_edges, ns, own_lo, cont);
+        d_row_ptr, n_vertices, n_edges, ns, own_lo, cont, e_start);
     PMB_CUDA_TRY(cudaGetLastError());
     return PMB_SUCCESS;
 }
 
 extern "C" size_t pmb_pagerank_work_bytes(uint32_t n_vertices, uint64_t n_edges) {
-    return 8ull * n_vertices + 4ull * slices_for(n_edges) + 256;
+    return 8ull * n_vertices + 4ull * slices_for(n_vertices, n_edges) + 256;
 }
 
 extern "C" int pmb_pagerank(const uint32_t* d_row_ptr, const uint32_t* d_col, const uint32_t* d_out_degree,
@@ -339,9 +354,10 @@ extern "C" int pmb_pagerank(const uint32_t* d_row_ptr, const uint32_t* d_col, co
         PMB_CUDA_TRY(cudaMemcpyAsync(d_rank_out, d_rank_in, 4ull * n_vertices, cudaMemcpyDeviceToDevice, s));
         return PMB_SUCCESS;
     }
-    const uint32_t ns = slices_for(n_edges);
+    const uint32_t ns = slices_for(n_vertices, n_edges);
     const int32_t* own_lo = static_cast<const int32_t*>(d_plan);
     const int32_t* cont = own_lo + ns + 1;
+    const uint32_t* e_start = reinterpret_cast<const uint32_t*>(cont + ns + 1);
     float* ca = static_cast<float*>(d_work);
     float* cbuf = ca + n_vertices;
     float* carry = cbuf + n_vertices;
@@ -355,7 +371,7 @@ extern "C" int pmb_pagerank(const uint32_t* d_row_ptr, const uint32_t* d_col, co
         if (ns == 0) {
             PMB_CUDA_TRY(cudaMemsetAsync(dst, 0, 4ull * n_vertices, s));
         } else {
-            pull_kernel<<<pgrid, kCtaThreads, 0, s>>>(d_row_ptr, d_col, d_out_degree, ca, own_lo, cont, ns, n_edges,
+            pull_kernel<<<pgrid, kCtaThreads, 0, s>>>(d_row_ptr, d_col, d_out_degree, ca, own_lo, cont, e_start, ns,
                                                       n_vertices, damping, last, dst, carry);
             PMB_CUDA_TRY(cudaGetLastError());
             fixup_kernel<<<grid_for(ns, 256, 0x7fffffffu), 256, 0, s>>>(cont, ns, d_out_degree, damping, last, carry,
