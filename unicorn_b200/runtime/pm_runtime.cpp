@@ -168,6 +168,9 @@ struct Stats {
     std::atomic<unsigned long long> h2d{0}, d2h{0}, gpu_subtasks{0}, batched{0};
     // nanoseconds: stub thread issuing tasks, stub waiting for admission, pinned allocation
     std::atomic<unsigned long long> stub_ns{0}, admit_ns{0}, pin_ns{0}, pin_bytes{0};
+    // admission: waiting for a slot, waiting for memory; mirrors evicted to make room
+    std::atomic<unsigned long long> slot_ns{0}, mem_ns{0}, evictions{0}, evicted_bytes{0};
+    std::atomic<unsigned long long> callback_ns{0};  // inside GPU callbacks (the apps' launches)
 };
 
 static unsigned long long ns_since(double t0);
@@ -197,6 +200,12 @@ struct Controller {
     std::atomic<uint64_t> next_stream{0};  // compute streams are handed out round robin
     void* fetch_stream = nullptr;
     size_t reserve_bytes = 0;
+    // Device memory the runtime may hold (mirrors + reserved subtask memory):
+    // free memory at initialisation minus the reserve, with 10 % headroom for
+    // pool fragmentation.  Admission is decided against this budget and the
+    // runtime's own count, not by querying the device per task.
+    int64_t dev_budget = 0;
+    std::atomic<int64_t> dev_held{0};
     size_t max_inflight = 64;              // GPU tasks on the device at once (admission slots)
     std::atomic<bool> eager_writeback{false};  // copy written bytes to the host at task end
     // pinned host buffers of released address spaces, kept for reuse
@@ -328,6 +337,7 @@ static void free_space(AddressSpace* a) {
     if (a->dev) {
         if (a->last_access) pmb_stream_wait_event(ctl().fetch_stream, a->last_access);
         pmb_free_async(a->dev, ctl().fetch_stream);
+        ctl().dev_held -= static_cast<int64_t>(a->length);
     }
     if (a->host) release_host(a->host, a->host_cap);
     if (a->last_write) pmb_event_destroy(a->last_write);
@@ -479,23 +489,12 @@ static pmStatus fetch_range(AddressSpace* a, size_t lo, size_t hi) {
 }
 
 // Free device mirrors of idle address spaces (least recently used first)
-// until `need` bytes are available beyond the reserve.  Mirrors come from the
-// device's stream-ordered pool, which keeps freed blocks for reuse; those count
-// as available, but the reserve (memory left to the app's own allocations) must
-// be physically free, so idle pool memory beyond `need` is trimmed when it eats
-// into it.
+// until `need` more bytes fit in the runtime's device budget (dev_held counts
+// the mirrors and reserved subtask memory the runtime holds).
 static bool make_room(size_t need, const std::vector<AddressSpace*>& keep) {
     Controller& c = ctl();
     for (;;) {
-        size_t avail = 0, fr = 0, tot = 0;
-        if (pmb_mem_available(c.device, &avail) != PMB_SUCCESS) return false;
-        if (avail >= need + c.reserve_bytes) {
-            if (pmb_mem_get_info(&fr, &tot) == PMB_SUCCESS && fr < c.reserve_bytes) {
-                pmb_stream_synchronize(c.copy_stream);
-                pmb_mempool_trim(c.device, need);
-            }
-            return true;
-        }
+        if (c.dev_held.load() + static_cast<int64_t>(need) <= c.dev_budget) return true;
         AddressSpace* victim = nullptr;
         {
             std::lock_guard<std::mutex> g(c.mu);
@@ -511,6 +510,9 @@ static bool make_room(size_t need, const std::vector<AddressSpace*>& keep) {
         if (victim->last_access) pmb_event_synchronize(victim->last_access);
         pmb_free_async(victim->dev, c.fetch_stream);
         pmb_stream_synchronize(c.fetch_stream);
+        c.dev_held -= static_cast<int64_t>(victim->length);
+        c.stats.evictions++;
+        c.stats.evicted_bytes += victim->length;
         victim->dev = nullptr;
         victim->dev_valid.clear();
     }
@@ -568,6 +570,7 @@ static pmStatus stage_and_launch_gpu(Task* t) {
             void* p = nullptr;  // stream-ordered: no device-wide synchronisation
             PMR_DEV(pmb_malloc_async(&p, a->length ? a->length : 1, c.copy_stream));
             a->dev = static_cast<char*>(p);
+            c.dev_held += static_cast<int64_t>(a->length);
         }
         a->lru = ++c.lru;
     }
@@ -669,6 +672,8 @@ static pmStatus stage_and_launch_gpu(Task* t) {
         PMR_DEV(pmb_stream_wait_event(stream, staged));
         if (s.reserved) {
             PMR_DEV(pmb_malloc_async(&s.dev_reserved, s.reserved, stream));
+            c.dev_held += static_cast<int64_t>(s.reserved);  // returned when the task finishes
+            t->reserved_held += s.reserved;
             info.gpuContext.reservedGlobalMem = s.dev_reserved;
         }
         auto sc = s.scratch.find(PRE_SUBTASK_TO_SUBTASK);
@@ -683,7 +688,9 @@ static pmStatus stage_and_launch_gpu(Task* t) {
         s.info = info;
         pmStatus st = pmSuccess;
         if (cb.subtask_gpu_custom) {
+            const double tcb = now_s();
             st = cb.subtask_gpu_custom(t->info, c.gpu_info, info, stream);
+            c.stats.callback_ns += ns_since(tcb);
         } else {
             const pmCudaLaunchConf lc = s.has_conf ? s.conf : pmCudaLaunchConf();
             pmTaskInfo ti = t->dev_info;
@@ -910,6 +917,8 @@ static pmStatus run_cpu_task(Task* t) {
 
 static void finish_task(Task* t, pmStatus st, const std::string& msg) {
     Controller& c = ctl();
+    c.dev_held -= static_cast<int64_t>(t->reserved_held);
+    t->reserved_held = 0;
     for (AddressSpace* a : t->spaces) {
         bool free_now = false;
         {
@@ -960,6 +969,8 @@ static void stub_main() {
                     std::unique_lock<std::mutex> lk(c.qmu);
                     c.icv.wait(lk, [&] { return c.inflight.size() < c.max_inflight; });
                 }
+                c.stats.slot_ns += ns_since(ta);
+                const double tm = now_s();
                 size_t need = 0;
                 for (;;) {
                     if (admit(t, &need)) break;
@@ -969,6 +980,7 @@ static void stub_main() {
                     c.icv.wait_for(lk, std::chrono::milliseconds(50), [&] { return c.inflight.size() < before; });
                 }
                 const bool fits = admit(t, &need);
+                c.stats.mem_ns += ns_since(tm);
                 c.stats.admit_ns += ns_since(ta);
                 const double tl = now_s();
                 st = fits ? stage_and_launch_gpu(t)
@@ -1076,6 +1088,10 @@ pmStatus pmInitialize() {
         PMR_DEV(pmb_stream_synchronize(c.copy_stream));
         const char* rv = getenv("PMLIB_CUDA_MEM_PER_CARD_RESERVED_FOR_EXTERNAL_USE");
         c.reserve_bytes = rv ? static_cast<size_t>(atoll(rv)) : (size_t(512) << 20);
+        size_t fr = 0, tot = 0;
+        PMR_DEV(pmb_mem_get_info(&fr, &tot));
+        c.dev_budget = fr > c.reserve_bytes ? static_cast<int64_t>((fr - c.reserve_bytes) / 10 * 9) : 0;
+        c.dev_held = 0;
         const char* pv = getenv("PMB_PINNED_CACHE_BYTES");
         c.pin_limit = pv ? static_cast<size_t>(atoll(pv)) : (size_t(16) << 30);
         c.eager_writeback = env_flag("PMB_EAGER_WRITEBACK");
@@ -1518,8 +1534,24 @@ extern "C" void pmb_runtime_timers(double* stub_s, double* admit_wait_s, double*
     if (pinned_alloc_bytes) *pinned_alloc_bytes = c.stats.pin_bytes;
 }
 
+extern "C" void pmb_runtime_admission(double* slot_wait_s, double* memory_wait_s, unsigned long long* evictions,
+                                      unsigned long long* evicted_bytes) {
+    pmr::Controller& c = pmr::ctl();
+    if (slot_wait_s) *slot_wait_s = c.stats.slot_ns * 1e-9;
+    if (memory_wait_s) *memory_wait_s = c.stats.mem_ns * 1e-9;
+    if (evictions) *evictions = c.stats.evictions;
+    if (evicted_bytes) *evicted_bytes = c.stats.evicted_bytes;
+}
+
+extern "C" double pmb_runtime_callback_seconds(void) { return pmr::ctl().stats.callback_ns * 1e-9; }
+
 extern "C" void pmb_runtime_reset_stats(void) {
     pmr::Controller& c = pmr::ctl();
+    c.stats.slot_ns = 0;
+    c.stats.callback_ns = 0;
+    c.stats.mem_ns = 0;
+    c.stats.evictions = 0;
+    c.stats.evicted_bytes = 0;
     c.stats.stub_ns = 0;
     c.stats.admit_ns = 0;
     c.stats.pin_ns = 0;

@@ -106,6 +106,7 @@ struct Task {
     bool on_gpu = false;
     void* done_event = nullptr;
     double t_submit = 0, t_start = 0, t_end = 0;
+    size_t reserved_held = 0;    // reserved subtask memory counted against the device budget
     double deadline = 0;         // 0: none
     std::atomic<int> state{0};   // 0 queued, 1 running, 2 done
     pmStatus status = pmSuccess;
@@ -138,5 +139,11 @@ void pmb_runtime_set_eager_writeback(int on);
 // bytes); for benchmarks.
 void pmb_runtime_timers(double* stub_s, double* admit_wait_s, double* pinned_alloc_s,
                         unsigned long long* pinned_alloc_bytes);
+// Admission: seconds waiting for a slot and for device memory, and the idle
+// mirrors evicted to make room (count, bytes).
+void pmb_runtime_admission(double* slot_wait_s, double* memory_wait_s, unsigned long long* evictions,
+                           unsigned long long* evicted_bytes);
+// Seconds spent inside subtask_gpu_custom callbacks (the apps' own launches).
+double pmb_runtime_callback_seconds(void);
 void pmb_runtime_reset_stats(void);
 }

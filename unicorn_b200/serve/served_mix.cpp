@@ -64,6 +64,9 @@ extern "C" void pmb_runtime_stats(unsigned long long* h2d_bytes, unsigned long l
                                   unsigned long long* gpu_subtasks, unsigned long long* batched_launches);
 extern "C" void pmb_runtime_reset_stats(void);
 extern "C" void pmb_runtime_set_eager_writeback(int on);
+extern "C" double pmb_runtime_callback_seconds(void);
+extern "C" void pmb_runtime_admission(double* slot_wait_s, double* memory_wait_s, unsigned long long* evictions,
+                                      unsigned long long* evicted_bytes);
 extern "C" void pmb_runtime_timers(double* stub_s, double* admit_wait_s, double* pinned_alloc_s,
                                    unsigned long long* pinned_alloc_bytes);
 extern "C" int sm_prepare_lu(const float* pool, int64_t ldp, float* out, int n, float diag, void* stream);
@@ -617,9 +620,12 @@ int main(int argc, char** argv) {
         pmb_runtime_reset_stats();
         const Run r = run_stream(specs, SERVED, sampled, true);
         unsigned long long h2d = 0, d2h = 0, subs = 0, bat = 0, pin_b = 0;
-        double stub_s = 0, admit_s = 0, pin_s = 0;
+        double stub_s = 0, admit_s = 0, pin_s = 0, slot_s = 0, mem_s = 0;
+        unsigned long long ev = 0, ev_b = 0;
         pmb_runtime_stats(&h2d, &d2h, &subs, &bat);
         pmb_runtime_timers(&stub_s, &admit_s, &pin_s, &pin_b);
+        pmb_runtime_admission(&slot_s, &mem_s, &ev, &ev_b);
+        const double cb_s = pmb_runtime_callback_seconds();
         js += ", " + stream_json("served", specs, r, dp, &served_tps, &ge, &lr);
         // Alone vs. in the mix: recompute each sampled task by itself.
         int same = 0, compared = 0;
@@ -634,12 +640,13 @@ int main(int argc, char** argv) {
                 std::memcmp(jt->second.data(), it->second.data(), 4 * it->second.size()) == 0)
                 ++same;
         }
-        char b[512];
+        char b[768];
         snprintf(b, sizeof(b), ", \"served_alone_vs_mix\": {\"compared\": %d, \"bit_identical\": %d}, "
                                "\"served_h2d_bytes\": %llu, \"served_d2h_bytes\": %llu, \"served_runtime\": "
-                               "{\"stub_issue_s\": %.4f, \"admission_wait_s\": %.4f, \"pinned_alloc_s\": %.4f, "
-                               "\"pinned_alloc_bytes\": %llu}",
-                 compared, same, h2d, d2h, stub_s, admit_s, pin_s, pin_b);
+                               "{\"stub_issue_s\": %.4f, \"admission_wait_s\": %.4f, \"slot_wait_s\": %.4f, "
+                               "\"memory_wait_s\": %.4f, \"evictions\": %llu, \"evicted_bytes\": %llu, "
+                               "\"pinned_alloc_s\": %.4f, \"pinned_alloc_bytes\": %llu, \"callback_s\": %.4f}",
+                 compared, same, h2d, d2h, stub_s, admit_s, slot_s, mem_s, ev, ev_b, pin_s, pin_b, cb_s);
         js += b;
     }
     if (o.run_plain) {
