@@ -314,10 +314,12 @@ size_t pmb_lu_workspace_bytes(int n, int nb);
  * Block size nb in [1,128].  Replaces the three task stages
  * luDecomposition_cudaLaunchFunc / horizVertComp_cudaLaunchFunc /
  * diagComp_cudaLaunchFunc (luDecompositionCUDA.cu:66-193): the nb x nb
- * diagonal blocks are factored (and inverted) in FP64, panels and trailing
- * updates run as BF16x3 tensor-core GEMMs.  Word 1 of the workspace gets flags
- * (pmb_scratch_error): 1 = partial pivoting (FP64 comparison) would have
- * exchanged rows in some column, 2 = a zero pivot. */
+ * diagonal blocks are factored in FP64, the panels are solved in FP64 from
+ * those factors (nb <= 64; larger blocks use FP64 inverses and BF16x3 GEMMs)
+ * and the trailing updates run as BF16x3 tensor-core GEMMs.  Word 1 of the
+ * workspace gets flags (pmb_scratch_error): 1 = partial pivoting (FP64
+ * comparison) would have exchanged rows in some column, 2 = a zero pivot,
+ * 4 = a kernel's bounded wait expired (the result is not valid). */
 int pmb_lu_decompose(float* d_A, int n, int64_t lda, int nb, void* d_workspace, size_t ws_bytes, void* stream);
 
 /* Same factorization with FP32 SIMT GEMMs (the plain one-task-at-a-time form). */

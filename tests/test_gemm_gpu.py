@@ -86,6 +86,38 @@ def test_submatrix_views_with_leading_dimensions(cuda):
     assert norm <= NORM_TOL and elem <= ELEM_TOL, (norm, elem)
 
 
+@pytest.mark.parametrize("M,N,K,alpha,beta", [(300, 520, 64, -1.0, 1.0), (1000, 1536, 40, 0.5, -2.0),
+                                              (256, 256, 16, 1.0, 0.0), (77, 1000, 64, -1.0, 1.0),
+                                              (2000, 4, 8, 2.0, 1.0)])
+def test_short_k_update(cuda, M, N, K, alpha, beta):
+    """K <= 64 with an aligned C takes the kernel that moves C by TMA (the LU
+    trailing update's shape); ragged M and N exercise its clipped boxes."""
+    A, B = mats(M, N, K, 11 + M)
+    C0 = np.random.default_rng(M + N).uniform(-1, 1, (M, N)).astype(np.float32)
+    norm, elem = errors(run(cuda, A, B, C0, alpha, beta), A, B, C0, alpha, beta)
+    assert norm <= NORM_TOL, norm
+
+
+def test_short_k_update_into_view_leaves_the_rest(cuda):
+    """C as an aligned view inside a larger matrix: only the view changes."""
+    from unicorn_b200 import ops
+
+    M, N, K = 300, 520, 64
+    A, B = mats(M, N, K, 21)
+    big = np.random.default_rng(5).uniform(-1, 1, (600, 800)).astype(np.float32)
+    dbig = cuda.from_numpy(big.copy()).cuda()
+    view = dbig[8:8 + M, 16:16 + N]
+    _, ws = ops.sgemm(cuda.from_numpy(A).cuda(), cuda.from_numpy(B).cuda(), view, -1.0, 1.0)
+    cuda.cuda.synchronize()
+    assert ops.scratch_error(ws) == 0
+    got = dbig.cpu().numpy()
+    norm, _ = errors(got[8:8 + M, 16:16 + N], A, B, big[8:8 + M, 16:16 + N], -1.0, 1.0)
+    assert norm <= NORM_TOL, norm
+    mask = np.ones_like(big, dtype=bool)
+    mask[8:8 + M, 16:16 + N] = False
+    assert np.array_equal(got[mask], big[mask])
+
+
 @pytest.mark.parametrize("M,N,K", [(64, 64, 64), (100, 300, 77), (512, 512, 512)])
 def test_plain_sgemm(cuda, M, N, K):
     A, B = mats(M, N, K, 2)

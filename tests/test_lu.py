@@ -44,7 +44,7 @@ def test_oracle_reconstructs(oracle, n):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("n,nb", [(1, 128), (5, 4), (64, 32), (100, 64), (128, 128), (129, 128), (300, 64),
-                                  (512, 128), (1000, 96)])
+                                  (512, 128), (1000, 96), (1001, 64), (515, 48), (257, 64)])
 def test_gpu_lu_matches_oracle(cuda, oracle, n, nb):
     from unicorn_b200 import ops
 
@@ -60,14 +60,15 @@ def test_gpu_lu_matches_oracle(cuda, oracle, n, nb):
 
 
 @pytest.mark.gpu
-def test_gpu_lu_plain_form(cuda, oracle):
+@pytest.mark.parametrize("nb", [128, 64])
+def test_gpu_lu_plain_form(cuda, oracle, nb):
     from unicorn_b200 import ops
 
     n = 700
     a = dd_matrix(n, 4)
     d = cuda.from_numpy(a.copy()).cuda()
     d0 = cuda.from_numpy(a.copy()).cuda()
-    ops.lu_decompose(d, 128, plain=True)
+    ops.lu_decompose(d, nb, plain=True)
     assert ops.lu_residual(d0, d) <= 1e-5
     assert np.allclose(d.cpu().numpy(), crout_f64(oracle, a), rtol=1e-4, atol=1e-5)
 
@@ -85,13 +86,28 @@ def test_pivot_check_flags_non_dominant_matrix(cuda):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("n", [2048, 4096])
-def test_gpu_lu_large_residual(cuda, n):
+@pytest.mark.parametrize("row", [10, 150])
+def test_pivot_check_one_large_entry(cuda, row):
+    """One L entry larger than its pivot, inside the diagonal block (row 10)
+    or below it (row 150): both halves of the check must see it."""
+    from unicorn_b200 import ops
+
+    n = 200
+    a = dd_matrix(n, 7)
+    a[5, row] = 10.0 * n  # memory is column-major: matrix element (row, 5)
+    d = cuda.from_numpy(a).cuda()
+    _, _, flags = ops.lu_decompose(d, 64)
+    assert flags & 1
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,nb", [(2048, 128), (4096, 128), (4096, 64)])
+def test_gpu_lu_large_residual(cuda, n, nb):
     from unicorn_b200 import ops
 
     a = dd_matrix(n, n)
     d = cuda.from_numpy(a.copy()).cuda()
     d0 = cuda.from_numpy(a).cuda()
-    _, _, flags = ops.lu_decompose(d, 128)
+    _, _, flags = ops.lu_decompose(d, nb)
     assert flags == 0
     assert ops.lu_residual(d0, d) <= 1e-5

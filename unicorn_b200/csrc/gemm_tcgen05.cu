@@ -32,6 +32,8 @@
 //             signals each finished accumulator segment;
 //   warps 2-5 epilogue: tcgen05.ld each segment (one row per thread), apply
 //             alpha/beta and accumulate into C, then hand the buffer back.
+// Products with K <= 64 (one K slice: the LU trailing update) take a third
+// kernel that moves C through shared memory by TMA (gemm_update_2sm_kernel).
 // Every mbarrier wait is bounded: on expiry the kernel records an error in the
 // workspace header, skips the remaining work, waits (bounded) for its own
 // in-flight tensor-core work and frees its TMEM before returning.
@@ -374,6 +376,20 @@ __device__ __forceinline__ void umma_commit_pair(uint32_t bar) {
         : "memory");
 }
 
+// Grouped tile order of the 2-SM kernels: CTA pair blockIdx.x / 2 -> 256 x 256
+// tile (pm, pn).  Consecutive pairs sweep the columns of a band of kGroupRows
+// tile rows.
+__device__ __forceinline__ void pair_tile(int M, int N, int& pm, int& pn) {
+    const int num_pm = (M + 255) / 256, num_pn = (N + 255) / 256;
+    const int pid = static_cast<int>(blockIdx.x >> 1);
+    const int per_group = kGroupRows * num_pn;
+    const int first = (pid / per_group) * kGroupRows;
+    const int rows = min(num_pm - first, kGroupRows);
+    const int in_group = pid % per_group;
+    pm = first + in_group % rows;
+    pn = in_group / rows;
+}
+
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
 gemm_bf16x3_2sm_kernel(const __grid_constant__ GemmMaps maps, int M, int N, int KT, float alpha, float beta,
                        float* __restrict__ C, int64_t ldc, uint32_t* __restrict__ err) {
@@ -396,16 +412,7 @@ gemm_bf16x3_2sm_kernel(const __grid_constant__ GemmMaps maps, int M, int N, int 
     // panels (read once from HBM, then from L2) instead of each wave reading
     // every row panel of A.
     int pm, pn;
-    {
-        const int num_pm = (M + 255) / 256, num_pn = (N + 255) / 256;
-        const int pid = static_cast<int>(blockIdx.x >> 1);
-        const int per_group = kGroupRows * num_pn;
-        const int first = (pid / per_group) * kGroupRows;
-        const int rows = min(num_pm - first, kGroupRows);
-        const int in_group = pid % per_group;
-        pm = first + in_group % rows;
-        pn = in_group / rows;
-    }
+    pair_tile(M, N, pm, pn);
     const int m0 = pm * 256 + 128 * static_cast<int>(rank);  // this CTA's rows of A and C
     const int n0 = pn * 256;                                 // the pair's columns
     const int nb0 = n0 + 128 * static_cast<int>(rank);       // this CTA's rows of B^T
@@ -563,6 +570,165 @@ gemm_bf16x3_2sm_kernel(const __grid_constant__ GemmMaps maps, int M, int N, int 
     }
 }
 
+// ---- 2-SM update kernel for short products (K <= 64) ------------------------
+// With a single 64-deep K slice per tile (the LU trailing update, K = block
+// size) the product is bound by reading and writing C, not by the MMAs.  The
+// kernel above reads C with plain loads in its epilogue, a few in flight per
+// thread, which leaves each SM far below its share of HBM bandwidth.  Here
+// each epilogue warp issues TMA loads of its 32 rows of the C tile into shared
+// memory at kernel start, so they overlap the operand loads and the MMAs,
+// updates the tile in shared memory and writes each finished 32 x 32 box back
+// with a TMA store (rows and columns outside M x N are neither read nor
+// written).  Shared memory holds one operand stage (64 KB) and the CTA's
+// 128 x 256 C tile (128 KB: 32 boxes of 32 x 32 fp32, SWIZZLE_128B, so that a
+// warp's row-per-lane float4 accesses are free of bank conflicts).
+constexpr int kBoxBytes = 32 * 32 * 4;
+constexpr int kUpdCBytes = 128 * 256 * 4;
+constexpr int kUpdSmemBytes = kStage2Bytes + kUpdCBytes + 1024 + 256;
+constexpr uint32_t kUpdTmemCols = 256;
+
+__device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, int x, int y, uint32_t src) {
+    asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
+                     reinterpret_cast<uint64_t>(map)),
+                 "r"(x), "r"(y), "r"(src)
+                 : "memory");
+}
+
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
+gemm_update_2sm_kernel(const __grid_constant__ GemmMaps maps, const __grid_constant__ CUtensorMap cmap, int M, int N,
+                       float alpha, float beta, uint32_t* __restrict__ err) {
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* ctile = smem + kStage2Bytes;  // 1024-byte aligned: kStage2Bytes is a multiple of 1024
+    uint64_t* bars = reinterpret_cast<uint64_t*>(ctile + kUpdCBytes);
+    uint64_t* full = bars;          // leader only: both CTAs' operand bytes
+    uint64_t* acc_full = bars + 1;  // both CTAs: multicast commit after the MMAs
+    uint64_t* cfull = bars + 2;     // [4] one per epilogue warp: its C rows landed
+    uint64_t* teardown = bars + 6;
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bars + 7);
+    __shared__ volatile int s_fail;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_rank();
+    int pm, pn;
+    pair_tile(M, N, pm, pn);
+    const int m0 = pm * 256 + 128 * static_cast<int>(rank);
+    const int n0 = pn * 256;
+    const int nb0 = n0 + 128 * static_cast<int>(rank);
+
+    if (threadIdx.x == 0) {
+        s_fail = 0;
+        mbar_init(smem_u32(full), 2);
+        mbar_init(smem_u32(acc_full), 1);
+        for (int q = 0; q < 4; ++q) mbar_init(smem_u32(&cfull[q]), 1);
+        mbar_init(smem_u32(teardown), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(kUpdTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    cluster_sync_all();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+
+    if (warp == 0 && lane == 0) {
+        // ---- producer (both CTAs): the one K slice ----
+        const uint32_t fbar = cluster_addr(smem_u32(full), 0);
+        mbar_arrive_expect_tx_cluster(fbar, kStage2Bytes);
+        tma_load_2d_pair(smem_u32(smem), &maps.ah, 0, m0, fbar);
+        tma_load_2d_pair(smem_u32(smem + kHalf2), &maps.al, 0, m0, fbar);
+        tma_load_2d_pair(smem_u32(smem + 2 * kHalf2), &maps.bh, 0, nb0, fbar);
+        tma_load_2d_pair(smem_u32(smem + 3 * kHalf2), &maps.bl, 0, nb0, fbar);
+    } else if (warp == 1 && lane == 0 && rank == 0) {
+        // ---- MMA issuer (leader CTA) ----
+        if (!mbar_wait(smem_u32(full), 0)) {
+            s_fail = 1;
+            atomicOr(err, kErrTimeout);
+        } else {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t st = smem_u32(smem);
+            const uint32_t a_hi = st, a_lo = st + kHalf2, b_hi = st + 2 * kHalf2, b_lo = st + 3 * kHalf2;
+#pragma unroll
+            for (int k16 = 0; k16 < BK2 / 16; ++k16) {
+                const uint32_t off = k16 * 32;
+                umma_bf16_pair(tmem, umma_desc_sw128(a_hi + off), umma_desc_sw128(b_hi + off), k16 != 0);
+                umma_bf16_pair(tmem, umma_desc_sw128(a_hi + off), umma_desc_sw128(b_lo + off), 1u);
+                umma_bf16_pair(tmem, umma_desc_sw128(a_lo + off), umma_desc_sw128(b_hi + off), 1u);
+            }
+            umma_commit_pair(smem_u32(acc_full));
+        }
+    } else if (warp >= 2) {
+        // ---- epilogue (both CTAs): rows 32q .. 32q+31 of this CTA's 128 ----
+        const int q = warp & 3;
+        uint8_t* mine = ctile + q * 8 * kBoxBytes;
+        const bool load_c = beta != 0.0f;
+        const uint32_t cbar = smem_u32(&cfull[q]);
+        if (lane == 0 && load_c) {
+            mbar_expect_tx(cbar, 8 * kBoxBytes);
+            for (int cb = 0; cb < 8; ++cb) tma_load_2d(smem_u32(mine + cb * kBoxBytes), &cmap, n0 + 32 * cb, m0 + 32 * q, cbar);
+        }
+        const bool ok = __all_sync(0xffffffffu, mbar_wait(smem_u32(acc_full), 0) && (!load_c || mbar_wait(cbar, 0)));
+        if (!ok || s_fail) {
+            s_fail = 1;
+            atomicOr(err, kErrTimeout);
+        } else {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll 1
+            for (int c = 0; c < 16; ++c) {
+                uint32_t r[16];
+                tmem_ld16(tmem + (static_cast<uint32_t>(32 * q) << 16) + 16 * c, r);
+                const int cb = c >> 1, h = c & 1;
+                uint8_t* rowp = mine + cb * kBoxBytes + lane * 128;  // this lane's row of the box
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    float4* p = reinterpret_cast<float4*>(rowp + ((((h << 2) | j) ^ (lane & 7)) << 4));
+                    float4 o = make_float4(alpha * __uint_as_float(r[4 * j]), alpha * __uint_as_float(r[4 * j + 1]),
+                                           alpha * __uint_as_float(r[4 * j + 2]), alpha * __uint_as_float(r[4 * j + 3]));
+                    if (load_c) {
+                        const float4 old = *p;
+                        o.x += beta * old.x;
+                        o.y += beta * old.y;
+                        o.z += beta * old.z;
+                        o.w += beta * old.w;
+                    }
+                    *p = o;
+                }
+                if (h == 1) {
+                    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                    __syncwarp();
+                    if (lane == 0) tma_store_2d(&cmap, n0 + 32 * cb, m0 + 32 * q, smem_u32(mine + cb * kBoxBytes));
+                }
+            }
+            if (lane == 0) {
+                asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+                asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+            }
+            __syncwarp();
+        }
+    }
+
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 1 && rank == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (s_fail && lane == 0) {
+            umma_commit_pair(smem_u32(teardown));
+            mbar_wait(smem_u32(teardown), 0);
+        }
+        __syncwarp();
+    }
+    cluster_sync_all();
+    if (warp == 1) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kUpdTmemCols) : "memory");
+    }
+}
+
 // ---- split passes -----------------------------------------------------------
 // Both splits in one launch: blocks [0, row_blocks) split the rows of A
 // (M x K) as split_rows_kernel does, the others take one 32 x 32 tile of B
@@ -694,6 +860,49 @@ int make_map(CUtensorMap* map, const void* base, int rows, int kp, int box_rows,
 size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
 int padded_k(int K) { return (K + BK - 1) / BK * BK; }
 
+// Row-major fp32 C (M x N, ldc) in 32 x 32 boxes, SWIZZLE_128B; TMA needs a
+// 16-byte aligned base and a row pitch that is a multiple of 16 bytes.
+bool c_map_ok(const float* C, int64_t ldc) { return (reinterpret_cast<uintptr_t>(C) & 15) == 0 && (ldc & 3) == 0; }
+
+int make_c_map(CUtensorMap* map, float* C, int M, int N, int64_t ldc) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return pmb::fail(PMB_GRAPHICS_CARD_ERROR, "cuTensorMapEncodeTiled unavailable");
+    const cuuint64_t dims[2] = {static_cast<cuuint64_t>(N), static_cast<cuuint64_t>(M)};
+    const cuuint64_t strides[1] = {static_cast<cuuint64_t>(ldc) * 4};
+    const cuuint32_t box[2] = {32, 32};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, C, dims, strides, box, estr,
+                          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return pmb::fail(PMB_GRAPHICS_CARD_ERROR, "cuTensorMapEncodeTiled (C) failed (%d)", (int)r);
+    return PMB_SUCCESS;
+}
+
+// The short-product kernel on split operands ah/al (M x kp) and bh/bl (N x kp),
+// kp <= 64, C satisfying c_map_ok.
+int launch_update(int M, int N, int kp, float alpha, const __nv_bfloat16* ah, const __nv_bfloat16* al,
+                  const __nv_bfloat16* bh, const __nv_bfloat16* bl, float beta, float* C, int64_t ldc, uint32_t* err,
+                  cudaStream_t s) {
+    GemmMaps maps;
+    CUtensorMap cmap;
+    int st;
+    if ((st = make_map(&maps.ah, ah, M, kp, 128, BK2)) != PMB_SUCCESS) return st;
+    if ((st = make_map(&maps.al, al, M, kp, 128, BK2)) != PMB_SUCCESS) return st;
+    if ((st = make_map(&maps.bh, bh, N, kp, 128, BK2)) != PMB_SUCCESS) return st;
+    if ((st = make_map(&maps.bl, bl, N, kp, 128, BK2)) != PMB_SUCCESS) return st;
+    if ((st = make_c_map(&cmap, C, M, N, ldc)) != PMB_SUCCESS) return st;
+    static std::once_flag attr_once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(attr_once, [] {
+        attr_err = cudaFuncSetAttribute(gemm_update_2sm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kUpdSmemBytes);
+    });
+    PMB_CUDA_TRY(attr_err);
+    const dim3 grid(2 * ((M + 255) / 256) * ((N + 255) / 256));
+    gemm_update_2sm_kernel<<<grid, kThreads, kUpdSmemBytes, s>>>(maps, cmap, M, N, alpha, beta, err);
+    PMB_CUDA_TRY(cudaGetLastError());
+    return PMB_SUCCESS;
+}
+
 }  // namespace
 
 extern "C" size_t pmb_gemm_workspace_bytes(int M, int N, int K) {
@@ -713,7 +922,27 @@ int sgemm_bf16x3_launch(int M, int N, int K, float alpha, const float* A, int64_
                         float beta, float* C, int64_t ldc, void* workspace, size_t ws_bytes, cudaStream_t s,
                         bool clear_error);
 
+// C = alpha * (Ahi + Alo)(Bhi + Blo)^T + beta * C without the split pass, for a
+// caller that already holds the split operands: ah/al M x kp and bh/bl N x kp,
+// K-major bf16 with zero padding beyond K, kp a multiple of 8 and at most 64.
+// C (row-major, ldc) must have a 16-byte aligned base and ldc a multiple of 4.
+// Errors of the kernel are OR-ed into *err.
+int gemm_presplit_launch(int M, int N, int kp, float alpha, const __nv_bfloat16* ah, const __nv_bfloat16* al,
+                         const __nv_bfloat16* bh, const __nv_bfloat16* bl, float beta, float* C, int64_t ldc,
+                         uint32_t* err, cudaStream_t s);
+
 }  // namespace pmb
+
+int pmb::gemm_presplit_launch(int M, int N, int kp, float alpha, const __nv_bfloat16* ah, const __nv_bfloat16* al,
+                              const __nv_bfloat16* bh, const __nv_bfloat16* bl, float beta, float* C, int64_t ldc,
+                              uint32_t* err, cudaStream_t s) {
+    PMB_CHECK_ARG(M >= 0 && N >= 0, "negative GEMM size");
+    if (M == 0 || N == 0) return PMB_SUCCESS;
+    PMB_CHECK_ARG(kp > 0 && kp <= BK2 && kp % 8 == 0, "split depth %d: need a multiple of 8 up to %d", kp, BK2);
+    PMB_CHECK_ARG(ah && al && bh && bl && C && err, "null pointer");
+    PMB_CHECK_ARG(ldc >= N && c_map_ok(C, ldc), "C needs a 16-byte aligned base and ldc a multiple of 4");
+    return launch_update(M, N, kp, alpha, ah, al, bh, bl, beta, C, ldc, err, s);
+}
 
 extern "C" int pmb_sgemm_bf16x3(int M, int N, int K, float alpha, const float* A, int64_t lda, const float* B,
                                 int64_t ldb, float beta, float* C, int64_t ldc, void* workspace, size_t ws_bytes,
@@ -754,13 +983,18 @@ int pmb::sgemm_bf16x3_launch(int M, int N, int K, float alpha, const float* A, i
         PMB_CUDA_TRY(cudaGetLastError());
     }
 
-    GemmMaps maps;
-    int st;
-    // Tiles of 256 rows per CTA pair for M > 128 (PMB_GEMM_KERNEL=1sm keeps the 1-SM kernel).
+    // PMB_GEMM_KERNEL=1sm keeps the 1-SM kernel for every shape.
     static const bool force_1sm = [] {
         const char* v = getenv("PMB_GEMM_KERNEL");
         return v && std::string(v) == "1sm";
     }();
+    // A single K slice: bound by C traffic, read and written by TMA.
+    if (kp <= BK2 && c_map_ok(C, ldc) && !force_1sm)
+        return launch_update(M, N, kp, alpha, ah, al, bh, bl, beta, C, ldc, err, s);
+
+    GemmMaps maps;
+    int st;
+    // Tiles of 256 rows per CTA pair for M > 128.
     if (M > BM && !force_1sm) {
         if ((st = make_map(&maps.ah, ah, M, kp, 128, BK2)) != PMB_SUCCESS) return st;
         if ((st = make_map(&maps.al, al, M, kp, 128, BK2)) != PMB_SUCCESS) return st;

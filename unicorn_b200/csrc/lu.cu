@@ -11,18 +11,30 @@
 // cublasSscal, cublasSger}), solve the row and column panels (cublasStrsm,
 // :99-151), update the trailing matrix (cublasSgemm, :153-193).
 //
-// B200 design, per nb-step:
-//  1. one CTA factors the nb x nb diagonal block in FP64, held in registers
-//     (one barrier per column) and, in the same launch, inverts both
-//     triangles in FP64 (W = L11^-1, V = U11^-1), written as fp32.  nb = 64
-//     (256 threads) is the default: the step chain is serial, so a smaller
-//     block halves its length and lets the CTA share an SM with GEMM tiles;
-//  2. U12 = W * A12 and L21 = A21 * V run as tensor-core GEMMs (BF16x3);
-//  3. A22 -= L21 * U12 runs as a tensor-core GEMM with alpha=-1, beta=1.
-// An FP64 scan of each finished L column checks that partial pivoting would
-// have chosen the diagonal (P = I, as diagonally dominant inputs guarantee);
+// B200 design, per nb-step (nb <= 64, the default 64):
+//  1. one CTA factors the diagonal block in FP64, held in registers (one
+//     barrier per column), and writes the factors as fp32 into A11 and in
+//     FP64 to the workspace;
+//  2. one launch solves both panels in FP64 from those factors -- U12 =
+//     L11^-1 A12 by forward substitution (a warp per column) and L21 =
+//     A21 U11^-1 by substitution with the unit upper U11 (a warp per row) --
+//     and writes them both as fp32 and as the BF16 hi/lo operands of step 3;
+//  3. A22 -= L21 * U12 runs on the tensor cores (BF16x3, K = 64) in the
+//     short-product GEMM kernel, which streams A22 through shared memory by
+//     TMA.  (An A22 that TMA cannot address -- unaligned base or row pitch --
+//     takes a split pass and the general GEMM kernel instead.)
+// Block sizes above 64 factor in a 512-thread CTA that also inverts both
+// triangles (W = L11^-1, V = U11^-1, FP64, written as fp32) and solve the
+// panels as BF16x3 GEMMs U12 = W * A12, L21 = A21 * V.
+// An FP64 check of each finished L column (inside steps 1 and 2, or a
+// separate scan for large blocks) tests that partial pivoting would have
+// chosen the diagonal (P = I, as diagonally dominant inputs guarantee);
 // if not, the factorization still completes unpivoted (the reference never
 // pivots) and the call reports it through the workspace flag word.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+
 #include "pmb_common.cuh"
 
 extern "C" size_t pmb_gemm_workspace_bytes(int M, int N, int K);
@@ -33,6 +45,9 @@ namespace pmb {
 int sgemm_bf16x3_launch(int M, int N, int K, float alpha, const float* A, int64_t lda, const float* B, int64_t ldb,
                         float beta, float* C, int64_t ldc, void* workspace, size_t ws_bytes, cudaStream_t s,
                         bool clear_error);
+int gemm_presplit_launch(int M, int N, int kp, float alpha, const __nv_bfloat16* ah, const __nv_bfloat16* al,
+                         const __nv_bfloat16* bh, const __nv_bfloat16* bl, float beta, float* C, int64_t ldc,
+                         uint32_t* err, cudaStream_t s);
 }
 extern "C" int pmb_sgemm_plain(int M, int N, int K, float alpha, const float* A, int64_t lda, const float* B,
                                int64_t ldb, float beta, float* C, int64_t ldc, void* stream);
@@ -253,23 +268,24 @@ lu_diag_kernel(float* __restrict__ A, int64_t lda, int kb, float* __restrict__ W
     }
 }
 
-// The 64 x 64 diagonal block with every step unrolled: the block is always
-// factored as 64 x 64 (a smaller block is padded with the identity, whose
-// factors and inverses are the identity, and only its kb x kb corner is
-// written), so every step's owner warp, owner lane and register index are
-// compile-time constants -- no select chains to reach a register, and only
-// warp-uniform tests besides the per-lane row ranges.  Same algorithm and
-// shared-memory protocol as lu_diag_kernel: 256 threads, thread (tx, ty) owns
-// rows tx, tx + 32 of columns ty + 8*jj.
+// The 64 x 64 diagonal block with every step unrolled: Crout factorization in
+// FP64, the factors written to A11 (fp32) and, in FP64, to F (64 x 64,
+// column-major: L with its diagonal, U's strict upper part) for the panel
+// solves.  The block is always factored as 64 x 64 (a smaller block is padded
+// with the identity, whose factors are the identity), so every step's owner
+// warp, owner lane and register index are compile-time constants -- no select
+// chains to reach a register.  Same algorithm and shared-memory protocol as
+// the factorization half of lu_diag_kernel: 256 threads, thread (tx, ty) owns
+// rows tx, tx + 32 of columns ty + 8*jj.  The in-block part of the pivot check
+// (L entries below a pivot inside the block) is done here; lu_panel_kernel
+// checks the rows below the block.
 __global__ void __launch_bounds__(256, 1)
-lu_diag64_kernel(float* __restrict__ A, int64_t lda, int kb, float* __restrict__ W, float* __restrict__ V,
-                 uint32_t* __restrict__ flags) {
+lu_diag64_kernel(float* __restrict__ A, int64_t lda, int kb, double* __restrict__ F, uint32_t* __restrict__ flags) {
     constexpr int NB = 64, WARPS = 8, RI = 2, CJ = 8;
     __shared__ double s_col[2][NB];
     __shared__ double s_row[2][NB];
-    __shared__ double s_ucol[2][NB];
-    __shared__ double s_vrow[2][NB];
     __shared__ double s_inv[NB];
+    __shared__ double s_piv[NB];
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
     double a[RI][CJ];
 #pragma unroll
@@ -295,6 +311,7 @@ lu_diag64_kernel(float* __restrict__ A, int64_t lda, int kb, float* __restrict__
                 if (r == i) {
                     if (v == 0.0) atomicOr(flags, kFlagZeroPivot);
                     s_inv[i] = v != 0.0 ? 1.0 / v : 0.0;
+                    s_piv[i] = v;
                 }
             }
         }
@@ -335,85 +352,110 @@ lu_diag64_kernel(float* __restrict__ A, int64_t lda, int kb, float* __restrict__
     }
 
 #pragma unroll
-    for (int st = 0; st < NB; ++st) {
-        const int buf = st & 1;
-        const int k = st, q = NB - 1 - st;
-        const double dinv = s_inv[k];
-        if (tx == (k & 31)) {
-#pragma unroll
-            for (int jj = 0; jj < CJ; ++jj) {
-                const int c = ty + WARPS * jj;
-                const double x = a[k >> 5][jj];
-                s_row[buf][c] = c < k ? x : 0.0;
-                if (c < k) a[k >> 5][jj] = x * dinv;
-            }
-        }
-        if (ty == k % WARPS) {
-#pragma unroll
-            for (int ii = 0; ii < RI; ++ii) {
-                const int r = tx + 32 * ii;
-                s_col[buf][r] = r > k ? a[ii][k / WARPS] : 0.0;
-            }
-        }
-        if (tx == (q & 31)) {
-#pragma unroll
-            for (int jj = 0; jj < CJ; ++jj) {
-                const int c = ty + WARPS * jj;
-                s_vrow[buf][c] = c > q ? a[q >> 5][jj] : 0.0;
-            }
-        }
-        if (ty == q % WARPS) {
-#pragma unroll
-            for (int ii = 0; ii < RI; ++ii) {
-                const int r = tx + 32 * ii;
-                s_ucol[buf][r] = r < q ? a[ii][q / WARPS] : 0.0;
-            }
-        }
-        __syncthreads();
-        double lc[RI], uc[RI];
-#pragma unroll
-        for (int ii = 0; ii < RI; ++ii) {
-            lc[ii] = s_col[buf][tx + 32 * ii];
-            uc[ii] = s_ucol[buf][tx + 32 * ii];
-        }
-#pragma unroll
-        for (int jj = 0; jj < CJ; ++jj) {
-            const int c = ty + WARPS * jj;
-            if (c < k) {
-                const double w = s_row[buf][c] * dinv;
-#pragma unroll
-                for (int ii = 0; ii < RI; ++ii) a[ii][jj] = fma(-lc[ii], w, a[ii][jj]);
-            } else if (c == k) {
-#pragma unroll
-                for (int ii = 0; ii < RI; ++ii) {
-                    const int r = tx + 32 * ii;
-                    a[ii][jj] = r == k ? dinv : (r > k ? -lc[ii] * dinv : a[ii][jj]);
-                }
-            }
-            if (c > q) {
-                const double v = s_vrow[buf][c];
-#pragma unroll
-                for (int ii = 0; ii < RI; ++ii) a[ii][jj] = fma(-uc[ii], v, a[ii][jj]);
-            } else if (c == q) {
-#pragma unroll
-                for (int ii = 0; ii < RI; ++ii) {
-                    const int r = tx + 32 * ii;
-                    a[ii][jj] = r < q ? -uc[ii] : a[ii][jj];
-                }
-            }
-        }
-    }
-#pragma unroll
     for (int jj = 0; jj < CJ; ++jj) {
         const int c = ty + WARPS * jj;
 #pragma unroll
         for (int ii = 0; ii < RI; ++ii) {
             const int r = tx + 32 * ii;
-            if (r < kb && c < kb) {
-                const int64_t e = static_cast<int64_t>(c) * kb + r;
-                W[e] = r >= c ? static_cast<float>(a[ii][jj]) : 0.0f;
-                V[e] = r < c ? static_cast<float>(a[ii][jj]) : (r == c ? 1.0f : 0.0f);
+            F[c * NB + r] = a[ii][jj];  // the whole padded block: identity outside kb x kb
+            // Partial pivoting would swap rows if an L entry below a pivot were larger.
+            if (r > c && c < kb && fabs(a[ii][jj]) > fabs(s_piv[c])) atomicOr(flags, kFlagPivot);
+        }
+    }
+}
+
+// hi/lo bf16 split of two values per lane into a 64-wide operand row.
+__device__ __forceinline__ void split_row(__nv_bfloat16* hi, __nv_bfloat16* lo, int64_t base, int lane, float f0,
+                                          float f1) {
+    const __nv_bfloat16 h0 = __float2bfloat16_rn(f0), h1 = __float2bfloat16_rn(f1);
+    hi[base + lane] = h0;
+    hi[base + lane + 32] = h1;
+    lo[base + lane] = __float2bfloat16_rn(f0 - __bfloat162float(h0));
+    lo[base + lane + 32] = __float2bfloat16_rn(f1 - __bfloat162float(h1));
+}
+
+// Panel solves of one block step from the FP64 factors F of the diagonal
+// block (replacing products with explicit inverses):
+//   U12 = L11^-1 A12  -- one warp per column of A12 (kb x rest): forward
+//                        substitution, lane l holding rows l and l + 32;
+//   L21 = A21 U11^-1  -- one warp per row of A21 (rest x kb): U11 unit upper,
+//                        lane l holding columns l and l + 32.
+// Blocks [0, col_blocks) take columns and need only L11; the others take rows
+// and need only U11, so each block stages one 64 x 64 factor in shared memory
+// (L column-major, U transposed: the lanes' reads of a step are consecutive).
+// Each step broadcasts the finished unknown with a shuffle.  Rows of L21 also
+// finish the pivot check: an entry larger than its column's pivot means
+// partial pivoting would have swapped rows.  T = double on the split-precision
+// path, float for the plain FP32 form.  Launched with 256 threads.
+//
+// With uh non-null the kernel also writes the trailing update's operands in
+// the GEMM's split form (hi = bf16(x), lo = bf16(x - hi) of the stored fp32 x,
+// K-major, 64 wide, zero beyond kb): uh/ul row m = U12 column m, lh/ll row r =
+// L21 row r -- what a split pass over the fp32 panels would produce.
+template <typename T>
+__global__ void __launch_bounds__(256)
+lu_panel_kernel(float* __restrict__ A, int64_t lda, int k0, int kb, int rest, int col_blocks,
+                const double* __restrict__ F, uint32_t* __restrict__ flags, __nv_bfloat16* __restrict__ uh,
+                __nv_bfloat16* __restrict__ ul, __nv_bfloat16* __restrict__ lh, __nv_bfloat16* __restrict__ ll) {
+    constexpr int NB = 64;
+    __shared__ T sF[NB * NB];
+    __shared__ T sDiag[NB];
+    const bool cols = blockIdx.x < col_blocks;
+#pragma unroll
+    for (int k = 0; k < NB * NB / 256; ++k) {  // 16 independent loads in flight per thread
+        const int e = threadIdx.x + 256 * k;
+        const int c = e / NB, r = e - c * NB;
+        const double f = F[e];
+        if (cols) sF[e] = r >= c ? static_cast<T>(f) : T(0);        // sF[c * 64 + r] = L_rc
+        else sF[r * NB + c] = r < c ? static_cast<T>(f) : T(0);     // sF[r * 64 + c] = U_rc
+        if (r == c) sDiag[r] = cols ? T(1) / static_cast<T>(f) : static_cast<T>(fabs(f));
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    constexpr int wpb = 256 / 32;
+    if (cols) {
+        for (int item = blockIdx.x * wpb + (threadIdx.x >> 5); item < rest; item += col_blocks * wpb) {
+            float* col = A + static_cast<int64_t>(k0 + kb + item) * lda + k0;  // rows k0.. of column k0+kb+item
+            T x0 = lane < kb ? static_cast<T>(col[lane]) : T(0);
+            T x1 = lane + 32 < kb ? static_cast<T>(col[lane + 32]) : T(0);
+#pragma unroll 8
+            for (int i = 0; i < NB; ++i) {
+                const T xi = __shfl_sync(0xffffffffu, i < 32 ? x0 : x1, i & 31) * sDiag[i];
+                if (lane == (i & 31)) {
+                    if (i < 32) x0 = xi; else x1 = xi;
+                }
+                if (lane > i) x0 -= sF[i * NB + lane] * xi;
+                if (lane + 32 > i) x1 -= sF[i * NB + lane + 32] * xi;
             }
+            const float f0 = static_cast<float>(x0), f1 = static_cast<float>(x1);
+            if (lane < kb) col[lane] = f0;
+            if (lane + 32 < kb) col[lane + 32] = f1;
+            if (uh) split_row(uh, ul, static_cast<int64_t>(item) * NB, lane, f0, f1);
+        }
+    } else {
+        const int row_blocks = gridDim.x - col_blocks;
+        for (int item = (blockIdx.x - col_blocks) * wpb + (threadIdx.x >> 5); item < rest; item += row_blocks * wpb) {
+            float* row = A + static_cast<int64_t>(k0) * lda + k0 + kb + item;  // columns k0.. of row k0+kb+item
+            T x0 = lane < kb ? static_cast<T>(row[static_cast<int64_t>(lane) * lda]) : T(0);
+            T x1 = lane + 32 < kb ? static_cast<T>(row[static_cast<int64_t>(lane + 32) * lda]) : T(0);
+#pragma unroll 8
+            for (int c = 0; c < NB; ++c) {
+                const T xc = __shfl_sync(0xffffffffu, c < 32 ? x0 : x1, c & 31);
+                if (lane > c) x0 -= xc * sF[c * NB + lane];
+                if (lane + 32 > c) x1 -= xc * sF[c * NB + lane + 32];
+            }
+            bool bigger = false;
+            const float f0 = static_cast<float>(x0), f1 = static_cast<float>(x1);
+            if (lane < kb) {
+                row[static_cast<int64_t>(lane) * lda] = f0;
+                bigger |= fabs(x0) > sDiag[lane];
+            }
+            if (lane + 32 < kb) {
+                row[static_cast<int64_t>(lane + 32) * lda] = f1;
+                bigger |= fabs(x1) > sDiag[lane + 32];
+            }
+            if (uh) split_row(lh, ll, static_cast<int64_t>(item) * NB, lane, f0, f1);
+            if (__any_sync(0xffffffffu, bigger) && lane == 0) atomicOr(flags, kFlagPivot);
         }
     }
 }
@@ -488,8 +530,12 @@ __global__ void lu_residual_kernel(const float* __restrict__ A0, int64_t lda0, c
 
 size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
 
+constexpr int kPanelNb = 64;  // block sizes up to this use the FP64 factor + panel-solve path
+
 struct LuWs {
     uint32_t* flags;
+    double* F;  // FP64 factors of the diagonal block (kPanelNb x kPanelNb)
+    __nv_bfloat16 *uh, *ul, *lh, *ll;  // split trailing-update operands, n x kPanelNb each
     float* W;
     float* V;
     float* panel;
@@ -502,6 +548,13 @@ LuWs carve(void* ws, int n, int nb) {
     LuWs w;
     w.flags = reinterpret_cast<uint32_t*>(p);  // word 1 = flags (pmb_scratch_error)
     p += 256;
+    w.F = reinterpret_cast<double*>(p);
+    p += align256(static_cast<size_t>(kPanelNb) * kPanelNb * 8);
+    __nv_bfloat16** split[4] = {&w.uh, &w.ul, &w.lh, &w.ll};
+    for (auto* b : split) {
+        *b = reinterpret_cast<__nv_bfloat16*>(p);
+        p += align256(static_cast<size_t>(n) * kPanelNb * 2);
+    }
     w.W = reinterpret_cast<float*>(p);
     p += align256(static_cast<size_t>(nb) * nb * 4);
     w.V = reinterpret_cast<float*>(p);
@@ -517,12 +570,18 @@ LuWs carve(void* ws, int n, int nb) {
 
 extern "C" size_t pmb_lu_workspace_bytes(int n, int nb) {
     if (n <= 0 || nb <= 0) return 256;
-    return 256 + 2 * align256(static_cast<size_t>(nb) * nb * 4) + align256(static_cast<size_t>(nb) * n * 4) +
+    return 256 + align256(static_cast<size_t>(kPanelNb) * kPanelNb * 8) +
+           4 * align256(static_cast<size_t>(n) * kPanelNb * 2) + 2 * align256(static_cast<size_t>(nb) * nb * 4) + align256(static_cast<size_t>(nb) * n * 4) +
            pmb_gemm_workspace_bytes(n, n, nb);
 }
 
-// Blocked LU; `plain` selects FP32 SIMT GEMMs for the panel solves and the
-// trailing update (the one-task-at-a-time baseline) instead of tcgen05.
+// Blocked LU.  Block sizes up to 64 take three launches a step: the FP64
+// diagonal factorization (with the in-block pivot check), the panel solves
+// (U12, L21 and the rest of the pivot check) and the trailing update
+// A22 -= L21 U12.  Larger blocks form explicit inverses W = L11^-1 and
+// V = U11^-1 and solve the panels as products.  `plain` selects FP32 solves
+// and the FP32 SIMT GEMM (the one-task-at-a-time baseline) instead of FP64
+// solves and the tcgen05 BF16x3 GEMM.
 static int lu_impl(float* A, int n, int64_t lda, int nb, void* workspace, size_t ws_bytes, cudaStream_t s,
                    bool plain) {
     PMB_CHECK_ARG(n >= 0, "negative size");
@@ -539,45 +598,71 @@ static int lu_impl(float* A, int n, int64_t lda, int nb, void* workspace, size_t
         const int kb = n - k0 < nb ? n - k0 : nb;
         const int rest = n - k0 - kb;
         float* A11 = A + static_cast<int64_t>(k0) * lda + k0;
-        if (nb <= 64) lu_diag64_kernel<<<1, 256, 0, s>>>(A11, lda, kb, w.W, w.V, &w.flags[1]);
-        else lu_diag_kernel<128, 512><<<1, 512, 0, s>>>(A11, lda, kb, w.W, w.V, &w.flags[1]);
-        PMB_CUDA_TRY(cudaGetLastError());
-        if (rest > 0) {
-            float* A12 = A + static_cast<int64_t>(k0 + kb) * lda + k0;  // kb x rest
-            float* A21 = A + static_cast<int64_t>(k0) * lda + k0 + kb;  // rest x kb
-            float* A22 = A + static_cast<int64_t>(k0 + kb) * lda + k0 + kb;
-            int st;
+        float* A12 = A + static_cast<int64_t>(k0 + kb) * lda + k0;  // kb x rest
+        float* A21 = A + static_cast<int64_t>(k0) * lda + k0 + kb;  // rest x kb
+        float* A22 = A + static_cast<int64_t>(k0 + kb) * lda + k0 + kb;
+        int st;
+        if (nb <= kPanelNb) {
+            lu_diag64_kernel<<<1, 256, 0, s>>>(A11, lda, kb, w.F, &w.flags[1]);
+            PMB_CUDA_TRY(cudaGetLastError());
+            if (rest == 0) continue;
+            const int half = std::min((rest + 7) / 8, 4 * 148);  // blocks per side, 8 warps (items) each
             if (plain) {
-                // The SIMT kernel reads its operands in place: solve into the panel buffer, copy back.
-                st = pmb_sgemm_plain(rest, kb, kb, 1.0f, A12, lda, w.W, kb, 0.0f, w.panel, kb, s);
-                if (st != PMB_SUCCESS) return st;
-                copy_block_kernel<<<296, 256, 0, s>>>(w.panel, kb, A12, lda, kb, rest);
+                lu_panel_kernel<float><<<2 * half, 256, 0, s>>>(A, lda, k0, kb, rest, half, w.F, &w.flags[1], nullptr,
+                                                                 nullptr, nullptr, nullptr);
                 PMB_CUDA_TRY(cudaGetLastError());
-                st = pmb_sgemm_plain(kb, rest, kb, 1.0f, w.V, kb, A21, lda, 0.0f, w.panel, rest, s);
-                if (st != PMB_SUCCESS) return st;
-                copy_block_kernel<<<296, 256, 0, s>>>(w.panel, rest, A21, lda, rest, kb);
-                PMB_CUDA_TRY(cudaGetLastError());
-                st = pmb_sgemm_plain(rest, rest, kb, -1.0f, A12, lda, A21, lda, 1.0f, A22, lda, s);
-                if (st != PMB_SUCCESS) return st;
             } else {
-                // The split pass copies the operands first, so each panel solve writes
-                // over its own operand: two launches per product, no copy back.
-                // U12 = W * A12 (column-major) == row-major (A12^T)(W^T): M = rest, N = kb, K = kb
-                st = pmb::sgemm_bf16x3_launch(rest, kb, kb, 1.0f, A12, lda, w.W, kb, 0.0f, A12, lda, w.gemm,
-                                              w.gemm_bytes, s, false);
-                if (st != PMB_SUCCESS) return st;
-                // L21 = A21 * V (column-major) == row-major (V^T)(A21^T): M = kb, N = rest, K = kb
-                st = pmb::sgemm_bf16x3_launch(kb, rest, kb, 1.0f, w.V, kb, A21, lda, 0.0f, A21, lda, w.gemm,
-                                              w.gemm_bytes, s, false);
-                if (st != PMB_SUCCESS) return st;
-                // A22 -= L21 * U12 (column-major) == row-major (U12^T)(L21^T): M = rest, N = rest, K = kb
-                st = pmb::sgemm_bf16x3_launch(rest, rest, kb, -1.0f, A12, lda, A21, lda, 1.0f, A22, lda, w.gemm,
-                                              w.gemm_bytes, s, false);
-                if (st != PMB_SUCCESS) return st;
+                // The update reads and writes A22 by TMA when it is 16-byte aligned with a
+                // row pitch that is a multiple of 16 bytes; the panel kernel then hands it
+                // the split operands directly.
+                const bool direct = (reinterpret_cast<uintptr_t>(A22) & 15) == 0 && (lda & 3) == 0;
+                lu_panel_kernel<double><<<2 * half, 256, 0, s>>>(A, lda, k0, kb, rest, half, w.F, &w.flags[1],
+                                                                  direct ? w.uh : nullptr, w.ul, w.lh, w.ll);
+                PMB_CUDA_TRY(cudaGetLastError());
+                if (direct) {
+                    // A22 -= L21 * U12 == row-major (U12^T)(L21^T); a timed-out wait shows as flag 4.
+                    st = pmb::gemm_presplit_launch(rest, rest, kPanelNb, -1.0f, w.uh, w.ul, w.lh, w.ll, 1.0f, A22,
+                                                   lda, &w.flags[1], s);
+                    if (st != PMB_SUCCESS) return st;
+                    continue;
+                }
             }
+        } else {
+            lu_diag_kernel<128, 512><<<1, 512, 0, s>>>(A11, lda, kb, w.W, w.V, &w.flags[1]);
+            PMB_CUDA_TRY(cudaGetLastError());
+            if (rest > 0) {
+                if (plain) {
+                    // The SIMT kernel reads its operands in place: solve into the panel buffer, copy back.
+                    st = pmb_sgemm_plain(rest, kb, kb, 1.0f, A12, lda, w.W, kb, 0.0f, w.panel, kb, s);
+                    if (st != PMB_SUCCESS) return st;
+                    copy_block_kernel<<<296, 256, 0, s>>>(w.panel, kb, A12, lda, kb, rest);
+                    PMB_CUDA_TRY(cudaGetLastError());
+                    st = pmb_sgemm_plain(kb, rest, kb, 1.0f, w.V, kb, A21, lda, 0.0f, w.panel, rest, s);
+                    if (st != PMB_SUCCESS) return st;
+                    copy_block_kernel<<<296, 256, 0, s>>>(w.panel, rest, A21, lda, rest, kb);
+                    PMB_CUDA_TRY(cudaGetLastError());
+                } else {
+                    // The split pass copies the operands first, so each panel solve writes
+                    // over its own operand: two launches per product, no copy back.
+                    // U12 = W * A12 (column-major) == row-major (A12^T)(W^T): M = rest, N = kb, K = kb
+                    st = pmb::sgemm_bf16x3_launch(rest, kb, kb, 1.0f, A12, lda, w.W, kb, 0.0f, A12, lda, w.gemm,
+                                                  w.gemm_bytes, s, false);
+                    if (st != PMB_SUCCESS) return st;
+                    // L21 = A21 * V (column-major) == row-major (V^T)(A21^T): M = kb, N = rest, K = kb
+                    st = pmb::sgemm_bf16x3_launch(kb, rest, kb, 1.0f, w.V, kb, A21, lda, 0.0f, A21, lda, w.gemm,
+                                                  w.gemm_bytes, s, false);
+                    if (st != PMB_SUCCESS) return st;
+                }
+            }
+            lu_pivot_check_kernel<<<(kb + 7) / 8, 256, 0, s>>>(A, lda, n, k0, kb, &w.flags[1]);
+            PMB_CUDA_TRY(cudaGetLastError());
+            if (rest == 0) continue;
         }
-        lu_pivot_check_kernel<<<(kb + 7) / 8, 256, 0, s>>>(A, lda, n, k0, kb, &w.flags[1]);
-        PMB_CUDA_TRY(cudaGetLastError());
+        // A22 -= L21 * U12 (column-major) == row-major (U12^T)(L21^T): M = rest, N = rest, K = kb
+        if (plain) st = pmb_sgemm_plain(rest, rest, kb, -1.0f, A12, lda, A21, lda, 1.0f, A22, lda, s);
+        else st = pmb::sgemm_bf16x3_launch(rest, rest, kb, -1.0f, A12, lda, A21, lda, 1.0f, A22, lda, w.gemm,
+                                           w.gemm_bytes, s, false);
+        if (st != PMB_SUCCESS) return st;
     }
     return PMB_SUCCESS;
 }
