@@ -88,6 +88,14 @@ int pmb_device_synchronize(void);
 /* Keep blocks freed with pmb_free_async in the device's default pool for
  * reuse (release threshold = unlimited). */
 int pmb_mempool_retain(int dev);
+/* Map device memory into the default pool now, until it holds `bytes` (less
+ * if the device cannot provide them); *reserved (may be null) gets the pool's
+ * size.  Growing the pool later, while kernels and copies are in flight,
+ * stalls them: the pm:: runtime reserves its device budget at pmInitialize,
+ * as the reference's CUDA stub reserves its chunk collections up front
+ * (source/code/src/pmExecutionStub.cpp:3616-3640 pmStubCUDA::ReserveMemory,
+ * chunks from pmDataTypes.cpp:505-509). */
+int pmb_mempool_reserve(int dev, size_t bytes, size_t* reserved);
 /* Return idle pool memory beyond keep_bytes to the device. */
 int pmb_mempool_trim(int dev, size_t keep_bytes);
 /* Free device memory plus memory the default pool holds but does not use. */

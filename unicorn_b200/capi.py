@@ -88,6 +88,7 @@ _SIGS = {
                                   ctypes.c_uint, ctypes.c_uint, ctypes.POINTER(c_void_p), c_void_p]),
     "pmb_device_synchronize": (c_int, []),
     "pmb_mempool_retain": (c_int, [c_int]),
+    "pmb_mempool_reserve": (c_int, [c_int, c_size_t, c_void_p]),
     "pmb_mempool_trim": (c_int, [c_int, c_size_t]),
     "pmb_mem_available": (c_int, [c_int, ctypes.POINTER(c_size_t)]),
     "pmb_graph_begin_capture": (c_int, [c_void_p]),

@@ -234,6 +234,38 @@ extern "C" int pmb_mempool_retain(int dev) {
     return PMB_SUCCESS;
 }
 
+extern "C" int pmb_mempool_reserve(int dev, size_t bytes, size_t* reserved) {
+    cudaMemPool_t pool;
+    PMB_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, dev));
+    uint64_t cur = 0;
+    PMB_CUDA_TRY(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &cur));
+    if (cur < bytes) {
+        cudaStream_t s;
+        PMB_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+        // One allocation maps the memory; freeing it at once leaves it in the
+        // pool (release threshold: keep everything).  Halve on failure.
+        for (size_t want = bytes - cur; want >= (size_t(64) << 20); want /= 2) {
+            void* p = nullptr;
+            const cudaError_t e = cudaMallocAsync(&p, want, s);
+            if (e == cudaSuccess) {
+                cudaFreeAsync(p, s);
+                break;
+            }
+            cudaGetLastError();
+            if (e != cudaErrorMemoryAllocation) {
+                cudaStreamDestroy(s);
+                return pmb::cuda_fail(e, "cudaMallocAsync (pool reservation)");
+            }
+        }
+        const cudaError_t e = cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+        PMB_CUDA_TRY(e);
+        PMB_CUDA_TRY(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &cur));
+    }
+    if (reserved) *reserved = static_cast<size_t>(cur);
+    return PMB_SUCCESS;
+}
+
 extern "C" int pmb_mempool_trim(int dev, size_t keep_bytes) {
     cudaMemPool_t pool;
     PMB_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, dev));

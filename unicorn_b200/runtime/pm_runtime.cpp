@@ -171,6 +171,9 @@ struct Stats {
     // admission: waiting for a slot, waiting for memory; mirrors evicted to make room
     std::atomic<unsigned long long> slot_ns{0}, mem_ns{0}, evictions{0}, evicted_bytes{0};
     std::atomic<unsigned long long> callback_ns{0};  // inside GPU callbacks (the apps' launches)
+    // write-back (pmFetchMemory and friends): host buffer, waiting for the
+    // producing task's event, the copies themselves
+    std::atomic<unsigned long long> fetch_host_ns{0}, fetch_wait_ns{0}, fetch_copy_ns{0}, fetches{0};
 };
 
 static unsigned long long ns_since(double t0);
@@ -476,14 +479,21 @@ static pmStatus fetch_range(AddressSpace* a, size_t lo, size_t hi) {
     std::vector<std::pair<size_t, size_t>> st;
     a->host_stale.present(lo, hi, st);
     if (st.empty()) return pmSuccess;
+    const double t0 = now_s();
     const pmStatus hs = ensure_host(a);
     if (hs != pmSuccess) return hs;
+    const double t1 = now_s();
     if (a->last_write) PMR_DEV(pmb_event_synchronize(a->last_write));
+    const double t2 = now_s();
     for (auto& r : st) {
         PMR_DEV(pmb_memcpy_async(a->host + r.first, a->dev + r.first, r.second - r.first, PMB_D2H, c.fetch_stream));
         c.stats.d2h += r.second - r.first;
     }
     PMR_DEV(pmb_stream_synchronize(c.fetch_stream));
+    c.stats.fetch_host_ns += static_cast<unsigned long long>((t1 - t0) * 1e9);
+    c.stats.fetch_wait_ns += static_cast<unsigned long long>((t2 - t1) * 1e9);
+    c.stats.fetch_copy_ns += ns_since(t2);
+    c.stats.fetches++;
     for (auto& r : st) a->host_stale.remove(r.first, r.second);
     return pmSuccess;
 }
@@ -1092,6 +1102,12 @@ pmStatus pmInitialize() {
         PMR_DEV(pmb_mem_get_info(&fr, &tot));
         c.dev_budget = fr > c.reserve_bytes ? static_cast<int64_t>((fr - c.reserve_bytes) / 10 * 9) : 0;
         c.dev_held = 0;
+        // Map the budget into the stream-ordered pool now: growing the pool
+        // while tasks run stalls their kernels and copies.
+        const char* pr = getenv("PMB_POOL_RESERVE_BYTES");
+        const size_t pool_want = std::min(pr ? static_cast<size_t>(atoll(pr)) : static_cast<size_t>(c.dev_budget),
+                                          static_cast<size_t>(c.dev_budget));
+        if (pool_want) PMR_DEV(pmb_mempool_reserve(c.device, pool_want, nullptr));
         const char* pv = getenv("PMB_PINNED_CACHE_BYTES");
         c.pin_limit = pv ? static_cast<size_t>(atoll(pv)) : (size_t(16) << 30);
         c.eager_writeback = env_flag("PMB_EAGER_WRITEBACK");
@@ -1545,10 +1561,22 @@ extern "C" void pmb_runtime_admission(double* slot_wait_s, double* memory_wait_s
 
 extern "C" double pmb_runtime_callback_seconds(void) { return pmr::ctl().stats.callback_ns * 1e-9; }
 
+extern "C" void pmb_runtime_fetch_timers(double* host_s, double* wait_s, double* copy_s, unsigned long long* fetches) {
+    pmr::Controller& c = pmr::ctl();
+    if (host_s) *host_s = c.stats.fetch_host_ns * 1e-9;
+    if (wait_s) *wait_s = c.stats.fetch_wait_ns * 1e-9;
+    if (copy_s) *copy_s = c.stats.fetch_copy_ns * 1e-9;
+    if (fetches) *fetches = c.stats.fetches;
+}
+
 extern "C" void pmb_runtime_reset_stats(void) {
     pmr::Controller& c = pmr::ctl();
     c.stats.slot_ns = 0;
     c.stats.callback_ns = 0;
+    c.stats.fetch_host_ns = 0;
+    c.stats.fetch_wait_ns = 0;
+    c.stats.fetch_copy_ns = 0;
+    c.stats.fetches = 0;
     c.stats.mem_ns = 0;
     c.stats.evictions = 0;
     c.stats.evicted_bytes = 0;

@@ -145,5 +145,9 @@ void pmb_runtime_admission(double* slot_wait_s, double* memory_wait_s, unsigned 
                            unsigned long long* evicted_bytes);
 // Seconds spent inside subtask_gpu_custom callbacks (the apps' own launches).
 double pmb_runtime_callback_seconds(void);
+// Write-back of device results to host memory (pmFetchMemory, eviction):
+// seconds getting host buffers, waiting for the producing tasks, copying
+// (issue to completion); and the number of write-backs.
+void pmb_runtime_fetch_timers(double* host_s, double* wait_s, double* copy_s, unsigned long long* fetches);
 void pmb_runtime_reset_stats(void);
 }

@@ -65,6 +65,7 @@ extern "C" void pmb_runtime_stats(unsigned long long* h2d_bytes, unsigned long l
 extern "C" void pmb_runtime_reset_stats(void);
 extern "C" void pmb_runtime_set_eager_writeback(int on);
 extern "C" double pmb_runtime_callback_seconds(void);
+extern "C" void pmb_runtime_fetch_timers(double* host_s, double* wait_s, double* copy_s, unsigned long long* fetches);
 extern "C" void pmb_runtime_admission(double* slot_wait_s, double* memory_wait_s, unsigned long long* evictions,
                                       unsigned long long* evicted_bytes);
 extern "C" void pmb_runtime_timers(double* stub_s, double* admit_wait_s, double* pinned_alloc_s,
@@ -626,6 +627,9 @@ int main(int argc, char** argv) {
         pmb_runtime_timers(&stub_s, &admit_s, &pin_s, &pin_b);
         pmb_runtime_admission(&slot_s, &mem_s, &ev, &ev_b);
         const double cb_s = pmb_runtime_callback_seconds();
+        double fh_s = 0, fw_s = 0, fc_s = 0;
+        unsigned long long nfetch = 0;
+        pmb_runtime_fetch_timers(&fh_s, &fw_s, &fc_s, &nfetch);
         js += ", " + stream_json("served", specs, r, dp, &served_tps, &ge, &lr);
         // Alone vs. in the mix: recompute each sampled task by itself.
         int same = 0, compared = 0;
@@ -640,13 +644,15 @@ int main(int argc, char** argv) {
                 std::memcmp(jt->second.data(), it->second.data(), 4 * it->second.size()) == 0)
                 ++same;
         }
-        char b[768];
+        char b[1024];
         snprintf(b, sizeof(b), ", \"served_alone_vs_mix\": {\"compared\": %d, \"bit_identical\": %d}, "
                                "\"served_h2d_bytes\": %llu, \"served_d2h_bytes\": %llu, \"served_runtime\": "
                                "{\"stub_issue_s\": %.4f, \"admission_wait_s\": %.4f, \"slot_wait_s\": %.4f, "
                                "\"memory_wait_s\": %.4f, \"evictions\": %llu, \"evicted_bytes\": %llu, "
-                               "\"pinned_alloc_s\": %.4f, \"pinned_alloc_bytes\": %llu, \"callback_s\": %.4f}",
-                 compared, same, h2d, d2h, stub_s, admit_s, slot_s, mem_s, ev, ev_b, pin_s, pin_b, cb_s);
+                               "\"pinned_alloc_s\": %.4f, \"pinned_alloc_bytes\": %llu, \"callback_s\": %.4f, "
+                               "\"fetches\": %llu, \"fetch_host_s\": %.4f, \"fetch_wait_s\": %.4f, \"fetch_copy_s\": %.4f}",
+                 compared, same, h2d, d2h, stub_s, admit_s, slot_s, mem_s, ev, ev_b, pin_s, pin_b, cb_s, nfetch, fh_s,
+                 fw_s, fc_s);
         js += b;
     }
     if (o.run_plain) {
