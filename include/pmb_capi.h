@@ -185,11 +185,14 @@ int pmb_image_filter_plain(const uint8_t* d_in, uint8_t* d_out, int width, int h
 /* ------------------------------------------------------------------------ */
 
 /* Bytes of device scratch pmb_inclusive_scan_u32_u64 needs for n elements
- * (a 256-byte header plus 8 bytes per 4096-element tile). */
+ * (a 256-byte header, one 64-bit carry per 2^24-element chunk and one 64-bit
+ * sum per 16384-element segment). */
 size_t pmb_scan_scratch_bytes(size_t n);
 
-/* out[i] = in[0] + ... + in[i] with 64-bit sums, n <= 2^30, one launch on
- * `stream` (plus a memset of the scratch).  d_in, d_out and d_scratch are
+/* out[i] = in[0] + ... + in[i] with 64-bit sums, n <= 2^30, ceil(n / 2^24) + 1
+ * launches on `stream` (reduce-then-scan over L2-sized chunks, chained by
+ * programmatic dependent launch; no memset, no inter-block spinning).  d_in,
+ * d_out and d_scratch are
  * device pointers, 16-byte aligned.  Replaces prefixSum_cudaLaunchFunc /
  * prefixSum_cuda / elemAdd_cuda and the host scan of subtask totals
  * (testSuite/prefixSum/source/code/src/prefixSumCUDA.cu:68-267,
@@ -203,16 +206,17 @@ int pmb_inclusive_scan_u32_u64(const uint32_t* d_in, uint64_t* d_out, size_t n, 
  * pm:: subtask_gpu_custom callback may only enqueue work on the stream it is
  * handed (cudaMalloc/cudaFree synchronise the device and would stall every
  * subtask in flight), and a service that fixes its memory budget up front
- * cannot let a library grow it.  The look-back scratch is a fixed 1 MiB
- * device array inside libpmb.so, held by every GPU that loads the library
+ * cannot let a library grow it.  The scan's scratch (chunk carries and
+ * segment sums) is a fixed 1 MiB device array inside libpmb.so, held by every
+ * GPU that loads the library
  * until the process exits; the call allocates nothing, which limits n to
  * PMB_SCAN_NOALLOC_MAX_ELEMS (longer inputs return PMB_BEYOND_LIMITS).  The
  * first call on a device looks up the array's device address with that
  * device current; make that first call before any stream capture.  All calls
- * share the one array (each clears the part it uses before its kernel runs),
+ * share the one array (each writes the words it reads before reading them),
  * so calls whose work overlaps on the GPU -- on different streams, or from
  * different threads -- race and must be serialised by the caller. */
-#define PMB_SCAN_NOALLOC_MAX_ELEMS 536739840ull /* (1 MiB - 256 B) / 8 B per 4096-element tile */
+#define PMB_SCAN_NOALLOC_MAX_ELEMS 536739840ull /* about 2^29; its scratch (257 KB) fits the 1 MiB array */
 int pmb_inclusive_scan_u32_u64_noalloc(const uint32_t* d_in, uint64_t* d_out, size_t n, void* stream);
 
 /* Copy the error word of a scan/sort scratch buffer to the host (synchronous).

@@ -1,4 +1,4 @@
-"""GPU parity tests of the single-pass scan and the onesweep radix sort.
+"""GPU parity tests of the chunked reduce-then-scan and the onesweep radix sort.
 
 Integer results must be bit-exact against the oracles (restatements of the
 reference's serialPrefixSum / serialRadixSortRound); every run also checks
@@ -33,7 +33,8 @@ def to_dev(cuda, x):
     return cuda.from_numpy(x.view(np.int32)).cuda()
 
 
-@pytest.mark.parametrize("n", [1, 3, 4, 5, 4095, 4096, 4097, 8192 + 17, 1 << 20, (1 << 22) + 3])
+@pytest.mark.parametrize("n", [1, 3, 4, 5, 4095, 4096, 4097, 8192 + 17, 32768 + 1, 1 << 20, (1 << 22) + 3,
+                               (1 << 23) + 5, 3 * (1 << 23) + 12345])
 def test_scan_matches_oracle(cuda, oracle, n):
     from unicorn_b200 import ops
 
@@ -43,6 +44,19 @@ def test_scan_matches_oracle(cuda, oracle, n):
     got = out.cpu().numpy().view(np.uint64)
     assert np.array_equal(got, orc_scan(oracle, x))
     assert ops.scratch_error(scratch) == 0
+
+
+def test_scan_carries_of_maximal_values(cuda):
+    """All keys 2^32-1 across a chunk boundary: carries and segment sums
+    need their full 64 bits."""
+    from unicorn_b200 import ops
+
+    n = (1 << 23) + 4099
+    x = np.full(n, 0xFFFFFFFF, dtype=np.uint32)
+    out, scratch = ops.inclusive_scan_u32_u64(to_dev(cuda, x))
+    cuda.cuda.synchronize()
+    got = out.cpu().numpy().view(np.uint64)
+    assert np.array_equal(got, np.arange(1, n + 1, dtype=np.uint64) * np.uint64(0xFFFFFFFF))
 
 
 def test_scan_repeated_calls_reuse_scratch(cuda):

@@ -3,8 +3,8 @@
 pmb_inclusive_scan_u32_u64_noalloc exists for callers that may not allocate
 device memory (a pm:: subtask_gpu_custom callback must only enqueue work on
 its stream; cudaMalloc would synchronise the device and stall the other
-subtasks in flight) -- it keeps its look-back scratch in a fixed array inside
-libpmb.so.  Its results must equal the allocating entry point's bit for bit
+subtasks in flight) -- it keeps its scratch (carries and segment sums) in a
+fixed array inside libpmb.so.  Its results must equal the allocating entry point's bit for bit
 (integer scan), on two calls in a row that reuse the shared array.  This file
 is collected last so that a failure here comes after every other test has
 run; it also passes on its own in a fresh process.
