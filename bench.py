@@ -319,7 +319,19 @@ def app_measurements(torch, L, stream):
         torch.cuda.synchronize()
         resid = ops.lu_residual(A0, Aw)
         res["lu_4096"] = {"gflops": round((2.0 / 3.0) * nl ** 3 / lu_ms / 1e6, 1), "ms": round(lu_ms, 3),
-                          "residual_fro": resid}
+                          "residual_fro": resid, "launches": 3 * (nl // 64) - 2}
+        del Aw, A0, lws
+        # The LU trailing update alone at its largest step (rest = 4032, K = 64):
+        # A22 -= L21*U12 streams A22 in and out (8 bytes per element); the split
+        # pass over the two 4032 x 64 panels runs in the timed region too.
+        m = nl - 64
+        U = torch.rand(m, 64, device="cuda", generator=g) * 2 - 1
+        V = torch.rand(64, m, device="cuda", generator=g) * 2 - 1
+        C = torch.rand(m, m, device="cuda", generator=g) * 2 - 1
+        uws = ops._scratch(L.pmb_gemm_workspace_bytes(m, m, 64))
+        up_ms = _timed(torch, stream, lambda: ops.sgemm(U, V, C, -1.0, 1.0, workspace=uws), 20)
+        res["lu_trailing_update_4032_k64"] = _hbm_entry(8 * m * m, up_ms, hbm)
+        del U, V, C, uws
     return res
 
 
@@ -585,6 +597,7 @@ def main():
             app_cpu_baselines(torch, apps)
         line["apps"] = apps
     if rank == 0 and world == 1 and not args.no_served:
+        torch.cuda.empty_cache()  # the served stream runs in its own process: leave it the device
         line["served_mix"] = served_measurement()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(img, f, os.cpu_count() or 1)
