@@ -95,13 +95,18 @@ onesweep_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, con
     __shared__ uint32_t s_vals[VALUES ? kTile : 1];
     __shared__ uint32_t s_whist[kWarps][RADIX];
     __shared__ uint32_t s_dummy[kWarps][32];
-    __shared__ uint32_t s_tile_start[RADIX];
+    __shared__ uint32_t s_mdummy[kWarps][32];
+    // Per warp and digit, the lanes holding it (two items in turn); used only
+    // while ranking, so it shares its storage with s_keys.
+    static_assert(2 * kWarps * RADIX <= kTile, "match words fit in the key buffer");
+    auto s_match = reinterpret_cast<uint32_t (*)[kWarps][RADIX]>(s_keys);
     __shared__ uint32_t s_goff[RADIX];
     __shared__ uint32_t s_tmp[kWarps];
     __shared__ uint32_t s_tile;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
     for (int i = tid; i < kWarps * RADIX; i += kThreads) (&s_whist[0][0])[i] = 0;
+    for (int i = tid; i < 2 * kWarps * RADIX; i += kThreads) (&s_match[0][0][0])[i] = 0;
     __syncthreads();
     const uint32_t tile = s_tile;
     const size_t wbase = static_cast<size_t>(tile) * kTile + static_cast<size_t>(warp) * (kItems * 32);
@@ -121,29 +126,35 @@ onesweep_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, con
             key[i] = idx < n ? in[idx] : 0u;
         }
     }
-    // Stable warp-level ranking in (warp, item, lane) order.  Lanes holding the
-    // same digit are found with BITS ballots; the lowest of them (the leader)
-    // advances the warp's running count for that digit.  Every lane performs the
-    // same load and store -- the others on a private dummy slot -- so the update
-    // has no divergent branch.
+    // Stable warp-level ranking in (warp, item, lane) order.  Every lane ORs
+    // its bit into the word of its digit (shared-memory atomic OR: the order
+    // of the lanes does not matter), and reads back the set of lanes holding
+    // the same digit.  The lowest of them (the leader) advances the warp's
+    // running count for that digit and, one item later, clears the word;
+    // consecutive items use alternate word sets, so a clear is ordered before
+    // the word's next use by the syncs in between.  Invalid lanes of a ragged
+    // last tile, and lanes that are not leaders, do the same loads and stores
+    // on private dummy words: no divergent branch.
+    uint32_t* prev_clear = &s_mdummy[warp][lane];
 #pragma unroll
     for (int i = 0; i < kItems; ++i) {
         const bool valid = full || wbase + i * 32 + lane < n;
         const uint32_t d = (key[i] >> shift) & MASK;
-        uint32_t peers = __ballot_sync(0xffffffffu, valid);
-#pragma unroll
-        for (int b = 0; b < BITS; ++b) {
-            const bool bit = (d >> b) & 1u;
-            const uint32_t m = __ballot_sync(0xffffffffu, bit);
-            peers &= bit ? m : ~m;
-        }
-        const int leader = (__ffs(peers) - 1) & 31;
-        uint32_t* slot = (valid && lane == leader) ? &s_whist[warp][d] : &s_dummy[warp][lane];
+        uint32_t* mw = valid ? &s_match[i & 1][warp][d] : &s_mdummy[warp][lane];
+        atomicOr(mw, 1u << lane);
+        __syncwarp();
+        const uint32_t peers = valid ? *mw : (1u << lane);
+        *prev_clear = 0;  // the previous item's word, if this lane led it
+        const int leader = __ffs(peers) - 1;
+        const bool lead = valid && lane == leader;
+        uint32_t* slot = lead ? &s_whist[warp][d] : &s_dummy[warp][lane];
         const uint32_t cnt = *slot;
         *slot = cnt + __popc(peers);
+        prev_clear = lead ? mw : &s_mdummy[warp][lane];
         __syncwarp();
         rank[i] = __shfl_sync(0xffffffffu, cnt, leader) + __popc(peers & pmb::lanemask_lt());
     }
+    *prev_clear = 0;
     __syncthreads();
 
     // Per digit: warp offsets within the tile and the tile's digit count.
@@ -162,7 +173,10 @@ onesweep_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, con
     const uint32_t digit_base = block_exclusive_scan(tid < RADIX ? hist_pass[tid] : 0u, s_tmp);
 
     if (tid < RADIX) {
-        s_tile_start[tid] = tile_start;
+        // One table per lookup below: each is a shared load at a data-dependent
+        // (bank-conflicting) address, so the offsets are pre-added.
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) s_whist[w][tid] += tile_start;
         uint32_t excl = 0;
         if (tile > 0) {
             // kLook predecessors per round, loaded together; only those nearer
@@ -204,7 +218,7 @@ onesweep_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, con
             pmb::st_relaxed_u32(&status[static_cast<size_t>(tile) * RADIX + tid],
                                 kFlagInc | ((excl + my_cnt) & kCountMask));
         }
-        s_goff[tid] = digit_base + excl;
+        s_goff[tid] = digit_base + excl - tile_start;  // output index = s_goff[d] + tile position
     }
     __syncthreads();
 
@@ -212,7 +226,7 @@ onesweep_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, con
     for (int i = 0; i < kItems; ++i) {
         if (full || wbase + i * 32 + lane < n) {
             const uint32_t d = (key[i] >> shift) & MASK;
-            const uint32_t pos = s_tile_start[d] + s_whist[warp][d] + rank[i];
+            const uint32_t pos = s_whist[warp][d] + rank[i];
             s_keys[pos] = key[i];
             if constexpr (VALUES) s_vals[pos] = vin[wbase + i * 32 + lane];
         }
@@ -225,7 +239,7 @@ onesweep_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, con
             const int p = tid + j * kThreads;
             const uint32_t k = s_keys[p];
             const uint32_t d = (k >> shift) & MASK;
-            const uint32_t g = s_goff[d] + (p - s_tile_start[d]);
+            const uint32_t g = s_goff[d] + p;
             out[g] = k;
             if constexpr (VALUES) vout[g] = s_vals[p];
         }
@@ -234,7 +248,7 @@ onesweep_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, con
         for (int p = tid; p < tile_n; p += kThreads) {
             const uint32_t k = s_keys[p];
             const uint32_t d = (k >> shift) & MASK;
-            const uint32_t g = s_goff[d] + (p - s_tile_start[d]);
+            const uint32_t g = s_goff[d] + p;
             out[g] = k;
             if constexpr (VALUES) vout[g] = s_vals[p];
         }
