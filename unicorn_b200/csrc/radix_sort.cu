@@ -91,9 +91,9 @@ onesweep_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, con
     constexpr int RADIX = 1 << BITS;
     constexpr uint32_t MASK = RADIX - 1;
     static_assert(RADIX <= kThreads, "one digit per thread");
-    __shared__ uint32_t s_keys[kTile];
+    __shared__ __align__(16) uint32_t s_keys[kTile];
     __shared__ uint32_t s_vals[VALUES ? kTile : 1];
-    __shared__ uint32_t s_whist[kWarps][RADIX];
+    __shared__ __align__(16) uint32_t s_whist[kWarps][RADIX];
     __shared__ uint32_t s_dummy[kWarps][32];
     __shared__ uint32_t s_mdummy[kWarps][32];
     // Per warp and digit, the lanes holding it (two items in turn); used only
@@ -105,8 +105,12 @@ onesweep_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, con
     __shared__ uint32_t s_tile;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) s_tile = atomicAdd(tile_counter, 1u);
-    for (int i = tid; i < kWarps * RADIX; i += kThreads) (&s_whist[0][0])[i] = 0;
-    for (int i = tid; i < 2 * kWarps * RADIX; i += kThreads) (&s_match[0][0][0])[i] = 0;
+    {
+        static_assert((kWarps * RADIX) % 4 == 0, "16-byte clears");
+        const uint4 z = make_uint4(0u, 0u, 0u, 0u);
+        for (int i = tid; i < kWarps * RADIX / 4; i += kThreads) reinterpret_cast<uint4*>(&s_whist[0][0])[i] = z;
+        for (int i = tid; i < 2 * kWarps * RADIX / 4; i += kThreads) reinterpret_cast<uint4*>(&s_match[0][0][0])[i] = z;
+    }
     __syncthreads();
     const uint32_t tile = s_tile;
     const size_t wbase = static_cast<size_t>(tile) * kTile + static_cast<size_t>(warp) * (kItems * 32);
@@ -148,8 +152,7 @@ onesweep_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, con
         const int leader = __ffs(peers) - 1;
         const bool lead = valid && lane == leader;
         uint32_t* slot = lead ? &s_whist[warp][d] : &s_dummy[warp][lane];
-        const uint32_t cnt = *slot;
-        *slot = cnt + __popc(peers);
+        const uint32_t cnt = atomicAdd(slot, static_cast<uint32_t>(__popc(peers)));
         prev_clear = lead ? mw : &s_mdummy[warp][lane];
         __syncwarp();
         rank[i] = __shfl_sync(0xffffffffu, cnt, leader) + __popc(peers & pmb::lanemask_lt());
