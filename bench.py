@@ -85,7 +85,7 @@ def bf16_peak():
 
 def profiled_traffic():
     """Per-launch DRAM bytes of the stencil kernel from the committed ncu summary."""
-    path = os.path.join(ROOT, "profiles", "image_filter_8192_r2.md")
+    path = os.path.join(ROOT, "profiles", "image_filter_8192_5x5.md")
     try:
         with open(path) as fh:
             for line in fh:
