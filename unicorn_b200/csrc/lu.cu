@@ -403,11 +403,14 @@ lu_panel_kernel(float* __restrict__ A, int64_t lda, int k0, int kb, int rest, in
     const bool cols = blockIdx.x < col_blocks;
 #pragma unroll
     for (int k = 0; k < NB * NB / 256; ++k) {  // 16 independent loads in flight per thread
+        // Consecutive threads write consecutive shared words (no bank conflicts);
+        // the row blocks read F transposed for that (strided, from L2).
         const int e = threadIdx.x + 256 * k;
-        const int c = e / NB, r = e - c * NB;
-        const double f = F[e];
-        if (cols) sF[e] = r >= c ? static_cast<T>(f) : T(0);        // sF[c * 64 + r] = L_rc
-        else sF[r * NB + c] = r < c ? static_cast<T>(f) : T(0);     // sF[r * 64 + c] = U_rc
+        const int hi = e / NB, lo = e - hi * NB;
+        const int c = cols ? hi : lo, r = cols ? lo : hi;
+        const double f = F[c * NB + r];
+        sF[e] = cols ? (r >= c ? static_cast<T>(f) : T(0))    // sF[c * 64 + r] = L_rc
+                     : (r < c ? static_cast<T>(f) : T(0));    // sF[r * 64 + c] = U_rc
         if (r == c) sDiag[r] = cols ? T(1) / static_cast<T>(f) : static_cast<T>(fabs(f));
     }
     __syncthreads();
