@@ -614,6 +614,11 @@ __device__ __forceinline__ void umma_bf16_pair_upd(uint32_t tmem_d, uint64_t ade
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 3)
 gemm_update_2sm_kernel(const __grid_constant__ GemmMaps maps, const __grid_constant__ CUtensorMap cmap, int M, int N,
                        float alpha, float beta, uint32_t* __restrict__ err) {
+    // Launched as a programmatic dependent of the kernel that wrote the
+    // operands (the LU panel solve), this returns once that grid is complete
+    // and its writes are visible; otherwise it returns at once.
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* ctile = smem;  // the operand region, reused for C after the MMAs
@@ -904,7 +909,7 @@ int make_c_map(CUtensorMap* map, float* C, int M, int N, int64_t ldc) {
 // kp <= 64, C satisfying c_map_ok.
 int launch_update(int M, int N, int kp, float alpha, const __nv_bfloat16* ah, const __nv_bfloat16* al,
                   const __nv_bfloat16* bh, const __nv_bfloat16* bl, float beta, float* C, int64_t ldc, uint32_t* err,
-                  cudaStream_t s) {
+                  cudaStream_t s, bool dependent = false) {
     GemmMaps maps;
     CUtensorMap cmap;
     int st;
@@ -919,9 +924,17 @@ int launch_update(int M, int N, int kp, float alpha, const __nv_bfloat16* ah, co
         attr_err = cudaFuncSetAttribute(gemm_update_2sm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kUpdSmemBytes);
     });
     PMB_CUDA_TRY(attr_err);
-    const dim3 grid(2 * ((M + 255) / 256) * ((N + kUpdN - 1) / kUpdN));
-    gemm_update_2sm_kernel<<<grid, kThreads, kUpdSmemBytes, s>>>(maps, cmap, M, N, alpha, beta, err);
-    PMB_CUDA_TRY(cudaGetLastError());
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2 * ((M + 255) / 256) * ((N + kUpdN - 1) / kUpdN));
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = kUpdSmemBytes;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = dependent ? 1 : 0;
+    PMB_CUDA_TRY(cudaLaunchKernelEx(&cfg, gemm_update_2sm_kernel, maps, cmap, M, N, alpha, beta, err));
     return PMB_SUCCESS;
 }
 
@@ -948,22 +961,25 @@ int sgemm_bf16x3_launch(int M, int N, int K, float alpha, const float* A, int64_
 // caller that already holds the split operands: ah/al M x kp and bh/bl N x kp,
 // K-major bf16 with zero padding beyond K, kp a multiple of 8 and at most 64.
 // C (row-major, ldc) must have a 16-byte aligned base and ldc a multiple of 4.
-// Errors of the kernel are OR-ed into *err.
+// Errors of the kernel are OR-ed into *err.  dependent = launch as a
+// programmatic dependent of the previous kernel on s: the kernel waits for
+// that grid to complete before it touches any data, so only the launch
+// latency overlaps the previous kernel.
 int gemm_presplit_launch(int M, int N, int kp, float alpha, const __nv_bfloat16* ah, const __nv_bfloat16* al,
                          const __nv_bfloat16* bh, const __nv_bfloat16* bl, float beta, float* C, int64_t ldc,
-                         uint32_t* err, cudaStream_t s);
+                         uint32_t* err, cudaStream_t s, bool dependent);
 
 }  // namespace pmb
 
 int pmb::gemm_presplit_launch(int M, int N, int kp, float alpha, const __nv_bfloat16* ah, const __nv_bfloat16* al,
                               const __nv_bfloat16* bh, const __nv_bfloat16* bl, float beta, float* C, int64_t ldc,
-                              uint32_t* err, cudaStream_t s) {
+                              uint32_t* err, cudaStream_t s, bool dependent) {
     PMB_CHECK_ARG(M >= 0 && N >= 0, "negative GEMM size");
     if (M == 0 || N == 0) return PMB_SUCCESS;
     PMB_CHECK_ARG(kp > 0 && kp <= BK2 && kp % 8 == 0, "split depth %d: need a multiple of 8 up to %d", kp, BK2);
     PMB_CHECK_ARG(ah && al && bh && bl && C && err, "null pointer");
     PMB_CHECK_ARG(ldc >= N && c_map_ok(C, ldc), "C needs a 16-byte aligned base and ldc a multiple of 4");
-    return launch_update(M, N, kp, alpha, ah, al, bh, bl, beta, C, ldc, err, s);
+    return launch_update(M, N, kp, alpha, ah, al, bh, bl, beta, C, ldc, err, s, dependent);
 }
 
 extern "C" int pmb_sgemm_bf16x3(int M, int N, int K, float alpha, const float* A, int64_t lda, const float* B,

@@ -47,7 +47,7 @@ int sgemm_bf16x3_launch(int M, int N, int K, float alpha, const float* A, int64_
                         bool clear_error);
 int gemm_presplit_launch(int M, int N, int kp, float alpha, const __nv_bfloat16* ah, const __nv_bfloat16* al,
                          const __nv_bfloat16* bh, const __nv_bfloat16* bl, float beta, float* C, int64_t ldc,
-                         uint32_t* err, cudaStream_t s);
+                         uint32_t* err, cudaStream_t s, bool dependent);
 }
 extern "C" int pmb_sgemm_plain(int M, int N, int K, float alpha, const float* A, int64_t lda, const float* B,
                                int64_t ldb, float beta, float* C, int64_t ldc, void* stream);
@@ -55,6 +55,32 @@ extern "C" int pmb_sgemm_plain(int M, int N, int K, float alpha, const float* A,
 namespace {
 
 constexpr int kMaxNb = 128;
+
+// The block-step kernels are chained by programmatic dependent launch: each
+// waits here until the previous grid on the stream is complete and its
+// writes are visible (at once when it was launched normally), then lets the
+// next kernel's launch begin.
+__device__ __forceinline__ void grid_dependency_wait() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// Launch on s, as a programmatic dependent of the previous kernel when `dependent`.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_chained(void (*kernel)(KArgs...), unsigned grid, unsigned block, cudaStream_t s, bool dependent,
+                           Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = dependent ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
 constexpr uint32_t kFlagPivot = 1;      // partial pivoting would have swapped rows
 constexpr uint32_t kFlagZeroPivot = 2;  // a pivot was exactly zero
 
@@ -281,6 +307,7 @@ lu_diag_kernel(float* __restrict__ A, int64_t lda, int kb, float* __restrict__ W
 // checks the rows below the block.
 __global__ void __launch_bounds__(256, 1)
 lu_diag64_kernel(float* __restrict__ A, int64_t lda, int kb, double* __restrict__ F, uint32_t* __restrict__ flags) {
+    grid_dependency_wait();
     constexpr int NB = 64, WARPS = 8, RI = 2, CJ = 8;
     __shared__ double s_col[2][NB];
     __shared__ double s_row[2][NB];
@@ -397,6 +424,7 @@ __global__ void __launch_bounds__(256)
 lu_panel_kernel(float* __restrict__ A, int64_t lda, int k0, int kb, int rest, int col_blocks,
                 const double* __restrict__ F, uint32_t* __restrict__ flags, __nv_bfloat16* __restrict__ uh,
                 __nv_bfloat16* __restrict__ ul, __nv_bfloat16* __restrict__ lh, __nv_bfloat16* __restrict__ ll) {
+    grid_dependency_wait();
     constexpr int NB = 64;
     __shared__ T sF[NB * NB];
     __shared__ T sDiag[NB];
@@ -606,26 +634,27 @@ static int lu_impl(float* A, int n, int64_t lda, int nb, void* workspace, size_t
         float* A22 = A + static_cast<int64_t>(k0 + kb) * lda + k0 + kb;
         int st;
         if (nb <= kPanelNb) {
-            lu_diag64_kernel<<<1, 256, 0, s>>>(A11, lda, kb, w.F, &w.flags[1]);
-            PMB_CUDA_TRY(cudaGetLastError());
+            // The first diagonal block waits for all earlier work on the stream;
+            // later ones follow the previous step's update as dependents.
+            PMB_CUDA_TRY(launch_chained(lu_diag64_kernel, 1, 256, s, k0 > 0, A11, lda, kb, w.F, &w.flags[1]));
             if (rest == 0) continue;
             const int half = std::min((rest + 7) / 8, 4 * 148);  // blocks per side, 8 warps (items) each
             if (plain) {
-                lu_panel_kernel<float><<<2 * half, 256, 0, s>>>(A, lda, k0, kb, rest, half, w.F, &w.flags[1], nullptr,
-                                                                 nullptr, nullptr, nullptr);
-                PMB_CUDA_TRY(cudaGetLastError());
+                PMB_CUDA_TRY(launch_chained(lu_panel_kernel<float>, 2 * half, 256, s, true, A, lda, k0, kb, rest, half,
+                                            w.F, &w.flags[1], static_cast<__nv_bfloat16*>(nullptr),
+                                            static_cast<__nv_bfloat16*>(nullptr), static_cast<__nv_bfloat16*>(nullptr),
+                                            static_cast<__nv_bfloat16*>(nullptr)));
             } else {
                 // The update reads and writes A22 by TMA when it is 16-byte aligned with a
                 // row pitch that is a multiple of 16 bytes; the panel kernel then hands it
                 // the split operands directly.
                 const bool direct = (reinterpret_cast<uintptr_t>(A22) & 15) == 0 && (lda & 3) == 0;
-                lu_panel_kernel<double><<<2 * half, 256, 0, s>>>(A, lda, k0, kb, rest, half, w.F, &w.flags[1],
-                                                                  direct ? w.uh : nullptr, w.ul, w.lh, w.ll);
-                PMB_CUDA_TRY(cudaGetLastError());
+                PMB_CUDA_TRY(launch_chained(lu_panel_kernel<double>, 2 * half, 256, s, true, A, lda, k0, kb, rest,
+                                            half, w.F, &w.flags[1], direct ? w.uh : nullptr, w.ul, w.lh, w.ll));
                 if (direct) {
                     // A22 -= L21 * U12 == row-major (U12^T)(L21^T); a timed-out wait shows as flag 4.
                     st = pmb::gemm_presplit_launch(rest, rest, kPanelNb, -1.0f, w.uh, w.ul, w.lh, w.ll, 1.0f, A22,
-                                                   lda, &w.flags[1], s);
+                                                   lda, &w.flags[1], s, true);
                     if (st != PMB_SUCCESS) return st;
                     continue;
                 }

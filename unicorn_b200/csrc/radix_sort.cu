@@ -84,7 +84,7 @@ __device__ __forceinline__ uint32_t block_exclusive_scan(uint32_t x, uint32_t* s
 }
 
 template <int BITS, bool VALUES>
-__global__ void __launch_bounds__(kThreads, 3)
+__global__ void __launch_bounds__(kThreads, VALUES ? 3 : 4)
 onesweep_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, const uint32_t* __restrict__ vin,
                 uint32_t* __restrict__ vout, size_t n, int shift, const uint32_t* __restrict__ hist_pass,
                 uint32_t* __restrict__ tile_counter, uint32_t* __restrict__ err, uint32_t* __restrict__ status) {
