@@ -139,6 +139,7 @@ struct GemmMaps {
 __global__ void __launch_bounds__(kThreads, 1)
 gemm_bf16x3_kernel(const __grid_constant__ GemmMaps maps, int M, int N, int KT, float alpha, float beta,
                    float* __restrict__ C, int64_t ldc, uint32_t* __restrict__ err) {
+    asm volatile("griddepcontrol.wait;" ::: "memory");  // the split pass launched before it
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kStages * kStageBytes);
@@ -393,6 +394,7 @@ __device__ __forceinline__ void pair_tile(int M, int N, int tn, int& pm, int& pn
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
 gemm_bf16x3_2sm_kernel(const __grid_constant__ GemmMaps maps, int M, int N, int KT, float alpha, float beta,
                        float* __restrict__ C, int64_t ldc, uint32_t* __restrict__ err) {
+    asm volatile("griddepcontrol.wait;" ::: "memory");  // the split pass launched before it
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     float* stage_out = reinterpret_cast<float*>(smem + kStages2 * kStage2Bytes);
@@ -764,6 +766,9 @@ __global__ void __launch_bounds__(256)
 split_both_kernel(const float* __restrict__ A, int64_t lda, int M, const float* __restrict__ B, int64_t ldb, int N,
                   int K, int Kp, int row_blocks, __nv_bfloat16* __restrict__ ah, __nv_bfloat16* __restrict__ al,
                   __nv_bfloat16* __restrict__ bh, __nv_bfloat16* __restrict__ bl) {
+    // The product kernel is launched as a programmatic dependent of this pass:
+    // let its launch begin (it waits for this grid before reading anything).
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     __shared__ float t[32][33];
     if (static_cast<int>(blockIdx.x) < row_blocks) {
         const int64_t total = static_cast<int64_t>(M) * Kp;
@@ -886,6 +891,23 @@ int make_map(CUtensorMap* map, const void* base, int rows, int kp, int box_rows,
 
 size_t align256(size_t x) { return (x + 255) & ~static_cast<size_t>(255); }
 int padded_k(int K) { return (K + BK - 1) / BK * BK; }
+
+// Launch on s as a programmatic dependent of the previous kernel when `dependent`.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_dep(void (*kernel)(KArgs...), dim3 grid, int threads, int smem, cudaStream_t s, bool dependent,
+                       Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = dependent ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
 
 // Row-major fp32 C (M x N, ldc) in 32 x 32 boxes, SWIZZLE_128B; TMA needs a
 // 16-byte aligned base and a row pitch that is a multiple of 16 bytes.
@@ -1028,7 +1050,7 @@ int pmb::sgemm_bf16x3_launch(int M, int N, int K, float alpha, const float* A, i
     }();
     // A single K slice: bound by C traffic, read and written by TMA.
     if (kp <= BK2 && c_map_ok(C, ldc) && !force_1sm)
-        return launch_update(M, N, kp, alpha, ah, al, bh, bl, beta, C, ldc, err, s);
+        return launch_update(M, N, kp, alpha, ah, al, bh, bl, beta, C, ldc, err, s, true);
 
     GemmMaps maps;
     int st;
@@ -1046,9 +1068,8 @@ int pmb::sgemm_bf16x3_launch(int M, int N, int K, float alpha, const float* A, i
         });
         PMB_CUDA_TRY(attr2_err);
         const dim3 grid2(2 * ((M + 255) / 256) * ((N + 255) / 256));
-        gemm_bf16x3_2sm_kernel<<<grid2, kThreads, kSmem2Bytes, s>>>(maps, M, N, (kp + BK2 - 1) / BK2, alpha, beta, C,
-                                                                     ldc, err);
-        PMB_CUDA_TRY(cudaGetLastError());
+        PMB_CUDA_TRY(launch_dep(gemm_bf16x3_2sm_kernel, grid2, kThreads, kSmem2Bytes, s, true, maps, M, N,
+                                (kp + BK2 - 1) / BK2, alpha, beta, C, ldc, err));
         return PMB_SUCCESS;
     }
     if ((st = make_map(&maps.ah, ah, M, kp, BM)) != PMB_SUCCESS) return st;
@@ -1063,8 +1084,8 @@ int pmb::sgemm_bf16x3_launch(int M, int N, int K, float alpha, const float* A, i
     });
     PMB_CUDA_TRY(attr_err);
     const dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
-    gemm_bf16x3_kernel<<<grid, kThreads, kSmemBytes, s>>>(maps, M, N, kp / BK, alpha, beta, C, ldc, err);
-    PMB_CUDA_TRY(cudaGetLastError());
+    PMB_CUDA_TRY(launch_dep(gemm_bf16x3_kernel, grid, kThreads, kSmemBytes, s, true, maps, M, N, kp / BK, alpha, beta, C,
+                            ldc, err));
     return PMB_SUCCESS;
 }
 

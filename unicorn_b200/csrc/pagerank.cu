@@ -160,6 +160,28 @@ __device__ __forceinline__ float finish(float r, uint32_t v, const uint32_t* __r
     return od ? (damping * r) / static_cast<float>(od) : 0.0f;
 }
 
+// The iteration kernels are chained by programmatic dependent launch: each
+// waits here for the previous grid on the stream (at once when launched
+// normally), then lets the next kernel's launch begin.
+__device__ __forceinline__ void chain_wait() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <typename... KArgs, typename... Args>
+cudaError_t launch_dep(void (*kernel)(KArgs...), unsigned grid, unsigned threads, cudaStream_t s, Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(threads);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+}
+
 // One iteration over all slices.  out[v] receives r'[v] (last iteration) or
 // the next contrib d*r'[v]/outdeg(v); split vertices get their owner partial
 // in out[v] and their later pieces in carry[slice].
@@ -168,6 +190,7 @@ pull_kernel(const uint32_t* __restrict__ row_ptr, const uint32_t* __restrict__ c
             const uint32_t* __restrict__ outdeg, const float* __restrict__ contrib, const int32_t* __restrict__ own_lo,
             const int32_t* __restrict__ cont, const uint32_t* __restrict__ e_start, uint32_t n_slices,
             uint32_t n_vertices, float damping, int last, float* __restrict__ out, float* __restrict__ carry) {
+    chain_wait();
     const uint32_t w = blockIdx.x * kWarpsPerCta + (threadIdx.x >> 5);
     if (w >= n_slices) return;
     const int lane = threadIdx.x & 31;
@@ -242,6 +265,7 @@ pull_kernel(const uint32_t* __restrict__ row_ptr, const uint32_t* __restrict__ c
 // vertex whose first continuation slice is w, adding carries in slice order.
 __global__ void fixup_kernel(const int32_t* __restrict__ cont, uint32_t n_slices, const uint32_t* __restrict__ outdeg,
                              float damping, int last, const float* __restrict__ carry, float* __restrict__ out) {
+    chain_wait();
     const uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= n_slices) return;
     const int32_t v = cont[w];
@@ -371,12 +395,11 @@ extern "C" int pmb_pagerank(const uint32_t* d_row_ptr, const uint32_t* d_col, co
         if (ns == 0) {
             PMB_CUDA_TRY(cudaMemsetAsync(dst, 0, 4ull * n_vertices, s));
         } else {
-            pull_kernel<<<pgrid, kCtaThreads, 0, s>>>(d_row_ptr, d_col, d_out_degree, ca, own_lo, cont, e_start, ns,
-                                                      n_vertices, damping, last, dst, carry);
-            PMB_CUDA_TRY(cudaGetLastError());
-            fixup_kernel<<<grid_for(ns, 256, 0x7fffffffu), 256, 0, s>>>(cont, ns, d_out_degree, damping, last, carry,
-                                                                         dst);
-            PMB_CUDA_TRY(cudaGetLastError());
+            PMB_CUDA_TRY(launch_dep(pull_kernel, pgrid, kCtaThreads, s, d_row_ptr, d_col, d_out_degree,
+                                    static_cast<const float*>(ca), own_lo, cont, e_start, ns, n_vertices, damping, last,
+                                    dst, carry));
+            PMB_CUDA_TRY(launch_dep(fixup_kernel, grid_for(ns, 256, 0x7fffffffu), 256, s, cont, ns, d_out_degree,
+                                    damping, last, static_cast<const float*>(carry), dst));
         }
         float* t = ca;
         ca = cbuf;
