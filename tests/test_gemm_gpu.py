@@ -135,3 +135,24 @@ def test_k_zero_scales_c(cuda):
     ops.sgemm(dA, dB, dC, 1.0, 3.0)
     cuda.cuda.synchronize()
     assert np.allclose(dC.cpu().numpy(), 3.0)
+
+
+@pytest.mark.parametrize("M,N,K", [(1024, 1024, 1024), (300, 520, 64)])
+def test_product_after_producer_on_same_stream(cuda, M, N, K):
+    """The product kernel is a programmatic dependent of the split pass; the
+    split pass itself must wait for a kernel that writes A earlier on the
+    stream."""
+    from unicorn_b200 import ops
+
+    A, B = mats(M, N, K, 41)
+    srcA = cuda.from_numpy(A).cuda()
+    dA = cuda.zeros_like(srcA)
+    dB = cuda.from_numpy(B).cuda()
+    s = cuda.cuda.Stream()
+    with cuda.cuda.stream(s):
+        dA.copy_(srcA)
+        C, ws = ops.sgemm(dA, dB, stream=s)
+        dA.zero_()
+    s.synchronize()
+    norm, _ = errors(C.cpu().numpy(), A, B)
+    assert norm <= NORM_TOL, norm

@@ -111,3 +111,28 @@ def test_gpu_lu_large_residual(cuda, n, nb):
     _, _, flags = ops.lu_decompose(d, nb)
     assert flags == 0
     assert ops.lu_residual(d0, d) <= 1e-5
+
+
+@pytest.mark.gpu
+def test_gpu_lu_after_producer_on_same_stream(cuda, oracle):
+    """The block steps are chained by programmatic dependent launch; the first
+    step must still wait for a kernel that writes A earlier on the same stream
+    (no host synchronisation in between), and a second factorization queued
+    right behind the first must see its own input."""
+    from unicorn_b200 import ops
+
+    n = 1000
+    a = dd_matrix(n, 31)
+    src = cuda.from_numpy(a.copy()).cuda()
+    d = cuda.zeros_like(src)
+    s = cuda.cuda.Stream()
+    with cuda.cuda.stream(s):
+        d.copy_(src)                     # the producer, on s
+        _, ws, _ = ops.lu_decompose(d, 64, stream=s)
+        d2 = d.clone()                   # reads the first result on s
+        d.copy_(src)                     # a fresh input, on s again
+        ops.lu_decompose(d, 64, workspace=ws, stream=s)
+    s.synchronize()
+    ref = crout_f64(oracle, a)
+    assert np.allclose(d.cpu().numpy(), ref, rtol=1e-4, atol=1e-5)
+    assert np.allclose(d2.cpu().numpy(), ref, rtol=1e-4, atol=1e-5)

@@ -125,3 +125,21 @@ def test_sort_then_scan_full_configuration(cuda):
     del x
     assert np.array_equal(out.cpu().numpy().view(np.uint64), np.cumsum(ref_sorted, dtype=np.uint64))
     assert ops.scratch_error(s1) == 0 and ops.scratch_error(s2) == 0
+
+
+def test_scan_after_producer_on_same_stream(cuda):
+    """The chunk launches overlap by programmatic dependent launch; the first
+    one must wait for a kernel that writes the input earlier on the stream."""
+    from unicorn_b200 import ops
+
+    n = 3 * (1 << 24) + 77
+    x = keys(n, 9)
+    src = to_dev(cuda, x)
+    d = cuda.zeros_like(src)
+    s = cuda.cuda.Stream()
+    with cuda.cuda.stream(s):
+        d.copy_(src)
+        out, scratch = ops.inclusive_scan_u32_u64(d, stream=s)
+        d.zero_()                        # queued behind the scan: must not change its result
+    s.synchronize()
+    assert np.array_equal(out.cpu().numpy().view(np.uint64), np.cumsum(x.astype(np.uint64)))

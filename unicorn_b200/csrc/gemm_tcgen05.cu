@@ -303,7 +303,9 @@ gemm_bf16x3_kernel(const __grid_constant__ GemmMaps maps, int M, int N, int KT, 
 // shared memory, and each CTA's tensor memory receives its 128 rows of the
 // tile.  Per CTA and K-slice that is 64 KB of operands for the work the 1-SM
 // kernel needs 96 KB for, and the 128-byte K slices (SWIZZLE_128B) halve the
-// number of TMA requests; three stages fill the shared memory.
+// number of TMA requests; three stages fill the shared memory.  Products with
+// few tiles use N = 128 per pair instead (Pair2<128>: twice the pairs busy,
+// four 48 KB stages).
 //   full[s]     leader only: one arrive.expect_tx from each CTA's producer plus
 //               both CTAs' TMA bytes (the peer's loads signal it remotely);
 //   empty[s]    both CTAs: multicast tcgen05.commit from the leader;
@@ -317,11 +319,25 @@ constexpr int kHalf2 = 128 * BK2 * 2;                     // 16 KB: 128 rows of 
 constexpr int kStage2Bytes = 4 * kHalf2;                  // A hi, A lo, B hi, B lo halves
 constexpr int kStageOutFloats = 4 * 32 * 20;              // per-warp 32 x 16 staging, row stride 20
 constexpr int kSmem2Bytes = kStages2 * kStage2Bytes + kStageOutFloats * 4 + 1024 + 256;
+
+// Tile shape of the pair kernel: 256 x TN outputs per CTA pair (TN = 256, or
+// 128 when a product has too few 256 x 256 tiles to occupy the SM pairs).
+// Each CTA stages TN/2 rows of B^T; 192 KB of stages either way (3 x 64 KB or
+// 4 x 48 KB); two TN-column accumulators in tensor memory.
+template <int TN>
+struct Pair2 {
+    static_assert(TN == 256 || TN == 128, "pair tile width");
+    static constexpr int kBHalf = (TN / 2) * BK2 * 2;
+    static constexpr int kStageBytes = 2 * kHalf2 + 2 * kBHalf;
+    static constexpr int kStages = TN == 256 ? 3 : 4;
+    static constexpr int kSmemBytes = kStages * kStageBytes + kStageOutFloats * 4 + 1024 + 256;
+    static constexpr uint32_t kTmemCols = 2 * TN;
+    static constexpr uint32_t kIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) |
+                                       ((uint32_t)(256 >> 4) << 24);
+};
+static_assert(Pair2<256>::kSmemBytes == kSmem2Bytes && Pair2<128>::kSmemBytes <= kSmem2Bytes, "pair shared memory");
 constexpr int kFlush2 = 16;                               // K = 1024 per accumulator segment
 constexpr int kGroupRows = 8;                             // tile rows per raster group
-constexpr uint32_t kIdesc2 = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(256 >> 3) << 17) |
-                             ((uint32_t)(256 >> 4) << 24);
-
 // K-major SWIZZLE_128B tile: rows of 128 bytes, 8-row core groups 1024 bytes apart.
 __device__ __forceinline__ uint64_t umma_desc_sw128(uint32_t saddr) {
     uint64_t d = 0;
@@ -361,12 +377,13 @@ __device__ __forceinline__ void tma_load_2d_pair(uint32_t dst, const CUtensorMap
         "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(cbar)
         : "memory");
 }
-__device__ __forceinline__ void umma_bf16_pair(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+__device__ __forceinline__ void umma_bf16_pair_i(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                                 uint32_t accumulate) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
         "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(kIdesc2), "r"(accumulate)
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
         : "memory");
 }
 // Arrive once on the mbarrier at this shared offset in both CTAs of the pair.
@@ -391,9 +408,12 @@ __device__ __forceinline__ void pair_tile(int M, int N, int tn, int& pm, int& pn
     pn = in_group / rows;
 }
 
+template <int TN>
 __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
 gemm_bf16x3_2sm_kernel(const __grid_constant__ GemmMaps maps, int M, int N, int KT, float alpha, float beta,
                        float* __restrict__ C, int64_t ldc, uint32_t* __restrict__ err) {
+    using P = Pair2<TN>;
+    constexpr int kStages2 = P::kStages, kStage2Bytes = P::kStageBytes, kBHalf = P::kBHalf;
     asm volatile("griddepcontrol.wait;" ::: "memory");  // the split pass launched before it
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -414,10 +434,10 @@ gemm_bf16x3_2sm_kernel(const __grid_constant__ GemmMaps maps, int M, int N, int 
     // panels (read once from HBM, then from L2) instead of each wave reading
     // every row panel of A.
     int pm, pn;
-    pair_tile(M, N, 256, pm, pn);
-    const int m0 = pm * 256 + 128 * static_cast<int>(rank);  // this CTA's rows of A and C
-    const int n0 = pn * 256;                                 // the pair's columns
-    const int nb0 = n0 + 128 * static_cast<int>(rank);       // this CTA's rows of B^T
+    pair_tile(M, N, TN, pm, pn);
+    const int m0 = pm * 256 + 128 * static_cast<int>(rank);     // this CTA's rows of A and C
+    const int n0 = pn * TN;                                     // the pair's columns
+    const int nb0 = n0 + (TN / 2) * static_cast<int>(rank);     // this CTA's rows of B^T
 
     if (threadIdx.x == 0) {
         s_fail = 0;
@@ -434,7 +454,7 @@ gemm_bf16x3_2sm_kernel(const __grid_constant__ GemmMaps maps, int M, int N, int 
     }
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
-                     "r"(kTmemCols)
+                     "r"(P::kTmemCols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
     }
@@ -461,7 +481,7 @@ gemm_bf16x3_2sm_kernel(const __grid_constant__ GemmMaps maps, int M, int N, int 
             tma_load_2d_pair(smem_u32(st), &maps.ah, k, m0, fbar);
             tma_load_2d_pair(smem_u32(st + kHalf2), &maps.al, k, m0, fbar);
             tma_load_2d_pair(smem_u32(st + 2 * kHalf2), &maps.bh, k, nb0, fbar);
-            tma_load_2d_pair(smem_u32(st + 3 * kHalf2), &maps.bl, k, nb0, fbar);
+            tma_load_2d_pair(smem_u32(st + 2 * kHalf2 + kBHalf), &maps.bl, k, nb0, fbar);
         }
     } else if (warp == 1 && lane == 0 && rank == 0) {
         // ---- MMA issuer (leader CTA) ----
@@ -479,15 +499,16 @@ gemm_bf16x3_2sm_kernel(const __grid_constant__ GemmMaps maps, int M, int N, int 
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t acc = tmem + 256u * b;
+            const uint32_t acc = tmem + static_cast<uint32_t>(TN) * b;
             const uint32_t st = smem_u32(smem + s * kStage2Bytes);
-            const uint32_t a_hi = st, a_lo = st + kHalf2, b_hi = st + 2 * kHalf2, b_lo = st + 3 * kHalf2;
+            const uint32_t a_hi = st, a_lo = st + kHalf2, b_hi = st + 2 * kHalf2, b_lo = st + 2 * kHalf2 + kBHalf;
 #pragma unroll
             for (int k16 = 0; k16 < BK2 / 16; ++k16) {
                 const uint32_t off = k16 * 32;  // 16 bf16 = 32 bytes along the swizzled row
-                umma_bf16_pair(acc, umma_desc_sw128(a_hi + off), umma_desc_sw128(b_hi + off), (seg_k | k16) != 0);
-                umma_bf16_pair(acc, umma_desc_sw128(a_hi + off), umma_desc_sw128(b_lo + off), 1u);
-                umma_bf16_pair(acc, umma_desc_sw128(a_lo + off), umma_desc_sw128(b_hi + off), 1u);
+                umma_bf16_pair_i(acc, umma_desc_sw128(a_hi + off), umma_desc_sw128(b_hi + off), P::kIdesc,
+                                 (seg_k | k16) != 0);
+                umma_bf16_pair_i(acc, umma_desc_sw128(a_hi + off), umma_desc_sw128(b_lo + off), P::kIdesc, 1u);
+                umma_bf16_pair_i(acc, umma_desc_sw128(a_lo + off), umma_desc_sw128(b_hi + off), P::kIdesc, 1u);
             }
             umma_commit_pair(smem_u32(&empty[s]));
             if (seg_k == kFlush2 - 1 || kt == KT - 1) umma_commit_pair(smem_u32(&acc_full[b]));
@@ -509,9 +530,9 @@ gemm_bf16x3_2sm_kernel(const __grid_constant__ GemmMaps maps, int M, int N, int 
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const float bscale = seg == 0 ? beta : 1.0f;
 #pragma unroll 1
-            for (int c = 0; c < 256 / 16; ++c) {
+            for (int c = 0; c < TN / 16; ++c) {
                 uint32_t r[16];
-                tmem_ld16(tmem + 256u * b + (static_cast<uint32_t>(32 * q) << 16) + 16 * c, r);
+                tmem_ld16(tmem + static_cast<uint32_t>(TN) * b + (static_cast<uint32_t>(32 * q) << 16) + 16 * c, r);
                 float4* mine = reinterpret_cast<float4*>(stg + lane * 20);
 #pragma unroll
                 for (int j = 0; j < 4; ++j)
@@ -568,7 +589,7 @@ gemm_bf16x3_2sm_kernel(const __grid_constant__ GemmMaps maps, int M, int N, int 
     cluster_sync_all();
     if (warp == 1) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(P::kTmemCols) : "memory");
     }
 }
 
@@ -1056,20 +1077,40 @@ int pmb::sgemm_bf16x3_launch(int M, int N, int K, float alpha, const float* A, i
     int st;
     // Tiles of 256 rows per CTA pair for M > 128.
     if (M > BM && !force_1sm) {
+        // 256 x 128 tiles when 256 x 256 ones would leave at least half the SM
+        // pairs without a tile (e.g. 1024 x 1024: 16 tiles for 74 pairs).
+        static const int sm_pairs = [] {
+            int dev = 0, sms = 148;
+            if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+                cudaGetLastError();
+                sms = 148;
+            }
+            return sms / 2;
+        }();
+        const int64_t tiles256 = static_cast<int64_t>((M + 255) / 256) * ((N + 255) / 256);
+        const bool narrow = 2 * tiles256 <= sm_pairs;
+        const int tn = narrow ? 128 : 256;
         if ((st = make_map(&maps.ah, ah, M, kp, 128, BK2)) != PMB_SUCCESS) return st;
         if ((st = make_map(&maps.al, al, M, kp, 128, BK2)) != PMB_SUCCESS) return st;
-        if ((st = make_map(&maps.bh, bh, N, kp, 128, BK2)) != PMB_SUCCESS) return st;
-        if ((st = make_map(&maps.bl, bl, N, kp, 128, BK2)) != PMB_SUCCESS) return st;
+        if ((st = make_map(&maps.bh, bh, N, kp, tn / 2, BK2)) != PMB_SUCCESS) return st;
+        if ((st = make_map(&maps.bl, bl, N, kp, tn / 2, BK2)) != PMB_SUCCESS) return st;
         static std::once_flag attr2_once;
         static cudaError_t attr2_err = cudaSuccess;
         std::call_once(attr2_once, [] {
-            attr2_err =
-                cudaFuncSetAttribute(gemm_bf16x3_2sm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmem2Bytes);
+            attr2_err = cudaFuncSetAttribute(gemm_bf16x3_2sm_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             Pair2<256>::kSmemBytes);
+            if (attr2_err == cudaSuccess)
+                attr2_err = cudaFuncSetAttribute(gemm_bf16x3_2sm_kernel<128>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, Pair2<128>::kSmemBytes);
         });
         PMB_CUDA_TRY(attr2_err);
-        const dim3 grid2(2 * ((M + 255) / 256) * ((N + 255) / 256));
-        PMB_CUDA_TRY(launch_dep(gemm_bf16x3_2sm_kernel, grid2, kThreads, kSmem2Bytes, s, true, maps, M, N,
-                                (kp + BK2 - 1) / BK2, alpha, beta, C, ldc, err));
+        const dim3 grid2(2 * ((M + 255) / 256) * ((N + tn - 1) / tn));
+        if (narrow)
+            PMB_CUDA_TRY(launch_dep(gemm_bf16x3_2sm_kernel<128>, grid2, kThreads, Pair2<128>::kSmemBytes, s, true, maps,
+                                    M, N, (kp + BK2 - 1) / BK2, alpha, beta, C, ldc, err));
+        else
+            PMB_CUDA_TRY(launch_dep(gemm_bf16x3_2sm_kernel<256>, grid2, kThreads, Pair2<256>::kSmemBytes, s, true, maps,
+                                    M, N, (kp + BK2 - 1) / BK2, alpha, beta, C, ldc, err));
         return PMB_SUCCESS;
     }
     if ((st = make_map(&maps.ah, ah, M, kp, BM)) != PMB_SUCCESS) return st;
