@@ -80,3 +80,20 @@ def test_served_mix_admits_under_memory_pressure(served_bin):
     assert s["error"] == "" and s["completed"] == 24, s
     assert s["max_gemm_rel_err"] <= REL_TOL and s["max_lu_residual"] <= REL_TOL
     assert r["served_alone_vs_mix"]["bit_identical"] == r["served_alone_vs_mix"]["compared"] == 4
+
+
+@pytest.mark.gpu
+def test_served_mix_concurrent_lu_stream_completes(served_bin):
+    """Many LU tasks admitted at once: their block-step kernels from different
+    tasks share the SMs (a trailing-update kernel variant that packed three
+    CTAs per SM once stalled exactly this case).  Every task must finish,
+    exact and bit-identical to its run alone."""
+    p = subprocess.run([served_bin, "--tasks", "64", "--rate", "0", "--gemm-frac", "0", "--lu-min", "512",
+                        "--lu-max", "4096", "--warmup", "64", "--check", "4", "--mode", "served"],
+                       capture_output=True, text=True, timeout=900)
+    assert p.returncode == 0, p.stdout + p.stderr
+    r = json.loads(p.stdout.strip().splitlines()[-1])
+    s = r["served"]
+    assert s["error"] == "" and s["completed"] == 64, s
+    assert s["max_lu_residual"] <= REL_TOL
+    assert r["served_alone_vs_mix"]["bit_identical"] == r["served_alone_vs_mix"]["compared"] == 4

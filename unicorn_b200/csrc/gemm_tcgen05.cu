@@ -597,27 +597,18 @@ gemm_bf16x3_2sm_kernel(const __grid_constant__ GemmMaps maps, int M, int N, int 
 // With a single 64-deep K slice per tile (the LU trailing update, K = block
 // size) the product is bound by reading and writing C, not by the MMAs.  The
 // kernel above reads C with plain loads in its epilogue, a few in flight per
-// thread, which leaves each SM far below its share of HBM bandwidth.  Here a
-// CTA pair owns a 256 x 128 tile (M = 256, N = 128 per MMA); each CTA's
-// shared memory is one 64 KB region that first holds its operands (A rows
-// 128 x 64, B^T rows 64 x 64, hi and lo) and, once the MMAs are done, its
-// 128 x 128 C tile: each epilogue warp TMA-loads its 32 rows (four 32 x 32
-// fp32 boxes, SWIZZLE_128B, so a warp's row-per-lane float4 accesses are free
-// of bank conflicts), updates them in shared memory and TMA-stores each box
-// as it finishes (rows and columns outside M x N are neither read nor
-// written).  At 65 KB per CTA three CTAs share an SM, so one CTA's C loads
-// overlap another's stores.
+// thread, which leaves each SM far below its share of HBM bandwidth.  Here
+// each epilogue warp issues TMA loads of its 32 rows of the C tile into shared
+// memory at kernel start, so they overlap the operand loads and the MMAs,
+// updates the tile in shared memory and writes each finished 32 x 32 box back
+// with a TMA store (rows and columns outside M x N are neither read nor
+// written).  Shared memory holds one operand stage (64 KB) and the CTA's
+// 128 x 256 C tile (128 KB: 32 boxes of 32 x 32 fp32, SWIZZLE_128B, so that a
+// warp's row-per-lane float4 accesses are free of bank conflicts).
 constexpr int kBoxBytes = 32 * 32 * 4;
-constexpr int kUpdN = 128;                                  // output columns per CTA pair
-constexpr int kUpdAHalf = 128 * BK2 * 2;                    // 16 KB: A hi or lo, this CTA's 128 rows
-constexpr int kUpdBHalf = (kUpdN / 2) * BK2 * 2;            // 8 KB: B^T hi or lo, this CTA's 64 rows
-constexpr int kUpdOpBytes = 2 * kUpdAHalf + 2 * kUpdBHalf;  // 48 KB
-constexpr int kUpdCBytes = 128 * kUpdN * 4;                 // 64 KB
-constexpr int kUpdRegion = kUpdOpBytes > kUpdCBytes ? kUpdOpBytes : kUpdCBytes;
-constexpr int kUpdSmemBytes = kUpdRegion + 1024 + 256;
-constexpr uint32_t kUpdTmemCols = kUpdN;
-constexpr uint32_t kIdescUpd = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(kUpdN >> 3) << 17) |
-                               ((uint32_t)(256 >> 4) << 24);
+constexpr int kUpdCBytes = 128 * 256 * 4;
+constexpr int kUpdSmemBytes = kStage2Bytes + kUpdCBytes + 1024 + 256;
+constexpr uint32_t kUpdTmemCols = 256;
 
 __device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, int x, int y, uint32_t src) {
     asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.bulk_group [%0, {%1, %2}], [%3];" ::"l"(
@@ -625,27 +616,19 @@ __device__ __forceinline__ void tma_store_2d(const CUtensorMap* map, int x, int 
                  "r"(x), "r"(y), "r"(src)
                  : "memory");
 }
-__device__ __forceinline__ void umma_bf16_pair_upd(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(kIdescUpd), "r"(accumulate)
-        : "memory");
-}
 
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 3)
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
 gemm_update_2sm_kernel(const __grid_constant__ GemmMaps maps, const __grid_constant__ CUtensorMap cmap, int M, int N,
                        float alpha, float beta, uint32_t* __restrict__ err) {
     // Launched as a programmatic dependent of the kernel that wrote the
-    // operands (the LU panel solve), this returns once that grid is complete
-    // and its writes are visible; otherwise it returns at once.
+    // operands (the split pass, or the LU panel solve), this returns once that
+    // grid is complete and its writes are visible; otherwise it returns at once.
     asm volatile("griddepcontrol.wait;" ::: "memory");
     asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint8_t* ctile = smem;  // the operand region, reused for C after the MMAs
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + kUpdRegion);
+    uint8_t* ctile = smem + kStage2Bytes;  // 1024-byte aligned: kStage2Bytes is a multiple of 1024
+    uint64_t* bars = reinterpret_cast<uint64_t*>(ctile + kUpdCBytes);
     uint64_t* full = bars;          // leader only: both CTAs' operand bytes
     uint64_t* acc_full = bars + 1;  // both CTAs: multicast commit after the MMAs
     uint64_t* cfull = bars + 2;     // [4] one per epilogue warp: its C rows landed
@@ -656,10 +639,10 @@ gemm_update_2sm_kernel(const __grid_constant__ GemmMaps maps, const __grid_const
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t rank = cluster_rank();
     int pm, pn;
-    pair_tile(M, N, kUpdN, pm, pn);
+    pair_tile(M, N, 256, pm, pn);
     const int m0 = pm * 256 + 128 * static_cast<int>(rank);
-    const int n0 = pn * kUpdN;
-    const int nb0 = n0 + (kUpdN / 2) * static_cast<int>(rank);
+    const int n0 = pn * 256;
+    const int nb0 = n0 + 128 * static_cast<int>(rank);
 
     if (threadIdx.x == 0) {
         s_fail = 0;
@@ -684,11 +667,11 @@ gemm_update_2sm_kernel(const __grid_constant__ GemmMaps maps, const __grid_const
     if (warp == 0 && lane == 0) {
         // ---- producer (both CTAs): the one K slice ----
         const uint32_t fbar = cluster_addr(smem_u32(full), 0);
-        mbar_arrive_expect_tx_cluster(fbar, kUpdOpBytes);
+        mbar_arrive_expect_tx_cluster(fbar, kStage2Bytes);
         tma_load_2d_pair(smem_u32(smem), &maps.ah, 0, m0, fbar);
-        tma_load_2d_pair(smem_u32(smem + kUpdAHalf), &maps.al, 0, m0, fbar);
-        tma_load_2d_pair(smem_u32(smem + 2 * kUpdAHalf), &maps.bh, 0, nb0, fbar);
-        tma_load_2d_pair(smem_u32(smem + 2 * kUpdAHalf + kUpdBHalf), &maps.bl, 0, nb0, fbar);
+        tma_load_2d_pair(smem_u32(smem + kHalf2), &maps.al, 0, m0, fbar);
+        tma_load_2d_pair(smem_u32(smem + 2 * kHalf2), &maps.bh, 0, nb0, fbar);
+        tma_load_2d_pair(smem_u32(smem + 3 * kHalf2), &maps.bl, 0, nb0, fbar);
     } else if (warp == 1 && lane == 0 && rank == 0) {
         // ---- MMA issuer (leader CTA) ----
         if (!mbar_wait(smem_u32(full), 0)) {
@@ -697,39 +680,34 @@ gemm_update_2sm_kernel(const __grid_constant__ GemmMaps maps, const __grid_const
         } else {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t st = smem_u32(smem);
-            const uint32_t a_hi = st, a_lo = st + kUpdAHalf, b_hi = st + 2 * kUpdAHalf,
-                           b_lo = st + 2 * kUpdAHalf + kUpdBHalf;
+            const uint32_t a_hi = st, a_lo = st + kHalf2, b_hi = st + 2 * kHalf2, b_lo = st + 3 * kHalf2;
 #pragma unroll
             for (int k16 = 0; k16 < BK2 / 16; ++k16) {
                 const uint32_t off = k16 * 32;
-                umma_bf16_pair_upd(tmem, umma_desc_sw128(a_hi + off), umma_desc_sw128(b_hi + off), k16 != 0);
-                umma_bf16_pair_upd(tmem, umma_desc_sw128(a_hi + off), umma_desc_sw128(b_lo + off), 1u);
-                umma_bf16_pair_upd(tmem, umma_desc_sw128(a_lo + off), umma_desc_sw128(b_hi + off), 1u);
+                umma_bf16_pair_i(tmem, umma_desc_sw128(a_hi + off), umma_desc_sw128(b_hi + off), Pair2<256>::kIdesc, k16 != 0);
+                umma_bf16_pair_i(tmem, umma_desc_sw128(a_hi + off), umma_desc_sw128(b_lo + off), Pair2<256>::kIdesc, 1u);
+                umma_bf16_pair_i(tmem, umma_desc_sw128(a_lo + off), umma_desc_sw128(b_hi + off), Pair2<256>::kIdesc, 1u);
             }
             umma_commit_pair(smem_u32(acc_full));
         }
     } else if (warp >= 2) {
         // ---- epilogue (both CTAs): rows 32q .. 32q+31 of this CTA's 128 ----
         const int q = warp & 3;
-        uint8_t* mine = ctile + q * (kUpdN / 32) * kBoxBytes;
+        uint8_t* mine = ctile + q * 8 * kBoxBytes;
         const bool load_c = beta != 0.0f;
         const uint32_t cbar = smem_u32(&cfull[q]);
-        // The MMAs (which read both CTAs' operand regions) are complete once
-        // acc_full fires, so the region can take C.
-        bool ok = __all_sync(0xffffffffu, mbar_wait(smem_u32(acc_full), 0));
-        if (ok && lane == 0 && load_c) {
-            mbar_expect_tx(cbar, (kUpdN / 32) * kBoxBytes);
-            for (int cb = 0; cb < kUpdN / 32; ++cb)
-                tma_load_2d(smem_u32(mine + cb * kBoxBytes), &cmap, n0 + 32 * cb, m0 + 32 * q, cbar);
+        if (lane == 0 && load_c) {
+            mbar_expect_tx(cbar, 8 * kBoxBytes);
+            for (int cb = 0; cb < 8; ++cb) tma_load_2d(smem_u32(mine + cb * kBoxBytes), &cmap, n0 + 32 * cb, m0 + 32 * q, cbar);
         }
-        ok = __all_sync(0xffffffffu, ok && (!load_c || mbar_wait(cbar, 0)));
+        const bool ok = __all_sync(0xffffffffu, mbar_wait(smem_u32(acc_full), 0) && (!load_c || mbar_wait(cbar, 0)));
         if (!ok || s_fail) {
             s_fail = 1;
             atomicOr(err, kErrTimeout);
         } else {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll 1
-            for (int c = 0; c < kUpdN / 16; ++c) {
+            for (int c = 0; c < 16; ++c) {
                 uint32_t r[16];
                 tmem_ld16(tmem + (static_cast<uint32_t>(32 * q) << 16) + 16 * c, r);
                 const int cb = c >> 1, h = c & 1;
@@ -958,8 +936,8 @@ int launch_update(int M, int N, int kp, float alpha, const __nv_bfloat16* ah, co
     int st;
     if ((st = make_map(&maps.ah, ah, M, kp, 128, BK2)) != PMB_SUCCESS) return st;
     if ((st = make_map(&maps.al, al, M, kp, 128, BK2)) != PMB_SUCCESS) return st;
-    if ((st = make_map(&maps.bh, bh, N, kp, kUpdN / 2, BK2)) != PMB_SUCCESS) return st;
-    if ((st = make_map(&maps.bl, bl, N, kp, kUpdN / 2, BK2)) != PMB_SUCCESS) return st;
+    if ((st = make_map(&maps.bh, bh, N, kp, 128, BK2)) != PMB_SUCCESS) return st;
+    if ((st = make_map(&maps.bl, bl, N, kp, 128, BK2)) != PMB_SUCCESS) return st;
     if ((st = make_c_map(&cmap, C, M, N, ldc)) != PMB_SUCCESS) return st;
     static std::once_flag attr_once;
     static cudaError_t attr_err = cudaSuccess;
@@ -968,7 +946,7 @@ int launch_update(int M, int N, int kp, float alpha, const __nv_bfloat16* ah, co
     });
     PMB_CUDA_TRY(attr_err);
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(2 * ((M + 255) / 256) * ((N + kUpdN - 1) / kUpdN));
+    cfg.gridDim = dim3(2 * ((M + 255) / 256) * ((N + 255) / 256));
     cfg.blockDim = dim3(kThreads);
     cfg.dynamicSmemBytes = kUpdSmemBytes;
     cfg.stream = s;
