@@ -220,9 +220,9 @@ int pmb_inclusive_scan_u32_u64(const uint32_t* d_in, uint64_t* d_out, size_t n, 
 int pmb_inclusive_scan_u32_u64_noalloc(const uint32_t* d_in, uint64_t* d_out, size_t n, void* stream);
 
 /* Copy the error word of a scan/sort scratch buffer to the host (synchronous).
- * 0 = clean; 1 = a look-back wait hit its poll limit (the result is then
- * not trustworthy).  Replaces nothing in the reference (its kernels never wait
- * on one another). */
+ * 0 = clean; 1 = a bounded wait hit its poll limit (the sort's look-back, the
+ * scan's tile staging; the result is then not trustworthy).  Replaces nothing
+ * in the reference (its kernels never wait on one another). */
 int pmb_scratch_error(const void* d_scratch, uint32_t* error_out);
 
 /* ------------------------------------------------------------------------ */
