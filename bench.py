@@ -332,6 +332,14 @@ def app_measurements(torch, L, stream):
         up_ms = _timed(torch, stream, lambda: ops.sgemm(U, V, C, -1.0, 1.0, workspace=uws), 20)
         res["lu_trailing_update_4032_k64"] = _hbm_entry(8 * m * m, up_ms, hbm)
         del U, V, C, uws
+        # Subtask reduction (REDUCE_ADD, FLOATS): 8 subtask copies of 2^24
+        # floats folded in order into the address space: 9 x 64 MiB moved.
+        nr, ns = 1 << 24, 8
+        copies = [torch.rand(nr, device="cuda", generator=g) for _ in range(ns)]
+        dst = torch.empty(nr, device="cuda")
+        red_ms = _timed(torch, stream, lambda: ops.reduce_elementwise(0, 4, dst, copies, nr, stream=stream), 10)
+        res["subtask_reduce_add_f32_8x2^24"] = _hbm_entry(4 * nr * (ns + 1), red_ms, hbm)
+        del copies, dst
     return res
 
 

@@ -181,6 +181,29 @@ int pmb_image_filter_plain(const uint8_t* d_in, uint8_t* d_out, int width, int h
                            const int8_t* filter, int radius, int mode, void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* Subtask reduction (REDUCE_* built-ins)                                   */
+/* ------------------------------------------------------------------------ */
+
+/* Bytes per element of a pmReductionDataType (INTS, UNSIGNED_INTS, LONGS,
+ * UNSIGNED_LONGS, FLOATS, DOUBLES = 0..5); 0 for an unknown type. */
+size_t pmb_reduce_element_size(int type);
+
+/* Element-wise fold of nsrc device arrays of `count` elements into d_dst, in
+ * source order: d_dst[e] = src0[e] (init_from_first) or d_dst[e] op src0[e],
+ * then op src1[e], ... .  op and type take the pmReductionOpType /
+ * pmReductionDataType values (bitwise ops on FLOATS / DOUBLES act on the
+ * values converted to uint32 / uint64, LOGICAL_XOR is a != b, as the
+ * reference's reducer defines them); `srcs` is a
+ * HOST array of nsrc device pointers (passed to the kernels by value, 128 per
+ * launch).  Every pointer must be aligned to the element size
+ * (PMB_INVALID_INDEX otherwise).  Launches on `stream`, no synchronisation.
+ * Replaces the host loops of the built-in reduction callbacks
+ * (source/code/src/pmReducer.cpp:1073-1320, pmPublicDefinitions.cpp:749-800)
+ * for subtask copies the pm:: runtime keeps in device memory. */
+int pmb_reduce_elementwise(int op, int type, void* d_dst, const void* const* d_srcs, int nsrc, size_t count,
+                           int init_from_first, void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* prefixSum: inclusive scan                                                */
 /* ------------------------------------------------------------------------ */
 

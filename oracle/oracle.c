@@ -222,3 +222,47 @@ void orc_lu_crout_f64(double* a, int n, long ld) {
         }
     }
 }
+
+/* ------------------------------------------------------------------------ */
+/* Subtask reduction: pmReducer::ReduceMemories                              */
+/* (source/code/src/pmReducer.cpp:590-700) folds subtask 2's shadow memory   */
+/* into subtask 1's element by element; bitwise operations on floats and     */
+/* doubles act on the values converted to uint32 / uint64                    */
+/* (pmReducer.cpp:408-423); LOGICAL_XOR is a != b.  op / type take the       */
+/* pmReductionOpType / pmReductionDataType values.  The reducer is a member  */
+/* of the reference runtime and does not compile on its own: this            */
+/* restatement is checked against hand-computed cases in the tests only.     */
+/* ------------------------------------------------------------------------ */
+#define ORC_FOLD(T, B)                                                                        \
+    do {                                                                                      \
+        T* x = (T*)a;                                                                         \
+        const T* y = (const T*)b;                                                             \
+        for (size_t i = 0; i < n; ++i) {                                                      \
+            switch (op) {                                                                     \
+                case 0: x[i] = x[i] + y[i]; break;                                            \
+                case 1: x[i] = y[i] < x[i] ? y[i] : x[i]; break;                              \
+                case 2: x[i] = x[i] < y[i] ? y[i] : x[i]; break;                              \
+                case 3: x[i] = x[i] * y[i]; break;                                            \
+                case 4: x[i] = (T)(x[i] && y[i]); break;                                      \
+                case 5: x[i] = (T)((B)x[i] & (B)y[i]); break;                                 \
+                case 6: x[i] = (T)(x[i] || y[i]); break;                                      \
+                case 7: x[i] = (T)((B)x[i] | (B)y[i]); break;                                 \
+                case 8: x[i] = (T)(x[i] != y[i]); break;                                      \
+                default: x[i] = (T)((B)x[i] ^ (B)y[i]); break;                                \
+            }                                                                                 \
+        }                                                                                     \
+    } while (0)
+
+int orc_reduce_fold(int op, int type, void* a, const void* b, size_t n) {
+    if (op < 0 || op > 9) return -1;
+    switch (type) {
+        case 0: ORC_FOLD(int32_t, int32_t); break;
+        case 1: ORC_FOLD(uint32_t, uint32_t); break;
+        case 2: ORC_FOLD(int64_t, int64_t); break;
+        case 3: ORC_FOLD(uint64_t, uint64_t); break;
+        case 4: ORC_FOLD(float, uint32_t); break;
+        case 5: ORC_FOLD(double, uint64_t); break;
+        default: return -1;
+    }
+    return 0;
+}

@@ -34,3 +34,22 @@ __global__ void rt_add_kernel(pmTaskInfo ti, pmDeviceInfo* di, pmSubtaskInfo si,
 }
 
 extern "C" void* rt_add_kernel_ptr() { return reinterpret_cast<void*>(&rt_add_kernel); }
+
+// Reduction self-test: subtask s reads row s of an N x words input and writes
+// its copy of the output range, out[j] = in[j] (copy) or out[j] += in[j]
+// (accumulate, int32: the copy starts from the address space's bytes).
+struct RtRowConf {
+    int words;       // 32-bit words per row
+    int accumulate;  // 0: copy, 1: add to the subscribed output
+    int type, op;    // reduction data type and operation
+};
+
+__global__ void rt_row_kernel(pmTaskInfo ti, pmDeviceInfo* di, pmSubtaskInfo si, pmStatus* st) {
+    const RtRowConf* conf = static_cast<const RtRowConf*>(ti.taskConf);
+    const unsigned* in = static_cast<const unsigned*>(si.memInfo[0].ptr);
+    unsigned* out = static_cast<unsigned*>(si.memInfo[1].ptr);
+    for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < conf->words; j += gridDim.x * blockDim.x)
+        out[j] = conf->accumulate ? out[j] + in[j] : in[j];
+}
+
+extern "C" void* rt_row_kernel_ptr() { return reinterpret_cast<void*>(&rt_row_kernel); }

@@ -8,9 +8,13 @@
 #include <cstring>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <vector>
+#include <algorithm>
+#include <cstdint>
 
 #include "pmPublicDefinitions.h"
+#include "pmPublicUtilities.h"
 #include "pmb_capi.h"
 
 using namespace pm;
@@ -269,12 +273,215 @@ void test_timeout() {
     CHECK(rel == pmStatusUnavailable, "released task status %d", rel);
 }
 
+// ---------------------------------------------------------------------------
+// Subtask reduction: N subtasks each write a private copy of one output range
+// (row s of the input, copied or added), folded with a built-in REDUCE_*
+// callback or the app's own.  The expected result is folded here in subtask
+// order, so float sums are compared bit for bit.
+
+extern "C" void* rt_row_kernel_ptr();
+
+struct RtRowConf {
+    int words, accumulate, type, op;
+};
+
+constexpr int kRowSubtasks = 7;
+constexpr int kRowWords = 2006;  // 8024 bytes: 2006 ints/floats, 1003 longs/doubles
+
+enum class OutSub { Whole, Inner, Scattered, Mismatched };
+OutSub g_out_sub = OutSub::Whole;
+
+pmStatus row_dd(pmTaskInfo ti, pmDeviceInfo di, pmSubtaskInfo si) {
+    const RtRowConf* conf = static_cast<const RtRowConf*>(ti.taskConf);
+    const size_t row = size_t(conf->words) * 4;
+    pmSubscribeToMemory(ti.taskHandle, di.deviceHandle, si.subtaskId, si.splitInfo, 0, READ_SUBSCRIPTION,
+                        pmSubscriptionInfo(si.subtaskId * row, row));
+    const pmSubscriptionInfo whole(0, row);
+    switch (g_out_sub) {
+        case OutSub::Whole:
+            pmSubscribeToMemory(ti.taskHandle, di.deviceHandle, si.subtaskId, si.splitInfo, 1,
+                                conf->accumulate ? READ_WRITE_SUBSCRIPTION : WRITE_SUBSCRIPTION, whole);
+            break;
+        case OutSub::Inner:  // reads everything, writes [64, row - 8): folded straight into the mirror
+            pmSubscribeToMemory(ti.taskHandle, di.deviceHandle, si.subtaskId, si.splitInfo, 1, READ_SUBSCRIPTION, whole);
+            pmSubscribeToMemory(ti.taskHandle, di.deviceHandle, si.subtaskId, si.splitInfo, 1, WRITE_SUBSCRIPTION,
+                                pmSubscriptionInfo(64, row - 72));
+            break;
+        case OutSub::Scattered:  // reads everything, writes 64 of every 128 bytes
+            pmSubscribeToMemory(ti.taskHandle, di.deviceHandle, si.subtaskId, si.splitInfo, 1, READ_SUBSCRIPTION, whole);
+            pmSubscribeToMemory(ti.taskHandle, di.deviceHandle, si.subtaskId, si.splitInfo, 1, WRITE_SUBSCRIPTION,
+                                pmScatteredSubscriptionInfo(0, 64, 128, row / 128));
+            break;
+        case OutSub::Mismatched:  // the last subtask writes a shorter range: the task fails
+            pmSubscribeToMemory(ti.taskHandle, di.deviceHandle, si.subtaskId, si.splitInfo, 1, WRITE_SUBSCRIPTION,
+                                pmSubscriptionInfo(0, si.subtaskId + 1 == kRowSubtasks ? row - 64 : row));
+            break;
+    }
+    if (di.deviceType == GPU_CUDA) {
+        pmCudaLaunchConf lc(4, 1, 1, 256, 1, 1);
+        pmSetCudaLaunchConf(ti.taskHandle, di.deviceHandle, si.subtaskId, si.splitInfo, lc);
+    }
+    return pmSuccess;
+}
+
+pmStatus row_cpu(pmTaskInfo ti, pmDeviceInfo, pmSubtaskInfo si) {
+    const RtRowConf* conf = static_cast<const RtRowConf*>(ti.taskConf);
+    const unsigned* in = static_cast<const unsigned*>(si.memInfo[0].ptr);
+    unsigned* out = static_cast<unsigned*>(si.memInfo[1].ptr);
+    for (int j = 0; j < conf->words; ++j) out[j] = conf->accumulate ? out[j] + in[j] : in[j];
+    return pmSuccess;
+}
+
+// The app's own callbacks: a = a + 3 b over int32, and one that calls
+// pmReduceSubtasks (BITWISE_OR, INTS) itself.
+pmStatus axpy3_reduction(pmTaskInfo ti, pmDeviceInfo, pmSubtaskInfo s1, pmDeviceInfo, pmSubtaskInfo s2) {
+    const RtRowConf* conf = static_cast<const RtRowConf*>(ti.taskConf);
+    int* a = static_cast<int*>(s1.memInfo[1].writePtr);
+    const int* b = static_cast<const int*>(s2.memInfo[1].writePtr);
+    if (!a || !b || s1.memInfo[1].length != size_t(conf->words) * 4) return pmUserError;
+    for (int j = 0; j < conf->words; ++j) a[j] += 3 * b[j];
+    return pmSuccess;
+}
+
+pmStatus or_reduction(pmTaskInfo ti, pmDeviceInfo d1, pmSubtaskInfo s1, pmDeviceInfo d2, pmSubtaskInfo s2) {
+    return pmReduceSubtasks(ti.taskHandle, d1.deviceHandle, s1.subtaskId, s1.splitInfo, d2.deviceHandle, s2.subtaskId,
+                            s2.splitInfo, REDUCE_BITWISE_OR, REDUCE_INTS);
+}
+
+template <typename T, typename B>
+T fold_ref(int op, T a, T b) {
+    switch (op) {
+        case REDUCE_ADD: return a + b;
+        case REDUCE_MIN: return b < a ? b : a;
+        case REDUCE_MAX: return a < b ? b : a;
+        case REDUCE_PRODUCT: return a * b;
+        case REDUCE_LOGICAL_AND: return (a != T(0) && b != T(0)) ? T(1) : T(0);
+        case REDUCE_BITWISE_AND: return T(B(a) & B(b));
+        case REDUCE_LOGICAL_OR: return (a != T(0) || b != T(0)) ? T(1) : T(0);
+        case REDUCE_BITWISE_OR: return T(B(a) | B(b));
+        case REDUCE_LOGICAL_XOR: return a != b ? T(1) : T(0);
+        default: return T(B(a) ^ B(b));
+    }
+}
+
+template <typename T>
+T row_value(int s, int j, int op) {
+    const unsigned h = unsigned(j) * 2654435761u + unsigned(s) * 40503u + 17u;
+    if (op == REDUCE_LOGICAL_AND || op == REDUCE_LOGICAL_OR || op == REDUCE_LOGICAL_XOR) return T(h % 3);
+    if (op == REDUCE_PRODUCT) return T(1 + h % 3);
+    if constexpr (std::is_floating_point<T>::value)
+        return (op == REDUCE_BITWISE_AND || op == REDUCE_BITWISE_OR || op == REDUCE_BITWISE_XOR)
+                   ? T(h % 100000u)
+                   : T(int(h % 20001u) - 10000) / T(7);
+    else if constexpr (sizeof(T) == 8)
+        return T((uint64_t(h) << 29) ^ (uint64_t(h) * 0x9E3779B97F4A7C15ull));
+    else
+        return T(int(h % 200001u) - 100000);
+}
+
+// One task: returns its status; on success compares the output with the fold.
+template <typename T, typename B>
+void reduce_case(bool gpu, int op, int type, pmDataReductionCallback custom, int custom_kind, int accumulate,
+                 OutSub sub) {
+    const int n = kRowWords * 4 / int(sizeof(T));
+    pmCallbacks cb;
+    cb.dataDistribution = row_dd;
+    cb.subtask_cpu = row_cpu;
+    if (gpu) cb.subtask_gpu_cuda = reinterpret_cast<pmSubtaskCallback_GPU_CUDA>(rt_row_kernel_ptr());
+    cb.dataReduction = custom ? custom : pmGetSubtaskReductionCallbackImpl(pmReductionOpType(op), pmReductionDataType(type));
+    CHECK(cb.dataReduction, "no reduction callback for op %d type %d", op, type);
+    char key[32];
+    std::snprintf(key, sizeof(key), "ROW_%d_%d_%d_%d", op, type, custom_kind, int(sub));
+    pmCallbackHandle h;
+    CHECK(pmRegisterCallbacks(key, cb, &h) == pmSuccess, "register");
+
+    pmMemHandle in, out;
+    CHECK(pmCreateMemory(size_t(kRowSubtasks) * kRowWords * 4, &in) == pmSuccess, "create in");
+    CHECK(pmCreateMemory(size_t(kRowWords) * 4, &out) == pmSuccess, "create out");
+    void *ip, *op_;
+    pmGetRawMemPtr(in, &ip);
+    pmGetRawMemPtr(out, &op_);
+    T* inp = static_cast<T*>(ip);
+    T* outp = static_cast<T*>(op_);
+    for (int s = 0; s < kRowSubtasks; ++s)
+        for (int j = 0; j < n; ++j) inp[size_t(s) * n + j] = row_value<T>(s, j, op);
+    std::vector<T> init(n);
+    for (int j = 0; j < n; ++j) init[j] = outp[j] = row_value<T>(100, j, op);
+
+    static RtRowConf conf;
+    conf = RtRowConf{kRowWords, accumulate, type, op};
+    g_out_sub = sub;
+    const bool reads_out = accumulate || sub == OutSub::Inner || sub == OutSub::Scattered;
+    pmTaskMem mem[2] = {pmTaskMem(in, READ_ONLY, SUBSCRIPTION_NATURAL),
+                        pmTaskMem(out, reads_out ? READ_WRITE : WRITE_ONLY, SUBSCRIPTION_NATURAL)};
+    pmTaskDetails td(&conf, sizeof(conf), mem, 2, h, kRowSubtasks);
+    pmTaskHandle t;
+    CHECK(pmSubmitTask(td, &t) == pmSuccess, "submit");
+    const pmStatus st = pmWaitForTaskCompletion(t);
+    if (sub == OutSub::Mismatched) {
+        CHECK(st == pmInvalidIndex, "mismatched subscriptions gave status %d", st);
+    } else {
+        CHECK(st == pmSuccess, "task failed (op %d type %d custom %d sub %d): %d", op, type, custom_kind, int(sub), st);
+        CHECK(pmFetchMemory(out) == pmSuccess, "fetch");
+        // the subtasks' copies (int32 words when accumulating), folded in order
+        std::vector<T> expect(n);
+        for (int j = 0; j < n; ++j) {
+            T acc{};
+            for (int s = 0; s < kRowSubtasks; ++s) {
+                T v = inp[size_t(s) * n + j];
+                if (accumulate) v = T(int(init[j]) + int(v));
+                if (s == 0) acc = v;
+                else if (custom_kind == 1) acc = T(int(acc) + 3 * int(v));
+                else if (custom_kind == 2) acc = T(int(acc) | int(v));
+                else acc = fold_ref<T, B>(op, acc, v);
+            }
+            const size_t byte = size_t(j) * sizeof(T);
+            bool written = true;
+            if (sub == OutSub::Inner) written = byte >= 64 && byte < size_t(kRowWords) * 4 - 8;
+            if (sub == OutSub::Scattered) written = byte % 128 < 64 && byte / 128 < size_t(kRowWords) * 4 / 128;
+            expect[j] = written ? acc : init[j];
+        }
+        CHECK(std::memcmp(expect.data(), outp, size_t(n) * sizeof(T)) == 0,
+              "op %d type %d custom %d sub %d: first mismatch at %d", op, type, custom_kind, int(sub),
+              int(std::mismatch(expect.begin(), expect.end(), outp,
+                                [](T a, T b) { return std::memcmp(&a, &b, sizeof(T)) == 0; }).first - expect.begin()));
+    }
+    CHECK(pmReleaseTask(t) == st, "release");
+    CHECK(pmReleaseMemory(in) == pmSuccess && pmReleaseMemory(out) == pmSuccess, "release memory");
+    CHECK(pmReleaseCallbacks(h) == pmSuccess, "release callbacks");
+}
+
+void test_reduce(bool gpu) {
+    CHECK(pmGetSubtaskReductionCallbackImpl(MAX_REDUCTION_OP_TYPES, REDUCE_INTS) == nullptr, "out-of-range op");
+    CHECK(pmGetSubtaskReductionCallbackImpl(REDUCE_ADD, MAX_REDUCTION_DATA_TYPES) == nullptr, "out-of-range type");
+    // every operation on every data type, whole-range writes
+    for (int op = 0; op < MAX_REDUCTION_OP_TYPES; ++op) {
+        reduce_case<int32_t, int32_t>(gpu, op, REDUCE_INTS, nullptr, 0, 0, OutSub::Whole);
+        reduce_case<uint32_t, uint32_t>(gpu, op, REDUCE_UNSIGNED_INTS, nullptr, 0, 0, OutSub::Whole);
+        reduce_case<int64_t, int64_t>(gpu, op, REDUCE_LONGS, nullptr, 0, 0, OutSub::Whole);
+        reduce_case<uint64_t, uint64_t>(gpu, op, REDUCE_UNSIGNED_LONGS, nullptr, 0, 0, OutSub::Whole);
+        reduce_case<float, uint32_t>(gpu, op, REDUCE_FLOATS, nullptr, 0, 0, OutSub::Whole);
+        reduce_case<double, uint64_t>(gpu, op, REDUCE_DOUBLES, nullptr, 0, 0, OutSub::Whole);
+    }
+    // copies that start from the address space's bytes (READ_WRITE)
+    reduce_case<int32_t, int32_t>(gpu, REDUCE_ADD, REDUCE_INTS, nullptr, 0, 1, OutSub::Whole);
+    // partial writes: contiguous (folded into the mirror) and scattered
+    reduce_case<float, uint32_t>(gpu, REDUCE_ADD, REDUCE_FLOATS, nullptr, 0, 0, OutSub::Inner);
+    reduce_case<double, uint64_t>(gpu, REDUCE_MAX, REDUCE_DOUBLES, nullptr, 0, 0, OutSub::Scattered);
+    // the app's own callbacks, run on the host
+    reduce_case<int32_t, int32_t>(gpu, REDUCE_ADD, REDUCE_INTS, axpy3_reduction, 1, 0, OutSub::Whole);
+    reduce_case<int32_t, int32_t>(gpu, REDUCE_BITWISE_OR, REDUCE_INTS, or_reduction, 2, 0, OutSub::Whole);
+    reduce_case<int32_t, int32_t>(gpu, REDUCE_ADD, REDUCE_INTS, axpy3_reduction, 1, 0, OutSub::Scattered);
+    // subtasks subscribing different ranges: the task fails before it runs
+    reduce_case<int32_t, int32_t>(gpu, REDUCE_ADD, REDUCE_INTS, nullptr, 0, 0, OutSub::Mismatched);
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
     if (argc < 2) {
         std::printf("usage: rt_selftest <views_cpu|views_cpu_compact|views_gpu|views_gpu_compact|chain|"
-                    "write_through|mix|errors|timeout>\n");
+                    "write_through|mix|errors|timeout|reduce_cpu|reduce_gpu>\n");
         return 2;
     }
     g_test = argv[1];
@@ -293,6 +500,8 @@ int main(int argc, char** argv) {
     else if (g_test == "mix") test_mix();
     else if (g_test == "errors") test_errors();
     else if (g_test == "timeout") test_timeout();
+    else if (g_test == "reduce_cpu") test_reduce(false);
+    else if (g_test == "reduce_gpu") test_reduce(true);
     else CHECK(false, "unknown test");
     CHECK(pmFinalize() == pmSuccess, "finalize");
     std::printf("PASS %s\n", g_test.c_str());

@@ -18,6 +18,7 @@ c_int64 = ctypes.c_int64
 c_size_t = ctypes.c_size_t
 
 PMB_SUCCESS = 0
+PMB_INVALID_INDEX = 7
 PMB_IMGF_WRAP = 0
 PMB_IMGF_CLAMP = 1
 PMB_IMGF_MAX_ITEMS = 256
@@ -89,6 +90,8 @@ _SIGS = {
     "pmb_device_synchronize": (c_int, []),
     "pmb_mempool_retain": (c_int, [c_int]),
     "pmb_mempool_reserve": (c_int, [c_int, c_size_t, c_void_p]),
+    "pmb_reduce_element_size": (c_size_t, [c_int]),
+    "pmb_reduce_elementwise": (c_int, [c_int, c_int, c_void_p, c_void_p, c_int, c_size_t, c_int, c_void_p]),
     "pmb_mempool_trim": (c_int, [c_int, c_size_t]),
     "pmb_mem_available": (c_int, [c_int, ctypes.POINTER(c_size_t)]),
     "pmb_graph_begin_capture": (c_int, [c_void_p]),

@@ -239,3 +239,19 @@ def lu_residual(d_A0, d_LU, stream=None) -> float:
                                               _dev_ptr(sums), _stream_ptr(stream)))
     s = sums.cpu().numpy()
     return float(np.sqrt(s[0] / s[1])) if s[1] > 0 else 0.0
+
+
+# pmReductionOpType / pmReductionDataType values (pmPublicUtilities.h)
+REDUCE_OPS = ("ADD", "MIN", "MAX", "PRODUCT", "LOGICAL_AND", "BITWISE_AND", "LOGICAL_OR", "BITWISE_OR",
+              "LOGICAL_XOR", "BITWISE_XOR")
+REDUCE_TYPES = {"int32": 0, "uint32": 1, "int64": 2, "uint64": 3, "float32": 4, "float64": 5}
+
+
+def reduce_elementwise(op: int, type_code: int, d_dst, srcs, count: int, init_from_first: bool = True,
+                       stream=None):
+    """Fold the device arrays `srcs` (in order) into d_dst over `count` elements
+    with a built-in REDUCE_* operation (pmb_reduce_elementwise)."""
+    ptrs = (ctypes.c_void_p * len(srcs))(*[_dev_ptr(s) for s in srcs])
+    capi.check(capi.lib().pmb_reduce_elementwise(op, type_code, _dev_ptr(d_dst), ctypes.cast(ptrs, ctypes.c_void_p),
+                                                 len(srcs), count, int(init_from_first), _stream_ptr(stream)))
+    return d_dst

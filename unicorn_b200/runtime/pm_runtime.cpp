@@ -221,9 +221,12 @@ struct Controller {
     std::map<std::string, std::pair<void*, size_t>> files;
 };
 
+// Never destroyed: an app that exits without pmFinalize (exit() on an error
+// path) must not run the destructors of condition variables the stub and
+// completer threads still wait on, which would block the exit.
 static Controller& ctl() {
-    static Controller c;
-    return c;
+    static Controller* c = new Controller;
+    return *c;
 }
 
 void register_batch(pmSubtaskCallback_GPU_Custom callback, BatchFn batch) {
@@ -549,6 +552,262 @@ static pmStatus run_dd(Task* t, const pmDeviceInfo& dev) {
     return pmSuccess;
 }
 
+// ---------------------------------------------------------------------------
+// subtask reduction (pmCallbacks::dataReduction)
+//
+// Every subtask that writes a writable address space of such a task writes a
+// private copy of its subscribed range; when all subtasks have run, the
+// copies are folded in subtask-id order and the written bytes committed to
+// the address space (pmReducer.cpp:1073-1296 reduces pairs of subtask shadow
+// memories over their unified read-write subscription and commits the
+// surviving one's write subscription).  Built-in REDUCE_* callbacks fold on
+// the device for GPU tasks (one pmb_reduce_elementwise pass); the app's own
+// callback runs on the host over host copies, pairwise into the first
+// subtask, as the reference calls it.
+
+static bool writable(pmMemType m) { return m != READ_ONLY && m != READ_ONLY_LAZY; }
+
+template <int OP, int TYPE>
+static pmStatus builtin_reduction(pmTaskInfo ti, pmDeviceInfo d1, pmSubtaskInfo s1, pmDeviceInfo d2, pmSubtaskInfo s2) {
+    return pmReduceSubtasks(ti.taskHandle, d1.deviceHandle, s1.subtaskId, s1.splitInfo, d2.deviceHandle, s2.subtaskId,
+                            s2.splitInfo, static_cast<pmReductionOpType>(OP), static_cast<pmReductionDataType>(TYPE));
+}
+
+#define PMR_REDUCTION_ROW(op)                                                                              \
+    {builtin_reduction<op, 0>, builtin_reduction<op, 1>, builtin_reduction<op, 2>, builtin_reduction<op, 3>, \
+     builtin_reduction<op, 4>, builtin_reduction<op, 5>}
+// [pmReductionOpType][pmReductionDataType] (pmPublicDefinitions.cpp:749-815)
+static const pmDataReductionCallback kBuiltinReduction[10][6] = {
+    PMR_REDUCTION_ROW(0), PMR_REDUCTION_ROW(1), PMR_REDUCTION_ROW(2), PMR_REDUCTION_ROW(3), PMR_REDUCTION_ROW(4),
+    PMR_REDUCTION_ROW(5), PMR_REDUCTION_ROW(6), PMR_REDUCTION_ROW(7), PMR_REDUCTION_ROW(8), PMR_REDUCTION_ROW(9)};
+#undef PMR_REDUCTION_ROW
+
+static bool builtin_of(pmDataReductionCallback cb, int* op, int* type) {
+    for (int o = 0; o < 10; ++o)
+        for (int d = 0; d < 6; ++d)
+            if (kBuiltinReduction[o][d] == cb) {
+                *op = o;
+                *type = d;
+                return true;
+            }
+    return false;
+}
+
+// Bitwise operations on floats and doubles act on the values converted to
+// 32- / 64-bit unsigned integers; LOGICAL_XOR is a != b (pmReducer.cpp:408-423, 590-700).
+template <typename T, typename B>
+static void host_fold(int op, T* a, const T* b, size_t n) {
+    switch (op) {
+        case REDUCE_ADD: for (size_t i = 0; i < n; ++i) a[i] += b[i]; break;
+        case REDUCE_MIN: for (size_t i = 0; i < n; ++i) a[i] = std::min(a[i], b[i]); break;
+        case REDUCE_MAX: for (size_t i = 0; i < n; ++i) a[i] = std::max(a[i], b[i]); break;
+        case REDUCE_PRODUCT: for (size_t i = 0; i < n; ++i) a[i] *= b[i]; break;
+        case REDUCE_LOGICAL_AND: for (size_t i = 0; i < n; ++i) a[i] = (a[i] && b[i]); break;
+        case REDUCE_BITWISE_AND: for (size_t i = 0; i < n; ++i) a[i] = static_cast<T>(static_cast<B>(a[i]) & static_cast<B>(b[i])); break;
+        case REDUCE_LOGICAL_OR: for (size_t i = 0; i < n; ++i) a[i] = (a[i] || b[i]); break;
+        case REDUCE_BITWISE_OR: for (size_t i = 0; i < n; ++i) a[i] = static_cast<T>(static_cast<B>(a[i]) | static_cast<B>(b[i])); break;
+        case REDUCE_LOGICAL_XOR: for (size_t i = 0; i < n; ++i) a[i] = (a[i] != b[i]); break;
+        default: for (size_t i = 0; i < n; ++i) a[i] = static_cast<T>(static_cast<B>(a[i]) ^ static_cast<B>(b[i])); break;
+    }
+}
+
+static pmStatus host_reduce(int op, int type, void* a, const void* b, size_t bytes) {
+    if (op < 0 || op >= MAX_REDUCTION_OP_TYPES) return fail(pmInvalidIndex, "unknown reduction operation %d", op);
+    const size_t es = pmb_reduce_element_size(type);
+    if (!es) return fail(pmInvalidIndex, "unknown reduction data type %d", type);
+    const size_t n = bytes / es;
+    switch (type) {
+        case REDUCE_INTS: host_fold<int32_t, int32_t>(op, static_cast<int32_t*>(a), static_cast<const int32_t*>(b), n); break;
+        case REDUCE_UNSIGNED_INTS: host_fold<uint32_t, uint32_t>(op, static_cast<uint32_t*>(a), static_cast<const uint32_t*>(b), n); break;
+        case REDUCE_LONGS: host_fold<int64_t, int64_t>(op, static_cast<int64_t*>(a), static_cast<const int64_t*>(b), n); break;
+        case REDUCE_UNSIGNED_LONGS: host_fold<uint64_t, uint64_t>(op, static_cast<uint64_t*>(a), static_cast<const uint64_t*>(b), n); break;
+        case REDUCE_FLOATS: host_fold<float, uint32_t>(op, static_cast<float*>(a), static_cast<const float*>(b), n); break;
+        default: host_fold<double, uint64_t>(op, static_cast<double*>(a), static_cast<const double*>(b), n); break;
+    }
+    return pmSuccess;
+}
+
+// The reducible address spaces of a task and the one range their writing
+// subtasks subscribe.  The reference reduces shadow memories positionally
+// and asserts equal lengths (pmReducer.cpp:1290); here the ranges must be
+// equal, so positions are addresses.
+static pmStatus plan_reduction(Task* t) {
+    t->reduce.clear();
+    t->reduce_op = t->reduce_type = -1;
+    const pmDataReductionCallback cb = t->callbacks->cb.dataReduction;
+    if (!cb) return pmSuccess;
+    builtin_of(cb, &t->reduce_op, &t->reduce_type);
+    for (size_t i = 0; i < t->spaces.size(); ++i) {
+        if (!writable(t->mem[i].memType)) continue;
+        ReduceSpace rs;
+        rs.index = i;
+        for (const Subtask& s : t->subtasks) {
+            const SubtaskMem& m = s.mem[i];
+            size_t rlo, rhi, wlo, whi;
+            consolidated(m.reads, rlo, rhi);
+            consolidated(m.writes, wlo, whi);
+            if (whi <= wlo) continue;
+            const size_t lo = rhi > rlo ? std::min(rlo, wlo) : wlo, hi = rhi > rlo ? std::max(rhi, whi) : whi;
+            if (rs.subtasks.empty()) {
+                rs.lo = lo, rs.hi = hi, rs.wlo = wlo, rs.whi = whi;
+            } else if (lo != rs.lo || hi != rs.hi || wlo != rs.wlo || whi != rs.whi) {
+                return fail(pmInvalidIndex,
+                            "reduction over address space %zu: subtasks %zu and %lu subscribe different ranges", i,
+                            rs.subtasks.front(), s.id);
+            }
+            rs.subtasks.push_back(s.id);
+        }
+        if (rs.subtasks.empty()) continue;
+        if (t->mem[i].subscriptionVisibilityType == SUBSCRIPTION_COMPACT)
+            return fail(pmInvalidIndex, "reduction over address space %zu needs a natural view", i);
+        t->reduce.push_back(rs);
+    }
+    return pmSuccess;
+}
+
+static size_t reduction_bytes(const Task* t) {
+    size_t b = 0;
+    for (const ReduceSpace& rs : t->reduce) b += (rs.hi - rs.lo) * rs.subtasks.size();
+    return b;
+}
+
+// memInfo of a reducible address space over a subtask's private copy.
+static pmMemInfo shadow_view(const SubtaskMem& m, const ReduceSpace& rs, char* base) {
+    pmMemInfo mi;
+    mi.visibilityType = SUBSCRIPTION_NATURAL;
+    size_t rlo, rhi;
+    consolidated(m.reads, rlo, rhi);
+    mi.ptr = base;
+    mi.readPtr = rhi > rlo ? base + (rlo - rs.lo) : nullptr;
+    mi.writePtr = base + (rs.wlo - rs.lo);
+    mi.length = rs.hi - rs.lo;
+    return mi;
+}
+
+// Folds the host copies of every reducible address space into the first
+// writing subtask's: the built-in operation in id order, or the app's
+// callback called pairwise (first, k) as pmReducer calls it.
+static pmStatus reduce_host_shadows(Task* t, const pmDeviceInfo& dev) {
+    if (t->reduce.empty()) return pmSuccess;
+    if (t->reduce_op >= 0) {
+        for (const ReduceSpace& rs : t->reduce) {
+            std::vector<char>& dst = t->subtasks[rs.subtasks.front()].host_shadow[rs.index];
+            for (size_t k = 1; k < rs.subtasks.size(); ++k) {
+                const std::vector<char>& src = t->subtasks[rs.subtasks[k]].host_shadow[rs.index];
+                const pmStatus st = host_reduce(t->reduce_op, t->reduce_type, dst.data(), src.data(), dst.size());
+                if (st != pmSuccess) return st;
+            }
+        }
+        return pmSuccess;
+    }
+    // The app's callback sees every reducible space of both subtasks; the
+    // subtasks it folds are those that wrote any of them.
+    std::vector<size_t> order;
+    for (const ReduceSpace& rs : t->reduce) order.insert(order.end(), rs.subtasks.begin(), rs.subtasks.end());
+    std::sort(order.begin(), order.end());
+    order.erase(std::unique(order.begin(), order.end()), order.end());
+    auto info_of = [&](size_t id) {
+        pmSubtaskInfo info;
+        info.subtaskId = id;
+        info.memCount = static_cast<uint>(t->spaces.size());
+        Subtask& s = t->subtasks[id];
+        for (const ReduceSpace& rs : t->reduce)
+            if (!s.host_shadow[rs.index].empty())
+                info.memInfo[rs.index] = shadow_view(s.mem[rs.index], rs, s.host_shadow[rs.index].data());
+        return info;
+    };
+    const pmSubtaskInfo first = info_of(order.front());
+    for (size_t k = 1; k < order.size(); ++k) {
+        const pmStatus st = t->callbacks->cb.dataReduction(t->info, dev, first, dev, info_of(order[k]));
+        if (st != pmSuccess)
+            return fail(st, "reduction callback of subtasks %zu and %zu returned %d", order.front(), order[k],
+                        static_cast<int>(st));
+    }
+    return pmSuccess;
+}
+
+// Commits the first writing subtask's host copy (its write records) to the
+// address space's host copy; the device mirror no longer holds those bytes.
+static pmStatus commit_host_shadows(Task* t) {
+    for (const ReduceSpace& rs : t->reduce) {
+        AddressSpace* a = t->spaces[rs.index];
+        const Subtask& s0 = t->subtasks[rs.subtasks.front()];
+        const std::vector<char>& sh = s0.host_shadow[rs.index];
+        std::lock_guard<std::mutex> g(a->mu);
+        const pmStatus hs = ensure_host(a);
+        if (hs != pmSuccess) return hs;
+        for (const Record& r : s0.mem[rs.index].writes)
+            for (size_t q = 0; q < std::max<size_t>(r.count, 1); ++q) {
+                const size_t off = r.offset + q * r.step;
+                memcpy(a->host + off, sh.data() + (off - rs.lo), r.size);
+                a->dev_valid.remove(off, off + r.size);
+                a->host_stale.remove(off, off + r.size);
+            }
+    }
+    for (Subtask& s : t->subtasks) s.host_shadow.clear();
+    return pmSuccess;
+}
+
+// GPU tasks: fold the device copies on `stream` (built-in operations) or
+// bring them to the host for the app's callback, then free them.
+static pmStatus reduce_device_shadows(Task* t, void* stream) {
+    if (t->reduce.empty()) return pmSuccess;
+    if (t->reduce_op >= 0) {
+        const size_t es = pmb_reduce_element_size(t->reduce_type);
+        for (const ReduceSpace& rs : t->reduce) {
+            AddressSpace* a = t->spaces[rs.index];
+            const Subtask& s0 = t->subtasks[rs.subtasks.front()];
+            const SubtaskMem& m0 = s0.mem[rs.index];
+            std::vector<const void*> srcs;
+            for (size_t id : rs.subtasks) srcs.push_back(t->subtasks[id].dev_shadow[rs.index]);
+            RangeSet w;
+            for (const Record& r : m0.writes) add_record(w, r);
+            std::lock_guard<std::mutex> g(a->mu);
+            // Contiguous, element-aligned writes fold straight into the mirror;
+            // otherwise into the first copy, whose written records are then copied.
+            if (w.covers(rs.wlo, rs.whi) && rs.wlo % es == 0 && (rs.wlo - rs.lo) % es == 0 &&
+                (rs.whi - rs.wlo) % es == 0) {
+                for (const void*& p : srcs) p = static_cast<const char*>(p) + (rs.wlo - rs.lo);
+                PMR_DEV(pmb_reduce_elementwise(t->reduce_op, t->reduce_type, a->dev + rs.wlo, srcs.data(),
+                                               static_cast<int>(srcs.size()), (rs.whi - rs.wlo) / es, 1, stream));
+            } else {
+                char* s0p = s0.dev_shadow[rs.index];
+                if (srcs.size() > 1)
+                    PMR_DEV(pmb_reduce_elementwise(t->reduce_op, t->reduce_type, s0p, srcs.data() + 1,
+                                                   static_cast<int>(srcs.size() - 1), (rs.hi - rs.lo) / es, 0, stream));
+                for (auto& piece : w.map())
+                    PMR_DEV(pmb_memcpy_async(a->dev + piece.first, s0p + (piece.first - rs.lo),
+                                             piece.second - piece.first, PMB_D2D, stream));
+            }
+            for (const Record& r : m0.writes) {
+                add_record(a->dev_valid, r);
+                add_record(a->host_stale, r);
+            }
+        }
+    } else {
+        PMR_DEV(pmb_stream_synchronize(stream));
+        for (const ReduceSpace& rs : t->reduce)
+            for (size_t id : rs.subtasks) {
+                Subtask& s = t->subtasks[id];
+                s.host_shadow.resize(t->spaces.size());
+                s.host_shadow[rs.index].resize(rs.hi - rs.lo);
+                PMR_DEV(pmb_memcpy_async(s.host_shadow[rs.index].data(), s.dev_shadow[rs.index], rs.hi - rs.lo,
+                                         PMB_D2H, stream));
+            }
+        PMR_DEV(pmb_stream_synchronize(stream));
+        pmStatus st = reduce_host_shadows(t, ctl().gpu_info);
+        if (st == pmSuccess) st = commit_host_shadows(t);
+        if (st != pmSuccess) return st;
+    }
+    for (Subtask& s : t->subtasks)
+        for (char*& p : s.dev_shadow)
+            if (p) {
+                PMR_DEV(pmb_free_async(p, stream));
+                p = nullptr;
+            }
+    return pmSuccess;
+}
+
 // Admission by free device memory: the task's missing mirrors and reserved
 // subtask memory must fit beside the reserve, after idle mirrors are evicted.
 static bool admit(Task* t, size_t* need_out) {
@@ -556,6 +815,7 @@ static bool admit(Task* t, size_t* need_out) {
     for (AddressSpace* a : t->spaces)
         if (!a->dev) need += a->length;
     for (Subtask& s : t->subtasks) need += s.reserved;
+    need += reduction_bytes(t);
     *need_out = need;
     return need == 0 || make_room(need, t->spaces);
 }
@@ -610,7 +870,10 @@ static pmStatus stage_and_launch_gpu(Task* t) {
             if (t->views[i] != SUBSCRIPTION_NATURAL) batch = nullptr;
         for (Subtask& s : t->subtasks)
             if (s.reserved || !s.scratch.empty()) batch = nullptr;
+        if (!t->reduce.empty()) batch = nullptr;  // each subtask writes its own copy
     }
+    std::vector<const ReduceSpace*> reducible(ns, nullptr);
+    for (const ReduceSpace& rs : t->reduce) reducible[rs.index] = &rs;
 
     std::vector<void*> events;
     auto new_event = [&]() -> void* {
@@ -628,6 +891,7 @@ static pmStatus stage_and_launch_gpu(Task* t) {
         info.subtaskId = s.id;
         info.memCount = static_cast<uint>(ns);
         s.dev_compact.assign(ns, nullptr);
+        s.dev_shadow.assign(ns, nullptr);
         std::vector<Compact> compacts(ns);
         // ---- stage (copy stream) ----
         for (size_t i = 0; i < ns; ++i) {
@@ -646,6 +910,18 @@ static pmStatus stage_and_launch_gpu(Task* t) {
             const bool has_r = rhi > rlo, has_w = whi > wlo;
             if (!has_r && !has_w) {
                 info.memInfo[i] = mi;
+                continue;
+            }
+            if (has_w && reducible[i]) {
+                // private copy of the subscribed range, holding the read bytes
+                const ReduceSpace& rs = *reducible[i];
+                void* p = nullptr;
+                PMR_DEV(pmb_malloc_async(&p, rs.hi - rs.lo, c.copy_stream));
+                s.dev_shadow[i] = static_cast<char*>(p);
+                c.dev_held += static_cast<int64_t>(rs.hi - rs.lo);  // returned when the task finishes
+                t->reserved_held += rs.hi - rs.lo;
+                if (has_r) PMR_DEV(pmb_memcpy_async(p, a->dev + rs.lo, rs.hi - rs.lo, PMB_D2D, c.copy_stream));
+                info.memInfo[i] = shadow_view(m, rs, s.dev_shadow[i]);
                 continue;
             }
             if (t->views[i] == SUBSCRIPTION_NATURAL) {
@@ -719,7 +995,7 @@ static pmStatus stage_and_launch_gpu(Task* t) {
         for (size_t i = 0; i < ns; ++i) {
             AddressSpace* a = t->spaces[i];
             const SubtaskMem& m = s.mem[i];
-            if (m.writes.empty()) continue;
+            if (m.writes.empty() || s.dev_shadow[i]) continue;  // private copies are folded after the join
             std::lock_guard<std::mutex> g(a->mu);
             if (t->views[i] == SUBSCRIPTION_COMPACT) {
                 for (const Record& r : m.writes) {
@@ -783,6 +1059,10 @@ static pmStatus stage_and_launch_gpu(Task* t) {
             if (used_stream[k]) js = join_on(c.streams[k]);
         if (js != pmSuccess) return js;
     }
+    {
+        const pmStatus rs = reduce_device_shadows(t, join);
+        if (rs != pmSuccess) return rs;
+    }
     // Write-back at task end: all stale bytes with the cache disabled (the
     // mirrors are then dropped); with eager write-back (PMB_EAGER_WRITEBACK=1)
     // the bytes of the address spaces this task writes, on the task's own
@@ -843,6 +1123,19 @@ static pmStatus run_cpu_task(Task* t) {
         st = fetch_range(a, 0, a->length);
         if (st != pmSuccess) return st;
     }
+    // Private copies of the reducible address spaces, holding the bytes of
+    // the address space (pmSubscriptionManager.cpp:1530-1537 fills them from
+    // the read subscriptions).
+    std::vector<const ReduceSpace*> reducible(ns, nullptr);
+    for (const ReduceSpace& rs : t->reduce) {
+        reducible[rs.index] = &rs;
+        const char* src = t->spaces[rs.index]->host;
+        for (size_t id : rs.subtasks) {
+            Subtask& s = t->subtasks[id];
+            s.host_shadow.resize(ns);
+            s.host_shadow[rs.index].assign(src + rs.lo, src + rs.hi);
+        }
+    }
     const unsigned nthreads = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(),
                                                               static_cast<unsigned>(t->subtasks.size())));
     std::atomic<size_t> next(0);
@@ -871,6 +1164,10 @@ static pmStatus run_cpu_task(Task* t) {
                 pmMemInfo mi;
                 mi.visibilityType = t->mem[i].subscriptionVisibilityType == SUBSCRIPTION_COMPACT ? SUBSCRIPTION_COMPACT
                                                                                                : SUBSCRIPTION_NATURAL;
+                if (has_w && reducible[i]) {
+                    info.memInfo[i] = shadow_view(m, *reducible[i], s.host_shadow[i].data());
+                    continue;
+                }
                 if (has_r || has_w) {
                     if (mi.visibilityType == SUBSCRIPTION_NATURAL) {
                         const size_t lo = has_r && has_w ? std::min(rlo, wlo) : (has_r ? rlo : wlo);
@@ -911,6 +1208,11 @@ static pmStatus run_cpu_task(Task* t) {
     for (unsigned k = 1; k < nthreads; ++k) pool.emplace_back(worker);
     worker();
     for (auto& th : pool) th.join();
+    if (err.load() == pmSuccess && !t->reduce.empty()) {
+        pmStatus rs = reduce_host_shadows(t, ctl().cpu_info);
+        if (rs == pmSuccess) rs = commit_host_shadows(t);
+        if (rs != pmSuccess) return rs;
+    }
     for (size_t i = 0; i < ns; ++i) {
         AddressSpace* a = t->spaces[i];
         std::lock_guard<std::mutex> g(a->mu);
@@ -927,6 +1229,12 @@ static pmStatus run_cpu_task(Task* t) {
 
 static void finish_task(Task* t, pmStatus st, const std::string& msg) {
     Controller& c = ctl();
+    for (Subtask& s : t->subtasks) {  // a failed task's private copies (its work has drained)
+        for (char* p : s.dev_shadow)
+            if (p) pmb_free_async(p, c.copy_stream);
+        s.dev_shadow.clear();
+        s.host_shadow.clear();
+    }
     c.dev_held -= static_cast<int64_t>(t->reserved_held);
     t->reserved_held = 0;
     for (AddressSpace* a : t->spaces) {
@@ -969,6 +1277,7 @@ static void stub_main() {
             continue;
         }
         pmStatus st = run_dd(t, t->on_gpu ? c.gpu_info : c.cpu_info);
+        if (st == pmSuccess) st = plan_reduction(t);
         if (st == pmSuccess) {
             if (t->on_gpu) {
                 // Admission: a free slot, then device memory.  While tasks are in
@@ -1465,11 +1774,39 @@ pmRedistributionMetadata* pmGetRedistributionMetadata(pmTaskHandle, uint, ulong*
     return nullptr;
 }
 
-pmDataReductionCallback pmGetSubtaskReductionCallbackImpl(pmReductionOpType, pmReductionDataType) { return nullptr; }
+// pmPublicDefinitions.cpp:779-815: the built-in callback of an (operation,
+// data type) pair, NULL for values outside the enums.
+pmDataReductionCallback pmGetSubtaskReductionCallbackImpl(pmReductionOpType pOperation, pmReductionDataType pDataType) {
+    if (pOperation < 0 || pOperation >= MAX_REDUCTION_OP_TYPES || pDataType < 0 || pDataType >= MAX_REDUCTION_DATA_TYPES)
+        return nullptr;
+    return kBuiltinReduction[pOperation][pDataType];
+}
 
-pmStatus pmReduceSubtasks(pmTaskHandle, pmDeviceHandle, unsigned long, pmSplitInfo&, pmDeviceHandle, unsigned long,
-                          pmSplitInfo&, pmReductionOpType, pmReductionDataType) {
-    return fail(pmStatusUnavailable, "subtask reduction is not supported by the B200 runtime");
+// Folds subtask 2's private copies into subtask 1's (host copies; called from
+// reduction callbacks), over every reducible address space both wrote
+// (pmReducer::ReduceSubtasks, pmReducer.cpp:1073-1296).
+pmStatus pmReduceSubtasks(pmTaskHandle pTaskHandle, pmDeviceHandle, unsigned long pSubtask1Id, pmSplitInfo&,
+                          pmDeviceHandle, unsigned long pSubtask2Id, pmSplitInfo&, pmReductionOpType pOperation,
+                          pmReductionDataType pDataType) {
+    Task* t = task_of(pTaskHandle);
+    if (!t) return fail(pmInvalidIndex, "unknown task handle");
+    if (pSubtask1Id >= t->subtasks.size() || pSubtask2Id >= t->subtasks.size())
+        return fail(pmInvalidIndex, "subtask %lu or %lu out of range", pSubtask1Id, pSubtask2Id);
+    Subtask& s1 = t->subtasks[pSubtask1Id];
+    Subtask& s2 = t->subtasks[pSubtask2Id];
+    for (const ReduceSpace& rs : t->reduce) {
+        const size_t i = rs.index;
+        if (s1.host_shadow.size() <= i || s2.host_shadow.size() <= i || s1.host_shadow[i].empty() ||
+            s2.host_shadow[i].empty())
+            return fail(pmInvalidIndex, "subtasks %lu and %lu have no reduction copies of address space %zu",
+                        pSubtask1Id, pSubtask2Id, i);
+        if (s1.host_shadow[i].size() != s2.host_shadow[i].size())
+            return fail(pmInvalidIndex, "reduction copies of address space %zu differ in length", i);
+        const pmStatus st = host_reduce(pOperation, pDataType, s1.host_shadow[i].data(), s2.host_shadow[i].data(),
+                                        s1.host_shadow[i].size());
+        if (st != pmSuccess) return st;
+    }
+    return pmSuccess;
 }
 
 void* pmGetMappedFile(const char* pPath) {

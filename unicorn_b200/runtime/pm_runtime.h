@@ -80,6 +80,21 @@ struct Subtask {
     std::vector<void*> dev_compact;  // per address space
     pmSubtaskInfo info;              // device view handed to the GPU callback
     pmStatus status = pmSuccess;
+    // Private copies of the reducible address spaces (tasks with a
+    // dataReduction callback), over the range every subtask subscribes:
+    // device copies for GPU subtasks, host copies on the CPU and for
+    // reduction callbacks that run on the host.  Per task address space.
+    std::vector<char*> dev_shadow;
+    std::vector<std::vector<char>> host_shadow;
+};
+
+// One writable address space of a task with a dataReduction callback: the
+// byte range [lo, hi) every writing subtask subscribes (reads and writes),
+// the written part [wlo, whi), and the writing subtasks in id order.
+struct ReduceSpace {
+    size_t index = 0;
+    size_t lo = 0, hi = 0, wlo = 0, whi = 0;
+    std::vector<size_t> subtasks;
 };
 
 struct CallbackSet {
@@ -106,7 +121,9 @@ struct Task {
     bool on_gpu = false;
     void* done_event = nullptr;
     double t_submit = 0, t_start = 0, t_end = 0;
-    size_t reserved_held = 0;    // reserved subtask memory counted against the device budget
+    size_t reserved_held = 0;    // reserved subtask memory and reduction copies counted against the device budget
+    std::vector<ReduceSpace> reduce;  // reducible address spaces (dataReduction tasks)
+    int reduce_op = -1, reduce_type = -1;  // built-in REDUCE_* callback, else -1 (the app's own callback)
     double deadline = 0;         // 0: none
     std::atomic<int> state{0};   // 0 queued, 1 running, 2 done
     pmStatus status = pmSuccess;
