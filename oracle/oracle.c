@@ -230,8 +230,9 @@ void orc_lu_crout_f64(double* a, int n, long ld) {
 /* doubles act on the values converted to uint32 / uint64                    */
 /* (pmReducer.cpp:408-423); LOGICAL_XOR is a != b.  op / type take the       */
 /* pmReductionOpType / pmReductionDataType values.  The reducer is a member  */
-/* of the reference runtime and does not compile on its own: this            */
-/* restatement is checked against hand-computed cases in the tests only.     */
+/* of the reference runtime and does not compile on its own: parity          */
+/* unpinned -- this restatement is checked against hand-computed cases in    */
+/* the tests only.                                                           */
 /* ------------------------------------------------------------------------ */
 #define ORC_FOLD(T, B)                                                                        \
     do {                                                                                      \
