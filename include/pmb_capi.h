@@ -293,6 +293,35 @@ int pmb_csr_by_destination(const uint32_t* d_src, const uint32_t* d_dst, uint32_
                            uint32_t* d_row_ptr, uint32_t* d_col, uint32_t* d_out_degree, void* d_scratch,
                            size_t scratch_bytes, void* stream);
 
+/* The reference's web-dump pages (pageRank.cpp:53-111, the page files
+ * mapped by pmMapFiles and read by pageRank_cpu / pageRank_cudaLaunchFunc):
+ * per page a u32 out-link count, then max_outlinks u32 slots whose first
+ * `count` hold 1-based target ids; pages max_outlinks + 1 words apart.
+ *
+ * pmb_csr_from_webdump: n_pages pages (sources 0..n_pages-1, n_pages <=
+ * n_vertices) -> CSR by destination over n_vertices rows, as
+ * pmb_csr_by_destination builds it (edges of one destination in page order).
+ * n_edges must be the sum of the counts.  Error word of d_scratch
+ * (pmb_scratch_error): bit 2 a target outside [1, n_vertices] (dropped) or a
+ * slot left unfilled, bit 4 a count above max_outlinks (clamped), bit 8 more
+ * edges than n_edges (dropped).  Replaces readWebPagesFile +
+ * the padded device copy of singleGpuPageRank (pageRankCUDA.cu:166-190). */
+size_t pmb_webdump_csr_scratch_bytes(uint32_t n_pages, uint32_t n_vertices, uint64_t n_edges);
+int pmb_csr_from_webdump(const uint32_t* d_dump, uint32_t n_pages, uint32_t max_outlinks, uint32_t n_vertices,
+                         uint64_t n_edges, uint32_t* d_row_ptr, uint32_t* d_col, uint32_t* d_out_degree,
+                         void* d_scratch, size_t scratch_bytes, void* stream);
+
+/* One push step of the reference over n_pages device-resident web-dump pages
+ * (zeroInit + pageRank_cuda, pageRankCUDA.cu:46-76): d_out[0..n_vertices) is
+ * zeroed, then every page with count > 0 adds (damping * r) / count to each of
+ * its targets, r = d_rank_in[page] or initial_rank when d_rank_in is NULL.
+ * fp32 adds in L2 in no fixed order (as the reference's atomics).  A target
+ * outside [1, n_vertices] is skipped and a count above max_outlinks clamped;
+ * either sets bit 2 of *d_err when d_err is not NULL. */
+int pmb_webdump_push(const uint32_t* d_dump, uint32_t n_pages, uint32_t max_outlinks, const float* d_rank_in,
+                     float initial_rank, float damping, float* d_out, uint32_t n_vertices, uint32_t* d_err,
+                     void* stream);
+
 /* Edge-slice partition of a CSR graph (once per graph). */
 size_t pmb_pagerank_plan_bytes(uint32_t n_vertices, uint64_t n_edges);
 int pmb_pagerank_plan(const uint32_t* d_row_ptr, uint32_t n_vertices, uint64_t n_edges, void* d_plan,

@@ -91,6 +91,11 @@ _SIGS = {
     "pmb_mempool_retain": (c_int, [c_int]),
     "pmb_mempool_reserve": (c_int, [c_int, c_size_t, c_void_p]),
     "pmb_reduce_element_size": (c_size_t, [c_int]),
+    "pmb_webdump_csr_scratch_bytes": (c_size_t, [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64]),
+    "pmb_csr_from_webdump": (c_int, [c_void_p, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64,
+                                     c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_void_p]),
+    "pmb_webdump_push": (c_int, [c_void_p, ctypes.c_uint32, ctypes.c_uint32, c_void_p, ctypes.c_float,
+                                 ctypes.c_float, c_void_p, ctypes.c_uint32, c_void_p, c_void_p]),
     "pmb_reduce_elementwise": (c_int, [c_int, c_int, c_void_p, c_void_p, c_int, c_size_t, c_int, c_void_p]),
     "pmb_mempool_trim": (c_int, [c_int, c_size_t]),
     "pmb_mem_available": (c_int, [c_int, ctypes.POINTER(c_size_t)]),

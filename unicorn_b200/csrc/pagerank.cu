@@ -35,6 +35,9 @@ extern "C" int pmb_radix_sort_pairs_u32(uint32_t* d_keys, uint32_t* d_alt, uint3
                                         size_t n, int begin_bit, int end_bit, int bits_per_pass, void* d_scratch,
                                         size_t scratch_bytes, void* stream);
 extern "C" size_t pmb_radix_sort_scratch_bytes(size_t n, int bits_per_pass);
+extern "C" size_t pmb_scan_scratch_bytes(size_t n);
+extern "C" int pmb_inclusive_scan_u32_u64(const uint32_t* d_in, uint64_t* d_out, size_t n, void* d_scratch,
+                                          size_t scratch_bytes, void* stream);
 
 namespace {
 
@@ -275,6 +278,84 @@ __global__ void fixup_kernel(const int32_t* __restrict__ cont, uint32_t n_slices
     out[v] = finish(r, static_cast<uint32_t>(v), outdeg, damping, last != 0);
 }
 
+// ---------------------------------------------------------------------------
+// The reference's web-dump pages (pageRank.cpp:53-111): per page a u32
+// out-link count followed by max_outlinks u32 slots, the first `count` of
+// them 1-based target ids; pages are `stride` = max_outlinks + 1 words apart.
+
+// counts[p] = the page's out-link count (clamped to the slots; bit 3 of *err
+// when a count exceeds them).
+__global__ void webdump_counts_kernel(const uint32_t* __restrict__ dump, uint32_t n_pages, uint32_t stride,
+                                      uint32_t* __restrict__ counts, uint32_t* __restrict__ err) {
+    for (uint64_t p = blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x; p < n_pages;
+         p += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        uint32_t c = dump[p * stride];
+        if (c > stride - 1) {
+            c = stride - 1;
+            atomicOr(err, 4u);
+        }
+        counts[p] = c;
+    }
+}
+
+// Edge list in page order: page p's edges at [incl[p] - counts[p], incl[p]),
+// (source p, 0-based target).  Targets outside [1, n_vertices] become
+// n_vertices, which the CSR builder drops (and flags); positions at or past
+// n_edges are skipped and set bit 4 of *err.  Eight lanes per page.
+__global__ void webdump_edges_kernel(const uint32_t* __restrict__ dump, uint32_t n_pages, uint32_t stride,
+                                     const uint32_t* __restrict__ counts, const uint64_t* __restrict__ incl,
+                                     uint32_t n_vertices, uint64_t n_edges, uint32_t* __restrict__ src,
+                                     uint32_t* __restrict__ dst, uint32_t* __restrict__ err) {
+    const uint64_t groups = static_cast<uint64_t>(gridDim.x) * blockDim.x / 8;
+    const uint32_t l8 = threadIdx.x & 7;
+    for (uint64_t p = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) / 8; p < n_pages; p += groups) {
+        const uint32_t c = counts[p];
+        const uint64_t base = incl[p] - c;
+        const uint32_t* row = dump + p * stride + 1;
+        for (uint32_t k = l8; k < c; k += 8) {
+            const uint64_t e = base + k;
+            if (e >= n_edges) {
+                atomicOr(err, 8u);
+                continue;
+            }
+            const uint32_t t = row[k];
+            src[e] = static_cast<uint32_t>(p);
+            dst[e] = (t >= 1 && t <= n_vertices) ? t - 1 : n_vertices;
+        }
+    }
+}
+
+__global__ void or_word_kernel(uint32_t* __restrict__ dst, const uint32_t* __restrict__ src) { *dst |= *src; }
+
+// One step of the reference's push (pageRankCUDA.cu:46-65, pageRank_cpu
+// :336-378): every page adds (d * r) / count to each target.  Eight lanes per
+// page read its slots coalesced; the adds are fire-and-forget fp32 reductions
+// in L2 (the order of the adds is not fixed, as with the reference's atomics).
+__global__ void webdump_push_kernel(const uint32_t* __restrict__ dump, uint32_t n_pages, uint32_t stride,
+                                    const float* __restrict__ rank_in, float init, float damping,
+                                    float* __restrict__ out, uint32_t n_vertices, uint32_t* __restrict__ err) {
+    const uint64_t groups = static_cast<uint64_t>(gridDim.x) * blockDim.x / 8;
+    const uint32_t l8 = threadIdx.x & 7;
+    bool bad = false;
+    for (uint64_t p = (blockIdx.x * static_cast<uint64_t>(blockDim.x) + threadIdx.x) / 8; p < n_pages; p += groups) {
+        const uint32_t* row = dump + p * stride;
+        uint32_t c = row[0];
+        if (c > stride - 1) {
+            c = stride - 1;
+            bad = true;
+        }
+        if (c == 0) continue;
+        const float r = rank_in ? rank_in[p] : init;
+        const float incr = (damping * r) / static_cast<float>(c);
+        for (uint32_t k = l8; k < c; k += 8) {
+            const uint32_t t = row[1 + k];
+            if (t >= 1 && t <= n_vertices) atomicAdd(&out[t - 1], incr);
+            else bad = true;
+        }
+    }
+    if (bad && err) atomicOr(err, 2u);
+}
+
 uint32_t slices_for(uint32_t n_vertices, uint64_t n_edges) {
     const uint64_t cost = n_edges + static_cast<uint64_t>(kVertexCost) * n_vertices;
     return static_cast<uint32_t>((cost + kSlice - 1) / kSlice);
@@ -405,5 +486,76 @@ extern "C" int pmb_pagerank(const uint32_t* d_row_ptr, const uint32_t* d_col, co
         ca = cbuf;
         cbuf = t;
     }
+    return PMB_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// Web-dump pages -> CSR by destination, and the reference's push step.
+
+namespace {
+size_t align256(size_t b) { return (b + 255) & ~static_cast<size_t>(255); }
+}  // namespace
+
+extern "C" size_t pmb_webdump_csr_scratch_bytes(uint32_t n_pages, uint32_t n_vertices, uint64_t n_edges) {
+    // CSR builder scratch (its header first) | counts | inclusive offsets | scan scratch | src | dst
+    return align256(pmb_csr_scratch_bytes(n_vertices, n_edges)) + align256(4ull * n_pages) +
+           align256(8ull * n_pages) + align256(pmb_scan_scratch_bytes(n_pages)) + 2 * align256(4ull * n_edges) + 256;
+}
+
+extern "C" int pmb_csr_from_webdump(const uint32_t* d_dump, uint32_t n_pages, uint32_t max_outlinks,
+                                    uint32_t n_vertices, uint64_t n_edges, uint32_t* d_row_ptr, uint32_t* d_col,
+                                    uint32_t* d_out_degree, void* d_scratch, size_t scratch_bytes, void* stream) {
+    PMB_CHECK_ARG(d_dump && d_row_ptr && d_col && d_out_degree && d_scratch, "null pointer");
+    PMB_CHECK_ARG(n_pages >= 1 && n_pages <= n_vertices, "pages %u outside [1, n_vertices = %u]", n_pages, n_vertices);
+    PMB_CHECK_ARG(max_outlinks >= 1 && max_outlinks < 0xffffffffu, "bad max_outlinks %u", max_outlinks);
+    PMB_CHECK_ARG(n_edges < (1ull << 30), "edge count above 2^30");
+    PMB_CHECK_ARG(scratch_bytes >= pmb_webdump_csr_scratch_bytes(n_pages, n_vertices, n_edges), "scratch too small");
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    char* p = static_cast<char*>(d_scratch);
+    const size_t csr_bytes = align256(pmb_csr_scratch_bytes(n_vertices, n_edges));
+    uint32_t* hdr = static_cast<uint32_t*>(d_scratch);
+    char* q = p + csr_bytes;
+    uint32_t* own_err = reinterpret_cast<uint32_t*>(q);
+    q += 256;
+    uint32_t* counts = reinterpret_cast<uint32_t*>(q);
+    q += align256(4ull * n_pages);
+    uint64_t* incl = reinterpret_cast<uint64_t*>(q);
+    q += align256(8ull * n_pages);
+    void* scan_scratch = q;
+    const size_t scan_bytes = align256(pmb_scan_scratch_bytes(n_pages));
+    q += scan_bytes;
+    uint32_t* src = reinterpret_cast<uint32_t*>(q);
+    q += align256(4ull * n_edges);
+    uint32_t* dst = reinterpret_cast<uint32_t*>(q);
+    const uint32_t stride = max_outlinks + 1;
+    PMB_CUDA_TRY(cudaMemsetAsync(own_err, 0, 4, s));
+    if (n_edges) PMB_CUDA_TRY(cudaMemsetAsync(dst, 0xff, 4ull * n_edges, s));  // unfilled slots are dropped
+    webdump_counts_kernel<<<grid_for(n_pages, 256, 148 * 32), 256, 0, s>>>(d_dump, n_pages, stride, counts, own_err);
+    PMB_CUDA_TRY(cudaGetLastError());
+    int st = pmb_inclusive_scan_u32_u64(counts, incl, n_pages, scan_scratch, scan_bytes, stream);
+    if (st != PMB_SUCCESS) return st;
+    webdump_edges_kernel<<<grid_for(8ull * n_pages, 256, 148 * 32), 256, 0, s>>>(
+        d_dump, n_pages, stride, counts, incl, n_vertices, n_edges, src, dst, own_err);
+    PMB_CUDA_TRY(cudaGetLastError());
+    st = pmb_csr_by_destination(src, dst, n_vertices, n_edges, d_row_ptr, d_col, d_out_degree, d_scratch,
+                                csr_bytes, stream);
+    if (st != PMB_SUCCESS) return st;
+    or_word_kernel<<<1, 1, 0, s>>>(&hdr[1], own_err);  // the builder cleared its header: fold ours in
+    PMB_CUDA_TRY(cudaGetLastError());
+    return PMB_SUCCESS;
+}
+
+extern "C" int pmb_webdump_push(const uint32_t* d_dump, uint32_t n_pages, uint32_t max_outlinks,
+                                const float* d_rank_in, float initial_rank, float damping, float* d_out,
+                                uint32_t n_vertices, uint32_t* d_err, void* stream) {
+    PMB_CHECK_ARG(d_dump && d_out, "null pointer");
+    PMB_CHECK_ARG(n_vertices >= 1, "no vertices");
+    PMB_CHECK_ARG(max_outlinks >= 1 && max_outlinks < 0xffffffffu, "bad max_outlinks %u", max_outlinks);
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    PMB_CUDA_TRY(cudaMemsetAsync(d_out, 0, 4ull * n_vertices, s));
+    if (n_pages == 0) return PMB_SUCCESS;
+    webdump_push_kernel<<<grid_for(8ull * n_pages, 256, 148 * 16), 256, 0, s>>>(
+        d_dump, n_pages, max_outlinks + 1, d_rank_in, initial_rank, damping, d_out, n_vertices, d_err);
+    PMB_CUDA_TRY(cudaGetLastError());
     return PMB_SUCCESS;
 }

@@ -42,6 +42,16 @@ __device__ __forceinline__ T combine(T a, T b) {
     else return static_cast<T>(static_cast<B>(a) ^ static_cast<B>(b));  // BITWISE_XOR
 }
 
+// 16-byte load of vector i of a source read once (evict-first streaming load).
+template <typename Vec>
+__device__ __forceinline__ Vec load_stream(const void* p, size_t i) {
+    const uint4 u = __ldcs(static_cast<const uint4*>(p) + i);
+    Vec v;
+    static_assert(sizeof(Vec) == sizeof(uint4), "16-byte vectors");
+    memcpy(&v, &u, sizeof(u));
+    return v;
+}
+
 // Grid-stride over 16-byte vectors of elements when every pointer is 16-byte
 // aligned (streaming loads: each source is read once), then the tail (or
 // everything, for unaligned pointers) one element per thread.  The sources
@@ -50,27 +60,25 @@ template <typename T, int OP>
 __global__ void __launch_bounds__(256)
 reduce_kernel(T* __restrict__ dst, const Sources srcs, int nsrc, size_t count, int init, int vec) {
     constexpr int V = 16 / sizeof(T);
-    union Vec {
-        uint4 u;
+    struct alignas(16) Vec {
         T v[V];
     };
     const size_t stride = static_cast<size_t>(gridDim.x) * blockDim.x;
     const size_t tid = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x;
     const size_t nv = vec ? count / V : 0;
     for (size_t i = tid; i < nv; i += stride) {
-        Vec a, b;
-        a.u = __ldcs(static_cast<const uint4*>(srcs.p[0]) + i);
+        Vec a = load_stream<Vec>(srcs.p[0], i), b;
         if (!init) {
-            b.u = reinterpret_cast<const uint4*>(dst)[i];
+            b = reinterpret_cast<const Vec*>(dst)[i];
 #pragma unroll
             for (int k = 0; k < V; ++k) a.v[k] = combine<T, OP>(b.v[k], a.v[k]);
         }
         for (int s = 1; s < nsrc; ++s) {
-            b.u = __ldcs(static_cast<const uint4*>(srcs.p[s]) + i);
+            b = load_stream<Vec>(srcs.p[s], i);
 #pragma unroll
             for (int k = 0; k < V; ++k) a.v[k] = combine<T, OP>(a.v[k], b.v[k]);
         }
-        reinterpret_cast<uint4*>(dst)[i] = a.u;
+        reinterpret_cast<Vec*>(dst)[i] = a;
     }
     for (size_t e = nv * V + tid; e < count; e += stride) {
         const T first = static_cast<const T*>(srcs.p[0])[e];
