@@ -10,7 +10,8 @@
   skewed graph gives ranks in the hundreds, so a lost subtask copy fails the
   app's |serial - parallel| < 1 check.
 * pmb_webdump_push (the reference's push step) against the oracle's fp32 push
-  (pageRank_cpu restated), relative 1e-5 (the device adds in no fixed order).
+  (pageRank_cpu restated), relative 2e-4 (the device adds in no fixed order;
+  hub pages sum thousands of fp32 terms).
 * pmb_csr_from_webdump against pmb_csr_by_destination of the same edges:
   identical arrays; out-of-range targets and over-long counts flagged.
 """
@@ -94,7 +95,7 @@ def test_webdump_push_matches_oracle(cuda, oracle, n, maxo, with_rank):
     oracle.orc_pagerank_push_f32(ptr(src), ptr(dst), ctypes.c_uint64(src.size), n, ptr(outdeg), 1,
                                  ctypes.c_float(0.85), ptr(rank), ptr(want))
     assert int(d_err.cpu()[0]) == 0
-    np.testing.assert_allclose(got, want, rtol=1e-5, atol=1e-6)
+    np.testing.assert_allclose(got, want, rtol=2e-4, atol=1e-6)
 
 
 @pytest.mark.gpu
@@ -155,7 +156,7 @@ def test_csr_from_webdump_flags_bad_pages(cuda):
     n, maxo = 50, 4
     dump = make_dump(n, maxo, seed=8)
     dump[3, 0], dump[3, 1] = 1, 0      # target 0 (outside [1, n])
-    dump[7, 0] = 6                     # count above the slots: clamped to 4
+    dump[7, 0], dump[7, 1:] = 6, [1, 2, 3, 4]   # count above the slots: clamped to 4
     E = int(np.minimum(dump[:, 0], maxo).sum())
     row_ptr = cuda.zeros(n + 1, dtype=cuda.int32, device="cuda")
     col = cuda.zeros(E, dtype=cuda.int32, device="cuda")
