@@ -53,3 +53,25 @@ __global__ void rt_row_kernel(pmTaskInfo ti, pmDeviceInfo* di, pmSubtaskInfo si,
 }
 
 extern "C" void* rt_row_kernel_ptr() { return reinterpret_cast<void*>(&rt_row_kernel); }
+
+// Redistribution self-test: subtask s groups its chunk of int keys by bucket
+// (key mod buckets, stable) into its output chunk and leaves the bucket sizes
+// in its SUBTASK_TO_POST_SUBTASK scratch buffer, as the reference radixSort's
+// subtasks do before their redistribution callback.  One thread: the chunks
+// are small and the order must be stable.
+__global__ void rt_bucket_kernel(pmTaskInfo ti, pmDeviceInfo* di, pmSubtaskInfo si, pmStatus* st) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const int buckets = *static_cast<const int*>(ti.taskConf);
+    const int* in = static_cast<const int*>(si.memInfo[0].ptr);
+    int* out = static_cast<int*>(si.memInfo[1].ptr);
+    int* bins = static_cast<int*>(si.gpuContext.scratchBuffer);
+    const int n = static_cast<int>(si.memInfo[0].length / 4);
+    for (int b = 0; b < buckets; ++b) bins[b] = 0;
+    for (int i = 0; i < n; ++i) bins[in[i] % buckets]++;
+    int pos = 0;
+    for (int b = 0; b < buckets; ++b)
+        for (int i = 0; i < n; ++i)
+            if (in[i] % buckets == b) out[pos++] = in[i];
+}
+
+extern "C" void* rt_bucket_kernel_ptr() { return reinterpret_cast<void*>(&rt_bucket_kernel); }

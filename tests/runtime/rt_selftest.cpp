@@ -476,12 +476,125 @@ void test_reduce(bool gpu) {
     reduce_case<int32_t, int32_t>(gpu, REDUCE_ADD, REDUCE_INTS, nullptr, 0, 0, OutSub::Mismatched);
 }
 
+// ---------------------------------------------------------------------------
+// Ordered redistribution: each subtask groups its chunk of keys by bucket and
+// its redistribution callback names each bucket's range with order
+// subtasks * bucket + subtask, as the reference radixSort does
+// (radixSort.cpp:150-162); the address space then holds all keys stably
+// grouped by bucket.
+
+extern "C" void* rt_bucket_kernel_ptr();
+
+constexpr int kBuckets = 5, kChunk = 1000, kKeys = 8500;
+pmStatus g_redist_bad = pmSuccess;  // status of a deliberately out-of-range pmRedistributeData
+
+int chunk_len(unsigned long id) { return std::min(kChunk, kKeys - int(id) * kChunk); }
+
+pmStatus bucket_dd(pmTaskInfo ti, pmDeviceInfo di, pmSubtaskInfo si) {
+    const pmSubscriptionInfo s(si.subtaskId * kChunk * 4, size_t(chunk_len(si.subtaskId)) * 4);
+    pmSubscribeToMemory(ti.taskHandle, di.deviceHandle, si.subtaskId, si.splitInfo, 0, READ_SUBSCRIPTION, s);
+    pmSubscribeToMemory(ti.taskHandle, di.deviceHandle, si.subtaskId, si.splitInfo, 1, WRITE_SUBSCRIPTION, s);
+    pmGetScratchBuffer(ti.taskHandle, di.deviceHandle, si.subtaskId, si.splitInfo, SUBTASK_TO_POST_SUBTASK,
+                       kBuckets * sizeof(int), nullptr);
+    if (di.deviceType == GPU_CUDA) {
+        pmCudaLaunchConf lc(1, 1, 1, 32, 1, 1);
+        pmSetCudaLaunchConf(ti.taskHandle, di.deviceHandle, si.subtaskId, si.splitInfo, lc);
+    }
+    return pmSuccess;
+}
+
+pmStatus bucket_cpu(pmTaskInfo ti, pmDeviceInfo di, pmSubtaskInfo si) {
+    const int* in = static_cast<const int*>(si.memInfo[0].ptr);
+    int* out = static_cast<int*>(si.memInfo[1].ptr);
+    int* bins = static_cast<int*>(pmGetScratchBuffer(ti.taskHandle, di.deviceHandle, si.subtaskId, si.splitInfo,
+                                                     SUBTASK_TO_POST_SUBTASK, 0, nullptr));
+    const int n = int(si.memInfo[0].length / 4);
+    for (int b = 0; b < kBuckets; ++b) bins[b] = 0;
+    for (int i = 0; i < n; ++i) bins[in[i] % kBuckets]++;
+    int pos = 0;
+    for (int b = 0; b < kBuckets; ++b)
+        for (int i = 0; i < n; ++i)
+            if (in[i] % kBuckets == b) out[pos++] = in[i];
+    return pmSuccess;
+}
+
+pmStatus bucket_redistribution(pmTaskInfo ti, pmDeviceInfo di, pmSubtaskInfo si) {
+    const int* bins = static_cast<const int*>(pmGetScratchBuffer(ti.taskHandle, di.deviceHandle, si.subtaskId,
+                                                                 si.splitInfo, SUBTASK_TO_POST_SUBTASK, 0, nullptr));
+    if (!bins) return pmUserError;
+    size_t off = 0;
+    for (int b = 0; b < kBuckets; ++b) {
+        const pmStatus st = pmRedistributeData(ti.taskHandle, di.deviceHandle, si.subtaskId, si.splitInfo, 1, off,
+                                               size_t(bins[b]) * 4, uint(ti.subtaskCount * b + si.subtaskId));
+        if (st != pmSuccess) return st;
+        off += size_t(bins[b]) * 4;
+    }
+    if (si.subtaskId == 0)  // a range past the end of the address space is refused
+        g_redist_bad = pmRedistributeData(ti.taskHandle, di.deviceHandle, 0, si.splitInfo, 1, size_t(kKeys) * 4, 4, 0);
+    return pmSuccess;
+}
+
+void test_redistribute(bool gpu) {
+    pmCallbacks cb;
+    cb.dataDistribution = bucket_dd;
+    cb.subtask_cpu = bucket_cpu;
+    if (gpu) cb.subtask_gpu_cuda = reinterpret_cast<pmSubtaskCallback_GPU_CUDA>(rt_bucket_kernel_ptr());
+    cb.dataRedistribution = bucket_redistribution;
+    pmCallbackHandle h;
+    CHECK(pmRegisterCallbacks("BUCKETS", cb, &h) == pmSuccess, "register");
+    pmMemHandle in, out;
+    CHECK(pmCreateMemory(size_t(kKeys) * 4, &in) == pmSuccess && pmCreateMemory(size_t(kKeys) * 4, &out) == pmSuccess,
+          "create");
+    void *ip, *op;
+    pmGetRawMemPtr(in, &ip);
+    int* keys = static_cast<int*>(ip);
+    for (int i = 0; i < kKeys; ++i) keys[i] = int((unsigned(i) * 2654435761u) % 100000u);
+    static int buckets = kBuckets;
+    pmTaskMem mem[2] = {pmTaskMem(in, READ_ONLY, SUBSCRIPTION_NATURAL), pmTaskMem(out, WRITE_ONLY, SUBSCRIPTION_NATURAL)};
+    const unsigned long nsub = (kKeys + kChunk - 1) / kChunk;
+    pmTaskDetails td(&buckets, sizeof(buckets), mem, 2, h, nsub);
+    pmTaskHandle t;
+    CHECK(pmSubmitTask(td, &t) == pmSuccess, "submit");
+    CHECK(pmWaitForTaskCompletion(t) == pmSuccess, "task failed");
+    CHECK(g_redist_bad == pmInvalidIndex, "out-of-range redistribution returned %d", g_redist_bad);
+    pmSplitInfo split;
+    CHECK(pmRedistributeData(t, nullptr, 0, split, 1, 0, 4, 0) == pmInvalidCommand,
+          "redistribution accepted after the task");
+    // expected: keys stably grouped by bucket over the whole array; metadata per (bucket, subtask)
+    std::vector<int> expect;
+    std::vector<std::pair<uint, uint>> meta;
+    for (int b = 0; b < kBuckets; ++b)
+        for (unsigned long s = 0; s < nsub; ++s) {
+            uint bytes = 0;
+            for (int i = int(s) * kChunk; i < int(s) * kChunk + chunk_len(s); ++i)
+                if (keys[i] % kBuckets == b) {
+                    expect.push_back(keys[i]);
+                    bytes += 4;
+                }
+            if (bytes) meta.emplace_back(uint(nsub * b + s), bytes);
+        }
+    CHECK(pmFetchMemory(out) == pmSuccess, "fetch");
+    pmGetRawMemPtr(out, &op);
+    CHECK(int(expect.size()) == kKeys && std::memcmp(expect.data(), op, size_t(kKeys) * 4) == 0,
+          "redistributed keys differ");
+    ulong count = 0;
+    const pmRedistributionMetadata* md = pmGetRedistributionMetadata(t, 1, &count);
+    CHECK(md && count == meta.size(), "metadata count %lu expected %zu", count, meta.size());
+    for (size_t k = 0; k < meta.size(); ++k)
+        CHECK(md[k].order == meta[k].first && md[k].count == meta[k].second, "metadata %zu: (%u, %u) expected (%u, %u)",
+              k, md[k].order, md[k].count, meta[k].first, meta[k].second);
+    ulong none = 7;
+    CHECK(pmGetRedistributionMetadata(t, 0, &none) == nullptr && none == 0, "metadata of an address space not redistributed");
+    CHECK(pmReleaseTask(t) == pmSuccess, "release");
+    CHECK(pmReleaseMemory(in) == pmSuccess && pmReleaseMemory(out) == pmSuccess, "release memory");
+}
+
 }  // namespace
 
 int main(int argc, char** argv) {
     if (argc < 2) {
         std::printf("usage: rt_selftest <views_cpu|views_cpu_compact|views_gpu|views_gpu_compact|chain|"
-                    "write_through|mix|errors|timeout|reduce_cpu|reduce_gpu>\n");
+                    "write_through|mix|errors|timeout|reduce_cpu|reduce_gpu|redistribute_cpu|redistribute_gpu>\n");
         return 2;
     }
     g_test = argv[1];
@@ -502,6 +615,8 @@ int main(int argc, char** argv) {
     else if (g_test == "timeout") test_timeout();
     else if (g_test == "reduce_cpu") test_reduce(false);
     else if (g_test == "reduce_gpu") test_reduce(true);
+    else if (g_test == "redistribute_cpu") test_redistribute(false);
+    else if (g_test == "redistribute_gpu") test_redistribute(true);
     else CHECK(false, "unknown test");
     CHECK(pmFinalize() == pmSuccess, "finalize");
     std::printf("PASS %s\n", g_test.c_str());

@@ -6,7 +6,9 @@
   chained tasks that stay device-resident, write-through with the CUDA cache
   disabled, many tasks in flight vs alone, error returns and timeouts, and
   subtask reduction (every built-in REDUCE_* operation and data type, partial
-  and scattered writes, the app's own callbacks) on the CPU and on the GPU.
+  and scattered writes, the app's own callbacks) and ordered redistribution
+  (pmRedistributeData / pmGetRedistributionMetadata, radixSort's bucket
+  pattern) on the CPU and on the GPU.
 * oracle/_ref/imageFiltering_b200.exe: the reference's own imageFiltering app
   and harness (imageFiltering.cpp + commonAPI.cpp, unchanged) linked against
   this runtime and the B200 GPU callbacks; it checks itself against its serial
@@ -36,14 +38,16 @@ def run(cmd, timeout=300):
     return p.returncode, p.stdout + p.stderr
 
 
-@pytest.mark.parametrize("name", ["views_cpu", "views_cpu_compact", "errors", "timeout", "reduce_cpu"])
+@pytest.mark.parametrize("name", ["views_cpu", "views_cpu_compact", "errors", "timeout", "reduce_cpu",
+                                  "redistribute_cpu"])
 def test_runtime_cpu(selftest, name):
     rc, out = run([selftest, name])
     assert rc == 0 and f"PASS {name}" in out, out
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("name", ["views_gpu", "views_gpu_compact", "chain", "write_through", "mix", "reduce_gpu"])
+@pytest.mark.parametrize("name", ["views_gpu", "views_gpu_compact", "chain", "write_through", "mix", "reduce_gpu",
+                                  "redistribute_gpu"])
 def test_runtime_gpu(selftest, name):
     rc, out = run([selftest, name])
     assert rc == 0 and f"PASS {name}" in out, out

@@ -808,6 +808,126 @@ static pmStatus reduce_device_shadows(Task* t, void* stream) {
     return pmSuccess;
 }
 
+// ---------------------------------------------------------------------------
+// ordered redistribution (pmCallbacks::dataRedistribution, pmRedistributeData)
+//
+// After a task's subtasks have run, the app's redistribution callback is
+// called for each subtask in id order (on the host) and names byte ranges of
+// an address space with an order number.  The address space is then rebuilt
+// with every order's ranges back to back, orders ascending, ranges within an
+// order by subtask id then call order, the rest zero
+// (pmRedistributor.cpp:88-121 sums each order's bytes, 123-145 assigns
+// running offsets, 240-283 copies the ranges into a new address space that
+// replaces the task's, pmTask.cpp:834-856).  A GPU task moves the bytes on
+// the device into a new mirror, one device copy per range.
+
+struct RedistCopy {
+    size_t src, dst, len;
+};
+
+// Copies and metadata of address space i; fails when the ranges add up to
+// more than the address space.
+static pmStatus redist_plan(Task* t, size_t i, std::vector<RedistCopy>& copies) {
+    std::vector<RedistRecord>& rs = t->redist[i];
+    std::sort(rs.begin(), rs.end(), [](const RedistRecord& a, const RedistRecord& b) {
+        return a.order != b.order ? a.order < b.order : (a.subtask != b.subtask ? a.subtask < b.subtask : a.seq < b.seq);
+    });
+    copies.clear();
+    t->redist_meta.resize(t->spaces.size());
+    std::vector<pmRedistributionMetadata>& meta = t->redist_meta[i];
+    meta.clear();
+    size_t run = 0;
+    for (const RedistRecord& r : rs) {
+        if (run + r.length > t->spaces[i]->length)
+            return fail(pmInvalidIndex, "redistribution of address space %zu: %zu bytes beyond its %zu", i,
+                        run + r.length, t->spaces[i]->length);
+        copies.push_back({r.offset, run, r.length});
+        if (meta.empty() || meta.back().order != r.order) meta.emplace_back(r.order, 0u);
+        meta.back().count += static_cast<uint>(r.length);
+        run += r.length;
+    }
+    return pmSuccess;
+}
+
+static pmStatus run_redistribution_callbacks(Task* t, const pmDeviceInfo& dev) {
+    const pmDataRedistributionCallback cb = t->callbacks->cb.dataRedistribution;
+    {
+        std::lock_guard<std::mutex> g(t->redist_mu);
+        t->redist.assign(t->spaces.size(), {});
+        t->redist_open = true;
+    }
+    pmStatus st = pmSuccess;
+    for (Subtask& s : t->subtasks) {
+        pmSubtaskInfo info;
+        info.subtaskId = s.id;
+        info.memCount = static_cast<uint>(t->spaces.size());
+        st = cb(t->info, dev, info);
+        if (st != pmSuccess) {
+            st = fail(st, "redistribution callback of subtask %lu returned %d", s.id, static_cast<int>(st));
+            break;
+        }
+    }
+    std::lock_guard<std::mutex> g(t->redist_mu);
+    t->redist_open = false;
+    return st;
+}
+
+// GPU task: after its work (the callbacks read SUBTASK_TO_POST_SUBTASK
+// scratch buffers, copied back on the task's streams), each redistributed
+// address space gets a new zeroed mirror filled by device copies on `stream`.
+static pmStatus redistribute_device(Task* t, void* stream) {
+    Controller& c = ctl();
+    PMR_DEV(pmb_stream_synchronize(stream));
+    pmStatus st = run_redistribution_callbacks(t, c.gpu_info);
+    if (st != pmSuccess) return st;
+    std::vector<RedistCopy> copies;
+    for (size_t i = 0; i < t->spaces.size(); ++i) {
+        if (t->redist[i].empty()) continue;
+        st = redist_plan(t, i, copies);
+        if (st != pmSuccess) return st;
+        AddressSpace* a = t->spaces[i];
+        std::lock_guard<std::mutex> g(a->mu);
+        for (const RedistCopy& k : copies) {  // source bytes the device does not hold come from the host
+            Record r;
+            r.offset = k.src, r.size = k.len, r.step = k.len, r.count = 1;
+            st = upload_record(a, r, stream);
+            if (st != pmSuccess) return st;
+        }
+        void* nd = nullptr;
+        PMR_DEV(pmb_malloc_async(&nd, a->length ? a->length : 1, stream));
+        PMR_DEV(pmb_memset_async(nd, 0, a->length, stream));
+        for (const RedistCopy& k : copies)
+            PMR_DEV(pmb_memcpy_async(static_cast<char*>(nd) + k.dst, a->dev + k.src, k.len, PMB_D2D, stream));
+        PMR_DEV(pmb_free_async(a->dev, stream));
+        a->dev = static_cast<char*>(nd);
+        a->dev_valid.clear();
+        a->dev_valid.add(0, a->length);
+        a->host_stale.clear();
+        a->host_stale.add(0, a->length);
+    }
+    return pmSuccess;
+}
+
+// CPU task: the same permutation of the host copy.
+static pmStatus redistribute_host(Task* t) {
+    pmStatus st = run_redistribution_callbacks(t, ctl().cpu_info);
+    if (st != pmSuccess) return st;
+    std::vector<RedistCopy> copies;
+    for (size_t i = 0; i < t->spaces.size(); ++i) {
+        if (t->redist[i].empty()) continue;
+        st = redist_plan(t, i, copies);
+        if (st != pmSuccess) return st;
+        AddressSpace* a = t->spaces[i];
+        std::lock_guard<std::mutex> g(a->mu);
+        const std::vector<char> old(a->host, a->host + a->length);
+        memset(a->host, 0, a->length);
+        for (const RedistCopy& k : copies) memcpy(a->host + k.dst, old.data() + k.src, k.len);
+        a->dev_valid.clear();
+        a->host_stale.clear();
+    }
+    return pmSuccess;
+}
+
 // Admission by free device memory: the task's missing mirrors and reserved
 // subtask memory must fit beside the reserve, after idle mirrors are evicted.
 static bool admit(Task* t, size_t* need_out) {
@@ -1060,7 +1180,8 @@ static pmStatus stage_and_launch_gpu(Task* t) {
         if (js != pmSuccess) return js;
     }
     {
-        const pmStatus rs = reduce_device_shadows(t, join);
+        pmStatus rs = reduce_device_shadows(t, join);
+        if (rs == pmSuccess && cb.dataRedistribution) rs = redistribute_device(t, join);
         if (rs != pmSuccess) return rs;
     }
     // Write-back at task end: all stale bytes with the cache disabled (the
@@ -1211,6 +1332,10 @@ static pmStatus run_cpu_task(Task* t) {
     if (err.load() == pmSuccess && !t->reduce.empty()) {
         pmStatus rs = reduce_host_shadows(t, ctl().cpu_info);
         if (rs == pmSuccess) rs = commit_host_shadows(t);
+        if (rs != pmSuccess) return rs;
+    }
+    if (err.load() == pmSuccess && t->callbacks->cb.dataRedistribution) {
+        const pmStatus rs = redistribute_host(t);
         if (rs != pmSuccess) return rs;
     }
     for (size_t i = 0; i < ns; ++i) {
@@ -1607,8 +1732,33 @@ pmStatus pmSubscribeToMemory(pmTaskHandle pTaskHandle, pmDeviceHandle, ulong pSu
     return subscribe(pTaskHandle, pSubtaskId, pMemIndex, pSubscriptionType, r);
 }
 
-pmStatus pmRedistributeData(pmTaskHandle, pmDeviceHandle, ulong, pmSplitInfo&, uint, size_t, size_t, uint) {
-    return fail(pmStatusUnavailable, "data redistribution is not supported by the B200 runtime");
+// pmSubscriptionManager::RegisterRedistribution (pmSubscriptionManager.cpp:861-877):
+// pOffset is relative to the start of the subtask's write range of the
+// address space; zero-length ranges are ignored.
+pmStatus pmRedistributeData(pmTaskHandle pTaskHandle, pmDeviceHandle, ulong pSubtaskId, pmSplitInfo&, uint pMemIndex,
+                            size_t pOffset, size_t pLength, uint pOrder) {
+    Task* t = task_of(pTaskHandle);
+    if (!t) return fail(pmInvalidIndex, "unknown task handle");
+    if (pMemIndex >= t->spaces.size() || pSubtaskId >= t->subtasks.size())
+        return fail(pmInvalidIndex, "address space %u or subtask %lu out of range", pMemIndex, pSubtaskId);
+    if (!pLength) return pmSuccess;
+    size_t wlo, whi;
+    consolidated(t->subtasks[pSubtaskId].mem[pMemIndex].writes, wlo, whi);
+    if (whi <= wlo) return fail(pmInvalidIndex, "subtask %lu writes nothing of address space %u", pSubtaskId, pMemIndex);
+    const size_t len = t->spaces[pMemIndex]->length;
+    if (pOffset > len || pLength > len || wlo + pOffset > len - pLength)
+        return fail(pmInvalidIndex, "redistributed range [%zu, +%zu) outside address space %u", wlo + pOffset, pLength,
+                    pMemIndex);
+    std::lock_guard<std::mutex> g(t->redist_mu);
+    if (!t->redist_open) return fail(pmInvalidCommand, "pmRedistributeData outside a data-redistribution callback");
+    RedistRecord r;
+    r.order = pOrder;
+    r.subtask = pSubtaskId;
+    r.seq = t->redist[pMemIndex].size();
+    r.offset = wlo + pOffset;
+    r.length = pLength;
+    t->redist[pMemIndex].push_back(r);
+    return pmSuccess;
 }
 
 pmStatus pmSetCudaLaunchConf(pmTaskHandle pTaskHandle, pmDeviceHandle, ulong pSubtaskId, pmSplitInfo&,
@@ -1769,9 +1919,14 @@ pmStatus pmReleaseScratchBuffer(pmTaskHandle pTaskHandle, pmDeviceHandle, ulong 
 
 void* pmGetLastReductionScratchBuffer(pmTaskHandle) { return nullptr; }
 
-pmRedistributionMetadata* pmGetRedistributionMetadata(pmTaskHandle, uint, ulong* pCount) {
+// pmRedistributor::GetRedistributionMetadata (pmRedistributor.cpp:296-322):
+// (order, bytes) per order, ascending; valid until the task is released.
+pmRedistributionMetadata* pmGetRedistributionMetadata(pmTaskHandle pTaskHandle, uint pMemIndex, ulong* pCount) {
     if (pCount) *pCount = 0;
-    return nullptr;
+    Task* t = task_of(pTaskHandle);
+    if (!t || pMemIndex >= t->redist_meta.size() || t->redist_meta[pMemIndex].empty()) return nullptr;
+    if (pCount) *pCount = t->redist_meta[pMemIndex].size();
+    return t->redist_meta[pMemIndex].data();
 }
 
 // pmPublicDefinitions.cpp:779-815: the built-in callback of an (operation,

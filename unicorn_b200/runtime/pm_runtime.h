@@ -97,6 +97,15 @@ struct ReduceSpace {
     std::vector<size_t> subtasks;
 };
 
+// One pmRedistributeData call: `length` bytes at `offset` of the address
+// space (the subtask's write range start + the offset it passed) go to order
+// `order`; ties broken by subtask id, then call sequence.
+struct RedistRecord {
+    unsigned int order = 0;
+    size_t subtask = 0, seq = 0;
+    size_t offset = 0, length = 0;
+};
+
 struct CallbackSet {
     std::string key;
     pmCallbacks cb;
@@ -124,6 +133,12 @@ struct Task {
     size_t reserved_held = 0;    // reserved subtask memory and reduction copies counted against the device budget
     std::vector<ReduceSpace> reduce;  // reducible address spaces (dataReduction tasks)
     int reduce_op = -1, reduce_type = -1;  // built-in REDUCE_* callback, else -1 (the app's own callback)
+    // Ordered redistribution (dataRedistribution callback): records per
+    // address space, and after the task the (order, bytes) metadata of each.
+    std::mutex redist_mu;
+    std::vector<std::vector<RedistRecord>> redist;
+    std::vector<std::vector<pmRedistributionMetadata>> redist_meta;
+    bool redist_open = false;  // inside the redistribution callbacks
     double deadline = 0;         // 0: none
     std::atomic<int> state{0};   // 0 queued, 1 running, 2 done
     pmStatus status = pmSuccess;
