@@ -481,6 +481,54 @@ def served_measurement():
     return out
 
 
+class Ranks:
+    """One process per GPU (torchrun): rank and world size from the
+    environment, a barrier after the caller's device sync, the max of a float
+    over ranks, and the whole-job rate.  NCCL on the GPU box; the CPU tests
+    run the same code over gloo."""
+
+    def __init__(self, backend: str = "nccl", device=None):
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.device = device
+        self.dist = None
+        if self.world > 1:
+            import datetime
+
+            import torch.distributed as dist
+
+            kw = {"device_id": device} if backend == "nccl" else {}
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120), **kw)
+            self.dist = dist
+
+    def barrier(self, sync=None) -> None:
+        if sync is not None:
+            sync()
+        if self.dist is not None:
+            self.dist.barrier()
+
+    def max(self, x: float) -> float:
+        if self.dist is None:
+            return x
+        import torch
+
+        t = torch.tensor([x], dtype=torch.float64, device=self.device if self.device is not None else "cpu")
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def rate(self, units_per_rank: float, steps: int, max_ms: float) -> float:
+        """Whole-job units per second, in 1e9 units (GB/s for bytes): every
+        rank processes units_per_rank per step; max_ms is the slowest rank."""
+        return self.world * units_per_rank * steps / (max_ms / 1e3) / 1e9
+
+    def close(self) -> None:
+        if self.dist is not None:
+            self.dist.barrier()
+            self.dist.destroy_process_group()
+            self.dist = None
+
+
 def _hbm_entry(nbytes: int, ms: float, hbm: float):
     gbs = nbytes / (ms / 1e3) / 1e9
     return {"gbs": round(gbs, 1), "ms": round(ms, 4), "algorithmic_bytes": nbytes,
@@ -497,18 +545,10 @@ def main():
     import torch
     from unicorn_b200 import capi
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+    ranks = Ranks("nccl", torch.device("cuda", local))
+    world, rank = ranks.world, ranks.rank
     L = capi.lib()
     img, f = make_inputs()
     fb = np.zeros((32, 32), np.int8)
@@ -532,16 +572,9 @@ def main():
         capi.check(L.pmb_image_filter(items, len(rects), fp, R, capi.PMB_IMGF_CLAMP, sp))
 
     def barrier():
-        torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
+        ranks.barrier(torch.cuda.synchronize)
 
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    max_over_ranks = ranks.max
 
     # ---- device-resident timing -----------------------------------------
     with torch.cuda.stream(stream):
@@ -557,7 +590,7 @@ def main():
         barrier()
     dev_ms = max_over_ranks(ev0.elapsed_time(ev1))
     ms_per_step = dev_ms / args.steps
-    value = world * ALG_BYTES * args.steps / (dev_ms / 1e3) / 1e9
+    value = ranks.rate(ALG_BYTES, args.steps, dev_ms)
     kernel_gbs = ALG_BYTES / (ms_per_step / 1e3) / 1e9
 
     # ---- end to end: host buffers, copies inside the timed region --------
@@ -580,7 +613,7 @@ def main():
     e1.record(stream)
     barrier()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1))
-    e2e_value = world * ALG_BYTES * args.steps / (e2e_ms / 1e3) / 1e9
+    e2e_value = ranks.rate(ALG_BYTES, args.steps, e2e_ms)
     apps = app_measurements(torch, L, stream) if (rank == 0 and not args.no_apps) else None
 
     peak, peak_kind = peaks()
@@ -609,9 +642,7 @@ def main():
         line["served_mix"] = served_measurement()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(img, f, os.cpu_count() or 1)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    ranks.close()
     if rank == 0:
         print(json.dumps(line))
     return 0
