@@ -321,6 +321,10 @@ pmStatus row_dd(pmTaskInfo ti, pmDeviceInfo di, pmSubtaskInfo si) {
         pmCudaLaunchConf lc(4, 1, 1, 256, 1, 1);
         pmSetCudaLaunchConf(ti.taskHandle, di.deviceHandle, si.subtaskId, si.splitInfo, lc);
     }
+    // a counter that travels with the reductions: subtask id + 1
+    uint64_t* counter = static_cast<uint64_t*>(pmGetScratchBuffer(ti.taskHandle, di.deviceHandle, si.subtaskId,
+                                                                  si.splitInfo, REDUCTION_TO_REDUCTION, 8, nullptr));
+    *counter = si.subtaskId + 1;
     return pmSuccess;
 }
 
@@ -340,6 +344,12 @@ pmStatus axpy3_reduction(pmTaskInfo ti, pmDeviceInfo, pmSubtaskInfo s1, pmDevice
     const int* b = static_cast<const int*>(s2.memInfo[1].writePtr);
     if (!a || !b || s1.memInfo[1].length != size_t(conf->words) * 4) return pmUserError;
     for (int j = 0; j < conf->words; ++j) a[j] += 3 * b[j];
+    uint64_t* ca = static_cast<uint64_t*>(pmGetScratchBuffer(ti.taskHandle, nullptr, s1.subtaskId, s1.splitInfo,
+                                                             REDUCTION_TO_REDUCTION, 0, nullptr));
+    const uint64_t* cb = static_cast<const uint64_t*>(pmGetScratchBuffer(ti.taskHandle, nullptr, s2.subtaskId,
+                                                                         s2.splitInfo, REDUCTION_TO_REDUCTION, 0, nullptr));
+    if (!ca || !cb) return pmUserError;
+    *ca += *cb;
     return pmSuccess;
 }
 
@@ -445,6 +455,14 @@ void reduce_case(bool gpu, int op, int type, pmDataReductionCallback custom, int
               "op %d type %d custom %d sub %d: first mismatch at %d", op, type, custom_kind, int(sub),
               int(std::mismatch(expect.begin(), expect.end(), outp,
                                 [](T a, T b) { return std::memcmp(&a, &b, sizeof(T)) == 0; }).first - expect.begin()));
+    }
+    if (sub != OutSub::Mismatched) {
+        // the REDUCTION_TO_REDUCTION buffer of the subtask all others were folded into: the app's
+        // callback summed the counters; the built-in folds leave subtask 0's (1)
+        const uint64_t* last = static_cast<const uint64_t*>(pmGetLastReductionScratchBuffer(t));
+        const uint64_t want = custom_kind == 1 ? uint64_t(kRowSubtasks) * (kRowSubtasks + 1) / 2 : 1;
+        CHECK(last && *last == want, "last reduction scratch %llu expected %llu",
+              last ? (unsigned long long)*last : 0ull, (unsigned long long)want);
     }
     CHECK(pmReleaseTask(t) == st, "release");
     CHECK(pmReleaseMemory(in) == pmSuccess && pmReleaseMemory(out) == pmSuccess, "release memory");

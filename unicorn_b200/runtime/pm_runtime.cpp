@@ -684,6 +684,21 @@ static pmMemInfo shadow_view(const SubtaskMem& m, const ReduceSpace& rs, char* b
     return mi;
 }
 
+// The REDUCTION_TO_REDUCTION scratch buffer of the subtask every other one
+// was folded into (pmTask.cpp:1197-1206); the others' were dropped as they
+// were folded (pmExecutionStub.cpp:2573).
+static void keep_last_reduction_scratch(Task* t, size_t first) {
+    auto& m = t->subtasks[first].scratch;
+    auto it = m.find(REDUCTION_TO_REDUCTION);
+    t->last_reduction_scratch = it != m.end() && !it->second.empty() ? it->second.data() : nullptr;
+}
+
+static size_t first_reducing_subtask(const Task* t) {
+    size_t first = t->subtasks.size();
+    for (const ReduceSpace& rs : t->reduce) first = std::min(first, rs.subtasks.front());
+    return first;
+}
+
 // Folds the host copies of every reducible address space into the first
 // writing subtask's: the built-in operation in id order, or the app's
 // callback called pairwise (first, k) as pmReducer calls it.
@@ -698,6 +713,7 @@ static pmStatus reduce_host_shadows(Task* t, const pmDeviceInfo& dev) {
                 if (st != pmSuccess) return st;
             }
         }
+        keep_last_reduction_scratch(t, first_reducing_subtask(t));
         return pmSuccess;
     }
     // The app's callback sees every reducible space of both subtasks; the
@@ -722,7 +738,9 @@ static pmStatus reduce_host_shadows(Task* t, const pmDeviceInfo& dev) {
         if (st != pmSuccess)
             return fail(st, "reduction callback of subtasks %zu and %zu returned %d", order.front(), order[k],
                         static_cast<int>(st));
+        t->subtasks[order[k]].scratch.erase(REDUCTION_TO_REDUCTION);
     }
+    keep_last_reduction_scratch(t, order.front());
     return pmSuccess;
 }
 
@@ -784,6 +802,7 @@ static pmStatus reduce_device_shadows(Task* t, void* stream) {
                 add_record(a->host_stale, r);
             }
         }
+        keep_last_reduction_scratch(t, first_reducing_subtask(t));
     } else {
         PMR_DEV(pmb_stream_synchronize(stream));
         for (const ReduceSpace& rs : t->reduce)
@@ -1917,7 +1936,12 @@ pmStatus pmReleaseScratchBuffer(pmTaskHandle pTaskHandle, pmDeviceHandle, ulong 
     return pmSuccess;
 }
 
-void* pmGetLastReductionScratchBuffer(pmTaskHandle) { return nullptr; }
+// pmTask::GetLastReductionScratchBuffer (pmTask.cpp:862-865): NULL when the
+// task reduced nothing or its subtasks made no REDUCTION_TO_REDUCTION buffer.
+void* pmGetLastReductionScratchBuffer(pmTaskHandle pTaskHandle) {
+    Task* t = task_of(pTaskHandle);
+    return t ? t->last_reduction_scratch : nullptr;
+}
 
 // pmRedistributor::GetRedistributionMetadata (pmRedistributor.cpp:296-322):
 // (order, bytes) per order, ascending; valid until the task is released.

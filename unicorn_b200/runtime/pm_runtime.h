@@ -133,6 +133,7 @@ struct Task {
     size_t reserved_held = 0;    // reserved subtask memory and reduction copies counted against the device budget
     std::vector<ReduceSpace> reduce;  // reducible address spaces (dataReduction tasks)
     int reduce_op = -1, reduce_type = -1;  // built-in REDUCE_* callback, else -1 (the app's own callback)
+    void* last_reduction_scratch = nullptr;  // REDUCTION_TO_REDUCTION buffer of the subtask all others folded into
     // Ordered redistribution (dataRedistribution callback): records per
     // address space, and after the task the (order, bytes) metadata of each.
     std::mutex redist_mu;
