@@ -340,7 +340,50 @@ def app_measurements(torch, L, stream):
         red_ms = _timed(torch, stream, lambda: ops.reduce_elementwise(0, 4, dst, copies, nr, stream=stream), 10)
         res["subtask_reduce_add_f32_8x2^24"] = _hbm_entry(4 * nr * (ns + 1), red_ms, hbm)
         del copies, dst
+        try:
+            res.update(webdump_measurement(torch, L, stream, hbm))
+        except Exception as e:  # a failed extra measurement must not lose the others
+            res["webdump"] = {"error": f"{type(e).__name__}: {e}"}
     return res
+
+
+def webdump_measurement(torch, L, stream, hbm: float, device: str = "cuda"):
+    """The reference pageRank's own input format on the device: one push step
+    (pmb_webdump_push) over 2^22 padded page records of 32 out-link slots
+    (out-degrees uniform in [0, 32], so ~2^26 edges, the R-MAT 22 edge count),
+    and the CSR build from the same records (pmb_csr_from_webdump)."""
+    from unicorn_b200 import ops
+
+    n, maxo = 1 << 22, 32
+    g = torch.Generator(device=device).manual_seed(5)
+    dump = torch.randint(1, n + 1, (n, maxo + 1), dtype=torch.int32, device=device, generator=g)
+    counts = torch.randint(0, maxo + 1, (n,), dtype=torch.int32, device=device, generator=g)
+    dump[:, 0] = counts
+    edges = int(counts.sum().item())
+    out = torch.empty(n, dtype=torch.float32, device=device)
+    sp = ctypes.c_void_p(stream.cuda_stream)
+    push_ms = _timed(torch, stream, lambda: capi_check(L.pmb_webdump_push(
+        dump.data_ptr(), n, maxo, None, 1.0, 0.85, out.data_ptr(), n, None, sp)), 10)
+    # algorithmic bytes: the records read once, the rank array zeroed and written
+    push_bytes = 4 * n * (maxo + 1) + 4 * n
+    res = {"webdump_push_2^22x32": dict(_hbm_entry(push_bytes, push_ms, hbm), edges=edges)}
+    row_ptr = torch.empty(n + 1, dtype=torch.int32, device=device)
+    col = torch.empty(max(edges, 1), dtype=torch.int32, device=device)
+    deg = torch.empty(n, dtype=torch.int32, device=device)
+    sc = ops._scratch(L.pmb_webdump_csr_scratch_bytes(n, n, edges)) if device == "cuda" else \
+        torch.empty(L.pmb_webdump_csr_scratch_bytes(n, n, edges), dtype=torch.uint8)
+    csr_ms = _timed(torch, stream, lambda: capi_check(L.pmb_csr_from_webdump(
+        dump.data_ptr(), n, maxo, n, edges, row_ptr.data_ptr(), col.data_ptr(), deg.data_ptr(), sc.data_ptr(),
+        sc.numel(), sp)), 3)
+    res["csr_from_webdump_2^22x32"] = {"ms": round(csr_ms, 3), "edges": edges,
+                                       "medges_per_s": round(edges / (csr_ms / 1e3) / 1e6, 1)}
+    return res
+
+
+def capi_check(st: int) -> None:
+    from unicorn_b200 import capi
+
+    capi.check(st)
 
 
 def _oracle_lib():
