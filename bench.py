@@ -396,6 +396,22 @@ def _cpu_entry(value, unit, cores, kind, sample, seconds):
             "seconds": round(seconds, 3)}
 
 
+def reduce_cpu_baseline(orc, nr: int = 1 << 24, ns: int = 8):
+    """The reference's host fold (pmReducer::ReduceMemories REDUCE_ADD over
+    FLOATS, restated in oracle/oracle.c) on the same 8 copies of 2^24 floats:
+    copy k folded into copy 0 for k = 1..7, one thread."""
+    P = ctypes.c_void_p
+    rng = np.random.default_rng(4)
+    copies = [rng.random(nr, dtype=np.float32) for _ in range(ns)]
+    t0 = time.perf_counter()
+    for k in range(1, ns):
+        orc.orc_reduce_fold(0, 4, copies[0].ctypes.data_as(P), copies[k].ctypes.data_as(P), ctypes.c_size_t(nr))
+    dt = time.perf_counter() - t0
+    return _cpu_entry(4.0 * nr * (ns + 1) / dt / 1e9, "GB/s", 1, "port",
+                      "pmReducer::ReduceMemories REDUCE_ADD restated (oracle/oracle.c), 8 copies of 2^24 floats "
+                      "folded pairwise into the first, one thread", dt)
+
+
 def app_cpu_baselines(torch, res):
     """CPU figures next to each app kernel, on the box's host cores: the
     restated reference algorithms of oracle/ (bounded samples of the same
@@ -446,6 +462,8 @@ def app_cpu_baselines(torch, res):
             "pageRank_cpu push arithmetic (oracle/oracle.c, bit-identical to the reference's), one iteration of "
             "the full R-MAT 2^22/2^26 graph, one thread", dt)
         del s_, d_, src, dst, order
+        if "subtask_reduce_add_f32_8x2^24" in res:
+            res["subtask_reduce_add_f32_8x2^24"]["cpu_baseline"] = reduce_cpu_baseline(orc)
     # GEMM: the reference CPU callback is cblas_sgemm (matrixMultiplyBlas.cpp:62-65).
     dim = 2048
     A = rng.random((dim, dim), dtype=np.float32) * 2 - 1
