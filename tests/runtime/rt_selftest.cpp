@@ -552,6 +552,62 @@ pmStatus bucket_redistribution(pmTaskInfo ti, pmDeviceInfo di, pmSubtaskInfo si)
     return pmSuccess;
 }
 
+// Each subtask names its chunk as two halves with orders 2 id and 2 id + 1:
+// the address space keeps its bytes (ranges that continue one another are
+// moved as one copy).
+pmStatus halves_redistribution(pmTaskInfo ti, pmDeviceInfo di, pmSubtaskInfo si) {
+    const size_t bytes = size_t(chunk_len(si.subtaskId)) * 4, half = bytes / 8 * 4;
+    pmStatus st = pmRedistributeData(ti.taskHandle, di.deviceHandle, si.subtaskId, si.splitInfo, 1, 0, half,
+                                     uint(2 * si.subtaskId));
+    if (st == pmSuccess)
+        st = pmRedistributeData(ti.taskHandle, di.deviceHandle, si.subtaskId, si.splitInfo, 1, half, bytes - half,
+                                uint(2 * si.subtaskId + 1));
+    return st;
+}
+
+void test_redistribute_halves(bool gpu) {
+    pmCallbacks cb;
+    cb.dataDistribution = bucket_dd;
+    cb.subtask_cpu = bucket_cpu;
+    if (gpu) cb.subtask_gpu_cuda = reinterpret_cast<pmSubtaskCallback_GPU_CUDA>(rt_bucket_kernel_ptr());
+    cb.dataRedistribution = halves_redistribution;
+    pmCallbackHandle h;
+    CHECK(pmRegisterCallbacks("HALVES", cb, &h) == pmSuccess, "register");
+    pmMemHandle in, out;
+    CHECK(pmCreateMemory(size_t(kKeys) * 4, &in) == pmSuccess && pmCreateMemory(size_t(kKeys) * 4, &out) == pmSuccess,
+          "create");
+    void *ip, *op;
+    pmGetRawMemPtr(in, &ip);
+    int* keys = static_cast<int*>(ip);
+    for (int i = 0; i < kKeys; ++i) keys[i] = int((unsigned(i) * 40503u + 7u) % 100000u);
+    static int buckets = kBuckets;
+    pmTaskMem mem[2] = {pmTaskMem(in, READ_ONLY, SUBSCRIPTION_NATURAL), pmTaskMem(out, WRITE_ONLY, SUBSCRIPTION_NATURAL)};
+    const unsigned long nsub = (kKeys + kChunk - 1) / kChunk;
+    pmTaskDetails td(&buckets, sizeof(buckets), mem, 2, h, nsub);
+    pmTaskHandle t;
+    CHECK(pmSubmitTask(td, &t) == pmSuccess, "submit");
+    CHECK(pmWaitForTaskCompletion(t) == pmSuccess, "task failed");
+    // each chunk stays where it is, grouped by bucket inside the chunk
+    std::vector<int> expect;
+    for (unsigned long sub = 0; sub < nsub; ++sub)
+        for (int b = 0; b < kBuckets; ++b)
+            for (int i = int(sub) * kChunk; i < int(sub) * kChunk + chunk_len(sub); ++i)
+                if (keys[i] % kBuckets == b) expect.push_back(keys[i]);
+    CHECK(pmFetchMemory(out) == pmSuccess, "fetch");
+    pmGetRawMemPtr(out, &op);
+    CHECK(std::memcmp(expect.data(), op, size_t(kKeys) * 4) == 0, "halves redistribution moved bytes");
+    ulong count = 0;
+    const pmRedistributionMetadata* md = pmGetRedistributionMetadata(t, 1, &count);
+    CHECK(md && count == 2 * nsub, "metadata count %lu", count);
+    for (unsigned long sub = 0; sub < nsub; ++sub) {
+        const uint bytes = uint(chunk_len(sub)) * 4, half = bytes / 8 * 4;
+        CHECK(md[2 * sub].order == 2 * sub && md[2 * sub].count == half && md[2 * sub + 1].count == bytes - half,
+              "metadata of subtask %lu", sub);
+    }
+    CHECK(pmReleaseTask(t) == pmSuccess, "release");
+    CHECK(pmReleaseMemory(in) == pmSuccess && pmReleaseMemory(out) == pmSuccess, "release memory");
+}
+
 void test_redistribute(bool gpu) {
     pmCallbacks cb;
     cb.dataDistribution = bucket_dd;
@@ -633,8 +689,13 @@ int main(int argc, char** argv) {
     else if (g_test == "timeout") test_timeout();
     else if (g_test == "reduce_cpu") test_reduce(false);
     else if (g_test == "reduce_gpu") test_reduce(true);
-    else if (g_test == "redistribute_cpu") test_redistribute(false);
-    else if (g_test == "redistribute_gpu") test_redistribute(true);
+    else if (g_test == "redistribute_cpu") {
+        test_redistribute(false);
+        test_redistribute_halves(false);
+    } else if (g_test == "redistribute_gpu") {
+        test_redistribute(true);
+        test_redistribute_halves(true);
+    }
     else CHECK(false, "unknown test");
     CHECK(pmFinalize() == pmSuccess, "finalize");
     std::printf("PASS %s\n", g_test.c_str());

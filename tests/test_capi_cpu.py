@@ -61,3 +61,34 @@ def test_image_filter_argument_checks(pmb):
     assert b"input view" in pmb.pmb_last_error()
     # too many items
     assert pmb.pmb_image_filter(it, capi.PMB_IMGF_MAX_ITEMS + 1, ptr(f), 1, 0, None) == 7
+
+
+def test_reduce_argument_checks(pmb):
+    """pmb_reduce_elementwise refuses bad operations, types, counts and
+    misaligned pointers on the host (the fake device addresses are never
+    dereferenced)."""
+    srcs = (ctypes.c_void_p * 2)(0x1000, 0x2000)
+    arr = ctypes.cast(srcs, ctypes.c_void_p)
+    assert pmb.pmb_reduce_element_size(0) == 4 and pmb.pmb_reduce_element_size(5) == 8
+    assert pmb.pmb_reduce_element_size(6) == 0
+    assert pmb.pmb_reduce_elementwise(0, 0, None, arr, 2, 16, 1, None) == 7       # null destination
+    assert pmb.pmb_reduce_elementwise(0, 0, 0x3000, arr, 0, 16, 1, None) == 7     # no sources
+    assert pmb.pmb_reduce_elementwise(0, 9, 0x3000, arr, 2, 16, 1, None) == 7     # unknown type
+    assert pmb.pmb_reduce_elementwise(0, 3, 0x3004, arr, 2, 16, 1, None) == 7     # 8-byte elements, 4-aligned
+    bad = (ctypes.c_void_p * 2)(0x1000, 0x2002)
+    assert pmb.pmb_reduce_elementwise(0, 0, 0x3000, ctypes.cast(bad, ctypes.c_void_p), 2, 16, 1, None) == 7
+    assert b"aligned" in pmb.pmb_last_error()
+
+
+def test_webdump_argument_checks(pmb):
+    d = 0x1000
+    # more pages than vertices; no slots; scratch too small
+    assert pmb.pmb_csr_from_webdump(d, 10, 4, 5, 8, d, d, d, d, 1 << 30, None) == 7
+    assert pmb.pmb_csr_from_webdump(d, 10, 0, 10, 8, d, d, d, d, 1 << 30, None) == 7
+    need = pmb.pmb_webdump_csr_scratch_bytes(10, 10, 8)
+    assert need > 0
+    assert pmb.pmb_csr_from_webdump(d, 10, 4, 10, 8, d, d, d, d, need - 1, None) == 7
+    assert pmb.pmb_csr_from_webdump(None, 10, 4, 10, 8, d, d, d, d, need, None) == 7
+    # push: null output, no vertices
+    assert pmb.pmb_webdump_push(d, 10, 4, None, 1.0, 0.85, None, 10, None, None) == 7
+    assert pmb.pmb_webdump_push(d, 10, 4, None, 1.0, 0.85, d, 0, None, None) == 7

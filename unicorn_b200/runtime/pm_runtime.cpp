@@ -860,7 +860,10 @@ static pmStatus redist_plan(Task* t, size_t i, std::vector<RedistCopy>& copies) 
         if (run + r.length > t->spaces[i]->length)
             return fail(pmInvalidIndex, "redistribution of address space %zu: %zu bytes beyond its %zu", i,
                         run + r.length, t->spaces[i]->length);
-        copies.push_back({r.offset, run, r.length});
+        if (!copies.empty() && copies.back().src + copies.back().len == r.offset)
+            copies.back().len += r.length;  // continues the previous range in both places: one copy
+        else
+            copies.push_back({r.offset, run, r.length});
         if (meta.empty() || meta.back().order != r.order) meta.emplace_back(r.order, 0u);
         meta.back().count += static_cast<uint>(r.length);
         run += r.length;
