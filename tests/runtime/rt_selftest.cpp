@@ -392,8 +392,8 @@ T row_value(int s, int j, int op) {
 // One task: returns its status; on success compares the output with the fold.
 template <typename T, typename B>
 void reduce_case(bool gpu, int op, int type, pmDataReductionCallback custom, int custom_kind, int accumulate,
-                 OutSub sub) {
-    const int n = kRowWords * 4 / int(sizeof(T));
+                 OutSub sub, int words = kRowWords) {
+    const int n = words * 4 / int(sizeof(T));
     pmCallbacks cb;
     cb.dataDistribution = row_dd;
     cb.subtask_cpu = row_cpu;
@@ -406,8 +406,8 @@ void reduce_case(bool gpu, int op, int type, pmDataReductionCallback custom, int
     CHECK(pmRegisterCallbacks(key, cb, &h) == pmSuccess, "register");
 
     pmMemHandle in, out;
-    CHECK(pmCreateMemory(size_t(kRowSubtasks) * kRowWords * 4, &in) == pmSuccess, "create in");
-    CHECK(pmCreateMemory(size_t(kRowWords) * 4, &out) == pmSuccess, "create out");
+    CHECK(pmCreateMemory(size_t(kRowSubtasks) * words * 4, &in) == pmSuccess, "create in");
+    CHECK(pmCreateMemory(size_t(words) * 4, &out) == pmSuccess, "create out");
     void *ip, *op_;
     pmGetRawMemPtr(in, &ip);
     pmGetRawMemPtr(out, &op_);
@@ -419,7 +419,7 @@ void reduce_case(bool gpu, int op, int type, pmDataReductionCallback custom, int
     for (int j = 0; j < n; ++j) init[j] = outp[j] = row_value<T>(100, j, op);
 
     static RtRowConf conf;
-    conf = RtRowConf{kRowWords, accumulate, type, op};
+    conf = RtRowConf{words, accumulate, type, op};
     g_out_sub = sub;
     const bool reads_out = accumulate || sub == OutSub::Inner || sub == OutSub::Scattered;
     pmTaskMem mem[2] = {pmTaskMem(in, READ_ONLY, SUBSCRIPTION_NATURAL),
@@ -447,8 +447,8 @@ void reduce_case(bool gpu, int op, int type, pmDataReductionCallback custom, int
             }
             const size_t byte = size_t(j) * sizeof(T);
             bool written = true;
-            if (sub == OutSub::Inner) written = byte >= 64 && byte < size_t(kRowWords) * 4 - 8;
-            if (sub == OutSub::Scattered) written = byte % 128 < 64 && byte / 128 < size_t(kRowWords) * 4 / 128;
+            if (sub == OutSub::Inner) written = byte >= 64 && byte < size_t(words) * 4 - 8;
+            if (sub == OutSub::Scattered) written = byte % 128 < 64 && byte / 128 < size_t(words) * 4 / 128;
             expect[j] = written ? acc : init[j];
         }
         CHECK(std::memcmp(expect.data(), outp, size_t(n) * sizeof(T)) == 0,
@@ -490,6 +490,8 @@ void test_reduce(bool gpu) {
     reduce_case<int32_t, int32_t>(gpu, REDUCE_ADD, REDUCE_INTS, axpy3_reduction, 1, 0, OutSub::Whole);
     reduce_case<int32_t, int32_t>(gpu, REDUCE_BITWISE_OR, REDUCE_INTS, or_reduction, 2, 0, OutSub::Whole);
     reduce_case<int32_t, int32_t>(gpu, REDUCE_ADD, REDUCE_INTS, axpy3_reduction, 1, 0, OutSub::Scattered);
+    // a 4 MiB copy per subtask: the host fold splits it over the cores
+    reduce_case<float, uint32_t>(gpu, REDUCE_ADD, REDUCE_FLOATS, nullptr, 0, 0, OutSub::Whole, 1 << 20);
     // subtasks subscribing different ranges: the task fails before it runs
     reduce_case<int32_t, int32_t>(gpu, REDUCE_ADD, REDUCE_INTS, nullptr, 0, 0, OutSub::Mismatched);
 }

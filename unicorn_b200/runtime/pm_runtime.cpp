@@ -611,20 +611,39 @@ static void host_fold(int op, T* a, const T* b, size_t n) {
     }
 }
 
+static void host_fold_range(int op, int type, char* a, const char* b, size_t n);
+
+// Large folds are split over the host cores in contiguous element ranges (the
+// reference's loops are OpenMP-parallel, pmReducer.cpp:593-700).
 static pmStatus host_reduce(int op, int type, void* a, const void* b, size_t bytes) {
     if (op < 0 || op >= MAX_REDUCTION_OP_TYPES) return fail(pmInvalidIndex, "unknown reduction operation %d", op);
     const size_t es = pmb_reduce_element_size(type);
     if (!es) return fail(pmInvalidIndex, "unknown reduction data type %d", type);
     const size_t n = bytes / es;
-    switch (type) {
-        case REDUCE_INTS: host_fold<int32_t, int32_t>(op, static_cast<int32_t*>(a), static_cast<const int32_t*>(b), n); break;
-        case REDUCE_UNSIGNED_INTS: host_fold<uint32_t, uint32_t>(op, static_cast<uint32_t*>(a), static_cast<const uint32_t*>(b), n); break;
-        case REDUCE_LONGS: host_fold<int64_t, int64_t>(op, static_cast<int64_t*>(a), static_cast<const int64_t*>(b), n); break;
-        case REDUCE_UNSIGNED_LONGS: host_fold<uint64_t, uint64_t>(op, static_cast<uint64_t*>(a), static_cast<const uint64_t*>(b), n); break;
-        case REDUCE_FLOATS: host_fold<float, uint32_t>(op, static_cast<float*>(a), static_cast<const float*>(b), n); break;
-        default: host_fold<double, uint64_t>(op, static_cast<double*>(a), static_cast<const double*>(b), n); break;
+    const size_t parts = std::min<size_t>(std::max(1u, std::thread::hardware_concurrency()), n >> 18);
+    if (parts <= 1) {
+        host_fold_range(op, type, static_cast<char*>(a), static_cast<const char*>(b), n);
+        return pmSuccess;
     }
+    std::vector<std::thread> pool;
+    for (size_t p = 0; p < parts; ++p) {
+        const size_t lo = n * p / parts, hi = n * (p + 1) / parts;
+        pool.emplace_back(host_fold_range, op, type, static_cast<char*>(a) + lo * es,
+                          static_cast<const char*>(b) + lo * es, hi - lo);
+    }
+    for (auto& th : pool) th.join();
     return pmSuccess;
+}
+
+static void host_fold_range(int op, int type, char* a, const char* b, size_t n) {
+    switch (type) {
+        case REDUCE_INTS: host_fold<int32_t, int32_t>(op, reinterpret_cast<int32_t*>(a), reinterpret_cast<const int32_t*>(b), n); break;
+        case REDUCE_UNSIGNED_INTS: host_fold<uint32_t, uint32_t>(op, reinterpret_cast<uint32_t*>(a), reinterpret_cast<const uint32_t*>(b), n); break;
+        case REDUCE_LONGS: host_fold<int64_t, int64_t>(op, reinterpret_cast<int64_t*>(a), reinterpret_cast<const int64_t*>(b), n); break;
+        case REDUCE_UNSIGNED_LONGS: host_fold<uint64_t, uint64_t>(op, reinterpret_cast<uint64_t*>(a), reinterpret_cast<const uint64_t*>(b), n); break;
+        case REDUCE_FLOATS: host_fold<float, uint32_t>(op, reinterpret_cast<float*>(a), reinterpret_cast<const float*>(b), n); break;
+        default: host_fold<double, uint64_t>(op, reinterpret_cast<double*>(a), reinterpret_cast<const double*>(b), n); break;
+    }
 }
 
 // The reducible address spaces of a task and the one range their writing
