@@ -1,10 +1,17 @@
-"""Generate the imageFilter golden fixtures from the reference's own CPU code.
+"""Generate golden fixtures from the reference's own CPU code.
 
-Runs the reference's imageFilterDataDistribution + imageFilter_cpu (compiled
-unchanged from testSuite/imageFiltering/source/code/src/imageFiltering.cpp into
-oracle/_ref/libref_imgf.so by oracle/ref/Makefile) on small seeded inputs and
-stores inputs, filters and outputs in imgf_golden.npz, plus the reference's
-subscription geometry for a few image shapes in imgf_subscriptions.json.
+* imageFilter: runs the reference's imageFilterDataDistribution +
+  imageFilter_cpu (compiled unchanged from
+  testSuite/imageFiltering/source/code/src/imageFiltering.cpp into
+  oracle/_ref/libref_imgf.so by oracle/ref/Makefile) on small seeded inputs and
+  stores inputs, filters and outputs in imgf_golden.npz, plus the reference's
+  subscription geometry for a few image shapes in imgf_subscriptions.json.
+* matrixMultiplyBlas and luDecomposition: runs the reference's
+  matrixMultiplyDataDistribution + matrixMultiply_cpu and serialLUDecomposition
+  (matrixMultiplyBlas.cpp, luDecomposition.cpp, compiled unchanged into
+  oracle/_ref/libref_mm.so and libref_lu.so over a CBLAS shim on numpy's
+  OpenBLAS) on small seeded inputs, and records the GEMM subscription geometry
+  of the 1024 (blocks of 256) and 4096 (blocks of 2048) tasks: blas_golden.npz.
 
 Usage (in a tree where the reference is available):
     make -C oracle/ref && python tests/golden/make_golden.py
@@ -60,5 +67,46 @@ def main() -> None:
         json.dump(subs, fh)
 
 
+# GEMM (n, block, seed) and LU (n, ld, seed) cases of blas_golden.npz.
+MM_CASES = [(64, 32, 21), (96, 48, 22)]
+LU_CASES = [(7, 7, 23), (48, 50, 24)]
+MM_SUB_SHAPES = [(1024, 256), (4096, 2048)]
+
+
+def main_blas() -> None:
+    P = ctypes.c_void_p
+    mm = ctypes.CDLL(os.path.join(ROOT, "oracle", "_ref", "libref_mm.so"))
+    lu = ctypes.CDLL(os.path.join(ROOT, "oracle", "_ref", "libref_lu.so"))
+    out = {}
+    for idx, (n, block, seed) in enumerate(MM_CASES):
+        rng = np.random.default_rng(seed)
+        a = rng.uniform(-1, 1, (n, n)).astype(np.float32)
+        b = rng.uniform(-1, 1, (n, n)).astype(np.float32)
+        c = np.zeros_like(a)
+        st = mm.ref_mm_task(a.ctypes.data_as(P), b.ctypes.data_as(P), c.ctypes.data_as(P), ctypes.c_ulong(n),
+                            ctypes.c_ulong(block))
+        assert st == 0, st
+        out[f"mm{idx}_meta"] = np.array([n, block, seed], np.int64)
+        out[f"mm{idx}_a"], out[f"mm{idx}_b"], out[f"mm{idx}_c"] = a, b, c
+    for idx, (n, ld, seed) in enumerate(LU_CASES):
+        rng = np.random.default_rng(seed)
+        a = rng.uniform(-1, 1, (n, ld)).astype(np.float32)  # row k of this array = column k (column-major)
+        a[np.arange(n), np.arange(n)] += n
+        r = a.copy()
+        assert lu.ref_lu_serial(r.ctypes.data_as(P), ctypes.c_ulong(n), ctypes.c_ulong(ld)) == 0
+        out[f"lu{idx}_meta"] = np.array([n, ld, seed], np.int64)
+        out[f"lu{idx}_in"], out[f"lu{idx}_out"] = a, r
+    buf = (ctypes.c_ulonglong * 15)()
+    for idx, (n, block) in enumerate(MM_SUB_SHAPES):
+        rows = []
+        for sid in range((n // block) ** 2):
+            assert mm.ref_mm_subscriptions(ctypes.c_ulong(n), ctypes.c_ulong(block), ctypes.c_ulong(sid), buf) == 0
+            rows.append([int(x) for x in buf])
+        out[f"mmsub{idx}_meta"] = np.array([n, block], np.int64)
+        out[f"mmsub{idx}"] = np.array(rows, np.uint64)
+    np.savez_compressed(os.path.join(HERE, "blas_golden.npz"), **out)
+
+
 if __name__ == "__main__":
     main()
+    main_blas()
