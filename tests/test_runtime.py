@@ -13,6 +13,11 @@
   and harness (imageFiltering.cpp + commonAPI.cpp, unchanged) linked against
   this runtime and the B200 GPU callbacks; it checks itself against its serial
   CPU implementation and prints "Serial Comparison Test Passed".
+* oracle/_ref/matrixMultiplyBlas_b200.exe and luDecomposition_cpu.exe: the
+  reference's BLAS apps (matrixMultiplyBlas.cpp, luDecomposition.cpp +
+  commonAPI.cpp, unchanged, CBLAS through the shim on numpy's OpenBLAS) on the
+  runtime's CPU stub: scattered row/column-block subscriptions, and the LU
+  app's three stage tasks per block step with pTaskInfo.taskId as the step.
 """
 from __future__ import annotations
 
@@ -25,6 +30,8 @@ from conftest import ROOT
 
 SELFTEST = os.path.join(ROOT, "tests", "runtime", "_build", "rt_selftest")
 APP = os.path.join(ROOT, "oracle", "_ref", "imageFiltering_b200.exe")
+MM_APP = os.path.join(ROOT, "oracle", "_ref", "matrixMultiplyBlas_b200.exe")
+LU_APP = os.path.join(ROOT, "oracle", "_ref", "luDecomposition_cpu.exe")
 
 
 @pytest.fixture(scope="module")
@@ -53,10 +60,10 @@ def test_runtime_gpu(selftest, name):
     assert rc == 0 and f"PASS {name}" in out, out
 
 
-def app_or_skip():
-    if not os.path.exists(APP):
+def app_or_skip(path=APP):
+    if not os.path.exists(path):
         pytest.skip("reference app not built (oracle/ref/Makefile needs the reference tree)")
-    return APP
+    return path
 
 
 def test_reference_app_cpu_mode_on_b200_runtime():
@@ -82,3 +89,22 @@ def test_reference_app_single_gpu_mode():
     """Run mode 4: the app's single-GPU path (singleGpuImageFilter) vs serial."""
     rc, out = run([app_or_skip(), "4", "2", "0", "2", "0", "3000", "1000", "1"])
     assert rc == 0 and "Single GPU Task's Sequential Comparison Test Passed" in out, out
+
+
+@pytest.mark.parametrize("n", ["300", "1024", "4096"])
+def test_reference_matrix_multiply_app_cpu_mode(n):
+    """The unchanged matrixMultiplyBlas app, parallel mode 1: (n / min(n, 2048))^2
+    subtasks (4 at 4096) over row-block / column-block / block subscriptions,
+    compared by the app with its serial cblas_sgemm (relative 1e-5 per element)."""
+    rc, out = run([app_or_skip(MM_APP), "1", "1", "0", n])
+    assert rc == 0 and "Serial Comparison Test Passed" in out and "Failed" not in out, out
+
+
+def test_reference_lu_app_cpu_mode():
+    """The unchanged luDecomposition app, parallel mode 1, 4096 = 2 x 2 blocks of
+    2048: LU_DECOMPOSE, HORZ_VERT_COMP (2 subtasks), DIAGONAL_COMP, LU_DECOMPOSE as
+    four tasks on one address space.  The app does not compare fp32 results
+    (luDecomposition.cpp:593-595); tests/test_blas_ref_oracle.py checks the same
+    stage sequence against the FP64 Crout factors."""
+    rc, out = run([app_or_skip(LU_APP), "1", "1", "0", "4096"])
+    assert rc == 0 and "Parallel Task 1 Execution Time" in out and "Failed" not in out, out
