@@ -464,6 +464,9 @@ def app_cpu_baselines(torch, res):
         del s_, d_, src, dst, order
         if "subtask_reduce_add_f32_8x2^24" in res:
             res["subtask_reduce_add_f32_8x2^24"]["cpu_baseline"] = reduce_cpu_baseline(orc)
+    if blas_reference_baselines(res, cores):
+        return
+    # Without oracle/_ref: the same BLAS calls on numpy's OpenBLAS.
     # GEMM: the reference CPU callback is cblas_sgemm (matrixMultiplyBlas.cpp:62-65).
     dim = 2048
     A = rng.random((dim, dim), dtype=np.float32) * 2 - 1
@@ -501,6 +504,75 @@ def app_cpu_baselines(torch, res):
     res["lu_4096"]["cpu_baseline"] = _cpu_entry(
         (2.0 / 3.0) * nl ** 3 / dt / 1e9, "GFLOP/s", cores, "port",
         f"blocked Crout LU n={nl}, nb={nb}: the reference's 3 stages on numpy/scipy BLAS, all cores", dt)
+
+
+def _time_reps(fn, min_seconds: float):
+    """Seconds per call of fn, over at least min_seconds (one untimed call first)."""
+    fn()
+    reps, t0 = 0, time.perf_counter()
+    while True:
+        fn()
+        reps += 1
+        dt = time.perf_counter() - t0
+        if dt >= min_seconds:
+            return dt / reps
+
+
+def blas_reference_baselines(res, cores: int, min_seconds: float = 2.0) -> bool:
+    """GEMM and LU CPU figures from the reference's own CPU callbacks,
+    compiled unchanged over numpy's OpenBLAS (oracle/_ref/libref_mm.so,
+    libref_lu.so), all host cores through the BLAS threads:
+    * gemm 1024: the task of 16 subtasks of 256 x 256 (matrixMultiply_cpu),
+      fp32 U[-1,1] from seed 0 -- the reference's CPU-runnable configuration;
+    * gemm 8192: a bounded sample, the 4096 task in the reference's own
+      2048 x 2048 blocks (4 subtasks);
+    * LU 4096: the app's LU_DECOMPOSE / HORZ_VERT_COMP / DIAGONAL_COMP sequence
+      at its BLOCK_DIM 2048 on a diagonally dominant matrix (fresh copy per
+      run, copy time excluded).
+    Returns False (and sets nothing) when the libraries are absent."""
+    mm_path = os.path.join(ROOT, "oracle", "_ref", "libref_mm.so")
+    lu_path = os.path.join(ROOT, "oracle", "_ref", "libref_lu.so")
+    if not (os.path.exists(mm_path) and os.path.exists(lu_path)):
+        return False
+    mm, lu = ctypes.CDLL(mm_path), ctypes.CDLL(lu_path)
+    P, U = ctypes.c_void_p, ctypes.c_ulong
+    entries = {}
+    for key, n, block, seed in (("gemm_bf16x3_1024", 1024, 256, 0), ("gemm_bf16x3_8192", 4096, 2048, 1)):
+        rng = np.random.default_rng(seed)
+        a = rng.uniform(-1, 1, (n, n)).astype(np.float32)
+        b = rng.uniform(-1, 1, (n, n)).astype(np.float32)
+        c = np.empty_like(a)
+        args = (a.ctypes.data_as(P), b.ctypes.data_as(P), c.ctypes.data_as(P), U(n), U(block))
+
+        def run(args=args):
+            if mm.ref_mm_task(*args) != 0:
+                raise RuntimeError("reference matrixMultiply task failed")
+
+        dt = _time_reps(run, min_seconds)
+        entries[key] = _cpu_entry(2.0 * n ** 3 / dt / 1e12, "TFLOP/s", cores, "reference",
+                                  f"reference matrixMultiply_cpu (oracle/_ref), {n}^2 fp32 in "
+                                  f"{(n // block) ** 2} subtasks of {block}^2, all cores (BLAS threads)", dt)
+    nl = 4096
+    rng = np.random.default_rng(5)
+    a0 = rng.uniform(-1, 1, (nl, nl)).astype(np.float32)
+    a0[np.arange(nl), np.arange(nl)] += nl
+    work = np.empty_like(a0)
+    total, runs = 0.0, 0
+    while total < min_seconds or runs < 2:
+        np.copyto(work, a0)
+        t0 = time.perf_counter()
+        if lu.ref_lu_blocked(work.ctypes.data_as(P), U(nl)) != 0:
+            raise RuntimeError("reference blocked LU failed")
+        total += time.perf_counter() - t0
+        runs += 1
+    dt = total / runs
+    entries["lu_4096"] = _cpu_entry(
+        (2.0 / 3.0) * nl ** 3 / dt / 1e9, "GFLOP/s", cores, "reference",
+        f"reference luDecomposition stages (oracle/_ref), n={nl} in blocks of 2048, all cores (BLAS threads)", dt)
+    for key, e in entries.items():
+        if key in res:
+            res[key]["cpu_baseline"] = e
+    return True
 
 
 SERVED_BIN = os.path.join(ROOT, "unicorn_b200", "serve", "_build", "served_mix")
@@ -675,7 +747,12 @@ def main():
     barrier()
     e2e_ms = max_over_ranks(e0.elapsed_time(e1))
     e2e_value = ranks.rate(ALG_BYTES, args.steps, e2e_ms)
-    apps = app_measurements(torch, L, stream) if (rank == 0 and not args.no_apps) else None
+    apps = None
+    if rank == 0 and not args.no_apps:
+        try:
+            apps = app_measurements(torch, L, stream)
+        except Exception as e:  # the extra kernels must not lose the headline line
+            apps = {"error": f"{type(e).__name__}: {e}"}
 
     peak, peak_kind = peaks()
     line = {
@@ -695,12 +772,18 @@ def main():
         "clocks": clk.summary(),
     }
     if apps is not None:
-        if not args.no_cpu_baseline:
-            app_cpu_baselines(torch, apps)
+        if not args.no_cpu_baseline and "error" not in apps:
+            try:
+                app_cpu_baselines(torch, apps)
+            except Exception as e:
+                apps["cpu_baseline_error"] = f"{type(e).__name__}: {e}"
         line["apps"] = apps
     if rank == 0 and world == 1 and not args.no_served:
         torch.cuda.empty_cache()  # the served stream runs in its own process: leave it the device
-        line["served_mix"] = served_measurement()
+        try:
+            line["served_mix"] = served_measurement()
+        except Exception as e:
+            line["served_mix"] = {"error": f"{type(e).__name__}: {e}"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(img, f, os.cpu_count() or 1)
     ranks.close()
