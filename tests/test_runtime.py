@@ -18,6 +18,9 @@
   commonAPI.cpp, unchanged, CBLAS through the shim on numpy's OpenBLAS) on the
   runtime's CPU stub: scattered row/column-block subscriptions, and the LU
   app's three stage tasks per block step with pTaskInfo.taskId as the step.
+* oracle/_ref/matrixMultiply_b200.exe: the reference's int matrixMultiply app
+  with its own subtask_gpu_cuda kernel file (unchanged), one output row per
+  subtask, on the runtime's CPU stub.
 """
 from __future__ import annotations
 
@@ -32,6 +35,7 @@ SELFTEST = os.path.join(ROOT, "tests", "runtime", "_build", "rt_selftest")
 APP = os.path.join(ROOT, "oracle", "_ref", "imageFiltering_b200.exe")
 MM_APP = os.path.join(ROOT, "oracle", "_ref", "matrixMultiplyBlas_b200.exe")
 LU_APP = os.path.join(ROOT, "oracle", "_ref", "luDecomposition_cpu.exe")
+INT_MM_APP = os.path.join(ROOT, "oracle", "_ref", "matrixMultiply_b200.exe")
 
 
 @pytest.fixture(scope="module")
@@ -108,3 +112,12 @@ def test_reference_lu_app_cpu_mode():
     stage sequence against the FP64 Crout factors."""
     rc, out = run([app_or_skip(LU_APP), "1", "1", "0", "4096"])
     assert rc == 0 and "Parallel Task 1 Execution Time" in out and "Failed" not in out, out
+
+
+@pytest.mark.parametrize("n", ["1000", "257"])
+def test_reference_int_matrix_multiply_app_cpu_mode(n):
+    """The unchanged int matrixMultiply app, parallel mode 1: n subtasks of one
+    output row each, every subtask subscribing the whole of B, compared by the
+    app with its serial run."""
+    rc, out = run([app_or_skip(INT_MM_APP), "1", "1", "0", n])
+    assert rc == 0 and "Serial Comparison Test Passed" in out and "Failed" not in out, out
