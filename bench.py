@@ -244,7 +244,7 @@ def _timed(torch, stream, fn, iters: int, warmup: int = 2) -> float:
 
 
 def app_measurements(torch, L, stream):
-    """The other kernels of the path on their SURVEY §8(d) configurations,
+    """The other kernels of the path on their own configurations (sizes below),
     each against its roofline (measured peaks)."""
     from unicorn_b200 import capi, ops
 

@@ -116,7 +116,7 @@ int run_one(imageFilterTaskConf* conf, unsigned long nsub, const uint8_t* in, ui
 
 extern "C" {
 
-/* Reference tile edge (TILE_DIM of imageFiltering.h) this build was compiled with. */
+/* Reference tile edge (TILE_DIM of imageFiltering.h) this library was compiled with. */
 int ref_imgf_tile_dim(void) { return TILE_DIM; }
 
 /* Number of subtasks the reference would create for a W x H image. */

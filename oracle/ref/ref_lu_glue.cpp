@@ -65,7 +65,7 @@ int run_stage(Cb dd, Cb cpu, float* A, size_t n, size_t task, unsigned long subt
 
 extern "C" {
 
-/* BLOCK_DIM of luDecomposition.h this build was compiled with. */
+/* BLOCK_DIM of luDecomposition.h this library was compiled with. */
 unsigned long ref_lu_block_dim(void) { return BLOCK_DIM; }
 
 /* In-place serialLUDecomposition of the leading n x n block of a

@@ -25,7 +25,7 @@ using namespace matrixMultiplyBlas;
 
 extern "C" {
 
-/* BLOCK_DIM of matrixMultiplyBlas.h this build was compiled with. */
+/* BLOCK_DIM of matrixMultiplyBlas.h this library was compiled with. */
 int ref_mm_block_dim(void) { return BLOCK_DIM; }
 
 /* The reference app's block size for an n x n product (getBlockSize, :52-55). */
