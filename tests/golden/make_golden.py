@@ -12,6 +12,10 @@
   oracle/_ref/libref_mm.so and libref_lu.so over a CBLAS shim on numpy's
   OpenBLAS) on small seeded inputs, and records the GEMM subscription geometry
   of the 1024 (blocks of 256) and 4096 (blocks of 2048) tasks: blas_golden.npz.
+* prefixSum and radixSort: runs the reference's serialPrefixSum and
+  serialLsbRadixSort / serialLsbRadixSortRound (cut unchanged out of
+  prefixSum.cpp and radixSort.cpp by oracle/ref/extract_serial.py into
+  oracle/_ref/libref_scan_sort.so) on seeded inputs: scan_sort_golden.npz.
 
 Usage (in a tree where the reference is available):
     make -C oracle/ref && python tests/golden/make_golden.py
@@ -107,6 +111,36 @@ def main_blas() -> None:
     np.savez_compressed(os.path.join(HERE, "blas_golden.npz"), **out)
 
 
+def main_scan_sort() -> None:
+    P = ctypes.c_void_p
+    ref = ctypes.CDLL(os.path.join(ROOT, "oracle", "_ref", "libref_scan_sort.so"))
+    out = {}
+    rng = np.random.default_rng(31)
+    # int32 scan (the reference's type) of values that cannot overflow it
+    x = rng.integers(0, 1 << 20, 1000, dtype=np.int32)
+    y = np.zeros_like(x)
+    ref.ref_serial_prefix_sum_i32(x.ctypes.data_as(P), y.ctypes.data_as(P), ctypes.c_uint(x.size))
+    out["scan_in"], out["scan_out"] = x, y
+    # full LSD sort (BITS_PER_ROUND-bit digits, TOTAL_ROUNDS rounds) and each single round
+    rng = np.random.default_rng(32)
+    keys = np.concatenate([rng.integers(0, 2**32, 2500, dtype=np.uint32),
+                           rng.integers(0, 8, 500, dtype=np.uint32) * np.uint32(0x10203041)])
+    rounds = ref.ref_radix_total_rounds()
+    srt = np.zeros_like(keys)
+    ref.ref_serial_lsb_radix_sort_u32(keys.ctypes.data_as(P), srt.ctypes.data_as(P), ctypes.c_uint(keys.size),
+                                      rounds)
+    out["sort_meta"] = np.array([ref.ref_radix_bits_per_round(), rounds], np.int64)
+    out["sort_in"], out["sort_out"] = keys, srt
+    for r in range(rounds):
+        o = np.zeros_like(keys)
+        bins = np.zeros(1 << ref.ref_radix_bits_per_round(), np.int32)
+        ref.ref_serial_lsb_radix_round_u32(keys.ctypes.data_as(P), o.ctypes.data_as(P), ctypes.c_uint(keys.size),
+                                           r, bins.ctypes.data_as(P))
+        out[f"round{r}_out"], out[f"round{r}_bins"] = o, bins
+    np.savez_compressed(os.path.join(HERE, "scan_sort_golden.npz"), **out)
+
+
 if __name__ == "__main__":
     main()
     main_blas()
+    main_scan_sort()
