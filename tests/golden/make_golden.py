@@ -16,6 +16,10 @@
   serialLsbRadixSort / serialLsbRadixSortRound (cut unchanged out of
   prefixSum.cpp and radixSort.cpp by oracle/ref/extract_serial.py into
   oracle/_ref/libref_scan_sort.so) on seeded inputs: scan_sort_golden.npz.
+* subtask reduction: runs the reference runtime's pmReducer::ReduceMemories
+  (cut unchanged out of pmReducer.cpp into oracle/_ref/libref_reduce.so) for
+  every operation and data type on the inputs tests/test_reduce_oracle.py
+  generates: reduce_golden.npz.
 
 Usage (in a tree where the reference is available):
     make -C oracle/ref && python tests/golden/make_golden.py
@@ -140,7 +144,27 @@ def main_scan_sort() -> None:
     np.savez_compressed(os.path.join(HERE, "scan_sort_golden.npz"), **out)
 
 
+def main_reduce() -> None:
+    import sys
+
+    sys.path.insert(0, os.path.dirname(HERE))
+    from test_reduce_oracle import DTYPES, values
+
+    P = ctypes.c_void_p
+    ref = ctypes.CDLL(os.path.join(ROOT, "oracle", "_ref", "libref_reduce.so"))
+    out = {}
+    for name, (code, dt) in DTYPES.items():
+        for op in range(10):
+            a, b = values(dt, op, 33, 1), values(dt, op, 33, 2)
+            r = a.copy()
+            assert ref.ref_reduce_memories(op, code, r.ctypes.data_as(P), b.copy().ctypes.data_as(P),
+                                           ctypes.c_size_t(a.size)) == 0
+            out[f"{name}_op{op}_a"], out[f"{name}_op{op}_b"], out[f"{name}_op{op}_out"] = a, b, r
+    np.savez_compressed(os.path.join(HERE, "reduce_golden.npz"), **out)
+
+
 if __name__ == "__main__":
     main()
     main_blas()
     main_scan_sort()
+    main_reduce()

@@ -1,10 +1,10 @@
 """CPU checks of the oracle's restatement of the reference reducer
 (pmReducer::ReduceMemories, source/code/src/pmReducer.cpp:590-700) on
 hand-computed cases, and the shared input generator of the GPU parity test.
-The reducer is a member of the reference runtime and does not compile on its
-own, so these cases pin the restatement: the operations' edge semantics
-(LOGICAL_XOR is a != b; bitwise operations on floats act on the values
-converted to unsigned integers; MIN/MAX are std::min/std::max)."""
+The cases spell out the operations' edge semantics (LOGICAL_XOR is a != b;
+bitwise operations on floats act on the values converted to unsigned
+integers; MIN/MAX are std::min/std::max); tests/test_reduce_ref.py checks the
+restatement bit for bit against the reference's own ReduceMemories."""
 from __future__ import annotations
 
 import ctypes
