@@ -229,10 +229,10 @@ void orc_lu_crout_f64(double* a, int n, long ld) {
 /* into subtask 1's element by element; bitwise operations on floats and     */
 /* doubles act on the values converted to uint32 / uint64                    */
 /* (pmReducer.cpp:408-423); LOGICAL_XOR is a != b.  op / type take the       */
-/* pmReductionOpType / pmReductionDataType values.  The reducer is a member  */
-/* of the reference runtime and does not compile on its own: parity          */
-/* unpinned -- this restatement is checked against hand-computed cases in    */
-/* the tests only.                                                           */
+/* pmReductionOpType / pmReductionDataType values.  Pinned bit for bit to   */
+/* the reference's own ReduceMemories, cut unchanged out of pmReducer.cpp    */
+/* into oracle/_ref/libref_reduce.so (tests/test_reduce_ref.py), and to its  */
+/* golden outputs (tests/golden/reduce_golden.npz).                          */
 /* ------------------------------------------------------------------------ */
 #define ORC_FOLD(T, B)                                                                        \
     do {                                                                                      \
