@@ -396,20 +396,72 @@ def _cpu_entry(value, unit, cores, kind, sample, seconds):
             "seconds": round(seconds, 3)}
 
 
-def reduce_cpu_baseline(orc, nr: int = 1 << 24, ns: int = 8):
+def _reference_lib(name: str):
+    path = os.path.join(ROOT, "oracle", "_ref", name)
+    return ctypes.CDLL(path) if os.path.exists(path) else None
+
+
+def reduce_cpu_baseline(orc, ref=None, nr: int = 1 << 24, ns: int = 8):
     """The reference's host fold (pmReducer::ReduceMemories REDUCE_ADD over
-    FLOATS, restated in oracle/oracle.c) on the same 8 copies of 2^24 floats:
-    copy k folded into copy 0 for k = 1..7, one thread."""
+    FLOATS: the reference's own function from oracle/_ref/libref_reduce.so
+    when given, else its restatement in oracle/oracle.c) on the same 8 copies
+    of 2^24 floats: copy k folded into copy 0 for k = 1..7, one thread (the
+    reference's loop is OpenMP-parallel only when built with
+    USE_OMP_FOR_REDUCTION)."""
     P = ctypes.c_void_p
     rng = np.random.default_rng(4)
     copies = [rng.random(nr, dtype=np.float32) for _ in range(ns)]
     t0 = time.perf_counter()
     for k in range(1, ns):
-        orc.orc_reduce_fold(0, 4, copies[0].ctypes.data_as(P), copies[k].ctypes.data_as(P), ctypes.c_size_t(nr))
+        a, b = copies[0].ctypes.data_as(P), copies[k].ctypes.data_as(P)
+        if ref is not None:
+            ref.ref_reduce_memories(0, 4, a, b, ctypes.c_size_t(nr))
+        else:
+            orc.orc_reduce_fold(0, 4, a, b, ctypes.c_size_t(nr))
     dt = time.perf_counter() - t0
-    return _cpu_entry(4.0 * nr * (ns + 1) / dt / 1e9, "GB/s", 1, "port",
-                      "pmReducer::ReduceMemories REDUCE_ADD restated (oracle/oracle.c), 8 copies of 2^24 floats "
-                      "folded pairwise into the first, one thread", dt)
+    what = ("pmReducer::ReduceMemories REDUCE_ADD (the reference's own, oracle/_ref)" if ref is not None else
+            "pmReducer::ReduceMemories REDUCE_ADD restated (oracle/oracle.c)")
+    return _cpu_entry(4.0 * nr * (ns + 1) / dt / 1e9, "GB/s", 1, "reference" if ref is not None else "port",
+                      f"{what}, 8 copies of 2^24 floats folded pairwise into the first, one thread", dt)
+
+
+def scan_sort_reference_baselines(res) -> bool:
+    """Radix-sort and prefix-sum CPU figures from the reference's own serial
+    functions (oracle/_ref/libref_scan_sort.so: serialLsbRadixSort with its
+    4-bit digits in 8 rounds, serialPrefixSum over int32), one thread as the
+    reference's per-subtask callbacks run, on bounded samples; rates in the
+    configurations' algorithmic bytes (sort 32 B per key over 4 passes of
+    8-bit digits, scan 12 B per element).  False when the library is absent."""
+    ref = _reference_lib("libref_scan_sort.so")
+    if ref is None:
+        return False
+    P, U = ctypes.c_void_p, ctypes.c_uint
+    rng = np.random.default_rng(2)
+    n = 1 << 24
+    keys = rng.integers(0, 2**32, n, dtype=np.uint32)
+    out = np.empty_like(keys)
+    for _ in range(2):  # the first call faults the output pages in; time the second
+        t0 = time.perf_counter()
+        ref.ref_serial_lsb_radix_sort_u32(keys.ctypes.data_as(P), out.ctypes.data_as(P), U(n),
+                                          ref.ref_radix_total_rounds())
+        dt = time.perf_counter() - t0
+    entries = {"radix_sort_2^28": _cpu_entry(
+        32.0 * n / dt / 1e9, "GB/s", 1, "reference", "serialLsbRadixSort (the reference's own, oracle/_ref), "
+        "4-bit digits x 8 rounds, 2^24 keys, one thread (the reference's per-subtask CPU sort)", dt)}
+    m = 1 << 26
+    vals = rng.integers(0, 16, m, dtype=np.int32)  # int32, the reference's type: sums stay below 2^31
+    outv = np.empty_like(vals)
+    for _ in range(2):
+        t0 = time.perf_counter()
+        ref.ref_serial_prefix_sum_i32(vals.ctypes.data_as(P), outv.ctypes.data_as(P), U(m))
+        dt = time.perf_counter() - t0
+    entries["prefix_sum_2^28"] = _cpu_entry(
+        12.0 * m / dt / 1e9, "GB/s", 1, "reference", "serialPrefixSum (the reference's own, oracle/_ref, int32), "
+        "2^26 elements, one thread", dt)
+    for key, e in entries.items():
+        if key in res:
+            res[key]["cpu_baseline"] = e
+    return True
 
 
 def app_cpu_baselines(torch, res):
@@ -423,10 +475,10 @@ def app_cpu_baselines(torch, res):
     P = ctypes.c_void_p
     cores = os.cpu_count() or 1
     rng = np.random.default_rng(2)
-    if orc is not None:
+    if orc is not None and not scan_sort_reference_baselines(res):
         n = 1 << 24
         keys = rng.integers(0, 2**32, n, dtype=np.uint32)
-        tmp = np.empty_like(keys)
+        tmp = np.ones_like(keys)  # touched, so page faults stay out of the timed call
         t0 = time.perf_counter()
         orc.orc_radix_sort_u32(keys.ctypes.data_as(P), tmp.ctypes.data_as(P), ctypes.c_size_t(n), 0, 32, 8)
         dt = time.perf_counter() - t0
@@ -434,7 +486,7 @@ def app_cpu_baselines(torch, res):
             32.0 * n / dt / 1e9, "GB/s", 1, "port", "serialRadixSortRound restated (oracle/oracle.c), 8-bit digits, "
             "2^24 keys, one thread (the reference's per-subtask CPU sort)", dt)
         vals = rng.integers(0, 2**32, 1 << 26, dtype=np.uint32)
-        outv = np.empty(vals.size, np.uint64)
+        outv = np.ones(vals.size, np.uint64)
         t0 = time.perf_counter()
         orc.orc_prefix_sum_u32_u64(vals.ctypes.data_as(P), outv.ctypes.data_as(P), ctypes.c_size_t(vals.size))
         dt = time.perf_counter() - t0
@@ -442,6 +494,7 @@ def app_cpu_baselines(torch, res):
             12.0 * vals.size / dt / 1e9, "GB/s", 1, "port", "serialPrefixSum restated (oracle/oracle.c), 2^26 "
             "elements, one thread", dt)
         del keys, tmp, vals, outv
+    if orc is not None:
         nv, ne = 1 << 22, 1 << 26
         s_, d_ = ops.rmat_edges(1, 22, ne)
         src = s_.cpu().numpy().view(np.uint32)
@@ -463,7 +516,8 @@ def app_cpu_baselines(torch, res):
             "the full R-MAT 2^22/2^26 graph, one thread", dt)
         del s_, d_, src, dst, order
         if "subtask_reduce_add_f32_8x2^24" in res:
-            res["subtask_reduce_add_f32_8x2^24"]["cpu_baseline"] = reduce_cpu_baseline(orc)
+            res["subtask_reduce_add_f32_8x2^24"]["cpu_baseline"] = reduce_cpu_baseline(
+                orc, _reference_lib("libref_reduce.so"))
     if blas_reference_baselines(res, cores):
         return
     # Without oracle/_ref: the same BLAS calls on numpy's OpenBLAS.
