@@ -20,6 +20,9 @@
   (cut unchanged out of pmReducer.cpp into oracle/_ref/libref_reduce.so) for
   every operation and data type on the inputs tests/test_reduce_oracle.py
   generates: reduce_golden.npz.
+* pageRank: runs the reference's pageRank_cpu (pageRank.cpp compiled unchanged
+  into oracle/_ref/libref_pagerank.so) on seeded hub-heavy graphs from
+  tests/test_pagerank_oracle.py: pagerank_golden.npz.
 
 Usage (in a tree where the reference is available):
     make -C oracle/ref && python tests/golden/make_golden.py
@@ -163,8 +166,29 @@ def main_reduce() -> None:
     np.savez_compressed(os.path.join(HERE, "reduce_golden.npz"), **out)
 
 
+def main_pagerank() -> None:
+    import sys
+
+    sys.path.insert(0, os.path.dirname(HERE))
+    from test_pagerank_oracle import out_lists, random_graph
+
+    P = ctypes.c_void_p
+    ref = ctypes.CDLL(os.path.join(ROOT, "oracle", "_ref", "libref_pagerank.so"))
+    out = {}
+    for idx, (n, e, iters) in enumerate([(64, 400, 1), (700, 9000, 3)]):
+        src, dst = random_graph(n, e, 7 * n + e)
+        out_ptr, out_dst, _ = out_lists(src, dst, n)
+        expect = np.zeros(n, np.float32)
+        assert ref.ref_pagerank(out_ptr.ctypes.data_as(P), out_dst.ctypes.data_as(P), n, iters,
+                                ctypes.c_float(1.0 / n), expect.ctypes.data_as(P)) == 0
+        out[f"g{idx}_meta"] = np.array([n, e, iters], np.int64)
+        out[f"g{idx}_src"], out[f"g{idx}_dst"], out[f"g{idx}_rank"] = src, dst, expect
+    np.savez_compressed(os.path.join(HERE, "pagerank_golden.npz"), **out)
+
+
 if __name__ == "__main__":
     main()
     main_blas()
     main_scan_sort()
     main_reduce()
+    main_pagerank()

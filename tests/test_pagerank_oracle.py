@@ -72,6 +72,23 @@ def test_push_oracle_matches_reference_callback(oracle, n, e, iters):
     assert np.array_equal(got, expect)  # same fp32 operations in the same order
 
 
+def test_push_oracle_matches_golden_reference_ranks(oracle):
+    """tests/golden/pagerank_golden.npz: the reference's pageRank_cpu ranks on
+    two seeded hub-heavy graphs (written by tests/golden/make_golden.py), for
+    machines without the reference tree.  Bit for bit."""
+    import os
+
+    from conftest import ROOT
+
+    g = np.load(os.path.join(ROOT, "tests", "golden", "pagerank_golden.npz"))
+    for idx in range(2):
+        n, _, iters = (int(v) for v in g[f"g{idx}_meta"])
+        src, dst = g[f"g{idx}_src"], g[f"g{idx}_dst"]
+        _, _, outdeg = csr_by_dst(src, dst, n)
+        got = oracle_push(oracle, src, dst, n, outdeg, iters, 1.0 / n)
+        assert np.array_equal(got, g[f"g{idx}_rank"]), idx
+
+
 def test_f64_oracle_close_to_push(oracle):
     n, e = 2000, 40000
     src, dst = random_graph(n, e, 3)
