@@ -208,16 +208,15 @@ int pmb_reduce_elementwise(int op, int type, void* d_dst, const void* const* d_s
 /* ------------------------------------------------------------------------ */
 
 /* Bytes of device scratch pmb_inclusive_scan_u32_u64 needs for n elements
- * (a 256-byte header, one 64-bit carry per 2^24-element chunk and one 64-bit
- * sum per 16384-element segment). */
+ * (a 256-byte header and one 64-bit status word per 16384-element tile). */
 size_t pmb_scan_scratch_bytes(size_t n);
 
-/* out[i] = in[0] + ... + in[i] with 64-bit sums, n <= 2^30, ceil(n / 2^24) + 1
- * launches on `stream` (reduce-then-scan over L2-sized chunks, chained by
- * programmatic dependent launch; no memset, no inter-block spinning).  d_in,
- * d_out and d_scratch are
- * device pointers, 16-byte aligned.  Replaces prefixSum_cudaLaunchFunc /
- * prefixSum_cuda / elemAdd_cuda and the host scan of subtask totals
+/* out[i] = in[0] + ... + in[i] with 64-bit sums, n <= 2^30: one memset of the
+ * scratch and one single-pass launch on `stream` (decoupled look-back over
+ * 16384-element tiles; every look-back wait is bounded and reported in the
+ * scratch error word).  d_in, d_out and d_scratch are device pointers,
+ * 16-byte aligned.  Replaces prefixSum_cudaLaunchFunc / prefixSum_cuda /
+ * elemAdd_cuda and the host scan of subtask totals
  * (testSuite/prefixSum/source/code/src/prefixSumCUDA.cu:68-267,
  * prefixSum.cpp:189-294); result equals serialPrefixSum (prefixSum.cpp:47-53)
  * widened to uint64. */
@@ -229,21 +228,28 @@ int pmb_inclusive_scan_u32_u64(const uint32_t* d_in, uint64_t* d_out, size_t n, 
  * pm:: subtask_gpu_custom callback may only enqueue work on the stream it is
  * handed (cudaMalloc/cudaFree synchronise the device and would stall every
  * subtask in flight), and a service that fixes its memory budget up front
- * cannot let a library grow it.  The scan's scratch (chunk carries and
- * segment sums) is a fixed 1 MiB device array inside libpmb.so, held by every
- * GPU that loads the library
- * until the process exits; the call allocates nothing, which limits n to
- * PMB_SCAN_NOALLOC_MAX_ELEMS (longer inputs return PMB_BEYOND_LIMITS).  The
- * first call on a device looks up the array's device address with that
- * device current; make that first call before any stream capture.  All calls
- * share the one array (each writes the words it reads before reading them),
- * so calls whose work overlaps on the GPU -- on different streams, or from
- * different threads -- race and must be serialised by the caller. */
-#define PMB_SCAN_NOALLOC_MAX_ELEMS 536739840ull /* about 2^29; its scratch (257 KB) fits the 1 MiB array */
+ * cannot let a library grow it.  The scan's scratch (tile counter, error word
+ * and tile status words) is a fixed 1 MiB device array inside libpmb.so, held
+ * by every GPU that loads the library until the process exits; the call
+ * allocates nothing, and n is limited to PMB_SCAN_NOALLOC_MAX_ELEMS (longer
+ * inputs return PMB_BEYOND_LIMITS).  The first call on a device looks up the
+ * array's device address with that device current and keeps it for the life
+ * of the process: make that first call before any stream capture, and do not
+ * use the entry point after cudaDeviceReset.  All calls share the one array
+ * (each clears it on its stream before use), so calls whose work overlaps on
+ * the GPU -- on different streams, or from different threads -- race and
+ * must be serialised by the caller. */
+#define PMB_SCAN_NOALLOC_MAX_ELEMS 1073741824ull /* 2^30; its scratch (513 KB) fits the 1 MiB array */
 int pmb_inclusive_scan_u32_u64_noalloc(const uint32_t* d_in, uint64_t* d_out, size_t n, void* stream);
 
+/* Error word of the allocation-free scan's fixed array on the current device
+ * (synchronous copy, no allocation): 0 = clean; 1 = a bounded wait of the
+ * last call hit its poll limit and its result is not trustworthy.  No
+ * counterpart in the reference. */
+int pmb_scan_noalloc_error(uint32_t* error_out);
+
 /* Copy the error word of a scan/sort scratch buffer to the host (synchronous).
- * 0 = clean; 1 = a bounded wait hit its poll limit (the sort's look-back, the
+ * 0 = clean; 1 = a bounded wait hit its poll limit (a look-back, or the
  * scan's tile staging; the result is then not trustworthy).  Replaces nothing
  * in the reference (its kernels never wait on one another). */
 int pmb_scratch_error(const void* d_scratch, uint32_t* error_out);

@@ -110,6 +110,16 @@ def test_single_round_matches_reference_round(cuda, oracle, bits):
         assert np.array_equal(d.cpu().numpy().view(np.uint32), expect), shift
 
 
+def scan_is_exact(cuda, d_in, out) -> bool:
+    """Size-independent check of an inclusive scan on the device: the first
+    sum is the first key and consecutive sums differ by exactly the next key
+    (64-bit sums of n <= 2^30 keys stay below 2^62, so int64 holds them)."""
+    x = d_in.to(cuda.int64) & 0xFFFFFFFF
+    if out.numel() != x.numel() or int(out[0]) != int(x[0]):
+        return False
+    return bool(cuda.equal(out[1:] - out[:-1], x[1:]))
+
+
 def test_sort_then_scan_full_configuration(cuda):
     """2^28 uint32 keys (seed 2): 8-bit LSD sort, then inclusive uint64 scan."""
     from unicorn_b200 import ops
@@ -120,11 +130,51 @@ def test_sort_then_scan_full_configuration(cuda):
     _, s1 = ops.radix_sort_u32(d)
     out, s2 = ops.inclusive_scan_u32_u64(d)
     cuda.cuda.synchronize()
+    assert ops.scratch_error(s1) == 0 and ops.scratch_error(s2) == 0
     ref_sorted = np.sort(x)
     assert np.array_equal(d.cpu().numpy().view(np.uint32), ref_sorted)
     del x
     assert np.array_equal(out.cpu().numpy().view(np.uint64), np.cumsum(ref_sorted, dtype=np.uint64))
-    assert ops.scratch_error(s1) == 0 and ops.scratch_error(s2) == 0
+
+
+@pytest.mark.parametrize("n,where", [(1 << 28, "created stream"), (1 << 28, "default stream"),
+                                     ((1 << 28) + 12345, "default stream"), (1 << 29, "created stream")])
+def test_scan_full_size(cuda, n, where):
+    """2^28 and 2^29 random keys (16 and 32 blocks of 2^24), alone on a
+    created stream or the default stream, and a ragged 2^28 + 12345."""
+    from unicorn_b200 import ops
+
+    g = cuda.Generator(device="cuda")
+    g.manual_seed(n)
+    d = cuda.randint(-(2**31), 2**31, (n,), dtype=cuda.int32, device="cuda", generator=g)
+    if where == "created stream":
+        s = cuda.cuda.Stream()
+        s.wait_stream(cuda.cuda.current_stream())
+        with cuda.cuda.stream(s):
+            out, scratch = ops.inclusive_scan_u32_u64(d, stream=s)
+        s.synchronize()
+    else:
+        out, scratch = ops.inclusive_scan_u32_u64(d)
+        cuda.cuda.synchronize()
+    assert ops.scratch_error(scratch) == 0
+    assert scan_is_exact(cuda, d, out)
+
+
+def test_scan_sorted_run_twice_same_scratch(cuda):
+    """Two scans of the full configuration back to back on one scratch buffer
+    (the second must clear what the first left behind)."""
+    from unicorn_b200 import ops
+
+    n = 1 << 28
+    g = cuda.Generator(device="cuda")
+    g.manual_seed(2)
+    d = cuda.randint(-(2**31), 2**31, (n,), dtype=cuda.int32, device="cuda", generator=g)
+    ops.radix_sort_u32(d)
+    out, scratch = ops.inclusive_scan_u32_u64(d)
+    out2, scratch = ops.inclusive_scan_u32_u64(d, scratch=scratch)
+    cuda.cuda.synchronize()
+    assert ops.scratch_error(scratch) == 0
+    assert scan_is_exact(cuda, d, out2) and cuda.equal(out, out2)
 
 
 def test_scan_after_producer_on_same_stream(cuda):

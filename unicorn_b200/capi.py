@@ -23,7 +23,7 @@ PMB_IMGF_WRAP = 0
 PMB_IMGF_CLAMP = 1
 PMB_IMGF_MAX_ITEMS = 256
 PMB_IMGF_MAX_FILTER_DIM = 32
-PMB_SCAN_NOALLOC_MAX_ELEMS = 536739840
+PMB_SCAN_NOALLOC_MAX_ELEMS = 1 << 30
 PMB_BEYOND_LIMITS = 15
 
 
@@ -111,6 +111,7 @@ _SIGS = {
     "pmb_scan_scratch_bytes": (c_size_t, [c_size_t]),
     "pmb_inclusive_scan_u32_u64": (c_int, [c_void_p, c_void_p, c_size_t, c_void_p, c_size_t, c_void_p]),
     "pmb_inclusive_scan_u32_u64_noalloc": (c_int, [c_void_p, c_void_p, c_size_t, c_void_p]),
+    "pmb_scan_noalloc_error": (c_int, [ctypes.POINTER(ctypes.c_uint32)]),
     "pmb_scratch_error": (c_int, [c_void_p, ctypes.POINTER(ctypes.c_uint32)]),
     "pmb_radix_sort_scratch_bytes": (c_size_t, [c_size_t, c_int]),
     "pmb_radix_sort_u32": (c_int, [c_void_p, c_void_p, c_size_t, c_int, c_int, c_int, c_void_p, c_size_t, c_void_p]),

@@ -5,28 +5,22 @@
 // two-task flow -- per-subtask serial scans :86-104, host scan of subtask
 // totals and elemAdd :106-133 -- produces the same global inclusive scan).
 //
-// Design: reduce-then-scan over chunks sized for the 126 MB L2.  The input is
-// cut into chunks of 2^24 elements (64 MB) and each chunk into segments of
-// 16384 elements.  Launch j (j = -1 .. chunks-1, all on one stream) runs two
-// kinds of 256-thread blocks side by side:
-//   reduce blocks sum two segments of chunk j+1 each, reading the input from
-//     HBM under an L2 evict-last policy so that it stays resident, and write
-//     one uint64 per segment;
-//   scan blocks scan one segment of chunk j each, from carry[j] (the sum of
-//     all earlier chunks) plus the sums of the segments before theirs; they
-//     read the input a second time -- mostly an L2 hit -- and stream the
-//     uint64 output out under an evict-first policy.  Scan block 0 also forms
-//     carry[j+1].
-// Launches after the first use programmatic dependent launch: their reduce
-// blocks start on SMs the previous launch has left, and their scan blocks
-// wait (griddepcontrol.wait) for the previous grid's results.  No block spins
-// on another block.  Each block stages its tiles through a 3-deep ring of
-// 16 KB shared-memory buffers filled by single bulk async copies (one thread
-// issues, an mbarrier completes), so ~48 KB per block is in flight while the
-// current tile is processed.  A tile (4096 elements) is scanned with
-// thread-local sums, warp shuffles and one warp scan of the 32 partial
-// totals.  Measured at 2^28 elements: 13.3 bytes of HBM traffic per element
-// (4 read, 8 written, ~1.3 of re-reads that missed L2).
+// Design: one launch, single pass, decoupled look-back (Merrill and Garland,
+// "Single-pass Parallel Prefix Scan with Decoupled Look-back", 2016).  Each
+// 256-thread block takes the next 16384-element tile from a global counter
+// (so every tile it waits on belongs to a block that started earlier), stages
+// the tile in shared memory with four 16 KB bulk async copies (one mbarrier
+// each), sums it, and publishes the sum in the tile's 64-bit status word
+// (2-bit flag | 62-bit value: AGGREGATE, or INCLUSIVE for tile 0).  Warp 0
+// then reads the status words of the 32 preceding tiles at once, adds the
+// aggregates back to the nearest inclusive prefix (waiting -- boundedly -- only
+// for tiles in between that have not published yet), and publishes the tile's
+// own inclusive prefix.  The block then scans the staged tile from that
+// offset: per 4096-element sub-tile, thread-local sums of four elements, warp
+// shuffle scans of the 32 row pieces and one warp scan of their totals, and
+// coalesced 16-byte stores of the uint64 results.  HBM traffic: 4 bytes read
+// and 8 written per element, plus 8 bytes of status per 16384 elements.  The
+// 62-bit status values hold any sum of n <= 2^30 uint32 values (< 2^62).
 #include <mutex>
 
 #include "lookback.cuh"
@@ -35,21 +29,16 @@
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kRows = 4;                          // 16-byte loads per thread per tile
-constexpr int kTile = kThreads * 4 * kRows;       // 4096 elements
-constexpr int kSeg = 4 * kTile;                   // 16384 elements per scan block
-constexpr size_t kChunk = size_t(1) << 24;        // 64 MB of input per launch
-constexpr int kSegsPerChunk = static_cast<int>(kChunk / kSeg);  // 1024
-constexpr int kReduceSegs = 2;                    // segments per reduce block
-constexpr int kStages = 3;                        // tiles staged in shared memory per block
-constexpr int kSmemBytes = kStages * kTile * 4;   // 48 KB (dynamic)
-constexpr size_t kHeaderBytes = 256;              // {unused, error word, padding}
+constexpr int kRows = 4;                          // 16-byte reads per thread per sub-tile
+constexpr int kSub = kThreads * 4 * kRows;        // 4096 elements per staged sub-tile
+constexpr int kSubs = 4;                          // sub-tiles per block tile
+constexpr int kTile = kSub * kSubs;               // 16384 elements per block
+constexpr int kSmemBytes = kTile * 4;             // 64 KB (dynamic)
+constexpr size_t kHeaderBytes = 256;              // {tile counter, error word, padding}
+constexpr uint64_t kFlagAgg = 1ull << 62;
+constexpr uint64_t kFlagInc = 2ull << 62;
+constexpr uint64_t kValueMask = (1ull << 62) - 1;
 
-__device__ __forceinline__ uint64_t policy_evict_last() {
-    uint64_t p;
-    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
-    return p;
-}
 __device__ __forceinline__ uint64_t policy_evict_first() {
     uint64_t p;
     asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
@@ -80,17 +69,17 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
     return false;
 }
 
-// Tile staging: one thread copies the 16-byte-aligned body of tile [t0, t0 +
-// kTile) clipped to `end` into shared memory with a single bulk async copy
-// completing on `bar`; the reading threads take the remaining 0-3 elements of
-// a ragged last tile straight from global memory.
-__device__ __forceinline__ size_t tile_body(size_t t0, size_t end) {
-    const size_t len = t0 + kTile <= end ? kTile : end - t0;
+// Sub-tile staging: one thread copies the 16-byte-aligned body of sub-tile
+// [t0, t0 + kSub) clipped to `end` into shared memory with a single bulk async
+// copy completing on `bar`; the reading threads take the remaining 0-3
+// elements of a ragged last sub-tile straight from global memory.
+__device__ __forceinline__ size_t sub_body(size_t t0, size_t end) {
+    const size_t len = t0 + kSub <= end ? kSub : end - t0;
     return len & ~size_t(3);
 }
-__device__ __forceinline__ void fetch_tile(uint32_t* dst, const uint32_t* __restrict__ in, size_t t0, size_t end,
-                                           uint64_t* bar, uint64_t pol) {
-    const uint32_t bytes = static_cast<uint32_t>(tile_body(t0, end) * 4);
+__device__ __forceinline__ void fetch_sub(uint32_t* dst, const uint32_t* __restrict__ in, size_t t0, size_t end,
+                                          uint64_t* bar, uint64_t pol) {
+    const uint32_t bytes = static_cast<uint32_t>(sub_body(t0, end) * 4);
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
                  : "memory");
     if (bytes)
@@ -100,14 +89,14 @@ __device__ __forceinline__ void fetch_tile(uint32_t* dst, const uint32_t* __rest
             "l"(in + t0), "r"(bytes), "r"(smem_u32(bar)), "l"(pol)
             : "memory");
 }
-// Element r*1024 + 4*tid + k of a staged tile, as q[r] component k; zero past `end`.
-__device__ __forceinline__ void read_tile(const uint32_t* tile, const uint32_t* __restrict__ in, size_t t0,
-                                          size_t end, int tid, uint4 (&q)[kRows]) {
-    if (t0 + kTile <= end) {
+// Element r*1024 + 4*tid + k of a staged sub-tile, as q[r] component k; zero past `end`.
+__device__ __forceinline__ void read_sub(const uint32_t* sub, const uint32_t* __restrict__ in, size_t t0,
+                                         size_t end, int tid, uint4 (&q)[kRows]) {
+    if (t0 + kSub <= end) {
 #pragma unroll
-        for (int r = 0; r < kRows; ++r) q[r] = reinterpret_cast<const uint4*>(tile)[r * kThreads + tid];
+        for (int r = 0; r < kRows; ++r) q[r] = reinterpret_cast<const uint4*>(sub)[r * kThreads + tid];
     } else {
-        const size_t body = t0 + tile_body(t0, end);
+        const size_t body = t0 + sub_body(t0, end);
 #pragma unroll
         for (int r = 0; r < kRows; ++r) {
             uint32_t e[4];
@@ -115,7 +104,7 @@ __device__ __forceinline__ void read_tile(const uint32_t* tile, const uint32_t* 
             for (int k = 0; k < 4; ++k) {
                 const int off = r * (kThreads * 4) + 4 * tid + k;
                 const size_t idx = t0 + off;
-                e[k] = idx < body ? tile[off] : (idx < end ? in[idx] : 0u);
+                e[k] = idx < body ? sub[off] : (idx < end ? in[idx] : 0u);
             }
             q[r] = make_uint4(e[0], e[1], e[2], e[3]);
         }
@@ -134,156 +123,150 @@ __device__ __forceinline__ uint64_t block_sum(uint64_t v, uint64_t* s_red) {
     return t;
 }
 
-__global__ void __launch_bounds__(kThreads)
-scan_chunks_kernel(const uint32_t* __restrict__ in, uint64_t* __restrict__ out, size_t n, int j, int scan_blocks,
-                   uint64_t* __restrict__ carry, uint64_t* __restrict__ sums, uint32_t* __restrict__ hdr) {
-    extern __shared__ __align__(128) unsigned char smem[];  // kStages staged tiles
-    __shared__ uint64_t s_bar[kStages];
-    __shared__ uint64_t s_red[2][kThreads / 32];
+// Exclusive prefix of tile `tile` from the status words of its predecessors,
+// run by one full warp.  Lane i looks at tile (base - i); a round sums the
+// aggregates of the tiles up to the nearest published inclusive prefix, and
+// waits only while one of those tiles has published nothing yet.  Sets
+// *gave_up (and counts the unpublished tiles as 0) once the poll limit is hit.
+__device__ __forceinline__ uint64_t lookback(const uint64_t* status, long long tile, int lane, bool* gave_up) {
+    uint64_t excl = 0;
+    for (long long base = tile - 1;; base -= 32) {
+        const long long idx = base - lane;
+        uint64_t s = idx >= 0 ? pmb::ld_relaxed_u64(&status[idx]) : kFlagInc;
+        uint32_t inc_mask, upto;
+        for (uint32_t polls = 0;; ++polls) {
+            inc_mask = __ballot_sync(0xffffffffu, (s >> 62) == 2);
+            // Lanes up to and including the first inclusive prefix (all 32 if none).
+            upto = inc_mask ? (inc_mask ^ (inc_mask - 1)) : 0xffffffffu;
+            const uint32_t pending = __ballot_sync(0xffffffffu, (s >> 62) == 0) & upto;
+            if (!pending) break;
+            if (polls >= pmb::kSpinLimit) {
+                *gave_up = true;
+                break;
+            }
+            __nanosleep(32);
+            if ((pending >> lane) & 1u) s = pmb::ld_relaxed_u64(&status[idx]);
+        }
+        excl += pmb::warp_sum_u64(((upto >> lane) & 1u) ? (s & kValueMask) : 0);
+        if (inc_mask || *gave_up) return excl;
+    }
+}
+
+__global__ void __launch_bounds__(kThreads, 3)
+scan_lookback_kernel(const uint32_t* __restrict__ in, uint64_t* __restrict__ out, size_t n,
+                     uint64_t* __restrict__ status, uint32_t* __restrict__ hdr) {
+    extern __shared__ __align__(128) unsigned char smem[];  // the block's staged tile
+    __shared__ uint64_t s_bar[kSubs];
+    __shared__ uint64_t s_red[kThreads / 32];
     __shared__ uint64_t s_wt[2][kRows][kThreads / 32];
     __shared__ uint64_t s_tot[2];
+    __shared__ uint64_t s_excl;
+    __shared__ uint32_t s_tile;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    uint32_t* tiles = reinterpret_cast<uint32_t*>(smem);
-    const bool reducer = static_cast<int>(blockIdx.x) >= scan_blocks;
-    // The next launch may start filling SMs as this one drains (programmatic
-    // dependent launch); its scan blocks wait for this grid before reading.
-    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    uint32_t* stage = reinterpret_cast<uint32_t*>(smem);
+    const uint64_t pol = policy_evict_first();  // input and output stream through L2 once
 
     if (tid == 0) {
-        if (reducer && j < 0 && blockIdx.x == static_cast<unsigned>(scan_blocks)) {
-            carry[0] = 0;
-            hdr[1] = 0;  // error word (set below only if a staging wait expires)
-        }
-        for (int st = 0; st < kStages; ++st) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_bar[st])));
+        s_tile = atomicAdd(&hdr[0], 1u);
+        for (int st = 0; st < kSubs; ++st) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_bar[st])));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     __syncthreads();
-
-    // The block's range [r0, r1) is staged tile by tile through the ring.
-    size_t r0, r1;
-    if (reducer) {
-        const size_t c1 = static_cast<size_t>(j + 1) * kChunk;
-        const size_t c1_end = c1 + kChunk < n ? c1 + kChunk : n;
-        r0 = c1 + static_cast<size_t>(blockIdx.x - scan_blocks) * kReduceSegs * kSeg;
-        r1 = r0 + static_cast<size_t>(kReduceSegs) * kSeg < c1_end ? r0 + static_cast<size_t>(kReduceSegs) * kSeg
-                                                                     : c1_end;
-    } else {
-        r0 = static_cast<size_t>(j) * kChunk + static_cast<size_t>(blockIdx.x) * kSeg;
-        r1 = r0 + kSeg < n ? r0 + kSeg : n;
-    }
-    const int ntiles = static_cast<int>((r1 - r0 + kTile - 1) / kTile);
-    const uint64_t pin = reducer ? policy_evict_last() : policy_evict_first();
+    const size_t tile = s_tile;
+    const size_t r0 = tile * kTile;
+    const size_t r1 = r0 + kTile < n ? r0 + kTile : n;
+    const int nsub = static_cast<int>((r1 - r0 + kSub - 1) / kSub);
     if (tid == 0)
-        for (int t = 0; t < kStages && t < ntiles; ++t)
-            fetch_tile(tiles + t * kTile, in, r0 + static_cast<size_t>(t) * kTile, r1, &s_bar[t], pin);
-    bool ok = true;
+        for (int st = 0; st < nsub; ++st)
+            fetch_sub(stage + st * kSub, in, r0 + static_cast<size_t>(st) * kSub, r1, &s_bar[st], pol);
 
-    if (reducer) {
-        // ---- reduce: one sum per kSeg segment of chunk j+1 ----
-        uint64_t acc = 0;
-        for (int t = 0; t < ntiles; ++t) {
-            const int st = t % kStages;
-            const size_t t0 = r0 + static_cast<size_t>(t) * kTile;
-            ok &= mbar_wait(smem_u32(&s_bar[st]), (t / kStages) & 1);
-            uint4 q[kRows];
-            read_tile(tiles + st * kTile, in, t0, r1, tid, q);
+    // ---- the tile's sum, published as soon as it is known ----
+    bool ok = true;
+    uint64_t acc = 0;
+    for (int st = 0; st < nsub; ++st) {
+        ok &= mbar_wait(smem_u32(&s_bar[st]), 0);
+        uint4 q[kRows];
+        read_sub(stage + st * kSub, in, r0 + static_cast<size_t>(st) * kSub, r1, tid, q);
 #pragma unroll
-            for (int r = 0; r < kRows; ++r) acc += static_cast<uint64_t>(q[r].x) + q[r].y + q[r].z + q[r].w;
-            __syncthreads();  // every thread has read stage st
-            if (tid == 0 && t + kStages < ntiles)
-                fetch_tile(tiles + st * kTile, in, t0 + static_cast<size_t>(kStages) * kTile, r1, &s_bar[st], pin);
-            if ((t + 1) % (kSeg / kTile) == 0 || t + 1 == ntiles) {
-                const uint64_t total = block_sum(acc, s_red[(t / (kSeg / kTile)) & 1]);
-                const size_t seg = (t0 - static_cast<size_t>(j + 1) * kChunk) / kSeg;
-                if (tid == 0) sums[static_cast<size_t>(j + 1) * kSegsPerChunk + seg] = total;
-                acc = 0;
+        for (int r = 0; r < kRows; ++r) acc += static_cast<uint64_t>(q[r].x) + q[r].y + q[r].z + q[r].w;
+    }
+    const uint64_t agg = block_sum(acc, s_red);
+    if (warp == 0) {
+        uint64_t excl = 0;
+        if (tile == 0) {
+            if (lane == 0) pmb::st_relaxed_u64(&status[0], kFlagInc | agg);
+        } else {
+            if (lane == 0) pmb::st_relaxed_u64(&status[tile], kFlagAgg | agg);
+            bool gave_up = false;
+            excl = lookback(status, static_cast<long long>(tile), lane, &gave_up);
+            if (lane == 0) {
+                pmb::st_relaxed_u64(&status[tile], kFlagInc | ((excl + agg) & kValueMask));
+                if (gave_up) atomicOr(&hdr[1], pmb::kErrLookbackTimeout);
             }
         }
-    } else {
-        // ---- scan one segment of chunk j ----
-        // The previous launch wrote this chunk's segment sums and carry[j].
-        asm volatile("griddepcontrol.wait;" ::: "memory");
-        const int seg = blockIdx.x;
-        const size_t c0 = static_cast<size_t>(j) * kChunk;
-        const uint64_t* cs = sums + static_cast<size_t>(j) * kSegsPerChunk;
-        const int nsegs = static_cast<int>(((c0 + kChunk < n ? c0 + kChunk : n) - c0 + kSeg - 1) / kSeg);
-        uint64_t before = 0, all = 0;
-        for (int t = tid; t < nsegs; t += kThreads) {
-            const uint64_t x = cs[t];
-            all += x;
-            if (t < seg) before += x;
-        }
-        const uint64_t cj = carry[j];
-        uint64_t base = cj + block_sum(before, s_red[0]);
-        if (seg == 0) {
-            const uint64_t tot = block_sum(all, s_red[1]);
-            if (tid == 0) carry[j + 1] = cj + tot;
-        }
-        const uint64_t pout = policy_evict_first();
-        for (int t = 0; t < ntiles; ++t) {
-            const int st = t % kStages, par = t & 1;
-            const size_t t0 = r0 + static_cast<size_t>(t) * kTile;
-            ok &= mbar_wait(smem_u32(&s_bar[st]), (t / kStages) & 1);
-            uint4 cur[kRows];
-            read_tile(tiles + st * kTile, in, t0, r1, tid, cur);
-            uint64_t lane_excl[kRows];  // this thread's offset inside its warp's row piece
+        if (lane == 0) s_excl = excl;
+    }
+    __syncthreads();
+
+    // ---- scan the staged tile from its exclusive prefix ----
+    uint64_t base = s_excl;
+    for (int st = 0; st < nsub; ++st) {
+        const int par = st & 1;
+        const size_t t0 = r0 + static_cast<size_t>(st) * kSub;
+        uint4 cur[kRows];
+        read_sub(stage + st * kSub, in, t0, r1, tid, cur);
+        uint64_t lane_excl[kRows];  // this thread's offset inside its warp's row piece
 #pragma unroll
-            for (int r = 0; r < kRows; ++r) {
-                const uint64_t own = static_cast<uint64_t>(cur[r].x) + cur[r].y + cur[r].z + cur[r].w;
-                const uint64_t incl = pmb::warp_inclusive_scan_u64(own, lane);
-                lane_excl[r] = incl - own;
-                if (lane == 31) s_wt[par][r][warp] = incl;
-            }
-            __syncthreads();  // s_wt complete; every thread has read stage st
-            if (tid == 0 && t + kStages < ntiles)
-                fetch_tile(tiles + st * kTile, in, t0 + static_cast<size_t>(kStages) * kTile, r1, &s_bar[st], pin);
-            if (warp == 0) {
-                // kRows * 8 warps == 32 partial totals, in element order (row-major).
-                const uint64_t x = s_wt[par][lane >> 3][lane & 7];
-                const uint64_t inc = pmb::warp_inclusive_scan_u64(x, lane);
-                s_wt[par][lane >> 3][lane & 7] = inc - x;
-                if (lane == 31) s_tot[par] = inc;
-            }
-            __syncthreads();
-#pragma unroll
-            for (int r = 0; r < kRows; ++r) {
-                const uint64_t o0 = base + s_wt[par][r][warp] + lane_excl[r] + cur[r].x;
-                const uint64_t o1 = o0 + cur[r].y, o2 = o1 + cur[r].z, o3 = o2 + cur[r].w;
-                const size_t idx = t0 + static_cast<size_t>(r) * (kThreads * 4) + 4 * tid;
-                if (idx + 3 < r1) {
-                    st_u64x2(out + idx, o0, o1, pout);
-                    st_u64x2(out + idx + 2, o2, o3, pout);
-                } else {
-                    const uint64_t o[4] = {o0, o1, o2, o3};
-#pragma unroll
-                    for (int k = 0; k < 4; ++k)
-                        if (idx + k < r1) out[idx + k] = o[k];
-                }
-            }
-            base += s_tot[par];
+        for (int r = 0; r < kRows; ++r) {
+            const uint64_t own = static_cast<uint64_t>(cur[r].x) + cur[r].y + cur[r].z + cur[r].w;
+            const uint64_t incl = pmb::warp_inclusive_scan_u64(own, lane);
+            lane_excl[r] = incl - own;
+            if (lane == 31) s_wt[par][r][warp] = incl;
         }
+        __syncthreads();  // s_wt[par] complete
+        if (warp == 0) {
+            // kRows * 8 warps == 32 partial totals, in element order (row-major).
+            const uint64_t x = s_wt[par][lane >> 3][lane & 7];
+            const uint64_t inc = pmb::warp_inclusive_scan_u64(x, lane);
+            s_wt[par][lane >> 3][lane & 7] = inc - x;
+            if (lane == 31) s_tot[par] = inc;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int r = 0; r < kRows; ++r) {
+            const uint64_t o0 = base + s_wt[par][r][warp] + lane_excl[r] + cur[r].x;
+            const uint64_t o1 = o0 + cur[r].y, o2 = o1 + cur[r].z, o3 = o2 + cur[r].w;
+            const size_t idx = t0 + static_cast<size_t>(r) * (kThreads * 4) + 4 * tid;
+            if (idx + 3 < r1) {
+                st_u64x2(out + idx, o0, o1, pol);
+                st_u64x2(out + idx + 2, o2, o3, pol);
+            } else {
+                const uint64_t o[4] = {o0, o1, o2, o3};
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if (idx + k < r1) out[idx + k] = o[k];
+            }
+        }
+        // s_wt[par] and s_tot[par] are rewritten two sub-tiles later, after the
+        // first barrier of the next sub-tile has ordered these reads.
+        base += s_tot[par];
     }
     if (!ok) atomicOr(&hdr[1], pmb::kErrLookbackTimeout);
 }
 
-constexpr size_t num_chunks(size_t n) { return (n + kChunk - 1) / kChunk; }
-constexpr int segs_of_chunk(size_t n, size_t c) {
-    return static_cast<int>(((c + 1) * kChunk < n ? kChunk : n - c * kChunk) + kSeg - 1) / kSeg;
-}
+constexpr size_t num_tiles(size_t n) { return (n + kTile - 1) / kTile; }
 
 }  // namespace
 
 namespace pmb {
 
-constexpr size_t scan_scratch_need(size_t n) {
-    return kHeaderBytes + 8 * (num_chunks(n) + 1) + 8 * num_chunks(n) * kSegsPerChunk;
-}
+constexpr size_t scan_scratch_need(size_t n) { return kHeaderBytes + 8 * num_tiles(n); }
 
 size_t scan_scratch_bytes(size_t n) { return scan_scratch_need(n); }
 
-// Shared by the public entry points: validates and runs the launch sequence.
-// The kernels write every scratch word they read, so nothing is cleared first.
+// Shared by the public entry points: validates, clears the tile counter, the
+// error word and the status words, and launches the single pass.
 int scan_launch(const uint32_t* d_in, uint64_t* d_out, size_t n, void* d_scratch, size_t scratch_bytes,
                 cudaStream_t s) {
     if (n == 0) return PMB_SUCCESS;
@@ -298,33 +281,15 @@ int scan_launch(const uint32_t* d_in, uint64_t* d_out, size_t n, void* d_scratch
     static std::once_flag attr_once;
     static cudaError_t attr_err = cudaSuccess;
     std::call_once(attr_once, [] {
-        attr_err = cudaFuncSetAttribute(scan_chunks_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+        attr_err = cudaFuncSetAttribute(scan_lookback_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
     });
     PMB_CUDA_TRY(attr_err);
+    PMB_CUDA_TRY(cudaMemsetAsync(d_scratch, 0, need, s));
     uint32_t* hdr = static_cast<uint32_t*>(d_scratch);
-    const size_t nc = num_chunks(n);
-    uint64_t* carry = reinterpret_cast<uint64_t*>(static_cast<char*>(d_scratch) + kHeaderBytes);
-    uint64_t* sums = carry + (nc + 1);
-    for (long long j = -1; j < static_cast<long long>(nc); ++j) {
-        const int sb = j >= 0 ? segs_of_chunk(n, static_cast<size_t>(j)) : 0;
-        const int rb = j + 1 < static_cast<long long>(nc)
-                           ? (segs_of_chunk(n, static_cast<size_t>(j + 1)) + kReduceSegs - 1) / kReduceSegs
-                           : 0;
-        // Launch -1 waits for all earlier work on the stream (the input may come
-        // from it); later launches overlap their predecessor's tail.
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(sb + rb);
-        cfg.blockDim = dim3(kThreads);
-        cfg.dynamicSmemBytes = kSmemBytes;
-        cfg.stream = s;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-        attr[0].val.programmaticStreamSerializationAllowed = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = j >= 0 ? 1 : 0;
-        PMB_CUDA_TRY(
-            cudaLaunchKernelEx(&cfg, scan_chunks_kernel, d_in, d_out, n, static_cast<int>(j), sb, carry, sums, hdr));
-    }
+    uint64_t* status = reinterpret_cast<uint64_t*>(static_cast<char*>(d_scratch) + kHeaderBytes);
+    const size_t tiles = num_tiles(n);
+    scan_lookback_kernel<<<static_cast<unsigned>(tiles), kThreads, kSmemBytes, s>>>(d_in, d_out, n, status, hdr);
+    PMB_CUDA_TRY(cudaGetLastError());
     return PMB_SUCCESS;
 }
 
@@ -350,8 +315,9 @@ extern "C" int pmb_scratch_error(const void* d_scratch, uint32_t* error_out) {
 // it is given (cudaMalloc and cudaFree synchronise the device and would stall
 // the stub's pipeline of in-flight subtasks), and services that fix their
 // memory budget up front cannot let a library grow it behind their back.  For
-// them the scan's look-back scratch lives in a fixed device array that every
-// GPU loading this library holds until the process exits.
+// them the scan's scratch (tile counter, error word, tile status words) lives
+// in a fixed device array that every GPU loading this library holds until the
+// process exits.
 namespace {
 
 constexpr size_t kNoAllocScratchBytes = size_t(1) << 20;  // 1 MiB per device
@@ -392,7 +358,17 @@ extern "C" int pmb_inclusive_scan_u32_u64_noalloc(const uint32_t* d_in, uint64_t
     void* scratch = nullptr;
     const int st = noalloc_scratch(&scratch);
     if (st != PMB_SUCCESS) return st;
-    // The shared array keeps the previous call's contents; the kernels write
-    // every word of it that they read (the carries and segment sums) first.
+    // The shared array keeps the previous call's contents; scan_launch clears
+    // the counter, the error word and the status words on the stream first.
     return pmb::scan_launch(d_in, d_out, n, scratch, kNoAllocScratchBytes, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int pmb_scan_noalloc_error(uint32_t* error_out) {
+    PMB_CHECK_ARG(error_out, "null pointer");
+    void* scratch = nullptr;
+    const int st = noalloc_scratch(&scratch);
+    if (st != PMB_SUCCESS) return st;
+    PMB_CUDA_TRY(cudaMemcpy(error_out, static_cast<const uint32_t*>(scratch) + 1, sizeof(uint32_t),
+                            cudaMemcpyDeviceToHost));
+    return PMB_SUCCESS;
 }
