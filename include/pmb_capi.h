@@ -158,6 +158,12 @@ typedef struct pmb_imgf_item {
 int pmb_image_filter(const pmb_imgf_item* items, int n_items,
                      const int8_t* filter, int radius, int mode, void* stream);
 
+/* Error word of the stencil kernels on the current device (synchronous copy;
+ * `clear` resets it): 0 = clean; 1 = a bounded wait of a tensor-core stencil
+ * launch (tile staging or its matrix products) expired, and that launch's
+ * output is not valid.  No counterpart in the reference. */
+int pmb_image_filter_error(int clear, uint32_t* error_out);
+
 /* Whole-image convenience form: one item covering the full image with
  * NATURAL views (in_pitch = out_pitch = 3W). */
 int pmb_image_filter_full(const uint8_t* d_in, uint8_t* d_out, int width, int height,
@@ -395,6 +401,28 @@ int pmb_lu_decompose(float* d_A, int n, int64_t lda, int nb, void* d_workspace, 
 /* Same factorization with FP32 SIMT GEMMs (the plain one-task-at-a-time form). */
 int pmb_lu_decompose_plain(float* d_A, int n, int64_t lda, int nb, void* d_workspace, size_t ws_bytes,
                            void* stream);
+
+/* Triangular solve in place, fp32 column-major, no transpose, alpha = 1:
+ *   side PMB_SIDE_LEFT,  uplo PMB_FILL_LOWER: B <- L^-1 B (L = the m x m lower
+ *     triangle of d_A, B m x n);
+ *   side PMB_SIDE_RIGHT, uplo PMB_FILL_UPPER: B <- B U^-1 (U = the n x n upper
+ *     triangle of d_A, B m x n);
+ * diag PMB_DIAG_UNIT ignores the stored diagonal.  64-wide diagonal blocks are
+ * solved in FP64, the remaining rows (left) or columns (right) are updated by
+ * BF16x3 tensor-core GEMMs.  d_workspace: pmb_trsm_workspace_bytes(side, m, n)
+ * bytes, 256-byte aligned.  Replaces cublasStrsm in horizVertComp_cudaLaunchFunc
+ * (testSuite/luDecomposition/source/code/src/luDecompositionCUDA.cu:99-151:
+ * left/lower/non-unit for U01 = L00^-1 A01, right/upper/unit for
+ * L10 = A10 U00^-1). */
+#define PMB_SIDE_LEFT 0
+#define PMB_SIDE_RIGHT 1
+#define PMB_FILL_LOWER 0
+#define PMB_FILL_UPPER 1
+#define PMB_DIAG_NON_UNIT 0
+#define PMB_DIAG_UNIT 1
+size_t pmb_trsm_workspace_bytes(int side, int m, int n);
+int pmb_trsm_f32(int side, int uplo, int diag, int m, int n, const float* d_A, int64_t lda, float* d_B, int64_t ldb,
+                 void* d_workspace, size_t ws_bytes, void* stream);
 
 /* FP64 residual: d_sums[0] = ||A0 - L*U||_F^2, d_sums[1] = ||A0||_F^2 (two
  * device doubles), L and U read from the packed factorization d_LU. */

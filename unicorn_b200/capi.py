@@ -25,6 +25,9 @@ PMB_IMGF_MAX_ITEMS = 256
 PMB_IMGF_MAX_FILTER_DIM = 32
 PMB_SCAN_NOALLOC_MAX_ELEMS = 1 << 30
 PMB_BEYOND_LIMITS = 15
+PMB_SIDE_LEFT, PMB_SIDE_RIGHT = 0, 1
+PMB_FILL_LOWER, PMB_FILL_UPPER = 0, 1
+PMB_DIAG_NON_UNIT, PMB_DIAG_UNIT = 0, 1
 
 
 class PmbError(RuntimeError):
@@ -107,6 +110,10 @@ _SIGS = {
     "pmb_image_filter_full": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_int, c_int, c_void_p]),
     "pmb_image_filter_host": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p, c_int, c_int,
                                       c_int, c_void_p]),
+    "pmb_image_filter_error": (c_int, [c_int, ctypes.POINTER(ctypes.c_uint32)]),
+    "pmb_trsm_workspace_bytes": (c_size_t, [c_int, c_int, c_int]),
+    "pmb_trsm_f32": (c_int, [c_int, c_int, c_int, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64, c_void_p,
+                             c_size_t, c_void_p]),
     "pmb_image_filter_plain": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_int, c_int, c_void_p]),
     "pmb_scan_scratch_bytes": (c_size_t, [c_size_t]),
     "pmb_inclusive_scan_u32_u64": (c_int, [c_void_p, c_void_p, c_size_t, c_void_p, c_size_t, c_void_p]),

@@ -412,6 +412,351 @@ imgf_fast_kernel(const __grid_constant__ ImgfParamsF<R, MAXI> p) {
 }
 
 // ---------------------------------------------------------------------------
+// Tensor-core path for R <= 8: the stencil as int8 matrix products on the
+// 5th-generation tensor cores (tcgen05.mma kind::i8, u8 pixels x s8 weights,
+// exact s32 sums in tensor memory), so integer parity is unchanged.
+//
+// One CTA (128 threads) owns a 128-row x 64-pixel output tile.  Per channel
+// plane P and filter row ky the tile is D += A_ky * B_ky with
+//   A_ky[i][k] = P[tile_r0 + i + ky - R][tile_c0 - 8 + 16t + k]   (M = 128 rows, K = 32 columns)
+//   B_ky[k][j] = f[ky][k - j + R - 8]  (zero outside [0, 2R])     (N = 16 output columns)
+// for each 16-column group t: the 32-column window of input bytes times a
+// banded Toeplitz slice of the filter row.  A is never materialised per ky:
+// the planes are stored in the canonical K-major no-swizzle layout with the
+// 8-row core groups packed back to back (row r of 16-byte chunk q at q * CH +
+// 16 r), so "rows shifted by ky" is the same descriptor with its start
+// address moved by 16 ky bytes.  B is 512 bytes per ky, built once per CTA.
+// 3 channels x 4 groups x (2R + 1) MMAs of 128 x 16 x 32 fill 12 accumulators
+// (192 of 256 allocated TMEM columns).
+//
+// Staging: the tile's 64 columns of each input row (plus an R-pixel halo) are
+// copied into a raw buffer -- one 192-byte bulk async copy per row when the
+// row piece is 16-byte aligned and the tile is full width, with the halo and
+// every other case (image borders: replicated pixels; ragged tiles) by plain
+// byte loads clamped to the subscription -- then de-interleaved by byte
+// permutes into the three planes.  Epilogue: each thread reads its output
+// row's 3 x 64 sums from TMEM, packs them to bytes (clamp: saturate; wrap:
+// low byte), re-interleaves RGB and stages the 192-byte row in shared memory;
+// the tile is then written with coalesced 16-byte stores.
+constexpr int kTcTW = 64, kTcTH = 128, kTcThreads = 128;
+constexpr int kTcMaxR = 8;
+constexpr int kTcMaxKD = 2 * kTcMaxR + 1;
+constexpr int kTcChunks = 5;        // plane columns tile_c0-8 .. tile_c0+71 in 16-byte chunks
+constexpr int kRawStride = 304;     // raw row: pixels tile_c0-16 .. tile_c0+79 (288 B) + padding
+constexpr int kOutStride = 208;     // staged output row: 192 B + padding (conflict-free 16-B stores)
+constexpr uint32_t kTcTmemCols = 256;
+constexpr uint32_t kTcWaitPolls = 1u << 21;
+constexpr uint32_t kImgfErrTimeout = 1;
+
+template <int R>
+struct TcGeo {
+    static constexpr int KD = 2 * R + 1;
+    static constexpr int ROWS = kTcTH + 2 * R;        // plane rows
+    static constexpr int CH = ROWS * 16;              // bytes per 16-column chunk of a plane
+    static constexpr int PLANE = kTcChunks * CH;
+    static constexpr int RAW = ROWS * kRawStride;
+    static constexpr int OUT = kTcTH * kOutStride;
+    static constexpr int OFF_RAW = 3 * PLANE;         // raw rows, later the staged output tile
+    static constexpr int OFF_B = OFF_RAW + (RAW > OUT ? RAW : OUT);
+    static constexpr int OFF_BAR = OFF_B + KD * 512;
+    static constexpr int SMEM = OFF_BAR + 64;
+    static_assert(CH % 16 == 0 && OFF_RAW % 16 == 0 && OFF_B % 16 == 0 && OFF_BAR % 8 == 0, "alignment");
+    static_assert(CH / 16 < (1 << 14), "leading byte offset field");
+};
+
+// Instruction descriptor, kind::i8: S32 accumulator, A u8, B s8, both
+// K-major, N = 16, M = 128.
+constexpr uint32_t kTcIdesc = (2u << 4) | (0u << 7) | (1u << 10) | ((16u >> 3) << 17) | ((128u >> 4) << 24);
+
+template <int MAXI>
+struct ImgfParamsTc {
+    int8_t f[kTcMaxKD][kTcMaxKD];
+    int n_items;
+    int tile_start[MAXI + 1];
+    int tiles_x[MAXI];
+    uint32_t* err;
+    pmb_imgf_item items[MAXI];
+};
+
+__device__ __forceinline__ uint32_t tc_smem(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Shared-memory descriptor of a K-major tile without swizzle: 8-row core
+// groups `sbo` bytes apart, 16-byte K chunks `lbo` bytes apart.
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = static_cast<uint64_t>((saddr >> 4) & 0x3FFF);
+    d |= static_cast<uint64_t>((lbo >> 4) & 0x3FFF) << 16;
+    d |= static_cast<uint64_t>((sbo >> 4) & 0x3FFF) << 32;
+    d |= static_cast<uint64_t>(1) << 46;  // descriptor version (sm_100); layout 0 = no swizzle
+    return d;
+}
+
+__device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity) {
+    for (uint32_t i = 0; i < kTcWaitPolls; ++i) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, 1000;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tc_mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(kTcIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+
+template <int R, int MODE, int MAXI>
+__global__ void __launch_bounds__(kTcThreads)
+imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
+    using G = TcGeo<R>;
+    extern __shared__ __align__(128) uint8_t smem[];
+    uint8_t* const planes = smem;
+    uint8_t* const raw = smem + G::OFF_RAW;
+    uint8_t* const bsm = smem + G::OFF_B;
+    uint64_t* const bars = reinterpret_cast<uint64_t*>(smem + G::OFF_BAR);  // [0] rows staged, [1] MMAs done
+    uint32_t* const tmem_slot = reinterpret_cast<uint32_t*>(bars + 2);
+    __shared__ int s_fail;
+
+    const int item = blockIdx.y;
+    const int local = blockIdx.x;
+    if (local >= p.tile_start[item + 1] - p.tile_start[item]) return;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const pmb_imgf_item& it = p.items[item];
+    const uint8_t* const in = it.in;
+    uint8_t* const out = it.out;
+    const int64_t ip = it.in_pitch, op = it.out_pitch;
+    const int H = it.height;
+    const int txs = p.tiles_x[item];
+    const int ty = local / txs, tx = local - ty * txs;
+    const int tile_c0 = it.c0 + tx * kTcTW, tile_r0 = it.r0 + ty * kTcTH;
+    const int mlo = max(0, it.r0 - R), mhi = min(H - 1, it.r1 - 1 + R);
+    const int clo = max(0, it.c0 - R), chi = min(it.width - 1, it.c1 - 1 + R);
+    const int tw = min(kTcTW, it.c1 - tile_c0);
+    // Row piece of the tile's 64 columns, as bulk copies: full width, 16-byte
+    // aligned source rows (the same for every row when the pitch is).
+    const bool bulk = tw == kTcTW && (ip & 15) == 0 &&
+                      ((reinterpret_cast<uintptr_t>(in) + 3 * static_cast<int64_t>(tile_c0 - it.in_col0)) & 15) == 0;
+    auto row_ptr = [&](int r) {  // input row of plane row r (replicated at the subscription's edges)
+        const int m = pmb::clampi(tile_r0 - R + r, mlo, mhi);
+        return in + static_cast<int64_t>(H - 1 - m - it.in_row0) * ip;
+    };
+
+    if (tid == 0) {
+        s_fail = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(&bars[0])));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(&bars[1])));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    // ---- stage input rows into the raw buffer (pixel x at byte 3x of a row:
+    //      image column tile_c0 - 16 + x) ----
+    if (bulk) {
+        if (warp == 0) {
+            if (lane == 0)
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc_smem(&bars[0])),
+                             "r"(static_cast<uint32_t>(G::ROWS * 3 * kTcTW))
+                             : "memory");
+            __syncwarp();
+            for (int r = lane; r < G::ROWS; r += 32) {
+                const uint8_t* src = row_ptr(r) + 3 * (tile_c0 - it.in_col0);
+                asm volatile(
+                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                        tc_smem(raw + r * kRawStride + 48)),
+                    "l"(src), "r"(3 * kTcTW), "r"(tc_smem(&bars[0]))
+                    : "memory");
+            }
+        }
+        for (int e = tid; e < G::ROWS * 2 * R; e += kTcThreads) {
+            const int r = e / (2 * R), k = e - r * (2 * R);
+            const int x = k < R ? 16 - R + k : 80 + (k - R);
+            const int n = pmb::clampi(tile_c0 - 16 + x, clo, chi);
+            const uint8_t* s = row_ptr(r) + 3 * (n - it.in_col0);
+            uint8_t* d = raw + r * kRawStride + 3 * x;
+            d[0] = __ldg(s);
+            d[1] = __ldg(s + 1);
+            d[2] = __ldg(s + 2);
+        }
+    } else {
+        const int span = kTcTW + 2 * R;
+        for (int e = tid; e < G::ROWS * span; e += kTcThreads) {
+            const int r = e / span, x = 16 - R + (e - r * span);
+            const int n = pmb::clampi(tile_c0 - 16 + x, clo, chi);
+            const uint8_t* s = row_ptr(r) + 3 * (n - it.in_col0);
+            uint8_t* d = raw + r * kRawStride + 3 * x;
+            d[0] = __ldg(s);
+            d[1] = __ldg(s + 1);
+            d[2] = __ldg(s + 2);
+        }
+    }
+
+    // ---- B: per filter row, the 16 x 32 banded slice, K-major core matrices
+    //      (8 output columns x 16 bytes; column groups 128 B, K chunks 256 B apart) ----
+    for (int w = tid; w < G::KD * 128; w += kTcThreads) {
+        const int ky = w >> 7, off = (w & 127) * 4;
+        uint32_t word = 0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int o = off + b;
+            const int k = (o >> 8) * 16 + (o & 15);
+            const int j = ((o >> 7) & 1) * 8 + ((o >> 4) & 7);
+            const int kx = k - j + R - 8;
+            const int v = (kx >= 0 && kx <= 2 * R) ? p.f[ky][kx] : 0;
+            word |= static_cast<uint32_t>(static_cast<uint8_t>(v)) << (8 * b);
+        }
+        *reinterpret_cast<uint32_t*>(bsm + ky * 512 + off) = word;
+    }
+    if (bulk && !tc_wait(tc_smem(&bars[0]), 0)) s_fail = 1;
+    __syncthreads();
+
+    // ---- de-interleave: plane c, chunk q, row r <- raw pixels 16q+8 .. 16q+23 ----
+    if (!s_fail) {
+        for (int e = tid; e < G::ROWS * kTcChunks; e += kTcThreads) {
+            const int q = e / G::ROWS, r = e - q * G::ROWS;
+            const uint8_t* s = raw + r * kRawStride + 48 * q + 24;
+            uint32_t w[12];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) {
+                const uint2 v = *reinterpret_cast<const uint2*>(s + 8 * k);
+                w[2 * k] = v.x;
+                w[2 * k + 1] = v.y;
+            }
+            uint32_t o[3][4];
+#pragma unroll
+            for (int g = 0; g < 4; ++g) deinterleave4(w[3 * g], w[3 * g + 1], w[3 * g + 2], o[0][g], o[1][g], o[2][g]);
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                *reinterpret_cast<uint4*>(planes + c * G::PLANE + q * G::CH + r * 16) =
+                    make_uint4(o[c][0], o[c][1], o[c][2], o[c][3]);
+        }
+    }
+    // Generic-proxy writes of the planes and B, then the tensor core reads them.
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (warp == 0) {
+        __syncwarp();
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc_smem(tmem_slot)),
+                     "r"(kTcTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    const bool failed = s_fail != 0;
+
+    // ---- MMAs: one thread issues 3 x 4 x (2R+1) products ----
+    if (tid == 0 && !failed) {
+        const uint32_t pl = tc_smem(planes), bb = tc_smem(bsm);
+#pragma unroll 1
+        for (int c = 0; c < 3; ++c)
+#pragma unroll 1
+            for (int t = 0; t < 4; ++t)
+#pragma unroll
+                for (int ky = 0; ky < G::KD; ++ky)
+                    tc_mma_i8(tmem + static_cast<uint32_t>((c * 4 + t) * 16),
+                              tc_desc(pl + c * G::PLANE + t * G::CH + ky * 16, G::CH, 128),
+                              tc_desc(bb + ky * 512, 256, 128), ky > 0 ? 1u : 0u);
+        tc_commit(tc_smem(&bars[1]));
+    }
+    // Block-uniform: the TMEM loads below are warp-collective.
+    const bool have = __syncthreads_and(!failed && tc_wait(tc_smem(&bars[1]), 0)) != 0;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+
+    // ---- epilogue: row 32*warp + lane, 3 x 64 sums -> 192 RGB bytes ----
+    uint8_t* const ost = raw;  // the raw rows are no longer needed
+    if (have) {
+        uint32_t pw[3][16];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                uint32_t v[16];
+                tc_ld16(tmem + (static_cast<uint32_t>(32 * warp) << 16) + static_cast<uint32_t>((c * 4 + t) * 16), v);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                for (int g = 0; g < 4; ++g) {
+                    const int a[4] = {static_cast<int>(v[4 * g]), static_cast<int>(v[4 * g + 1]),
+                                      static_cast<int>(v[4 * g + 2]), static_cast<int>(v[4 * g + 3])};
+                    pw[c][4 * t + g] = pack4<MODE>(a);
+                }
+            }
+        uint8_t* const orow = ost + (32 * warp + lane) * kOutStride;
+#pragma unroll
+        for (int g = 0; g < 16; g += 4) {
+            uint32_t d[12];
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+                const uint32_t A = pw[0][g + h], B = pw[1][g + h], C = pw[2][g + h];
+                d[3 * h + 0] = __byte_perm(__byte_perm(A, B, 0x0140), C, 0x2410);  // a0 b0 c0 a1
+                d[3 * h + 1] = __byte_perm(__byte_perm(B, C, 0x0251), A, 0x2610);  // b1 c1 a2 b2
+                d[3 * h + 2] = __byte_perm(C, __byte_perm(A, B, 0x0073), 0x3542);  // c2 a3 b3 c3
+            }
+#pragma unroll
+            for (int h = 0; h < 3; ++h)
+                *reinterpret_cast<uint4*>(orow + 12 * g + 16 * h) =
+                    make_uint4(d[4 * h], d[4 * h + 1], d[4 * h + 2], d[4 * h + 3]);
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (!failed && !have && lane == 0) {
+            // The MMAs did not report completion in time: wait (bounded) once
+            // more before freeing the tensor memory they write.
+            tc_wait(tc_smem(&bars[1]), 0);
+        }
+        __syncwarp();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTmemCols) : "memory");
+    }
+    if (!have) {
+        if (tid == 0) atomicOr(p.err, kImgfErrTimeout);
+        return;
+    }
+
+    // ---- write the tile: coalesced 16-byte stores, byte stores at ragged edges ----
+    const int rows = min(kTcTH, it.r1 - tile_r0);
+    uint8_t* const obase = out + static_cast<int64_t>(tile_r0 - it.out_row0) * op + 3 * (tile_c0 - it.out_col0);
+    if (tw == kTcTW && ((reinterpret_cast<uintptr_t>(obase) | static_cast<uintptr_t>(op)) & 15) == 0) {
+        for (int e = tid; e < rows * 12; e += kTcThreads) {
+            const int r = e / 12, k = e - r * 12;
+            *reinterpret_cast<uint4*>(obase + r * op + 16 * k) =
+                *reinterpret_cast<const uint4*>(ost + r * kOutStride + 16 * k);
+        }
+    } else {
+        const int nb = 3 * tw;
+        for (int e = tid; e < rows * nb; e += kTcThreads) {
+            const int r = e / nb, b = e - r * nb;
+            obase[r * op + b] = ost[r * kOutStride + b];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Plain GPU form: one thread per output pixel, byte loads straight from HBM.
 struct PlainFilter {
     int8_t f[PMB_IMGF_MAX_FILTER_DIM][PMB_IMGF_MAX_FILTER_DIM];
@@ -554,11 +899,69 @@ int launch_fast(const pmb_imgf_item* items, int n, const int8_t* filter, cudaStr
     return PMB_SUCCESS;
 }
 
+// Device address of the stencil's error word on the current device.
+__device__ uint32_t g_imgf_err;
+
+int imgf_err_word(uint32_t** out) {
+    static std::mutex mu;
+    static uint32_t* per_dev[64] = {};
+    int dev = 0;
+    PMB_CUDA_TRY(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return pmb::fail(PMB_BEYOND_LIMITS, "device ordinal %d", dev);
+    std::lock_guard<std::mutex> g(mu);
+    if (!per_dev[dev]) {
+        void* a = nullptr;
+        PMB_CUDA_TRY(cudaGetSymbolAddress(&a, g_imgf_err));
+        per_dev[dev] = static_cast<uint32_t*>(a);
+    }
+    *out = per_dev[dev];
+    return PMB_SUCCESS;
+}
+
+template <int R, int MODE, int MAXI>
+int launch_tc(const pmb_imgf_item* items, int n, const int8_t* filter, cudaStream_t s) {
+    using G = TcGeo<R>;
+    ImgfParamsTc<MAXI> p;
+    for (int ky = 0; ky < kTcMaxKD; ++ky)
+        for (int kx = 0; kx < kTcMaxKD; ++kx)
+            p.f[ky][kx] = ky < G::KD && kx < G::KD ? filter[ky * PMB_IMGF_MAX_FILTER_DIM + kx] : 0;
+    int64_t total = 0;
+    int m = 0, max_tiles = 0;
+    for (int i = 0; i < n; ++i) {
+        const pmb_imgf_item& it = items[i];
+        if (it.r0 == it.r1 || it.c0 == it.c1) continue;
+        const int txs = (it.c1 - it.c0 + kTcTW - 1) / kTcTW;
+        const int tys = (it.r1 - it.r0 + kTcTH - 1) / kTcTH;
+        p.items[m] = it;
+        p.tiles_x[m] = txs;
+        p.tile_start[m] = static_cast<int>(total);
+        total += static_cast<int64_t>(txs) * tys;
+        max_tiles = std::max(max_tiles, txs * tys);
+        ++m;
+    }
+    if (m == 0) return PMB_SUCCESS;
+    if (total > 0x7fffffffLL) return pmb::fail(PMB_BEYOND_LIMITS, "too many tiles: %lld", (long long)total);
+    p.n_items = m;
+    p.tile_start[m] = static_cast<int>(total);
+    int st = imgf_err_word(&p.err);
+    if (st != PMB_SUCCESS) return st;
+    static std::once_flag once;
+    static cudaError_t attr = cudaSuccess;
+    std::call_once(once, [] {
+        attr = cudaFuncSetAttribute(imgf_tc_kernel<R, MODE, MAXI>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
+    });
+    PMB_CUDA_TRY(attr);
+    imgf_tc_kernel<R, MODE, MAXI>
+        <<<dim3(static_cast<unsigned>(max_tiles), static_cast<unsigned>(m)), kTcThreads, G::SMEM, s>>>(p);
+    PMB_CUDA_TRY(cudaGetLastError());
+    return PMB_SUCCESS;
+}
+
 template <int R, int MAXI>
 int launch_mode(const pmb_imgf_item* items, int n, const int8_t* filter, int mode, cudaStream_t s) {
-    if constexpr (R <= 4) {
-        return mode == PMB_IMGF_WRAP ? launch_fast<R, PMB_IMGF_WRAP, MAXI>(items, n, filter, s)
-                                     : launch_fast<R, PMB_IMGF_CLAMP, MAXI>(items, n, filter, s);
+    if constexpr (R <= kTcMaxR) {
+        return mode == PMB_IMGF_WRAP ? launch_tc<R, PMB_IMGF_WRAP, MAXI>(items, n, filter, s)
+                                     : launch_tc<R, PMB_IMGF_CLAMP, MAXI>(items, n, filter, s);
     } else {
         return mode == PMB_IMGF_WRAP ? launch_t<R, PMB_IMGF_WRAP, MAXI>(items, n, filter, s)
                                      : launch_t<R, PMB_IMGF_CLAMP, MAXI>(items, n, filter, s);
@@ -612,6 +1015,16 @@ extern "C" int pmb_image_filter_full(const uint8_t* d_in, uint8_t* d_out, int wi
     it.c0 = 0;
     it.c1 = width;
     return pmb_image_filter(&it, 1, filter, radius, mode, stream);
+}
+
+extern "C" int pmb_image_filter_error(int clear, uint32_t* error_out) {
+    PMB_CHECK_ARG(error_out, "null pointer");
+    uint32_t* w = nullptr;
+    const int st = imgf_err_word(&w);
+    if (st != PMB_SUCCESS) return st;
+    PMB_CUDA_TRY(cudaMemcpy(error_out, w, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (clear) PMB_CUDA_TRY(cudaMemset(w, 0, sizeof(uint32_t)));
+    return PMB_SUCCESS;
 }
 
 extern "C" int pmb_image_filter_plain(const uint8_t* d_in, uint8_t* d_out, int width, int height,

@@ -211,6 +211,7 @@ struct Controller {
     std::atomic<int64_t> dev_held{0};
     size_t max_inflight = 64;              // GPU tasks on the device at once (admission slots)
     std::atomic<bool> eager_writeback{false};  // copy written bytes to the host at task end
+    size_t batch_groups = 16;              // launches a batched task is split into (pipelined staging)
     // pinned host buffers of released address spaces, kept for reuse
     std::mutex pin_mu;
     std::multimap<size_t, char*> pin_free;
@@ -981,6 +982,83 @@ static bool admit(Task* t, size_t* need_out) {
     return need == 0 || make_room(need, t->spaces);
 }
 
+// Upload what subtasks [g0, g1) of a batched task read and the device lacks.
+// Their read records are merged first: neighbouring tiles' rows join into
+// long contiguous copies (one per run of full rows for a row of image tiles)
+// instead of one narrow 2-D copy per subtask; when merging would not reduce
+// the number of copies, each record is uploaded on its own.
+static pmStatus upload_group(Task* t, size_t g0, size_t g1, void* stream) {
+    Controller& c = ctl();
+    for (size_t i = 0; i < t->spaces.size(); ++i) {
+        AddressSpace* a = t->spaces[i];
+        std::lock_guard<std::mutex> g(a->mu);
+        RangeSet need;
+        size_t records = 0;
+        for (size_t si = g0; si < g1; ++si)
+            for (const Record& r : t->subtasks[si].mem[i].reads)
+                if (r.count && r.size) {
+                    add_record(need, r);
+                    ++records;
+                }
+        if (need.empty()) continue;
+        if (need.map().size() > records) {
+            for (size_t si = g0; si < g1; ++si)
+                for (const Record& r : t->subtasks[si].mem[i].reads) {
+                    const pmStatus st = upload_record(a, r, stream);
+                    if (st != pmSuccess) return st;
+                }
+            continue;
+        }
+        for (auto& kv : need.map()) {
+            if (a->host) {  // never written by the host: contents are undefined either way
+                std::vector<std::pair<size_t, size_t>> miss;
+                a->dev_valid.missing(kv.first, kv.second, miss);
+                for (auto& m : miss) {
+                    PMR_DEV(pmb_memcpy_async(a->dev + m.first, a->host + m.first, m.second - m.first, PMB_H2D, stream));
+                    c.stats.h2d += m.second - m.first;
+                }
+            }
+            a->dev_valid.add(kv.first, kv.second);
+        }
+    }
+    return pmSuccess;
+}
+
+// Copy back, on `stream` right after their launch, the bytes subtasks
+// [g0, g1) of a batched task wrote, when results go to the host at task end
+// (cache disabled, or eager write-back): a group's results then cross to the
+// host while later groups compute.  Fragmented write sets are left to the
+// task-end write-back.
+static pmStatus writeback_group(Task* t, size_t g0, size_t g1, bool write_through, void* stream) {
+    Controller& c = ctl();
+    for (size_t i = 0; i < t->spaces.size(); ++i) {
+        if (!writable(t->mem[i].memType)) continue;
+        AddressSpace* a = t->spaces[i];
+        std::lock_guard<std::mutex> g(a->mu);
+        RangeSet done;
+        size_t records = 0;
+        for (size_t si = g0; si < g1; ++si)
+            for (const Record& r : t->subtasks[si].mem[i].writes)
+                if (r.count && r.size) {
+                    add_record(done, r);
+                    ++records;
+                }
+        if (done.empty() || done.map().size() > std::max<size_t>(records, 16)) continue;
+        if (write_through) {
+            const pmStatus hs = ensure_host(a);
+            if (hs != pmSuccess) return hs;
+        } else if (!host_from_cache(a)) {
+            continue;  // no pinned buffer at hand: pmFetchMemory copies it back later
+        }
+        for (auto& kv : done.map()) {
+            PMR_DEV(pmb_memcpy_async(a->host + kv.first, a->dev + kv.first, kv.second - kv.first, PMB_D2H, stream));
+            c.stats.d2h += kv.second - kv.first;
+            a->host_stale.remove(kv.first, kv.second);
+        }
+    }
+    return pmSuccess;
+}
+
 static pmStatus stage_and_launch_gpu(Task* t) {
     Controller& c = ctl();
     const pmCallbacks& cb = t->callbacks->cb;
@@ -1046,6 +1124,17 @@ static pmStatus stage_and_launch_gpu(Task* t) {
 
     std::vector<pmSubtaskInfo> infos(t->subtasks.size());
     std::vector<bool> used_stream(c.streams.size(), false);
+    // A batched task runs as up to c.batch_groups launches over consecutive
+    // subtasks; each launches once its own group is staged.
+    std::vector<size_t> group_begin;  // first subtask of each group, then the subtask count
+    std::vector<void*> group_staged;
+    if (batch) {
+        const size_t nsub = t->subtasks.size();
+        const size_t per = (nsub + std::max<size_t>(c.batch_groups, 1) - 1) / std::max<size_t>(c.batch_groups, 1);
+        for (size_t g0 = 0; g0 < nsub; g0 += std::max<size_t>(per, 1)) group_begin.push_back(g0);
+        group_begin.push_back(nsub);
+    }
+    size_t group = 0;
     for (size_t si = 0; si < t->subtasks.size(); ++si) {
         Subtask& s = t->subtasks[si];
         pmSubtaskInfo& info = infos[si];
@@ -1055,11 +1144,16 @@ static pmStatus stage_and_launch_gpu(Task* t) {
         s.dev_shadow.assign(ns, nullptr);
         std::vector<Compact> compacts(ns);
         // ---- stage (copy stream) ----
+        if (batch && si == group_begin[group]) {
+            const pmStatus st = upload_group(t, si, group_begin[group + 1], c.copy_stream);
+            if (st != pmSuccess) return st;
+        }
         for (size_t i = 0; i < ns; ++i) {
             AddressSpace* a = t->spaces[i];
             const SubtaskMem& m = s.mem[i];
             std::lock_guard<std::mutex> g(a->mu);
             for (const Record& r : m.reads) {
+                if (batch) break;  // staged with its group
                 const pmStatus st = upload_record(a, r, c.copy_stream);
                 if (st != pmSuccess) return st;
             }
@@ -1107,10 +1201,19 @@ static pmStatus stage_and_launch_gpu(Task* t) {
             }
             info.memInfo[i] = mi;
         }
+        if (batch) {  // launched per group below
+            if (si + 1 == group_begin[group + 1]) {
+                void* staged = new_event();
+                if (!staged) return fail(pmGraphicsCardError, "event creation failed: %s", pmb_last_error());
+                PMR_DEV(pmb_event_record(staged, c.copy_stream));
+                group_staged.push_back(staged);
+                ++group;
+            }
+            continue;
+        }
         void* staged = new_event();
         if (!staged) return fail(pmGraphicsCardError, "event creation failed: %s", pmb_last_error());
         PMR_DEV(pmb_event_record(staged, c.copy_stream));
-        if (batch) continue;  // launched once for the whole task below
 
         // ---- launch (compute stream) ----
         const size_t sidx = c.next_stream++ % c.streams.size();
@@ -1177,16 +1280,19 @@ static pmStatus stage_and_launch_gpu(Task* t) {
         if (s.dev_scratch) PMR_DEV(pmb_free_async(s.dev_scratch, stream));
     }
 
-    if (batch) {
+    for (size_t gi = 0; batch && gi + 1 < group_begin.size(); ++gi) {
+        const size_t g0 = group_begin[gi], g1 = group_begin[gi + 1];
         const size_t sidx = c.next_stream++ % c.streams.size();
         void* stream = c.streams[sidx];
         used_stream[sidx] = true;
-        PMR_DEV(pmb_stream_wait_event(stream, events.back()));  // copy stream is ordered: all staged
-        const pmStatus st = batch(&t->info, &c.gpu_info, infos.data(), infos.size(), stream);
+        PMR_DEV(pmb_stream_wait_event(stream, group_staged[gi]));  // the group's uploads are done
+        const double tcb = now_s();
+        const pmStatus st = batch(&t->info, &c.gpu_info, infos.data() + g0, g1 - g0, stream);
+        c.stats.callback_ns += ns_since(tcb);
         if (st != pmSuccess) return fail(st, "batched GPU callback returned %d", static_cast<int>(st));
         c.stats.batched++;
-        c.stats.gpu_subtasks += infos.size();
-        for (size_t si = 0; si < t->subtasks.size(); ++si) {
+        c.stats.gpu_subtasks += g1 - g0;
+        for (size_t si = g0; si < g1; ++si) {
             t->subtasks[si].info = infos[si];
             for (size_t i = 0; i < ns; ++i) {
                 AddressSpace* a = t->spaces[i];
@@ -1196,6 +1302,10 @@ static pmStatus stage_and_launch_gpu(Task* t) {
                     add_record(a->host_stale, r);
                 }
             }
+        }
+        if (write_through || c.eager_writeback) {
+            const pmStatus ws = writeback_group(t, g0, g1, write_through, stream);
+            if (ws != pmSuccess) return ws;
         }
     }
 
@@ -1586,6 +1696,8 @@ pmStatus pmInitialize() {
         const char* pv = getenv("PMB_PINNED_CACHE_BYTES");
         c.pin_limit = pv ? static_cast<size_t>(atoll(pv)) : (size_t(16) << 30);
         c.eager_writeback = env_flag("PMB_EAGER_WRITEBACK");
+        const char* bg = getenv("PMB_BATCH_GROUPS");
+        c.batch_groups = bg && atoi(bg) > 0 ? static_cast<size_t>(atoi(bg)) : 16;
         const char* mv = getenv("PMB_MAX_INFLIGHT");
         c.max_inflight = mv && atoi(mv) > 0 ? static_cast<size_t>(atoi(mv)) : 64;
     }
