@@ -141,3 +141,11 @@ def test_full_configuration_8192(cuda, oracle, mode):
     ops.image_filter(d_in, d_out, W, H, f[:5, :5], mode, items=tiles(W, H, 512))
     cuda.cuda.synchronize()
     assert np.array_equal(d_out.cpu().numpy(), run_oracle(oracle, img, W, H, R, f, mode))
+
+
+def test_zz_stencil_error_word_clear(cuda, pmb):
+    """Last in this file: no bounded wait of any tensor-core stencil launch
+    above expired (the error word is sticky until cleared)."""
+    err = ctypes.c_uint32(0xFFFFFFFF)
+    assert pmb.pmb_image_filter_error(1, ctypes.byref(err)) == 0
+    assert err.value == 0

@@ -121,3 +121,24 @@ def test_reference_int_matrix_multiply_app_cpu_mode(n):
     app with its serial run."""
     rc, out = run([app_or_skip(INT_MM_APP), "1", "1", "0", n])
     assert rc == 0 and "Serial Comparison Test Passed" in out and "Failed" not in out, out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", ["1024", "4096"])
+def test_reference_matrix_multiply_app_gpu_mode(n):
+    """The unchanged matrixMultiplyBlas app, parallel mode 2 (local GPU): its
+    subtasks run matrixMultiply_cudaLaunchFunc of libpmb_app_matrixMultiplyBlas
+    (the tcgen05 BF16x3 GEMM) and the app compares them with its serial
+    cblas_sgemm at relative 1e-5 per element."""
+    rc, out = run([app_or_skip(MM_APP), "1", "2", "0", n], timeout=600)
+    assert rc == 0 and "Serial Comparison Test Passed" in out and "Failed" not in out, out
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", ["1000", "257"])
+def test_reference_int_matrix_multiply_app_gpu_mode(n):
+    """The unchanged int matrixMultiply app, parallel mode 2: the runtime
+    launches the app's own subtask_gpu_cuda kernel (matrixMultiplyCUDA.cu,
+    compiled for sm_100a) per subtask and the app compares with its serial run."""
+    rc, out = run([app_or_skip(INT_MM_APP), "1", "2", "0", n], timeout=600)
+    assert rc == 0 and "Serial Comparison Test Passed" in out and "Failed" not in out, out
