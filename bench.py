@@ -817,6 +817,49 @@ def _hbm_entry(nbytes: int, ms: float, hbm: float):
             "roofline": {"bound": "hbm", "peak": hbm, "frac": round(gbs / hbm, 4)}}
 
 
+def summarize(line):
+    """Compact per-app figures: {app: [rate, unit, roofline frac, CPU value,
+    library or plain-form figure]} plus the served stream and the e2e path."""
+    out = {}
+    apps = line.get("apps") or {}
+
+    def cpu(v):
+        c = v.get("cpu_baseline") or {}
+        return c.get("value")
+
+    for key, v in apps.items():
+        if not isinstance(v, dict):
+            continue
+        if "error" in v:
+            out[key] = "error"
+        elif "gbs" in v:
+            lib = v.get("library_torch_sort_int64_ms") or v.get("library_torch_cumsum_int64_ms")
+            out[key] = [v["gbs"], "GB/s", v["roofline"]["frac"], cpu(v)] + ([f"torch {lib} ms"] if lib else [])
+        elif "tflops" in v:
+            out[key] = [v["tflops"], "TFLOP/s", v["roofline"]["frac"], cpu(v), f"cublas_sgemm {v['cublas_sgemm_fp32_tflops']}"]
+        elif "gflops" in v:
+            out[key] = [v["gflops"], "GFLOP/s", v.get("ms"), cpu(v), f"resid {v.get('residual_fro')}"]
+        elif "medges_per_s" in v:
+            out[key] = [v["medges_per_s"], "Medges/s"]
+    sm = line.get("served_mix") or {}
+    sat = sm.get("saturated")
+    if sat:
+        out["served"] = {"tasks_per_s": sat["served"]["tasks_per_s"], "plain": sat["plain"]["tasks_per_s"],
+                         "x": sat.get("served_over_plain_tasks_per_s"),
+                         "alone_vs_mix": f"{sat['alone_vs_mix']['bit_identical']}/{sat['alone_vs_mix']['compared']}"}
+        ld = sm.get("at_load")
+        if ld:
+            out["served"].update({"load_rate": ld["rate_per_s"], "p50_ms": ld["served"]["p50_ms"],
+                                  "p99_ms": ld["served"]["p99_ms"]})
+    elif sm:
+        out["served"] = "error"
+    e2e = line.get("e2e") or {}
+    out["e2e"] = {"pm_api_gbs": e2e.get("value") if "pm_api_error" not in e2e else None,
+                  "c_abi_gbs": (line.get("e2e_c_abi") or {}).get("value"),
+                  "runtime_stub_ms": (e2e.get("runtime_per_task") or {}).get("stub_host_ms")}
+    return out
+
+
 def main():
     args = parse()
     if args.warmup < 3:
@@ -963,6 +1006,9 @@ def main():
             line["served_mix"] = {"error": f"{type(e).__name__}: {e}"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(img, f, os.cpu_count() or 1)
+    # Last key of the line (so it survives a cut-off tail): one compact entry
+    # per app kernel -- rate, roofline fraction, CPU baseline, library figure.
+    line["summary"] = summarize(line)
     ranks.close()
     if rank == 0:
         print(json.dumps(line))

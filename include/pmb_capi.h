@@ -429,6 +429,21 @@ int pmb_trsm_f32(int side, int uplo, int diag, int m, int n, const float* d_A, i
 int pmb_lu_residual_f64(const float* d_A0, int64_t lda0, const float* d_LU, int64_t ldlu, int n, double* d_sums,
                         void* stream);
 
+/* FP64 refinement of a solve with fp32 LU factors: A x = b for the n x n
+ * column-major d_A0 (fp32, lda0) factored into d_LU by pmb_lu_decompose
+ * (Crout form, ldlu).  x_0 = U^-1 L^-1 b, then `iterations` steps of
+ * r = b - A x in FP64, x += U^-1 L^-1 r, all triangular solves in FP64.
+ * d_b, d_x: n device doubles; d_berr: iterations + 1 device doubles receiving
+ * the normwise backward error ||b - A x||_inf / (||A||_inf ||x||_inf +
+ * ||b||_inf) after each solve.  d_workspace: pmb_lu_refine_workspace_bytes(n).
+ * No counterpart in the reference, whose LU stays in fp32
+ * (luDecomposition.cpp:116-125); it is the FP64 residual / refinement step
+ * of the split-precision LU. */
+size_t pmb_lu_refine_workspace_bytes(int n);
+int pmb_lu_solve_refined(const float* d_A0, int64_t lda0, const float* d_LU, int64_t ldlu, int n, const double* d_b,
+                         double* d_x, int iterations, double* d_berr, void* d_workspace, size_t ws_bytes,
+                         void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -136,3 +136,32 @@ def test_gpu_lu_after_producer_on_same_stream(cuda, oracle):
     ref = crout_f64(oracle, a)
     assert np.allclose(d.cpu().numpy(), ref, rtol=1e-4, atol=1e-5)
     assert np.allclose(d2.cpu().numpy(), ref, rtol=1e-4, atol=1e-5)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n", [100, 1000, 2048])
+def test_fp64_refinement_recovers_fp64_accuracy(cuda, pmb, n):
+    """Refined solves with the BF16x3/FP64 LU factors: the backward error
+    falls from fp32 level to FP64 level, and x matches an FP64 solve."""
+    from unicorn_b200 import capi, ops
+
+    a = dd_matrix(n, 500 + n)
+    d0 = cuda.from_numpy(a.copy()).cuda()
+    d = cuda.from_numpy(a.copy()).cuda()
+    ops.lu_decompose(d, 64)
+    b = np.random.default_rng(n).uniform(-1, 1, n)
+    db = cuda.from_numpy(b).cuda()
+    dx = cuda.zeros(n, dtype=cuda.float64, device="cuda")
+    iters = 4
+    berr = cuda.zeros(iters + 1, dtype=cuda.float64, device="cuda")
+    wsb = pmb.pmb_lu_refine_workspace_bytes(n)
+    ws = ops._scratch(wsb)
+    capi.check(pmb.pmb_lu_solve_refined(d0.data_ptr(), n, d.data_ptr(), n, n, db.data_ptr(), dx.data_ptr(), iters,
+                                        berr.data_ptr(), ws.data_ptr(), wsb, cuda.cuda.current_stream().cuda_stream))
+    cuda.cuda.synchronize()
+    e = berr.cpu().numpy()
+    assert e[0] < 1e-5 and e[-1] < 1e-14, e
+    A = a.T.astype(np.float64)
+    ref = np.linalg.solve(A, b)
+    x = dx.cpu().numpy()
+    assert np.linalg.norm(x - ref) / np.linalg.norm(ref) < 1e-12

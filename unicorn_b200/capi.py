@@ -112,6 +112,9 @@ _SIGS = {
                                       c_int, c_void_p]),
     "pmb_image_filter_error": (c_int, [c_int, ctypes.POINTER(ctypes.c_uint32)]),
     "pmb_trsm_workspace_bytes": (c_size_t, [c_int, c_int, c_int]),
+    "pmb_lu_refine_workspace_bytes": (c_size_t, [c_int]),
+    "pmb_lu_solve_refined": (c_int, [c_void_p, c_int64, c_void_p, c_int64, c_int, c_void_p, c_void_p, c_int, c_void_p,
+                                     c_void_p, c_size_t, c_void_p]),
     "pmb_trsm_f32": (c_int, [c_int, c_int, c_int, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64, c_void_p,
                              c_size_t, c_void_p]),
     "pmb_image_filter_plain": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_int, c_int, c_void_p]),

@@ -590,15 +590,34 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
                     : "memory");
             }
         }
-        for (int e = tid; e < G::ROWS * 2 * R; e += kTcThreads) {
-            const int r = e / (2 * R), k = e - r * (2 * R);
-            const int x = k < R ? 16 - R + k : 80 + (k - R);
-            const int n = pmb::clampi(tile_c0 - 16 + x, clo, chi);
-            const uint8_t* s = row_ptr(r) + 3 * (n - it.in_col0);
-            uint8_t* d = raw + r * kRawStride + 3 * x;
-            d[0] = __ldg(s);
-            d[1] = __ldg(s + 1);
-            d[2] = __ldg(s + 2);
+        // Halo: R pixels left and right of every row, one (row, side) piece per
+        // thread and round, all loads of a thread issued before its stores.
+        constexpr int kPer = (2 * G::ROWS + kTcThreads - 1) / kTcThreads;
+        uint8_t hv[kPer][3 * R];
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) {
+            const int e = tid + q * kTcThreads;
+            if (e < 2 * G::ROWS) {
+                const uint8_t* rp = row_ptr(e >> 1);
+                const int x0 = (e & 1) ? 80 : 16 - R;
+#pragma unroll
+                for (int b = 0; b < R; ++b) {
+                    const int n = pmb::clampi(tile_c0 - 16 + x0 + b, clo, chi);
+                    const uint8_t* src = rp + 3 * (n - it.in_col0);
+                    hv[q][3 * b] = __ldg(src);
+                    hv[q][3 * b + 1] = __ldg(src + 1);
+                    hv[q][3 * b + 2] = __ldg(src + 2);
+                }
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < kPer; ++q) {
+            const int e = tid + q * kTcThreads;
+            if (e < 2 * G::ROWS) {
+                uint8_t* d = raw + (e >> 1) * kRawStride + 3 * ((e & 1) ? 80 : 16 - R);
+#pragma unroll
+                for (int b = 0; b < 3 * R; ++b) d[b] = hv[q][b];
+            }
         }
     } else {
         const int span = kTcTW + 2 * R;
@@ -691,19 +710,21 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
     if (have) {
         uint32_t pw[3][16];
 #pragma unroll
-        for (int c = 0; c < 3; ++c)
+        for (int c = 0; c < 3; ++c) {
+            uint32_t v[4][16];  // a channel's four accumulators in flight at once
 #pragma unroll
-            for (int t = 0; t < 4; ++t) {
-                uint32_t v[16];
-                tc_ld16(tmem + (static_cast<uint32_t>(32 * warp) << 16) + static_cast<uint32_t>((c * 4 + t) * 16), v);
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            for (int t = 0; t < 4; ++t)
+                tc_ld16(tmem + (static_cast<uint32_t>(32 * warp) << 16) + static_cast<uint32_t>((c * 4 + t) * 16), v[t]);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int t = 0; t < 4; ++t)
 #pragma unroll
                 for (int g = 0; g < 4; ++g) {
-                    const int a[4] = {static_cast<int>(v[4 * g]), static_cast<int>(v[4 * g + 1]),
-                                      static_cast<int>(v[4 * g + 2]), static_cast<int>(v[4 * g + 3])};
+                    const int a[4] = {static_cast<int>(v[t][4 * g]), static_cast<int>(v[t][4 * g + 1]),
+                                      static_cast<int>(v[t][4 * g + 2]), static_cast<int>(v[t][4 * g + 3])};
                     pw[c][4 * t + g] = pack4<MODE>(a);
                 }
-            }
+        }
         uint8_t* const orow = ost + (32 * warp + lane) * kOutStride;
 #pragma unroll
         for (int g = 0; g < 16; g += 4) {

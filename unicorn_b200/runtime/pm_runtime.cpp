@@ -374,6 +374,73 @@ static void add_record(RangeSet& s, const Record& r) {
     for (size_t k = 0; k < r.count; ++k) s.add(r.offset + k * r.step, r.offset + k * r.step + r.size);
 }
 
+// Union of the byte ranges of `recs`, as sorted disjoint [lo, hi) pieces with
+// touching pieces joined.  Records that are rows of one pitch (the 2-D tiles
+// of image and matrix subscriptions) are merged band by band: within a band
+// of rows the same records are active, so the band is one contiguous piece
+// when their columns cover the whole pitch, else the same column pieces
+// repeat on every row of the band.  This costs O(records^2 + pieces) instead
+// of one ordered-map insertion per row of every record.
+static void union_records(const std::vector<const Record*>& recs, std::vector<std::pair<size_t, size_t>>& out) {
+    out.clear();
+    size_t step = 0;
+    bool strided = true;
+    for (const Record* r : recs) {
+        if (!r->count || !r->size) continue;
+        if (r->contiguous() || r->size > r->step) {
+            strided = false;
+            break;
+        }
+        if (!step) step = r->step;
+        if (r->step != step || (r->offset % step) + r->size > step) {
+            strided = false;
+            break;
+        }
+    }
+    auto push = [&](size_t lo, size_t hi) {
+        if (!out.empty() && out.back().second >= lo) out.back().second = std::max(out.back().second, hi);
+        else out.emplace_back(lo, hi);
+    };
+    if (!strided || !step) {
+        RangeSet u;
+        for (const Record* r : recs) add_record(u, *r);
+        for (auto& kv : u.map()) out.emplace_back(kv.first, kv.second);
+        return;
+    }
+    std::vector<size_t> rows;  // band boundaries
+    for (const Record* r : recs) {
+        if (!r->count || !r->size) continue;
+        rows.push_back(r->offset / step);
+        rows.push_back(r->offset / step + r->count);
+    }
+    std::sort(rows.begin(), rows.end());
+    rows.erase(std::unique(rows.begin(), rows.end()), rows.end());
+    std::vector<std::pair<size_t, size_t>> cols;
+    for (size_t b = 0; b + 1 < rows.size(); ++b) {
+        const size_t b0 = rows[b], b1 = rows[b + 1];
+        cols.clear();
+        for (const Record* r : recs) {
+            if (!r->count || !r->size) continue;
+            const size_t r0 = r->offset / step;
+            if (r0 <= b0 && r0 + r->count >= b1) cols.emplace_back(r->offset % step, r->offset % step + r->size);
+        }
+        if (cols.empty()) continue;
+        std::sort(cols.begin(), cols.end());
+        size_t k = 0;  // merge the column pieces in place
+        for (size_t i = 1; i < cols.size(); ++i) {
+            if (cols[i].first <= cols[k].second) cols[k].second = std::max(cols[k].second, cols[i].second);
+            else cols[++k] = cols[i];
+        }
+        cols.resize(k + 1);
+        if (cols.size() == 1 && cols[0].first == 0 && cols[0].second == step) {
+            push(b0 * step, b1 * step);
+            continue;
+        }
+        for (size_t row = b0; row < b1; ++row)
+            for (auto& c : cols) push(row * step + c.first, row * step + c.second);
+    }
+}
+
 // Compact layout of one address space for one subtask: the union of its read
 // and write ranges, packed back to back in offset order
 // (pmSubscriptionManager::GetCompactedSubscription, pmSubscriptionManager.cpp:1978-2030).
@@ -989,27 +1056,25 @@ static bool admit(Task* t, size_t* need_out) {
 // the number of copies, each record is uploaded on its own.
 static pmStatus upload_group(Task* t, size_t g0, size_t g1, void* stream) {
     Controller& c = ctl();
+    std::vector<const Record*> recs;
+    std::vector<std::pair<size_t, size_t>> need;
     for (size_t i = 0; i < t->spaces.size(); ++i) {
         AddressSpace* a = t->spaces[i];
         std::lock_guard<std::mutex> g(a->mu);
-        RangeSet need;
-        size_t records = 0;
+        recs.clear();
         for (size_t si = g0; si < g1; ++si)
             for (const Record& r : t->subtasks[si].mem[i].reads)
-                if (r.count && r.size) {
-                    add_record(need, r);
-                    ++records;
-                }
-        if (need.empty()) continue;
-        if (need.map().size() > records) {
-            for (size_t si = g0; si < g1; ++si)
-                for (const Record& r : t->subtasks[si].mem[i].reads) {
-                    const pmStatus st = upload_record(a, r, stream);
-                    if (st != pmSuccess) return st;
-                }
+                if (r.count && r.size) recs.push_back(&r);
+        if (recs.empty()) continue;
+        union_records(recs, need);
+        if (need.size() > recs.size()) {
+            for (const Record* r : recs) {
+                const pmStatus st = upload_record(a, *r, stream);
+                if (st != pmSuccess) return st;
+            }
             continue;
         }
-        for (auto& kv : need.map()) {
+        for (auto& kv : need) {
             if (a->host) {  // never written by the host: contents are undefined either way
                 std::vector<std::pair<size_t, size_t>> miss;
                 a->dev_valid.missing(kv.first, kv.second, miss);
@@ -1024,33 +1089,40 @@ static pmStatus upload_group(Task* t, size_t g0, size_t g1, void* stream) {
     return pmSuccess;
 }
 
-// Copy back, on `stream` right after their launch, the bytes subtasks
-// [g0, g1) of a batched task wrote, when results go to the host at task end
-// (cache disabled, or eager write-back): a group's results then cross to the
-// host while later groups compute.  Fragmented write sets are left to the
-// task-end write-back.
+// Record what subtasks [g0, g1) of a batched task wrote (valid on the device,
+// newer than the host) and, when results go to the host at task end (cache
+// disabled, or eager write-back), copy those bytes back on `stream` right
+// after the group's launch: a group's results then cross to the host while
+// later groups compute.  Fragmented write sets are left to the task-end
+// write-back.
 static pmStatus writeback_group(Task* t, size_t g0, size_t g1, bool write_through, void* stream) {
     Controller& c = ctl();
+    std::vector<const Record*> recs;
+    std::vector<std::pair<size_t, size_t>> done;
     for (size_t i = 0; i < t->spaces.size(); ++i) {
         if (!writable(t->mem[i].memType)) continue;
         AddressSpace* a = t->spaces[i];
         std::lock_guard<std::mutex> g(a->mu);
-        RangeSet done;
-        size_t records = 0;
+        recs.clear();
         for (size_t si = g0; si < g1; ++si)
             for (const Record& r : t->subtasks[si].mem[i].writes)
-                if (r.count && r.size) {
-                    add_record(done, r);
-                    ++records;
-                }
-        if (done.empty() || done.map().size() > std::max<size_t>(records, 16)) continue;
+                if (r.count && r.size) recs.push_back(&r);
+        if (recs.empty()) continue;
+        union_records(recs, done);
+        // Mark the group's results valid on the device and newer than the host.
+        for (auto& kv : done) {
+            a->dev_valid.add(kv.first, kv.second);
+            a->host_stale.add(kv.first, kv.second);
+        }
+        if (!write_through && !c.eager_writeback) continue;
+        if (done.size() > std::max<size_t>(recs.size(), 16)) continue;  // fragmented: left to the task-end write-back
         if (write_through) {
             const pmStatus hs = ensure_host(a);
             if (hs != pmSuccess) return hs;
         } else if (!host_from_cache(a)) {
             continue;  // no pinned buffer at hand: pmFetchMemory copies it back later
         }
-        for (auto& kv : done.map()) {
+        for (auto& kv : done) {
             PMR_DEV(pmb_memcpy_async(a->host + kv.first, a->dev + kv.first, kv.second - kv.first, PMB_D2H, stream));
             c.stats.d2h += kv.second - kv.first;
             a->host_stale.remove(kv.first, kv.second);
@@ -1292,21 +1364,9 @@ static pmStatus stage_and_launch_gpu(Task* t) {
         if (st != pmSuccess) return fail(st, "batched GPU callback returned %d", static_cast<int>(st));
         c.stats.batched++;
         c.stats.gpu_subtasks += g1 - g0;
-        for (size_t si = g0; si < g1; ++si) {
-            t->subtasks[si].info = infos[si];
-            for (size_t i = 0; i < ns; ++i) {
-                AddressSpace* a = t->spaces[i];
-                std::lock_guard<std::mutex> g(a->mu);
-                for (const Record& r : t->subtasks[si].mem[i].writes) {
-                    add_record(a->dev_valid, r);
-                    add_record(a->host_stale, r);
-                }
-            }
-        }
-        if (write_through || c.eager_writeback) {
-            const pmStatus ws = writeback_group(t, g0, g1, write_through, stream);
-            if (ws != pmSuccess) return ws;
-        }
+        for (size_t si = g0; si < g1; ++si) t->subtasks[si].info = infos[si];
+        const pmStatus ws = writeback_group(t, g0, g1, write_through, stream);
+        if (ws != pmSuccess) return ws;
     }
 
     // ---- join the task's streams into its completion event ----
