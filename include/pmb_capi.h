@@ -80,6 +80,14 @@ int pmb_memcpy_async(void* dst, const void* src, size_t bytes, int kind, void* s
 int pmb_memcpy2d_async(void* dst, size_t dpitch, const void* src, size_t spitch, size_t width, size_t height,
                        int kind, void* stream);
 int pmb_memset_async(void* p, int value, size_t bytes, void* stream);
+/* Copy n_ranges byte ranges d_src + src -> d_dst + dst in one launch on
+ * `stream`; d_ranges is a device array.  Ranges must not overlap their
+ * destinations.  Replaces the range-by-range copies of ordered
+ * redistribution (source/code/src/pmRedistributor.cpp:240-283). */
+typedef struct pmb_copy_range {
+    uint64_t src, dst, len;
+} pmb_copy_range;
+int pmb_copy_ranges(void* d_dst, const void* d_src, const pmb_copy_range* d_ranges, int n_ranges, void* stream);
 /* cudaLaunchKernel of a __global__ function pointer (an app's
  * subtask_gpu_cuda kernel) with the argument array `args`. */
 int pmb_launch_kernel(const void* fn, unsigned gx, unsigned gy, unsigned gz, unsigned bx, unsigned by, unsigned bz,
@@ -209,6 +217,27 @@ size_t pmb_reduce_element_size(int type);
 int pmb_reduce_elementwise(int op, int type, void* d_dst, const void* const* d_srcs, int nsrc, size_t count,
                            int init_from_first, void* stream);
 
+/* Sentinel compression of a reduction output (zero is the sentinel) for its
+ * copy to the host, in the reference's compressed form: a uint32 count, the
+ * count non-zero elements, then their count uint32 indices, index order;
+ * compressed only when count < 0.4 x elements
+ * (source/code/src/pmCudaInterface.cu:380-472 CompressForSentinel,
+ * pmExecutionStub.cpp:3850-3950, pmInternalDefinitions.h:223-224).  `type` is
+ * a pmReductionDataType (INTS .. DOUBLES = 0..5); elements are stored as
+ * 32-bit words.  pmb_sentinel_compress writes the count word always and the
+ * rest only when the data compresses (three launches on `stream`, no
+ * synchronisation); read the count, then pmb_sentinel_compressed tells
+ * whether to copy 4 + count x (element size + 4) bytes or the data as it is.
+ * d_dst needs pmb_sentinel_capacity_bytes, d_scratch (16-byte aligned)
+ * pmb_sentinel_scratch_bytes.  pmb_sentinel_expand restores a host array
+ * (UncompressSentinelCompressedData, pmExecutionStub.cpp:3878-3950). */
+size_t pmb_sentinel_capacity_bytes(int type, size_t length);
+size_t pmb_sentinel_scratch_bytes(int type, size_t length);
+int pmb_sentinel_compress(int type, const void* d_src, size_t length, void* d_dst, size_t capacity, void* d_scratch,
+                          size_t scratch_bytes, void* stream);
+int pmb_sentinel_compressed(int type, size_t length, uint32_t count);
+int pmb_sentinel_expand(int type, const void* h_src, void* h_dst, size_t length);
+
 /* ------------------------------------------------------------------------ */
 /* prefixSum: inclusive scan                                                */
 /* ------------------------------------------------------------------------ */
@@ -260,6 +289,11 @@ int pmb_scan_noalloc_error(uint32_t* error_out);
  * in the reference (its kernels never wait on one another). */
 int pmb_scratch_error(const void* d_scratch, uint32_t* error_out);
 
+/* d_data[i] += *d_scalar for i < n (uint64; d_data 16-byte aligned, the
+ * scalar read on the device).  Replaces elemAdd_cuda, the prefix sum's second
+ * task (testSuite/prefixSum/source/code/src/prefixSumCUDA.cu:143-158). */
+int pmb_add_u64_scalar(uint64_t* d_data, size_t n, const uint64_t* d_scalar, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* radixSort: stable LSD sort of uint32 keys                                */
 /* ------------------------------------------------------------------------ */
@@ -282,6 +316,11 @@ int pmb_radix_sort_u32(uint32_t* d_keys, uint32_t* d_alt, size_t n, int begin_bi
 int pmb_radix_sort_pairs_u32(uint32_t* d_keys, uint32_t* d_alt, uint32_t* d_vals, uint32_t* d_vals_alt,
                              size_t n, int begin_bit, int end_bit, int bits_per_pass, void* d_scratch,
                              size_t scratch_bytes, void* stream);
+
+/* The digit counts (uint32, 2^bits_per_pass of them) of the first pass of the
+ * last sort run with d_scratch, copied on `stream` into d_counts: the
+ * per-subtask bins of a radixSort round (radixSort.cpp:127-148). */
+int pmb_radix_sort_histogram(const void* d_scratch, int bits_per_pass, void* d_counts, void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* pageRank: pull over CSR in-edges                                         */

@@ -374,9 +374,12 @@ T fold_ref(int op, T a, T b) {
     }
 }
 
+bool g_sparse = false;  // inputs mostly zero (sentinel-compressed copies)
+
 template <typename T>
 T row_value(int s, int j, int op) {
     const unsigned h = unsigned(j) * 2654435761u + unsigned(s) * 40503u + 17u;
+    if (g_sparse && (h >> 7) % 10 != 0) return T(0);
     if (op == REDUCE_LOGICAL_AND || op == REDUCE_LOGICAL_OR || op == REDUCE_LOGICAL_XOR) return T(h % 3);
     if (op == REDUCE_PRODUCT) return T(1 + h % 3);
     if constexpr (std::is_floating_point<T>::value)
@@ -494,6 +497,28 @@ void test_reduce(bool gpu) {
     reduce_case<float, uint32_t>(gpu, REDUCE_ADD, REDUCE_FLOATS, nullptr, 0, 0, OutSub::Whole, 1 << 20);
     // subtasks subscribing different ranges: the task fails before it runs
     reduce_case<int32_t, int32_t>(gpu, REDUCE_ADD, REDUCE_INTS, nullptr, 0, 0, OutSub::Mismatched);
+}
+
+// Sentinel-compressed copies: the app's own reduction callback on GPU
+// subtasks whose copies are ~90 % zero words; with the threshold lowered to
+// 0 every copy goes to the host compressed, and the folds still match.
+extern "C" void pmb_runtime_sentinel_stats(unsigned long long* copies, unsigned long long* bytes);
+
+void test_sentinel() {
+    g_sparse = true;
+    unsigned long long c0 = 0, b0 = 0, c1 = 0, b1 = 0;
+    pmb_runtime_sentinel_stats(&c0, &b0);
+    reduce_case<int32_t, int32_t>(true, REDUCE_ADD, REDUCE_INTS, axpy3_reduction, 1, 0, OutSub::Whole);
+    reduce_case<int32_t, int32_t>(true, REDUCE_BITWISE_OR, REDUCE_INTS, or_reduction, 2, 0, OutSub::Whole, 1 << 20);
+    pmb_runtime_sentinel_stats(&c1, &b1);
+    CHECK(c1 - c0 == 2 * kRowSubtasks, "compressed copies: %llu", c1 - c0);
+    CHECK(b1 - b0 < (size_t(kRowWords) + (size_t(1) << 20)) * 4 * kRowSubtasks / 4, "compressed bytes %llu", b1 - b0);
+    // dense copies stay uncompressed
+    g_sparse = false;
+    reduce_case<int32_t, int32_t>(true, REDUCE_ADD, REDUCE_INTS, axpy3_reduction, 1, 0, OutSub::Whole);
+    unsigned long long c2 = 0;
+    pmb_runtime_sentinel_stats(&c2, nullptr);
+    CHECK(c2 == c1, "a dense copy was compressed");
 }
 
 // ---------------------------------------------------------------------------
@@ -670,10 +695,11 @@ void test_redistribute(bool gpu) {
 int main(int argc, char** argv) {
     if (argc < 2) {
         std::printf("usage: rt_selftest <views_cpu|views_cpu_compact|views_gpu|views_gpu_compact|chain|"
-                    "write_through|mix|errors|timeout|reduce_cpu|reduce_gpu|redistribute_cpu|redistribute_gpu>\n");
+                    "write_through|mix|errors|timeout|reduce_cpu|reduce_gpu|sentinel_gpu|redistribute_cpu|redistribute_gpu>\n");
         return 2;
     }
     g_test = argv[1];
+    if (g_test == "sentinel_gpu") setenv("PMB_SENTINEL_THRESHOLD_BYTES", "0", 1);
     CHECK(pmInitialize() == pmSuccess, "init");
     int ndev = 0;
     pmb_device_count(&ndev);
@@ -691,6 +717,7 @@ int main(int argc, char** argv) {
     else if (g_test == "timeout") test_timeout();
     else if (g_test == "reduce_cpu") test_reduce(false);
     else if (g_test == "reduce_gpu") test_reduce(true);
+    else if (g_test == "sentinel_gpu") test_sentinel();
     else if (g_test == "redistribute_cpu") {
         test_redistribute(false);
         test_redistribute_halves(false);

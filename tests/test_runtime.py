@@ -58,7 +58,7 @@ def test_runtime_cpu(selftest, name):
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", ["views_gpu", "views_gpu_compact", "chain", "write_through", "mix", "reduce_gpu",
-                                  "redistribute_gpu"])
+                                  "sentinel_gpu", "redistribute_gpu"])
 def test_runtime_gpu(selftest, name):
     rc, out = run([selftest, name])
     assert rc == 0 and f"PASS {name}" in out, out

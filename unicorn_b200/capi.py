@@ -91,6 +91,7 @@ _SIGS = {
     "pmb_launch_kernel": (c_int, [c_void_p, ctypes.c_uint, ctypes.c_uint, ctypes.c_uint, ctypes.c_uint, ctypes.c_uint,
                                   ctypes.c_uint, ctypes.c_uint, ctypes.POINTER(c_void_p), c_void_p]),
     "pmb_device_synchronize": (c_int, []),
+    "pmb_copy_ranges": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p]),
     "pmb_mempool_retain": (c_int, [c_int]),
     "pmb_mempool_reserve": (c_int, [c_int, c_size_t, c_void_p]),
     "pmb_reduce_element_size": (c_size_t, [c_int]),
@@ -118,12 +119,19 @@ _SIGS = {
     "pmb_trsm_f32": (c_int, [c_int, c_int, c_int, c_int, c_int, c_void_p, c_int64, c_void_p, c_int64, c_void_p,
                              c_size_t, c_void_p]),
     "pmb_image_filter_plain": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_int, c_int, c_void_p]),
+    "pmb_sentinel_capacity_bytes": (c_size_t, [c_int, c_size_t]),
+    "pmb_sentinel_scratch_bytes": (c_size_t, [c_int, c_size_t]),
+    "pmb_sentinel_compress": (c_int, [c_int, c_void_p, c_size_t, c_void_p, c_size_t, c_void_p, c_size_t, c_void_p]),
+    "pmb_sentinel_compressed": (c_int, [c_int, c_size_t, ctypes.c_uint32]),
+    "pmb_sentinel_expand": (c_int, [c_int, c_void_p, c_void_p, c_size_t]),
     "pmb_scan_scratch_bytes": (c_size_t, [c_size_t]),
     "pmb_inclusive_scan_u32_u64": (c_int, [c_void_p, c_void_p, c_size_t, c_void_p, c_size_t, c_void_p]),
     "pmb_inclusive_scan_u32_u64_noalloc": (c_int, [c_void_p, c_void_p, c_size_t, c_void_p]),
     "pmb_scan_noalloc_error": (c_int, [ctypes.POINTER(ctypes.c_uint32)]),
     "pmb_scratch_error": (c_int, [c_void_p, ctypes.POINTER(ctypes.c_uint32)]),
     "pmb_radix_sort_scratch_bytes": (c_size_t, [c_size_t, c_int]),
+    "pmb_radix_sort_histogram": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
+    "pmb_add_u64_scalar": (c_int, [c_void_p, c_size_t, c_void_p, c_void_p]),
     "pmb_radix_sort_u32": (c_int, [c_void_p, c_void_p, c_size_t, c_int, c_int, c_int, c_void_p, c_size_t, c_void_p]),
     "pmb_radix_sort_pairs_u32": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_size_t, c_int, c_int, c_int,
                                          c_void_p, c_size_t, c_void_p]),

@@ -285,3 +285,49 @@ extern "C" int pmb_mem_available(int dev, size_t* available) {
     *available = fr + (reserved > used ? static_cast<size_t>(reserved - used) : 0);
     return PMB_SUCCESS;
 }
+
+// ---------------------------------------------------------------------------
+// Many byte ranges in one launch (the device side of ordered redistribution,
+// source/code/src/pmRedistributor.cpp:240-283, which copies range by range):
+// CTA k copies range k with 16-byte vector moves where source and
+// destination agree modulo 16, byte moves at the ends and otherwise.
+namespace {
+
+__global__ void __launch_bounds__(256)
+copy_ranges_kernel(char* __restrict__ dst, const char* __restrict__ src, const pmb_copy_range* __restrict__ ranges,
+                   int n) {
+    for (int k = blockIdx.x; k < n; k += gridDim.x) {
+        const pmb_copy_range r = ranges[k];
+        const char* s = src + r.src;
+        char* d = dst + r.dst;
+        size_t len = r.len;
+        if (((reinterpret_cast<uintptr_t>(s) ^ reinterpret_cast<uintptr_t>(d)) & 15) == 0) {
+            const size_t head = (16 - (reinterpret_cast<uintptr_t>(s) & 15)) & 15;
+            const size_t h = head < len ? head : len;
+            if (threadIdx.x < h) d[threadIdx.x] = s[threadIdx.x];
+            s += h;
+            d += h;
+            len -= h;
+            const size_t nv = len / 16;
+            const uint4* sv = reinterpret_cast<const uint4*>(s);
+            uint4* dv = reinterpret_cast<uint4*>(d);
+            for (size_t i = threadIdx.x; i < nv; i += blockDim.x) dv[i] = sv[i];
+            for (size_t i = nv * 16 + threadIdx.x; i < len; i += blockDim.x) d[i] = s[i];
+        } else {
+            for (size_t i = threadIdx.x; i < len; i += blockDim.x) d[i] = s[i];
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" int pmb_copy_ranges(void* d_dst, const void* d_src, const pmb_copy_range* d_ranges, int n_ranges,
+                               void* stream) {
+    if (n_ranges <= 0) return PMB_SUCCESS;
+    PMB_CHECK_ARG(d_dst && d_src && d_ranges, "null pointer");
+    const int grid = n_ranges < 65535 ? n_ranges : 65535;
+    copy_ranges_kernel<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(
+        static_cast<char*>(d_dst), static_cast<const char*>(d_src), d_ranges, n_ranges);
+    PMB_CUDA_TRY(cudaGetLastError());
+    return PMB_SUCCESS;
+}

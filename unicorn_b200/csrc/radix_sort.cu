@@ -349,3 +349,16 @@ extern "C" int pmb_radix_sort_pairs_u32(uint32_t* d_keys, uint32_t* d_alt, uint3
     return sort_checked(d_keys, d_alt, d_vals, d_vals_alt, n, begin_bit, end_bit, bits_per_pass, d_scratch,
                         scratch_bytes, static_cast<cudaStream_t>(stream));
 }
+
+// Digit counts of the first pass of the last sort run with `d_scratch`
+// (uint32 per digit, 2^bits of them), copied on the stream into d_counts:
+// the per-subtask bins the reference's radixSort round hands to its
+// redistribution callback (radixSort.cpp:127-148).
+extern "C" int pmb_radix_sort_histogram(const void* d_scratch, int bits_per_pass, void* d_counts, void* stream) {
+    PMB_CHECK_ARG(d_scratch && d_counts, "null pointer");
+    PMB_CHECK_ARG(bits_per_pass == 4 || bits_per_pass == 8, "digit width %d not 4 or 8", bits_per_pass);
+    PMB_CUDA_TRY(cudaMemcpyAsync(d_counts, static_cast<const char*>(d_scratch) + kHeaderBytes,
+                                 sizeof(uint32_t) << bits_per_pass, cudaMemcpyDeviceToDevice,
+                                 static_cast<cudaStream_t>(stream)));
+    return PMB_SUCCESS;
+}

@@ -21,6 +21,7 @@
 // coalesced 16-byte stores of the uint64 results.  HBM traffic: 4 bytes read
 // and 8 written per element, plus 8 bytes of status per 16384 elements.  The
 // 62-bit status values hold any sum of n <= 2^30 uint32 values (< 2^62).
+#include <algorithm>
 #include <mutex>
 
 #include "lookback.cuh"
@@ -370,5 +371,43 @@ extern "C" int pmb_scan_noalloc_error(uint32_t* error_out) {
     if (st != PMB_SUCCESS) return st;
     PMB_CUDA_TRY(cudaMemcpy(error_out, static_cast<const uint32_t*>(scratch) + 1, sizeof(uint32_t),
                             cudaMemcpyDeviceToHost));
+    return PMB_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// The prefix sum's second task: add the total of the preceding slices to
+// every element of a slice (elemAdd_cuda, testSuite/prefixSum/source/code/
+// src/prefixSumCUDA.cu:143-158, widened to uint64).  The total is read on the
+// device, so the task's data dependencies stay on the stream.
+namespace {
+
+__global__ void __launch_bounds__(256)
+add_scalar_kernel(uint64_t* __restrict__ d, size_t n, const uint64_t* __restrict__ scalar) {
+    const uint64_t v = *scalar;
+    const size_t n2 = n / 2;
+    ulonglong2* d2 = reinterpret_cast<ulonglong2*>(d);
+    for (size_t i = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; i < n2;
+         i += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        ulonglong2 x = d2[i];
+        x.x += v;
+        x.y += v;
+        d2[i] = x;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0 && (n & 1)) d[n - 1] += v;
+}
+
+}  // namespace
+
+extern "C" int pmb_add_u64_scalar(uint64_t* d_data, size_t n, const uint64_t* d_scalar, void* stream) {
+    if (n == 0) return PMB_SUCCESS;
+    PMB_CHECK_ARG(d_data && d_scalar, "null pointer");
+    PMB_CHECK_ARG((reinterpret_cast<uintptr_t>(d_data) & 15) == 0, "data must be 16-byte aligned");
+    int dev = 0, sms = 148;
+    PMB_CUDA_TRY(cudaGetDevice(&dev));
+    PMB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const size_t want = (n / 2 + 255) / 256;
+    const unsigned grid = static_cast<unsigned>(std::max<size_t>(1, std::min<size_t>(want, static_cast<size_t>(sms) * 8)));
+    add_scalar_kernel<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(d_data, n, d_scalar);
+    PMB_CUDA_TRY(cudaGetLastError());
     return PMB_SUCCESS;
 }

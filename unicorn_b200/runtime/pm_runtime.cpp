@@ -171,6 +171,8 @@ struct Stats {
     // admission: waiting for a slot, waiting for memory; mirrors evicted to make room
     std::atomic<unsigned long long> slot_ns{0}, mem_ns{0}, evictions{0}, evicted_bytes{0};
     std::atomic<unsigned long long> callback_ns{0};  // inside GPU callbacks (the apps' launches)
+    // subtask copies sent to the host sentinel-compressed, and the bytes they took
+    std::atomic<unsigned long long> sentinel_copies{0}, sentinel_bytes{0};
     // write-back (pmFetchMemory and friends): host buffer, waiting for the
     // producing task's event, the copies themselves
     std::atomic<unsigned long long> fetch_host_ns{0}, fetch_wait_ns{0}, fetch_copy_ns{0}, fetches{0};
@@ -855,6 +857,74 @@ static pmStatus commit_host_shadows(Task* t) {
 
 // GPU tasks: fold the device copies on `stream` (built-in operations) or
 // bring them to the host for the app's callback, then free them.
+// The device copies of an app's own reduction go to the host for its
+// callback.  As the reference does for reduction outputs
+// (pmExecutionStub.cpp:3850-3876, pmCudaInterface.cu:380-472), a copy of the
+// whole of a single reducible address space larger than the threshold (1 GB,
+// CUDA_SENTINEL_COMPRESSION_THRESHOLD; PMB_SENTINEL_THRESHOLD_BYTES
+// overrides) is compressed on the device first when fewer than 40 % of its
+// elements are non-zero, and expanded on the host.  The app's element type
+// is not known here, so the copy is compressed as 32-bit words, which
+// restores any data bit for bit.
+static pmStatus copy_shadows_to_host(Task* t, void* stream) {
+    Controller& c = ctl();
+    const char* tv = getenv("PMB_SENTINEL_THRESHOLD_BYTES");
+    const size_t threshold = tv ? static_cast<size_t>(atoll(tv)) : (size_t(1) << 30);
+    constexpr int kWords = 1;  // REDUCE_UNSIGNED_INTS: 32-bit words
+    struct Pending {
+        Subtask* s;
+        size_t index, len;
+        char* buf = nullptr;  // device: compressed form, then scratch
+        uint32_t count = 0;
+        std::vector<char> packed;
+    };
+    std::vector<Pending> pend;
+    for (const ReduceSpace& rs : t->reduce)
+        for (size_t id : rs.subtasks) {
+            Subtask& s = t->subtasks[id];
+            const size_t len = rs.hi - rs.lo;
+            s.host_shadow.resize(t->spaces.size());
+            s.host_shadow[rs.index].resize(len);
+            const bool whole = t->reduce.size() == 1 && rs.lo == 0 && rs.hi == t->spaces[rs.index]->length;
+            if (whole && len > threshold && len % 4 == 0 && len / 4 < (size_t(1) << 32) &&
+                (reinterpret_cast<uintptr_t>(s.dev_shadow[rs.index]) & 3) == 0) {
+                Pending p;
+                p.s = &s;
+                p.index = rs.index;
+                p.len = len;
+                const size_t cap = (pmb_sentinel_capacity_bytes(kWords, len) + 255) & ~size_t(255);
+                void* b = nullptr;
+                PMR_DEV(pmb_malloc_async(&b, cap + pmb_sentinel_scratch_bytes(kWords, len), stream));
+                p.buf = static_cast<char*>(b);
+                PMR_DEV(pmb_sentinel_compress(kWords, s.dev_shadow[rs.index], len, p.buf, cap, p.buf + cap,
+                                              pmb_sentinel_scratch_bytes(kWords, len), stream));
+                pend.push_back(std::move(p));
+            } else {
+                PMR_DEV(pmb_memcpy_async(s.host_shadow[rs.index].data(), s.dev_shadow[rs.index], len, PMB_D2H, stream));
+            }
+        }
+    for (Pending& p : pend) PMR_DEV(pmb_memcpy_async(&p.count, p.buf, sizeof(uint32_t), PMB_D2H, stream));
+    PMR_DEV(pmb_stream_synchronize(stream));
+    for (Pending& p : pend) {
+        char* host = p.s->host_shadow[p.index].data();
+        if (pmb_sentinel_compressed(kWords, p.len, p.count)) {
+            const size_t bytes = sizeof(uint32_t) + static_cast<size_t>(p.count) * 8;
+            p.packed.resize(bytes);
+            PMR_DEV(pmb_memcpy_async(p.packed.data(), p.buf, bytes, PMB_D2H, stream));
+            c.stats.sentinel_copies++;
+            c.stats.sentinel_bytes += bytes;
+        } else {
+            PMR_DEV(pmb_memcpy_async(host, p.s->dev_shadow[p.index], p.len, PMB_D2H, stream));
+        }
+        PMR_DEV(pmb_free_async(p.buf, stream));
+    }
+    PMR_DEV(pmb_stream_synchronize(stream));
+    for (Pending& p : pend)
+        if (!p.packed.empty())
+            PMR_DEV(pmb_sentinel_expand(kWords, p.packed.data(), p.s->host_shadow[p.index].data(), p.len));
+    return pmSuccess;
+}
+
 static pmStatus reduce_device_shadows(Task* t, void* stream) {
     if (t->reduce.empty()) return pmSuccess;
     if (t->reduce_op >= 0) {
@@ -892,15 +962,8 @@ static pmStatus reduce_device_shadows(Task* t, void* stream) {
         keep_last_reduction_scratch(t, first_reducing_subtask(t));
     } else {
         PMR_DEV(pmb_stream_synchronize(stream));
-        for (const ReduceSpace& rs : t->reduce)
-            for (size_t id : rs.subtasks) {
-                Subtask& s = t->subtasks[id];
-                s.host_shadow.resize(t->spaces.size());
-                s.host_shadow[rs.index].resize(rs.hi - rs.lo);
-                PMR_DEV(pmb_memcpy_async(s.host_shadow[rs.index].data(), s.dev_shadow[rs.index], rs.hi - rs.lo,
-                                         PMB_D2H, stream));
-            }
-        PMR_DEV(pmb_stream_synchronize(stream));
+        const pmStatus cs = copy_shadows_to_host(t, stream);
+        if (cs != pmSuccess) return cs;
         pmStatus st = reduce_host_shadows(t, ctl().gpu_info);
         if (st == pmSuccess) st = commit_host_shadows(t);
         if (st != pmSuccess) return st;
@@ -925,7 +988,7 @@ static pmStatus reduce_device_shadows(Task* t, void* stream) {
 // (pmRedistributor.cpp:88-121 sums each order's bytes, 123-145 assigns
 // running offsets, 240-283 copies the ranges into a new address space that
 // replaces the task's, pmTask.cpp:834-856).  A GPU task moves the bytes on
-// the device into a new mirror, one device copy per range.
+// the device into a new mirror, all ranges in one gather launch.
 
 struct RedistCopy {
     size_t src, dst, len;
@@ -1005,8 +1068,21 @@ static pmStatus redistribute_device(Task* t, void* stream) {
         void* nd = nullptr;
         PMR_DEV(pmb_malloc_async(&nd, a->length ? a->length : 1, stream));
         PMR_DEV(pmb_memset_async(nd, 0, a->length, stream));
-        for (const RedistCopy& k : copies)
-            PMR_DEV(pmb_memcpy_async(static_cast<char*>(nd) + k.dst, a->dev + k.src, k.len, PMB_D2D, stream));
+        if (copies.size() <= 4) {
+            for (const RedistCopy& k : copies)
+                PMR_DEV(pmb_memcpy_async(static_cast<char*>(nd) + k.dst, a->dev + k.src, k.len, PMB_D2D, stream));
+        } else {  // all ranges in one launch, the range table staged on the device
+            std::vector<pmb_copy_range> table(copies.size());
+            for (size_t k = 0; k < copies.size(); ++k) table[k] = {copies[k].src, copies[k].dst, copies[k].len};
+            void* dt = nullptr;
+            const size_t tb = table.size() * sizeof(pmb_copy_range);
+            PMR_DEV(pmb_malloc_async(&dt, tb, stream));
+            PMR_DEV(pmb_memcpy_async(dt, table.data(), tb, PMB_H2D, stream));
+            PMR_DEV(pmb_copy_ranges(nd, a->dev, static_cast<const pmb_copy_range*>(dt), static_cast<int>(table.size()),
+                                    stream));
+            PMR_DEV(pmb_stream_synchronize(stream));  // the table is a host vector (pageable copy)
+            PMR_DEV(pmb_free_async(dt, stream));
+        }
         PMR_DEV(pmb_free_async(a->dev, stream));
         a->dev = static_cast<char*>(nd);
         a->dev_valid.clear();
@@ -2267,6 +2343,11 @@ extern "C" void pmb_runtime_admission(double* slot_wait_s, double* memory_wait_s
     if (memory_wait_s) *memory_wait_s = c.stats.mem_ns * 1e-9;
     if (evictions) *evictions = c.stats.evictions;
     if (evicted_bytes) *evicted_bytes = c.stats.evicted_bytes;
+}
+
+extern "C" void pmb_runtime_sentinel_stats(unsigned long long* copies, unsigned long long* bytes) {
+    if (copies) *copies = pmr::ctl().stats.sentinel_copies;
+    if (bytes) *bytes = pmr::ctl().stats.sentinel_bytes;
 }
 
 extern "C" double pmb_runtime_callback_seconds(void) { return pmr::ctl().stats.callback_ns * 1e-9; }
