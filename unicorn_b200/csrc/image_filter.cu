@@ -416,8 +416,8 @@ imgf_fast_kernel(const __grid_constant__ ImgfParamsF<R, MAXI> p) {
 // 5th-generation tensor cores (tcgen05.mma kind::i8, u8 pixels x s8 weights,
 // exact s32 sums in tensor memory), so integer parity is unchanged.
 //
-// One CTA (128 threads) owns a 128-row x 64-pixel output tile.  Per channel
-// plane P and filter row ky the tile is D += A_ky * B_ky with
+// Output tiles are 128 rows x 64 pixels.  Per channel plane P and filter row
+// ky a tile is D += A_ky * B_ky with
 //   A_ky[i][k] = P[tile_r0 + i + ky - R][tile_c0 - 8 + 16t + k]   (M = 128 rows, K = 32 columns)
 //   B_ky[k][j] = f[ky][k - j + R - 8]  (zero outside [0, 2R])     (N = 16 output columns)
 // for each 16-column group t: the 32-column window of input bytes times a
@@ -427,26 +427,40 @@ imgf_fast_kernel(const __grid_constant__ ImgfParamsF<R, MAXI> p) {
 // 16 r), so "rows shifted by ky" is the same descriptor with its start
 // address moved by 16 ky bytes.  B is 512 bytes per ky, built once per CTA.
 // 3 channels x 4 groups x (2R + 1) MMAs of 128 x 16 x 32 fill 12 accumulators
-// (192 of 256 allocated TMEM columns).
+// (192 TMEM columns).
 //
-// Staging: the tile's 64 columns of each input row (plus an R-pixel halo) are
-// copied into a raw buffer -- one 192-byte bulk async copy per row when the
-// row piece is 16-byte aligned and the tile is full width, with the halo and
-// every other case (image borders: replicated pixels; ragged tiles) by plain
-// byte loads clamped to the subscription -- then de-interleaved by byte
-// permutes into the three planes.  Epilogue: each thread reads its output
-// row's 3 x 64 sums from TMEM, packs them to bytes (clamp: saturate; wrap:
-// low byte), re-interleaves RGB and stages the 192-byte row in shared memory;
-// the tile is then written with coalesced 16-byte stores.
-constexpr int kTcTW = 64, kTcTH = 128, kTcThreads = 128;
+// Persistent, warp-specialised: one CTA per SM walks its share of the
+// tiles of all items.  Warps 0-3 stage and multiply, warps 4-7 drain:
+//  - staging: lanes of warp 0 issue one bulk async copy per input row of the
+//    tile (its 96 columns tile_c0-16 .. tile_c0+79 clipped to the image, rows
+//    replicated at the subscription's edges by choosing the source row) into
+//    a ring of raw buffers, SLOTS - 1 tiles ahead; pixels beyond the image's
+//    left/right edge are filled from the edge pixel afterwards.  Views that a
+//    bulk copy cannot address (not a whole-row NATURAL view, or unaligned)
+//    are staged by plain clamped byte loads.  The rows are then
+//    de-interleaved by byte permutes into one of two plane buffers and one
+//    thread issues the tile's MMAs into one of two accumulator sets;
+//  - epilogue: each thread reads its output row's 3 x 64 sums from TMEM,
+//    packs them to bytes (clamp: saturate; wrap: low byte), re-interleaves
+//    RGB and stages the row in shared memory, frees the accumulator set, and
+//    the four warps write the tile with coalesced 16-byte stores.
+// mbarriers order the two roles: raw buffer filled, MMAs done (planes and
+// accumulators readable / planes reusable), accumulators drained.  Every
+// wait is bounded; a wait that expires sets the error word and the CTA
+// stops, waiting (bounded) for its own copies and MMAs before it frees its
+// tensor memory.  Reads outside the subscription but inside the image's rows
+// (NATURAL views hold whole rows) only meet zero filter weights.
+constexpr int kTcTW = 64, kTcTH = 128;
+constexpr int kTcThreads = 256;     // warps 0-3: staging and MMAs; warps 4-7: epilogue
 constexpr int kTcMaxR = 8;
 constexpr int kTcMaxKD = 2 * kTcMaxR + 1;
 constexpr int kTcChunks = 5;        // plane columns tile_c0-8 .. tile_c0+71 in 16-byte chunks
 constexpr int kRawStride = 304;     // raw row: pixels tile_c0-16 .. tile_c0+79 (288 B) + padding
 constexpr int kOutStride = 208;     // staged output row: 192 B + padding (conflict-free 16-B stores)
-constexpr uint32_t kTcTmemCols = 256;
+constexpr uint32_t kTcTmemCols = 512;  // two accumulator sets of 192 columns, 256 apart
 constexpr uint32_t kTcWaitPolls = 1u << 21;
 constexpr uint32_t kImgfErrTimeout = 1;
+constexpr int kSmemLimit = 227 * 1024;
 
 template <int R>
 struct TcGeo {
@@ -454,14 +468,20 @@ struct TcGeo {
     static constexpr int ROWS = kTcTH + 2 * R;        // plane rows
     static constexpr int CH = ROWS * 16;              // bytes per 16-column chunk of a plane
     static constexpr int PLANE = kTcChunks * CH;
+    static constexpr int PLANES = 3 * PLANE;          // one buffer of the three planes
     static constexpr int RAW = ROWS * kRawStride;
     static constexpr int OUT = kTcTH * kOutStride;
-    static constexpr int OFF_RAW = 3 * PLANE;         // raw rows, later the staged output tile
-    static constexpr int OFF_B = OFF_RAW + (RAW > OUT ? RAW : OUT);
+    static constexpr int FIXED = 2 * PLANES + OUT + KD * 512 + 128;
+    static constexpr int SLOTS = FIXED + 3 * RAW <= kSmemLimit ? 3 : 2;
+    static constexpr int OFF_RAW = 2 * PLANES;
+    static constexpr int OFF_OUT = OFF_RAW + SLOTS * RAW;
+    static constexpr int OFF_B = OFF_OUT + OUT;
     static constexpr int OFF_BAR = OFF_B + KD * 512;
-    static constexpr int SMEM = OFF_BAR + 64;
-    static_assert(CH % 16 == 0 && OFF_RAW % 16 == 0 && OFF_B % 16 == 0 && OFF_BAR % 8 == 0, "alignment");
+    static constexpr int SMEM = OFF_BAR + 128;
+    static_assert(CH % 16 == 0 && OFF_RAW % 16 == 0 && OFF_OUT % 16 == 0 && OFF_B % 16 == 0 && OFF_BAR % 8 == 0,
+                  "alignment");
     static_assert(CH / 16 < (1 << 14), "leading byte offset field");
+    static_assert(SMEM <= kSmemLimit, "shared memory");
 };
 
 // Instruction descriptor, kind::i8: S32 accumulator, A u8, B s8, both
@@ -472,6 +492,7 @@ template <int MAXI>
 struct ImgfParamsTc {
     int8_t f[kTcMaxKD][kTcMaxKD];
     int n_items;
+    int total_tiles;
     int tile_start[MAXI + 1];
     int tiles_x[MAXI];
     uint32_t* err;
@@ -507,6 +528,10 @@ __device__ __forceinline__ bool tc_wait(uint32_t bar, uint32_t parity) {
     return false;
 }
 
+__device__ __forceinline__ void tc_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
 __device__ __forceinline__ void tc_mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -528,112 +553,89 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t (&r)[16]) {
         : "r"(taddr));
 }
 
+// Barriers among the 128 threads of one role (id 1: epilogue, id 2: staging);
+// role_all / role_any also combine a flag, so every thread of the role takes
+// the same branch after them.
+__device__ __forceinline__ void role_sync(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
+__device__ __forceinline__ bool role_all(int id, bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.and.pred q, %2, 128, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"(static_cast<uint32_t>(v)), "r"(id)
+        : "memory");
+    return r != 0;
+}
+__device__ __forceinline__ bool role_any(int id, bool v) { return !role_all(id, !v); }
+
+struct TcTile {
+    int item, r0, c0, tw, rows;
+    bool bulk;  // rows staged by bulk copies
+};
+
+template <int MAXI>
+__device__ __forceinline__ TcTile tc_tile(const ImgfParamsTc<MAXI>& p, int g) {
+    int lo = 0, hi = p.n_items - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (p.tile_start[mid] <= g) lo = mid; else hi = mid - 1;
+    }
+    const pmb_imgf_item& it = p.items[lo];
+    const int local = g - p.tile_start[lo];
+    const int txs = p.tiles_x[lo];
+    const int ty = local / txs, tx = local - ty * txs;
+    TcTile t;
+    t.item = lo;
+    t.c0 = it.c0 + tx * kTcTW;
+    t.r0 = it.r0 + ty * kTcTH;
+    t.tw = min(kTcTW, it.c1 - t.c0);
+    t.rows = min(kTcTH, it.r1 - t.r0);
+    // A NATURAL view holds whole image rows; 16-byte aligned pixel 16k of
+    // every row and a width of whole 16-pixel groups make each row piece one
+    // bulk copy.
+    t.bulk = it.in_pitch == 3LL * it.width && (it.width & 15) == 0 && (t.c0 & 15) == 0 && (it.in_pitch & 15) == 0 &&
+             ((reinterpret_cast<uintptr_t>(it.in) - 3 * static_cast<int64_t>(it.in_col0)) & 15) == 0;
+    return t;
+}
+
 template <int R, int MODE, int MAXI>
-__global__ void __launch_bounds__(kTcThreads)
+__global__ void __launch_bounds__(kTcThreads, 1)
 imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
     using G = TcGeo<R>;
+    constexpr int SLOTS = G::SLOTS;
     extern __shared__ __align__(128) uint8_t smem[];
     uint8_t* const planes = smem;
-    uint8_t* const raw = smem + G::OFF_RAW;
+    uint8_t* const raws = smem + G::OFF_RAW;
+    uint8_t* const ost = smem + G::OFF_OUT;
     uint8_t* const bsm = smem + G::OFF_B;
-    uint64_t* const bars = reinterpret_cast<uint64_t*>(smem + G::OFF_BAR);  // [0] rows staged, [1] MMAs done
-    uint32_t* const tmem_slot = reinterpret_cast<uint32_t*>(bars + 2);
-    __shared__ int s_fail;
+    uint64_t* const bars = reinterpret_cast<uint64_t*>(smem + G::OFF_BAR);
+    uint64_t* const full = bars;              // [SLOTS]: raw buffer filled
+    uint64_t* const mma_done = bars + 3;      // [2]: accumulator set b written, planes b read
+    uint64_t* const acc_free = bars + 5;      // [2]: accumulator set b drained (4 epilogue warps)
+    uint64_t* const teardown = bars + 7;
+    uint32_t* const tmem_slot = reinterpret_cast<uint32_t*>(bars + 8);
+    __shared__ volatile int s_fail;
 
-    const int item = blockIdx.y;
-    const int local = blockIdx.x;
-    if (local >= p.tile_start[item + 1] - p.tile_start[item]) return;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const pmb_imgf_item& it = p.items[item];
-    const uint8_t* const in = it.in;
-    uint8_t* const out = it.out;
-    const int64_t ip = it.in_pitch, op = it.out_pitch;
-    const int H = it.height;
-    const int txs = p.tiles_x[item];
-    const int ty = local / txs, tx = local - ty * txs;
-    const int tile_c0 = it.c0 + tx * kTcTW, tile_r0 = it.r0 + ty * kTcTH;
-    const int mlo = max(0, it.r0 - R), mhi = min(H - 1, it.r1 - 1 + R);
-    const int clo = max(0, it.c0 - R), chi = min(it.width - 1, it.c1 - 1 + R);
-    const int tw = min(kTcTW, it.c1 - tile_c0);
-    // Row piece of the tile's 64 columns, as bulk copies: full width, 16-byte
-    // aligned source rows (the same for every row when the pitch is).
-    const bool bulk = tw == kTcTW && (ip & 15) == 0 &&
-                      ((reinterpret_cast<uintptr_t>(in) + 3 * static_cast<int64_t>(tile_c0 - it.in_col0)) & 15) == 0;
-    auto row_ptr = [&](int r) {  // input row of plane row r (replicated at the subscription's edges)
-        const int m = pmb::clampi(tile_r0 - R + r, mlo, mhi);
-        return in + static_cast<int64_t>(H - 1 - m - it.in_row0) * ip;
-    };
+    const int ntiles = (p.total_tiles - static_cast<int>(blockIdx.x) + static_cast<int>(gridDim.x) - 1) /
+                       static_cast<int>(gridDim.x);
+    auto tile_id = [&](int k) { return static_cast<int>(blockIdx.x) + k * static_cast<int>(gridDim.x); };
 
     if (tid == 0) {
         s_fail = 0;
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(&bars[0])));
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(&bars[1])));
+        for (int i = 0; i < SLOTS; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(&full[i])));
+        for (int i = 0; i < 2; ++i) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(&mma_done[i])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(tc_smem(&acc_free[i])));
+        }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(teardown)));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    __syncthreads();
-
-    // ---- stage input rows into the raw buffer (pixel x at byte 3x of a row:
-    //      image column tile_c0 - 16 + x) ----
-    if (bulk) {
-        if (warp == 0) {
-            if (lane == 0)
-                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(tc_smem(&bars[0])),
-                             "r"(static_cast<uint32_t>(G::ROWS * 3 * kTcTW))
-                             : "memory");
-            __syncwarp();
-            for (int r = lane; r < G::ROWS; r += 32) {
-                const uint8_t* src = row_ptr(r) + 3 * (tile_c0 - it.in_col0);
-                asm volatile(
-                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                        tc_smem(raw + r * kRawStride + 48)),
-                    "l"(src), "r"(3 * kTcTW), "r"(tc_smem(&bars[0]))
-                    : "memory");
-            }
-        }
-        // Halo: R pixels left and right of every row, one (row, side) piece per
-        // thread and round, all loads of a thread issued before its stores.
-        constexpr int kPer = (2 * G::ROWS + kTcThreads - 1) / kTcThreads;
-        uint8_t hv[kPer][3 * R];
-#pragma unroll
-        for (int q = 0; q < kPer; ++q) {
-            const int e = tid + q * kTcThreads;
-            if (e < 2 * G::ROWS) {
-                const uint8_t* rp = row_ptr(e >> 1);
-                const int x0 = (e & 1) ? 80 : 16 - R;
-#pragma unroll
-                for (int b = 0; b < R; ++b) {
-                    const int n = pmb::clampi(tile_c0 - 16 + x0 + b, clo, chi);
-                    const uint8_t* src = rp + 3 * (n - it.in_col0);
-                    hv[q][3 * b] = __ldg(src);
-                    hv[q][3 * b + 1] = __ldg(src + 1);
-                    hv[q][3 * b + 2] = __ldg(src + 2);
-                }
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < kPer; ++q) {
-            const int e = tid + q * kTcThreads;
-            if (e < 2 * G::ROWS) {
-                uint8_t* d = raw + (e >> 1) * kRawStride + 3 * ((e & 1) ? 80 : 16 - R);
-#pragma unroll
-                for (int b = 0; b < 3 * R; ++b) d[b] = hv[q][b];
-            }
-        }
-    } else {
-        const int span = kTcTW + 2 * R;
-        for (int e = tid; e < G::ROWS * span; e += kTcThreads) {
-            const int r = e / span, x = 16 - R + (e - r * span);
-            const int n = pmb::clampi(tile_c0 - 16 + x, clo, chi);
-            const uint8_t* s = row_ptr(r) + 3 * (n - it.in_col0);
-            uint8_t* d = raw + r * kRawStride + 3 * x;
-            d[0] = __ldg(s);
-            d[1] = __ldg(s + 1);
-            d[2] = __ldg(s + 2);
-        }
-    }
-
-    // ---- B: per filter row, the 16 x 32 banded slice, K-major core matrices
-    //      (8 output columns x 16 bytes; column groups 128 B, K chunks 256 B apart) ----
+    // B: per filter row, the 16 x 32 banded slice, K-major core matrices
+    // (8 output columns x 16 bytes; column groups 128 B, K chunks 256 B apart).
     for (int w = tid; w < G::KD * 128; w += kTcThreads) {
         const int ky = w >> 7, off = (w & 127) * 4;
         uint32_t word = 0;
@@ -648,34 +650,8 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
         }
         *reinterpret_cast<uint32_t*>(bsm + ky * 512 + off) = word;
     }
-    if (bulk && !tc_wait(tc_smem(&bars[0]), 0)) s_fail = 1;
-    __syncthreads();
-
-    // ---- de-interleave: plane c, chunk q, row r <- raw pixels 16q+8 .. 16q+23 ----
-    if (!s_fail) {
-        for (int e = tid; e < G::ROWS * kTcChunks; e += kTcThreads) {
-            const int q = e / G::ROWS, r = e - q * G::ROWS;
-            const uint8_t* s = raw + r * kRawStride + 48 * q + 24;
-            uint32_t w[12];
-#pragma unroll
-            for (int k = 0; k < 6; ++k) {
-                const uint2 v = *reinterpret_cast<const uint2*>(s + 8 * k);
-                w[2 * k] = v.x;
-                w[2 * k + 1] = v.y;
-            }
-            uint32_t o[3][4];
-#pragma unroll
-            for (int g = 0; g < 4; ++g) deinterleave4(w[3 * g], w[3 * g + 1], w[3 * g + 2], o[0][g], o[1][g], o[2][g]);
-#pragma unroll
-            for (int c = 0; c < 3; ++c)
-                *reinterpret_cast<uint4*>(planes + c * G::PLANE + q * G::CH + r * 16) =
-                    make_uint4(o[c][0], o[c][1], o[c][2], o[c][3]);
-        }
-    }
-    // Generic-proxy writes of the planes and B, then the tensor core reads them.
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     if (warp == 0) {
-        __syncwarp();
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc_smem(tmem_slot)),
                      "r"(kTcTmemCols)
                      : "memory");
@@ -685,95 +661,221 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
-    const bool failed = s_fail != 0;
+    int issued = 0;  // tiles whose staging warp 0 has started (warp 0 only)
 
-    // ---- MMAs: one thread issues 3 x 4 x (2R+1) products ----
-    if (tid == 0 && !failed) {
-        const uint32_t pl = tc_smem(planes), bb = tc_smem(bsm);
-#pragma unroll 1
-        for (int c = 0; c < 3; ++c)
-#pragma unroll 1
-            for (int t = 0; t < 4; ++t)
-#pragma unroll
-                for (int ky = 0; ky < G::KD; ++ky)
-                    tc_mma_i8(tmem + static_cast<uint32_t>((c * 4 + t) * 16),
-                              tc_desc(pl + c * G::PLANE + t * G::CH + ky * 16, G::CH, 128),
-                              tc_desc(bb + ky * 512, 256, 128), ky > 0 ? 1u : 0u);
-        tc_commit(tc_smem(&bars[1]));
-    }
-    // Block-uniform: the TMEM loads below are warp-collective.
-    const bool have = __syncthreads_and(!failed && tc_wait(tc_smem(&bars[1]), 0)) != 0;
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-
-    // ---- epilogue: row 32*warp + lane, 3 x 64 sums -> 192 RGB bytes ----
-    uint8_t* const ost = raw;  // the raw rows are no longer needed
-    if (have) {
-        uint32_t pw[3][16];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            uint32_t v[4][16];  // a channel's four accumulators in flight at once
-#pragma unroll
-            for (int t = 0; t < 4; ++t)
-                tc_ld16(tmem + (static_cast<uint32_t>(32 * warp) << 16) + static_cast<uint32_t>((c * 4 + t) * 16), v[t]);
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-            for (int t = 0; t < 4; ++t)
-#pragma unroll
-                for (int g = 0; g < 4; ++g) {
-                    const int a[4] = {static_cast<int>(v[t][4 * g]), static_cast<int>(v[t][4 * g + 1]),
-                                      static_cast<int>(v[t][4 * g + 2]), static_cast<int>(v[t][4 * g + 3])};
-                    pw[c][4 * t + g] = pack4<MODE>(a);
-                }
-        }
-        uint8_t* const orow = ost + (32 * warp + lane) * kOutStride;
-#pragma unroll
-        for (int g = 0; g < 16; g += 4) {
-            uint32_t d[12];
-#pragma unroll
-            for (int h = 0; h < 4; ++h) {
-                const uint32_t A = pw[0][g + h], B = pw[1][g + h], C = pw[2][g + h];
-                d[3 * h + 0] = __byte_perm(__byte_perm(A, B, 0x0140), C, 0x2410);  // a0 b0 c0 a1
-                d[3 * h + 1] = __byte_perm(__byte_perm(B, C, 0x0251), A, 0x2610);  // b1 c1 a2 b2
-                d[3 * h + 2] = __byte_perm(C, __byte_perm(A, B, 0x0073), 0x3542);  // c2 a3 b3 c3
+    if (warp < 4) {
+        // ================= staging and MMAs =================
+        // Warp 0 starts the staging of tile k: bulk copies of its rows into
+        // raw slot k % SLOTS (plain arrival for tiles staged by loads).
+        auto issue = [&](int k) {
+            const TcTile t = tc_tile(p, tile_id(k));
+            const int s = k % SLOTS;
+            const uint32_t bar = tc_smem(&full[s]);
+            if (!t.bulk) {
+                if (lane == 0) tc_arrive(bar);
+                return;
             }
+            const pmb_imgf_item& it = p.items[t.item];
+            const int x0 = max(0, 16 - t.c0), x1 = min(96, it.width - t.c0 + 16);
+            const uint32_t bytes = static_cast<uint32_t>(3 * (x1 - x0));
+            const int mlo = max(0, it.r0 - R), mhi = min(it.height - 1, it.r1 - 1 + R);
+            if (lane == 0)
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                             "r"(bytes * static_cast<uint32_t>(G::ROWS))
+                             : "memory");
+            __syncwarp();
+            uint8_t* raw = raws + s * G::RAW;
+            for (int r = lane; r < G::ROWS; r += 32) {
+                const int m = pmb::clampi(t.r0 - R + r, mlo, mhi);
+                const uint8_t* src = it.in + static_cast<int64_t>(it.height - 1 - m - it.in_row0) * it.in_pitch +
+                                     3 * static_cast<int64_t>(t.c0 - 16 + x0 - it.in_col0);
+                asm volatile(
+                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                        tc_smem(raw + r * kRawStride + 3 * x0)),
+                    "l"(src), "r"(bytes), "r"(bar)
+                    : "memory");
+            }
+        };
+        if (warp == 0)
+            for (; issued < SLOTS - 1 && issued < ntiles; ++issued) issue(issued);
+        for (int k = 0; k < ntiles; ++k) {
+            if (role_any(2, s_fail != 0)) break;
+            if (warp == 0 && issued < ntiles) issue(issued++);  // SLOTS - 1 tiles ahead
+            const TcTile t = tc_tile(p, tile_id(k));
+            const pmb_imgf_item& it = p.items[t.item];
+            const int s = k % SLOTS, b = k & 1;
+            uint8_t* raw = raws + s * G::RAW;
+            bool ok = tc_wait(tc_smem(&full[s]), (k / SLOTS) & 1);
+            const int mlo = max(0, it.r0 - R), mhi = min(it.height - 1, it.r1 - 1 + R);
+            const int clo = max(0, it.c0 - R), chi = min(it.width - 1, it.c1 - 1 + R);
+            if (!t.bulk) {
+                // Plain loads of the needed pixels, clamped to the subscription.
+                const int span = kTcTW + 2 * R;
+                for (int e = tid; e < G::ROWS * span; e += 128) {
+                    const int r = e / span, x = 16 - R + (e - r * span);
+                    const int m = pmb::clampi(t.r0 - R + r, mlo, mhi);
+                    const int n = pmb::clampi(t.c0 - 16 + x, clo, chi);
+                    const uint8_t* src = it.in + static_cast<int64_t>(it.height - 1 - m - it.in_row0) * it.in_pitch +
+                                         3 * (n - it.in_col0);
+                    uint8_t* d = raw + r * kRawStride + 3 * x;
+                    d[0] = __ldg(src);
+                    d[1] = __ldg(src + 1);
+                    d[2] = __ldg(src + 2);
+                }
+            } else if (t.c0 < 16 || t.c0 + 80 > it.width) {
+                // Pixels beyond the image's left or right edge repeat the edge pixel.
+                const int x0 = max(0, 16 - t.c0), x1 = min(96, it.width - t.c0 + 16);
+                for (int e = tid; e < G::ROWS * 2 * R; e += 128) {
+                    const int r = e / (2 * R), k2 = e - r * (2 * R);
+                    const int x = k2 < R ? 16 - R + k2 : 80 + (k2 - R);
+                    if (x >= x0 && x < x1) continue;
+                    const int xs = x < x0 ? x0 : x1 - 1;
+                    uint8_t* row = raw + r * kRawStride;
+                    row[3 * x] = row[3 * xs];
+                    row[3 * x + 1] = row[3 * xs + 1];
+                    row[3 * x + 2] = row[3 * xs + 2];
+                }
+            }
+            // Planes b are free once the MMAs of tile k - 2 have read them.
+            if (k >= 2) ok = tc_wait(tc_smem(&mma_done[b]), ((k - 2) >> 1) & 1) && ok;
+            if (!role_all(2, ok)) {  // also: raw rows complete (loads and edge fills)
+                s_fail = 1;
+                break;
+            }
+            uint8_t* pl = planes + b * G::PLANES;
+            for (int e = tid; e < G::ROWS * kTcChunks; e += 128) {
+                const int q = e / G::ROWS, r = e - q * G::ROWS;
+                const uint8_t* src = raw + r * kRawStride + 48 * q + 24;
+                uint32_t w[12];
 #pragma unroll
-            for (int h = 0; h < 3; ++h)
-                *reinterpret_cast<uint4*>(orow + 12 * g + 16 * h) =
-                    make_uint4(d[4 * h], d[4 * h + 1], d[4 * h + 2], d[4 * h + 3]);
+                for (int j = 0; j < 6; ++j) {
+                    const uint2 v = *reinterpret_cast<const uint2*>(src + 8 * j);
+                    w[2 * j] = v.x;
+                    w[2 * j + 1] = v.y;
+                }
+                uint32_t o[3][4];
+#pragma unroll
+                for (int g = 0; g < 4; ++g) deinterleave4(w[3 * g], w[3 * g + 1], w[3 * g + 2], o[0][g], o[1][g], o[2][g]);
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    *reinterpret_cast<uint4*>(pl + c * G::PLANE + q * G::CH + r * 16) =
+                        make_uint4(o[c][0], o[c][1], o[c][2], o[c][3]);
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // planes, then the tensor core reads them
+            role_sync(2);
+            if (tid == 0) {
+                // Accumulator set b is free once the epilogue has drained tile k - 2.
+                // On a timeout no MMAs are issued: the epilogue's wait then runs
+                // out too, and both roles stop at their next iteration.
+                if (k >= 2 && !tc_wait(tc_smem(&acc_free[b]), ((k - 2) >> 1) & 1)) {
+                    s_fail = 1;
+                    continue;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t pa = tc_smem(pl), bb = tc_smem(bsm), acc = tmem + 256u * b;
+#pragma unroll 1
+                for (int c = 0; c < 3; ++c)
+#pragma unroll 1
+                    for (int tg = 0; tg < 4; ++tg)
+#pragma unroll
+                        for (int ky = 0; ky < G::KD; ++ky)
+                            tc_mma_i8(acc + static_cast<uint32_t>((c * 4 + tg) * 16),
+                                      tc_desc(pa + c * G::PLANE + tg * G::CH + ky * 16, G::CH, 128),
+                                      tc_desc(bb + ky * 512, 256, 128), ky > 0 ? 1u : 0u);
+                tc_commit(tc_smem(&mma_done[b]));
+            }
+        }
+        // Bulk copies started for tiles that will not be consumed (after a
+        // failure) must land before the CTA's shared memory is released.
+        if (warp == 0 && s_fail) {
+            const int consumed_max = issued;
+            for (int k = max(0, consumed_max - (SLOTS - 1)); k < consumed_max; ++k)
+                tc_wait(tc_smem(&full[k % SLOTS]), (k / SLOTS) & 1);
+        }
+    } else {
+        // ================= epilogue =================
+        const int q = warp - 4, row = 32 * q + lane;
+        for (int k = 0; k < ntiles; ++k) {
+            if (role_any(1, s_fail != 0)) break;
+            const TcTile t = tc_tile(p, tile_id(k));
+            const pmb_imgf_item& it = p.items[t.item];
+            const int b = k & 1;
+            if (!role_all(1, tc_wait(tc_smem(&mma_done[b]), (k >> 1) & 1))) {
+                s_fail = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            uint32_t pw[3][16];
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                uint32_t v[4][16];
+#pragma unroll
+                for (int tg = 0; tg < 4; ++tg)
+                    tc_ld16(tmem + 256u * b + (static_cast<uint32_t>(32 * q) << 16) +
+                                static_cast<uint32_t>((c * 4 + tg) * 16),
+                            v[tg]);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                for (int tg = 0; tg < 4; ++tg)
+#pragma unroll
+                    for (int g = 0; g < 4; ++g) {
+                        const int a[4] = {static_cast<int>(v[tg][4 * g]), static_cast<int>(v[tg][4 * g + 1]),
+                                          static_cast<int>(v[tg][4 * g + 2]), static_cast<int>(v[tg][4 * g + 3])};
+                        pw[c][4 * tg + g] = pack4<MODE>(a);
+                    }
+            }
+            // The accumulator set is drained: the MMAs of tile k + 2 may start.
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) tc_arrive(tc_smem(&acc_free[b]));
+            uint8_t* const orow = ost + row * kOutStride;
+#pragma unroll
+            for (int g = 0; g < 16; g += 4) {
+                uint32_t d[12];
+#pragma unroll
+                for (int h = 0; h < 4; ++h) {
+                    const uint32_t A = pw[0][g + h], B = pw[1][g + h], C = pw[2][g + h];
+                    d[3 * h + 0] = __byte_perm(__byte_perm(A, B, 0x0140), C, 0x2410);  // a0 b0 c0 a1
+                    d[3 * h + 1] = __byte_perm(__byte_perm(B, C, 0x0251), A, 0x2610);  // b1 c1 a2 b2
+                    d[3 * h + 2] = __byte_perm(C, __byte_perm(A, B, 0x0073), 0x3542);  // c2 a3 b3 c3
+                }
+#pragma unroll
+                for (int h = 0; h < 3; ++h)
+                    *reinterpret_cast<uint4*>(orow + 12 * g + 16 * h) =
+                        make_uint4(d[4 * h], d[4 * h + 1], d[4 * h + 2], d[4 * h + 3]);
+            }
+            role_sync(1);  // the staged tile is complete
+            const int et = tid - 128;
+            uint8_t* const obase = it.out + static_cast<int64_t>(t.r0 - it.out_row0) * it.out_pitch +
+                                   3 * (t.c0 - it.out_col0);
+            if (t.tw == kTcTW && ((reinterpret_cast<uintptr_t>(obase) | static_cast<uintptr_t>(it.out_pitch)) & 15) == 0) {
+                for (int e = et; e < t.rows * 12; e += 128) {
+                    const int r = e / 12, c = e - r * 12;
+                    *reinterpret_cast<uint4*>(obase + r * it.out_pitch + 16 * c) =
+                        *reinterpret_cast<const uint4*>(ost + r * kOutStride + 16 * c);
+                }
+            } else {
+                const int nb = 3 * t.tw;
+                for (int e = et; e < t.rows * nb; e += 128) {
+                    const int r = e / nb, c = e - r * nb;
+                    obase[r * it.out_pitch + c] = ost[r * kOutStride + c];
+                }
+            }
+            role_sync(1);  // the staging buffer may be refilled
         }
     }
+
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        if (!failed && !have && lane == 0) {
-            // The MMAs did not report completion in time: wait (bounded) once
-            // more before freeing the tensor memory they write.
-            tc_wait(tc_smem(&bars[1]), 0);
+        if (s_fail && lane == 0) {
+            atomicOr(p.err, kImgfErrTimeout);
+            tc_commit(tc_smem(teardown));  // every MMA this CTA issued has retired once this arrives
+            tc_wait(tc_smem(teardown), 0);
         }
         __syncwarp();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcTmemCols) : "memory");
-    }
-    if (!have) {
-        if (tid == 0) atomicOr(p.err, kImgfErrTimeout);
-        return;
-    }
-
-    // ---- write the tile: coalesced 16-byte stores, byte stores at ragged edges ----
-    const int rows = min(kTcTH, it.r1 - tile_r0);
-    uint8_t* const obase = out + static_cast<int64_t>(tile_r0 - it.out_row0) * op + 3 * (tile_c0 - it.out_col0);
-    if (tw == kTcTW && ((reinterpret_cast<uintptr_t>(obase) | static_cast<uintptr_t>(op)) & 15) == 0) {
-        for (int e = tid; e < rows * 12; e += kTcThreads) {
-            const int r = e / 12, k = e - r * 12;
-            *reinterpret_cast<uint4*>(obase + r * op + 16 * k) =
-                *reinterpret_cast<const uint4*>(ost + r * kOutStride + 16 * k);
-        }
-    } else {
-        const int nb = 3 * tw;
-        for (int e = tid; e < rows * nb; e += kTcThreads) {
-            const int r = e / nb, b = e - r * nb;
-            obase[r * op + b] = ost[r * kOutStride + b];
-        }
     }
 }
 
@@ -947,7 +1049,7 @@ int launch_tc(const pmb_imgf_item* items, int n, const int8_t* filter, cudaStrea
         for (int kx = 0; kx < kTcMaxKD; ++kx)
             p.f[ky][kx] = ky < G::KD && kx < G::KD ? filter[ky * PMB_IMGF_MAX_FILTER_DIM + kx] : 0;
     int64_t total = 0;
-    int m = 0, max_tiles = 0;
+    int m = 0;
     for (int i = 0; i < n; ++i) {
         const pmb_imgf_item& it = items[i];
         if (it.r0 == it.r1 || it.c0 == it.c1) continue;
@@ -957,12 +1059,12 @@ int launch_tc(const pmb_imgf_item* items, int n, const int8_t* filter, cudaStrea
         p.tiles_x[m] = txs;
         p.tile_start[m] = static_cast<int>(total);
         total += static_cast<int64_t>(txs) * tys;
-        max_tiles = std::max(max_tiles, txs * tys);
         ++m;
     }
     if (m == 0) return PMB_SUCCESS;
     if (total > 0x7fffffffLL) return pmb::fail(PMB_BEYOND_LIMITS, "too many tiles: %lld", (long long)total);
     p.n_items = m;
+    p.total_tiles = static_cast<int>(total);
     p.tile_start[m] = static_cast<int>(total);
     int st = imgf_err_word(&p.err);
     if (st != PMB_SUCCESS) return st;
@@ -972,8 +1074,11 @@ int launch_tc(const pmb_imgf_item* items, int n, const int8_t* filter, cudaStrea
         attr = cudaFuncSetAttribute(imgf_tc_kernel<R, MODE, MAXI>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
     });
     PMB_CUDA_TRY(attr);
-    imgf_tc_kernel<R, MODE, MAXI>
-        <<<dim3(static_cast<unsigned>(max_tiles), static_cast<unsigned>(m)), kTcThreads, G::SMEM, s>>>(p);
+    int dev = 0, sms = 148;
+    PMB_CUDA_TRY(cudaGetDevice(&dev));
+    PMB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const unsigned grid = static_cast<unsigned>(std::min<int64_t>(total, sms));  // persistent: one CTA per SM
+    imgf_tc_kernel<R, MODE, MAXI><<<grid, kTcThreads, G::SMEM, s>>>(p);
     PMB_CUDA_TRY(cudaGetLastError());
     return PMB_SUCCESS;
 }
