@@ -943,6 +943,10 @@ int launch_update(int M, int N, int kp, float alpha, const __nv_bfloat16* ah, co
     static cudaError_t attr_err = cudaSuccess;
     std::call_once(attr_once, [] {
         attr_err = cudaFuncSetAttribute(gemm_update_2sm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kUpdSmemBytes);
+        if (attr_err == cudaSuccess &&
+            pmb::tmem_exclusive(reinterpret_cast<const void*>(gemm_update_2sm_kernel), kThreads, kUpdSmemBytes,
+                                "gemm_update_2sm_kernel") != PMB_SUCCESS)
+            attr_err = cudaErrorInvalidConfiguration;
     });
     PMB_CUDA_TRY(attr_err);
     cudaLaunchConfig_t cfg = {};
@@ -1080,6 +1084,12 @@ int pmb::sgemm_bf16x3_launch(int M, int N, int K, float alpha, const float* A, i
             if (attr2_err == cudaSuccess)
                 attr2_err = cudaFuncSetAttribute(gemm_bf16x3_2sm_kernel<128>,
                                                  cudaFuncAttributeMaxDynamicSharedMemorySize, Pair2<128>::kSmemBytes);
+            if (attr2_err == cudaSuccess &&
+                (pmb::tmem_exclusive(reinterpret_cast<const void*>(gemm_bf16x3_2sm_kernel<256>), kThreads,
+                                     Pair2<256>::kSmemBytes, "gemm_bf16x3_2sm_kernel<256>") != PMB_SUCCESS ||
+                 pmb::tmem_exclusive(reinterpret_cast<const void*>(gemm_bf16x3_2sm_kernel<128>), kThreads,
+                                     Pair2<128>::kSmemBytes, "gemm_bf16x3_2sm_kernel<128>") != PMB_SUCCESS))
+                attr2_err = cudaErrorInvalidConfiguration;
         });
         PMB_CUDA_TRY(attr2_err);
         const dim3 grid2(2 * ((M + 255) / 256) * ((N + tn - 1) / tn));
@@ -1100,6 +1110,10 @@ int pmb::sgemm_bf16x3_launch(int M, int N, int K, float alpha, const float* A, i
     static cudaError_t attr_err = cudaSuccess;
     std::call_once(attr_once, [] {
         attr_err = cudaFuncSetAttribute(gemm_bf16x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+        if (attr_err == cudaSuccess &&
+            pmb::tmem_exclusive(reinterpret_cast<const void*>(gemm_bf16x3_kernel), kThreads, kSmemBytes,
+                                "gemm_bf16x3_kernel") != PMB_SUCCESS)
+            attr_err = cudaErrorInvalidConfiguration;
     });
     PMB_CUDA_TRY(attr_err);
     const dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);

@@ -722,13 +722,15 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
                     d[1] = __ldg(src + 1);
                     d[2] = __ldg(src + 2);
                 }
-            } else if (t.c0 < 16 || t.c0 + 80 > it.width) {
-                // Pixels beyond the image's left or right edge repeat the edge pixel.
+            } else if (t.c0 < 16 || t.c0 + 80 + R > it.width + 16) {
+                // Needed pixels (x in [16 - R, 80 + R)) beyond the image's left or
+                // right edge -- the halo, or the part of a tile that overhangs the
+                // image -- repeat the edge pixel.
                 const int x0 = max(0, 16 - t.c0), x1 = min(96, it.width - t.c0 + 16);
-                for (int e = tid; e < G::ROWS * 2 * R; e += 128) {
-                    const int r = e / (2 * R), k2 = e - r * (2 * R);
-                    const int x = k2 < R ? 16 - R + k2 : 80 + (k2 - R);
-                    if (x >= x0 && x < x1) continue;
+                const int nl = max(0, x0 - (16 - R)), nr = max(0, 80 + R - x1), nx = nl + nr;
+                for (int e = tid; e < G::ROWS * nx; e += 128) {
+                    const int r = e / nx, k2 = e - r * nx;
+                    const int x = k2 < nl ? 16 - R + k2 : x1 + (k2 - nl);
                     const int xs = x < x0 ? x0 : x1 - 1;
                     uint8_t* row = raw + r * kRawStride;
                     row[3 * x] = row[3 * xs];
@@ -1072,6 +1074,10 @@ int launch_tc(const pmb_imgf_item* items, int n, const int8_t* filter, cudaStrea
     static cudaError_t attr = cudaSuccess;
     std::call_once(once, [] {
         attr = cudaFuncSetAttribute(imgf_tc_kernel<R, MODE, MAXI>, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
+        if (attr == cudaSuccess &&
+            pmb::tmem_exclusive(reinterpret_cast<const void*>(imgf_tc_kernel<R, MODE, MAXI>), kTcThreads, G::SMEM,
+                                "imgf_tc_kernel") != PMB_SUCCESS)
+            attr = cudaErrorInvalidConfiguration;
     });
     PMB_CUDA_TRY(attr);
     int dev = 0, sms = 148;

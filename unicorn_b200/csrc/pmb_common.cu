@@ -25,6 +25,18 @@ int cuda_fail(cudaError_t err, const char* what) {
 
 void clear_error() { t_last_error[0] = 0; }
 
+int tmem_exclusive(const void* kernel, int threads, size_t smem_bytes, const char* name) {
+    (void)kernel;
+    (void)threads;
+    int dev = 0, per_sm = 0;
+    PMB_CUDA_TRY(cudaGetDevice(&dev));
+    PMB_CUDA_TRY(cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev));
+    if (2 * smem_bytes <= static_cast<size_t>(per_sm))
+        return fail(PMB_BEYOND_LIMITS, "%s: %zu bytes of shared memory per CTA would let two CTAs holding tensor "
+                    "memory share an SM (%d bytes per SM)", name, smem_bytes, per_sm);
+    return PMB_SUCCESS;
+}
+
 }  // namespace pmb
 
 extern "C" const char* pmb_last_error(void) { return pmb::t_last_error; }

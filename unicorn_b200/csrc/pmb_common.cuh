@@ -21,6 +21,15 @@ int cuda_fail(cudaError_t err, const char* what);
 // Clear the calling thread's last error.
 void clear_error();
 
+// Tensor-memory exclusivity of a kernel that allocates TMEM: its CTAs take
+// more than half of an SM's shared memory, so no two TMEM-allocating CTAs of
+// this library (each of which satisfies the same) are ever resident on one
+// SM together.  Two TMEM-allocating CTAs on one SM could wait
+// on each other's columns -- for CTA pairs (cta_group::2) even across two
+// SMs -- so every TMEM-allocating launch checks this once and fails with
+// PMB_BEYOND_LIMITS otherwise.
+int tmem_exclusive(const void* kernel, int threads, size_t smem_bytes, const char* name);
+
 }  // namespace pmb
 
 #define PMB_CUDA_TRY(call)                                          \
