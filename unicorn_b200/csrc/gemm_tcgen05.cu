@@ -855,22 +855,8 @@ __global__ void __launch_bounds__(256) sgemm_plain_kernel(int M, int N, int K, f
 }
 
 // ---- host side ----------------------------------------------------------------
-using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
-                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
-                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_fn() {
-    static EncodeTiledFn fn = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<EncodeTiledFn>(p);
-    });
-    return fn;
-}
+using pmb::EncodeTiledFn;
+EncodeTiledFn encode_fn() { return pmb::tensor_map_encoder(); }
 
 // K-major bf16 operand [rows][kp]: boxes of box_k x box_rows, 64- or 128-byte swizzle.
 int make_map(CUtensorMap* map, const void* base, int rows, int kp, int box_rows, int box_k = BK) {

@@ -431,12 +431,13 @@ imgf_fast_kernel(const __grid_constant__ ImgfParamsF<R, MAXI> p) {
 //
 // Persistent, warp-specialised: one CTA per SM walks its share of the
 // tiles of all items.  Warps 0-3 stage and multiply, warps 4-7 drain:
-//  - staging: lanes of warp 0 issue one bulk async copy per input row of the
-//    tile (its 96 columns tile_c0-16 .. tile_c0+79 clipped to the image, rows
-//    replicated at the subscription's edges by choosing the source row) into
-//    a ring of raw buffers, SLOTS - 1 tiles ahead; pixels beyond the image's
-//    left/right edge are filled from the edge pixel afterwards.  Views that a
-//    bulk copy cannot address (not a whole-row NATURAL view, or unaligned)
+//  - staging: one thread loads the tile's input -- 96 pixels (tile_c0-16 ..
+//    tile_c0+79) of 128 + 2R rows of the bottom-up image -- as ONE 2-D TMA box
+//    (36 KB; a tensor map per distinct image, u32 elements, rows in buffer
+//    order) into a ring of raw buffers, SLOTS - 1 tiles ahead; rows and
+//    pixels beyond the image, which TMA fills with zeros, are replaced by the
+//    edge row / pixel afterwards.  Views a tensor map cannot describe (not a
+//    whole-row NATURAL view, unaligned, or more distinct images than maps)
 //    are staged by plain clamped byte loads.  The rows are then
 //    de-interleaved by byte permutes into one of two plane buffers and one
 //    thread issues the tile's MMAs into one of two accumulator sets;
@@ -455,7 +456,8 @@ constexpr int kTcThreads = 256;     // warps 0-3: staging and MMAs; warps 4-7: e
 constexpr int kTcMaxR = 8;
 constexpr int kTcMaxKD = 2 * kTcMaxR + 1;
 constexpr int kTcChunks = 5;        // plane columns tile_c0-8 .. tile_c0+71 in 16-byte chunks
-constexpr int kRawStride = 304;     // raw row: pixels tile_c0-16 .. tile_c0+79 (288 B) + padding
+constexpr int kRawStride = 288;     // raw row (a TMA box row): pixels tile_c0-16 .. tile_c0+79
+constexpr int kImgfMaps = 4;        // distinct images with a tensor map per launch
 constexpr int kOutStride = 208;     // staged output row: 192 B + padding (conflict-free 16-B stores)
 constexpr uint32_t kTcTmemCols = 512;  // two accumulator sets of 192 columns, 256 apart
 constexpr uint32_t kTcWaitPolls = 1u << 21;
@@ -469,16 +471,17 @@ struct TcGeo {
     static constexpr int CH = ROWS * 16;              // bytes per 16-column chunk of a plane
     static constexpr int PLANE = kTcChunks * CH;
     static constexpr int PLANES = 3 * PLANE;          // one buffer of the three planes
-    static constexpr int RAW = ROWS * kRawStride;
+    static constexpr int RAW = (ROWS * kRawStride + 127) / 128 * 128;  // slot stride (TMA destinations 128-B aligned)
     static constexpr int OUT = kTcTH * kOutStride;
-    static constexpr int FIXED = 2 * PLANES + OUT + KD * 512 + 128;
+    static constexpr int OFF_RAW = (2 * PLANES + 127) / 128 * 128;
+    static constexpr int FIXED = OFF_RAW + OUT + KD * 512 + 128;
     static constexpr int SLOTS = FIXED + 3 * RAW <= kSmemLimit ? 3 : 2;
-    static constexpr int OFF_RAW = 2 * PLANES;
     static constexpr int OFF_OUT = OFF_RAW + SLOTS * RAW;
     static constexpr int OFF_B = OFF_OUT + OUT;
     static constexpr int OFF_BAR = OFF_B + KD * 512;
     static constexpr int SMEM = OFF_BAR + 128;
-    static_assert(CH % 16 == 0 && OFF_RAW % 16 == 0 && OFF_OUT % 16 == 0 && OFF_B % 16 == 0 && OFF_BAR % 8 == 0,
+    static_assert(CH % 16 == 0 && OFF_RAW % 128 == 0 && RAW % 128 == 0 && OFF_OUT % 16 == 0 && OFF_B % 16 == 0 &&
+                      OFF_BAR % 8 == 0,
                   "alignment");
     static_assert(CH / 16 < (1 << 14), "leading byte offset field");
     static_assert(SMEM <= kSmemLimit, "shared memory");
@@ -490,6 +493,8 @@ constexpr uint32_t kTcIdesc = (2u << 4) | (0u << 7) | (1u << 10) | ((16u >> 3) <
 
 template <int MAXI>
 struct ImgfParamsTc {
+    CUtensorMap maps[kImgfMaps];  // the input images (u32 elements, 72 x (128 + 2R) boxes)
+    int map_of[MAXI];             // tensor map of each item, -1: plain loads
     int8_t f[kTcMaxKD][kTcMaxKD];
     int n_items;
     int total_tiles;
@@ -573,7 +578,7 @@ __device__ __forceinline__ bool role_any(int id, bool v) { return !role_all(id, 
 
 struct TcTile {
     int item, r0, c0, tw, rows;
-    bool bulk;  // rows staged by bulk copies
+    int map;  // tensor map that stages the tile, -1: plain loads
 };
 
 template <int MAXI>
@@ -593,11 +598,7 @@ __device__ __forceinline__ TcTile tc_tile(const ImgfParamsTc<MAXI>& p, int g) {
     t.r0 = it.r0 + ty * kTcTH;
     t.tw = min(kTcTW, it.c1 - t.c0);
     t.rows = min(kTcTH, it.r1 - t.r0);
-    // A NATURAL view holds whole image rows; 16-byte aligned pixel 16k of
-    // every row and a width of whole 16-pixel groups make each row piece one
-    // bulk copy.
-    t.bulk = it.in_pitch == 3LL * it.width && (it.width & 15) == 0 && (t.c0 & 15) == 0 && (it.in_pitch & 15) == 0 &&
-             ((reinterpret_cast<uintptr_t>(it.in) - 3 * static_cast<int64_t>(it.in_col0)) & 15) == 0;
+    t.map = p.map_of[lo];
     return t;
 }
 
@@ -665,36 +666,29 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
 
     if (warp < 4) {
         // ================= staging and MMAs =================
-        // Warp 0 starts the staging of tile k: bulk copies of its rows into
-        // raw slot k % SLOTS (plain arrival for tiles staged by loads).
+        // Warp 0 starts the staging of tile k: one 2-D TMA box into raw slot
+        // k % SLOTS (plain arrival for tiles staged by loads).  Box row j holds
+        // buffer row y0 + j, i.e. image row t.r0 - R + ROWS - 1 - j.
         auto issue = [&](int k) {
+            if (lane != 0) return;
             const TcTile t = tc_tile(p, tile_id(k));
             const int s = k % SLOTS;
             const uint32_t bar = tc_smem(&full[s]);
-            if (!t.bulk) {
-                if (lane == 0) tc_arrive(bar);
+            if (t.map < 0) {
+                tc_arrive(bar);
                 return;
             }
             const pmb_imgf_item& it = p.items[t.item];
-            const int x0 = max(0, 16 - t.c0), x1 = min(96, it.width - t.c0 + 16);
-            const uint32_t bytes = static_cast<uint32_t>(3 * (x1 - x0));
-            const int mlo = max(0, it.r0 - R), mhi = min(it.height - 1, it.r1 - 1 + R);
-            if (lane == 0)
-                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
-                             "r"(bytes * static_cast<uint32_t>(G::ROWS))
-                             : "memory");
-            __syncwarp();
-            uint8_t* raw = raws + s * G::RAW;
-            for (int r = lane; r < G::ROWS; r += 32) {
-                const int m = pmb::clampi(t.r0 - R + r, mlo, mhi);
-                const uint8_t* src = it.in + static_cast<int64_t>(it.height - 1 - m - it.in_row0) * it.in_pitch +
-                                     3 * static_cast<int64_t>(t.c0 - 16 + x0 - it.in_col0);
-                asm volatile(
-                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                        tc_smem(raw + r * kRawStride + 3 * x0)),
-                    "l"(src), "r"(bytes), "r"(bar)
-                    : "memory");
-            }
+            const int x = 3 * (t.c0 - 16) / 4;                          // u32 elements; 16-byte multiple
+            const int y = it.height - 1 - (t.r0 - R + G::ROWS - 1);     // may be negative: zero-filled rows
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                         "r"(static_cast<uint32_t>(G::ROWS * kRawStride))
+                         : "memory");
+            asm volatile(
+                "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+                    tc_smem(raws + s * G::RAW)),
+                "l"(reinterpret_cast<uint64_t>(&p.maps[t.map])), "r"(x), "r"(y), "r"(bar)
+                : "memory");
         };
         if (warp == 0)
             for (; issued < SLOTS - 1 && issued < ntiles; ++issued) issue(issued);
@@ -708,7 +702,7 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
             bool ok = tc_wait(tc_smem(&full[s]), (k / SLOTS) & 1);
             const int mlo = max(0, it.r0 - R), mhi = min(it.height - 1, it.r1 - 1 + R);
             const int clo = max(0, it.c0 - R), chi = min(it.width - 1, it.c1 - 1 + R);
-            if (!t.bulk) {
+            if (t.map < 0) {
                 // Plain loads of the needed pixels, clamped to the subscription.
                 const int span = kTcTW + 2 * R;
                 for (int e = tid; e < G::ROWS * span; e += 128) {
@@ -717,25 +711,42 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
                     const int n = pmb::clampi(t.c0 - 16 + x, clo, chi);
                     const uint8_t* src = it.in + static_cast<int64_t>(it.height - 1 - m - it.in_row0) * it.in_pitch +
                                          3 * (n - it.in_col0);
-                    uint8_t* d = raw + r * kRawStride + 3 * x;
+                    uint8_t* d = raw + (G::ROWS - 1 - r) * kRawStride + 3 * x;
                     d[0] = __ldg(src);
                     d[1] = __ldg(src + 1);
                     d[2] = __ldg(src + 2);
                 }
-            } else if (t.c0 < 16 || t.c0 + 80 + R > it.width + 16) {
-                // Needed pixels (x in [16 - R, 80 + R)) beyond the image's left or
-                // right edge -- the halo, or the part of a tile that overhangs the
-                // image -- repeat the edge pixel.
-                const int x0 = max(0, 16 - t.c0), x1 = min(96, it.width - t.c0 + 16);
-                const int nl = max(0, x0 - (16 - R)), nr = max(0, 80 + R - x1), nx = nl + nr;
-                for (int e = tid; e < G::ROWS * nx; e += 128) {
-                    const int r = e / nx, k2 = e - r * nx;
-                    const int x = k2 < nl ? 16 - R + k2 : x1 + (k2 - nl);
-                    const int xs = x < x0 ? x0 : x1 - 1;
-                    uint8_t* row = raw + r * kRawStride;
-                    row[3 * x] = row[3 * xs];
-                    row[3 * x + 1] = row[3 * xs + 1];
-                    row[3 * x + 2] = row[3 * xs + 2];
+            } else {
+                const bool top = t.r0 - R < 0, bottom = t.r0 - R + G::ROWS > it.height;
+                const bool left = t.c0 < 16, right = t.c0 + 80 + R > it.width + 16;
+                if (left || right) {
+                    // Needed pixels (x in [16 - R, 80 + R)) beyond the image's left or
+                    // right edge -- the halo, or the part of a tile that overhangs
+                    // the image -- repeat the edge pixel.
+                    const int x0 = max(0, 16 - t.c0), x1 = min(96, it.width - t.c0 + 16);
+                    const int nl = max(0, x0 - (16 - R)), nr = max(0, 80 + R - x1), nx = nl + nr;
+                    for (int e = tid; e < G::ROWS * nx; e += 128) {
+                        const int j = e / nx, k2 = e - j * nx;
+                        const int x = k2 < nl ? 16 - R + k2 : x1 + (k2 - nl);
+                        const int xs = x < x0 ? x0 : x1 - 1;
+                        uint8_t* row = raw + j * kRawStride;
+                        row[3 * x] = row[3 * xs];
+                        row[3 * x + 1] = row[3 * xs + 1];
+                        row[3 * x + 2] = row[3 * xs + 2];
+                    }
+                }
+                if (top || bottom) {
+                    // Rows beyond the image's top or bottom repeat the edge row.
+                    role_sync(2);  // edge pixels of the edge rows are in place
+                    const int j_top = t.r0 - R + G::ROWS - 1;             // box row of image row 0
+                    const int j_bot = t.r0 - R + G::ROWS - it.height;     // box row of image row H - 1
+                    for (int e = tid; e < G::ROWS * (kRawStride / 16); e += 128) {
+                        const int j = e / (kRawStride / 16), v = e - j * (kRawStride / 16);
+                        const int js = j > j_top ? j_top : (j < j_bot ? j_bot : j);
+                        if (js != j)
+                            *reinterpret_cast<uint4*>(raw + j * kRawStride + 16 * v) =
+                                *reinterpret_cast<const uint4*>(raw + js * kRawStride + 16 * v);
+                    }
                 }
             }
             // Planes b are free once the MMAs of tile k - 2 have read them.
@@ -747,7 +758,7 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
             uint8_t* pl = planes + b * G::PLANES;
             for (int e = tid; e < G::ROWS * kTcChunks; e += 128) {
                 const int q = e / G::ROWS, r = e - q * G::ROWS;
-                const uint8_t* src = raw + r * kRawStride + 48 * q + 24;
+                const uint8_t* src = raw + (G::ROWS - 1 - r) * kRawStride + 48 * q + 24;  // plane row r
                 uint32_t w[12];
 #pragma unroll
                 for (int j = 0; j < 6; ++j) {
@@ -1068,6 +1079,39 @@ int launch_tc(const pmb_imgf_item* items, int n, const int8_t* filter, cudaStrea
     p.n_items = m;
     p.total_tiles = static_cast<int>(total);
     p.tile_start[m] = static_cast<int>(total);
+    // Tensor maps: one per distinct image among the items whose view is a
+    // whole-row NATURAL view that TMA can address (16-byte aligned image and
+    // pitch, whole 16-pixel tile columns); the other items use plain loads.
+    int nmaps = 0;
+    const uint8_t* bases[kImgfMaps] = {};
+    int widths[kImgfMaps] = {}, heights[kImgfMaps] = {};
+    pmb::EncodeTiledFn enc = pmb::tensor_map_encoder();
+    for (int i = 0; i < m; ++i) {
+        const pmb_imgf_item& it = p.items[i];
+        p.map_of[i] = -1;
+        const uint8_t* base = it.in - it.in_row0 * it.in_pitch - 3 * static_cast<int64_t>(it.in_col0);
+        if (!enc || it.in_pitch != 3LL * it.width || (it.width & 3) || (it.c0 & 15) || (it.in_pitch & 15) ||
+            (reinterpret_cast<uintptr_t>(base) & 15))
+            continue;
+        int k = 0;
+        while (k < nmaps && !(bases[k] == base && widths[k] == it.width && heights[k] == it.height)) ++k;
+        if (k == nmaps) {
+            if (nmaps == kImgfMaps) continue;
+            const cuuint64_t dims[2] = {static_cast<cuuint64_t>(3 * it.width / 4), static_cast<cuuint64_t>(it.height)};
+            const cuuint64_t strides[1] = {static_cast<cuuint64_t>(it.in_pitch)};
+            const cuuint32_t box[2] = {kRawStride / 4, static_cast<cuuint32_t>(G::ROWS)};
+            const cuuint32_t estr[2] = {1, 1};
+            const CUresult r = enc(&p.maps[k], CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, const_cast<uint8_t*>(base), dims,
+                                   strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                   CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+            if (r != CUDA_SUCCESS) continue;
+            bases[k] = base;
+            widths[k] = it.width;
+            heights[k] = it.height;
+            ++nmaps;
+        }
+        p.map_of[i] = k;
+    }
     int st = imgf_err_word(&p.err);
     if (st != PMB_SUCCESS) return st;
     static std::once_flag once;

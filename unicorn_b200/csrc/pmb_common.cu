@@ -3,6 +3,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 
 #include "pmb_common.cuh"
 
@@ -35,6 +36,19 @@ int tmem_exclusive(const void* kernel, int threads, size_t smem_bytes, const cha
         return fail(PMB_BEYOND_LIMITS, "%s: %zu bytes of shared memory per CTA would let two CTAs holding tensor "
                     "memory share an SM (%d bytes per SM)", name, smem_bytes, per_sm);
     return PMB_SUCCESS;
+}
+
+EncodeTiledFn tensor_map_encoder() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    return fn;
 }
 
 }  // namespace pmb

@@ -2,6 +2,7 @@
 // translation, and small device utilities used by several kernels.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stddef.h>
@@ -29,6 +30,13 @@ void clear_error();
 // SMs -- so every TMEM-allocating launch checks this once and fails with
 // PMB_BEYOND_LIMITS otherwise.
 int tmem_exclusive(const void* kernel, int threads, size_t smem_bytes, const char* name);
+
+// cuTensorMapEncodeTiled, looked up once through the runtime's driver entry
+// point (null when the driver does not provide it).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn tensor_map_encoder();
 
 }  // namespace pmb
 
