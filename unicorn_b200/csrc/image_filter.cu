@@ -427,42 +427,47 @@ imgf_fast_kernel(const __grid_constant__ ImgfParamsF<R, MAXI> p) {
 // 16 r), so "rows shifted by ky" is the same descriptor with its start
 // address moved by 16 ky bytes.  B is 512 bytes per ky, built once per CTA.
 // 3 channels x 4 groups x (2R + 1) MMAs of 128 x 16 x 32 fill 12 accumulators
-// (192 TMEM columns).
+// (192 TMEM columns).  An MMA of this shape costs about as long as the
+// tensor core takes to read its 4.5 KB of operands from shared memory, so
+// the kernel keeps the rest of its shared-memory traffic conflict-free.
 //
-// Persistent, warp-specialised: one CTA per SM walks its share of the
-// tiles of all items.  Warps 0-3 stage and multiply, warps 4-7 drain:
-//  - staging: one thread loads the tile's input -- 96 pixels (tile_c0-16 ..
-//    tile_c0+79) of 128 + 2R rows of the bottom-up image -- as ONE 2-D TMA box
-//    (36 KB; a tensor map per distinct image, u32 elements, rows in buffer
-//    order) into a ring of raw buffers, SLOTS - 1 tiles ahead; rows and
-//    pixels beyond the image, which TMA fills with zeros, are replaced by the
-//    edge row / pixel afterwards.  Views a tensor map cannot describe (not a
-//    whole-row NATURAL view, unaligned, or more distinct images than maps)
-//    are staged by plain clamped byte loads.  The rows are then
-//    de-interleaved by byte permutes into one of two plane buffers and one
-//    thread issues the tile's MMAs into one of two accumulator sets;
-//  - epilogue: each thread reads its output row's 3 x 64 sums from TMEM,
-//    packs them to bytes (clamp: saturate; wrap: low byte), re-interleaves
-//    RGB and stages the row in shared memory, frees the accumulator set, and
+// Persistent and warp-specialised: one CTA per SM walks a contiguous range
+// of the launch's tiles (horizontal neighbours back to back, so their shared
+// input columns are L2 hits).  Ten warps in four roles:
+//  - loader (warp 8, one lane): loads the tile's input -- 96+ pixels
+//    (tile_c0-16 ..) of 128 + 2R rows of the bottom-up image -- as ONE 2-D
+//    TMA box (304-byte rows, a tensor map per distinct image) into a ring of
+//    raw buffers, up to SLOTS tiles ahead.  Views a tensor map cannot
+//    describe (not a whole-row NATURAL view, unaligned, or more distinct
+//    images than maps) are staged by the staging warps with plain loads;
+//  - staging (warps 4-7): replace rows and pixels beyond the image (TMA
+//    fills them with zeros) by the edge row / pixel, then de-interleave the
+//    rows by byte permutes into one of two plane buffers;
+//  - MMA (warp 9, one elected lane): issues the tile's MMAs into one of two
+//    accumulator sets and commits them;
+//  - epilogue (warps 0-3, TMEM lane quarter = warp): reads its row's 3 x 64
+//    sums, packs them to bytes (clamp: saturate; wrap: low byte),
+//    re-interleaves RGB into a staged row, frees the accumulator set, and
 //    the four warps write the tile with coalesced 16-byte stores.
-// mbarriers order the two roles: raw buffer filled, MMAs done (planes and
-// accumulators readable / planes reusable), accumulators drained.  Every
-// wait is bounded; a wait that expires sets the error word and the CTA
-// stops, waiting (bounded) for its own copies and MMAs before it frees its
-// tensor memory.  Reads outside the subscription but inside the image's rows
-// (NATURAL views hold whole rows) only meet zero filter weights.
+// mbarriers order the roles (raw buffer filled / drained, planes written,
+// MMAs done = planes and accumulators readable, accumulators drained).
+// Every wait is bounded; a wait that expires sets the error word and the
+// CTA stops, waiting (bounded) for its own copies and MMAs before it frees
+// its tensor memory.  Reads outside the subscription but inside the image's
+// rows (NATURAL views hold whole rows) only meet zero filter weights.
 constexpr int kTcTW = 64, kTcTH = 128;
-constexpr int kTcThreads = 256;     // warps 0-3: staging and MMAs; warps 4-7: epilogue
+constexpr int kTcThreads = 320;     // warps 0-3 epilogue, 4-7 staging, 8 loader, 9 MMA
+constexpr int kTcStageWarp0 = 4, kTcLoaderWarp = 8, kTcMmaWarp = 9;
 constexpr int kTcMaxR = 8;
 constexpr int kTcMaxKD = 2 * kTcMaxR + 1;
 constexpr int kTcChunks = 5;        // plane columns tile_c0-8 .. tile_c0+71 in 16-byte chunks
-constexpr int kRawStride = 288;     // raw row (a TMA box row): pixels tile_c0-16 .. tile_c0+79
+constexpr int kRawStride = 304;     // raw row (a TMA box row): pixels tile_c0-16 .. ; 19 x 16 B (odd: conflict-free)
 constexpr int kImgfMaps = 4;        // distinct images with a tensor map per launch
 constexpr int kOutStride = 208;     // staged output row: 192 B + padding (conflict-free 16-B stores)
 constexpr uint32_t kTcTmemCols = 512;  // two accumulator sets of 192 columns, 256 apart
 constexpr uint32_t kTcWaitPolls = 1u << 21;
 constexpr uint32_t kImgfErrTimeout = 1;
-constexpr int kSmemLimit = 227 * 1024;
+constexpr int kSmemLimit = 227 * 1024 - 256;  // per-block opt-in limit, less the kernel's static shared memory
 
 template <int R>
 struct TcGeo {
@@ -493,7 +498,7 @@ constexpr uint32_t kTcIdesc = (2u << 4) | (0u << 7) | (1u << 10) | ((16u >> 3) <
 
 template <int MAXI>
 struct ImgfParamsTc {
-    CUtensorMap maps[kImgfMaps];  // the input images (u32 elements, 72 x (128 + 2R) boxes)
+    CUtensorMap maps[kImgfMaps];  // the input images (u32 elements, 76 x (128 + 2R) boxes)
     int map_of[MAXI];             // tensor map of each item, -1: plain loads
     int8_t f[kTcMaxKD][kTcMaxKD];
     int n_items;
@@ -558,6 +563,17 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t (&r)[16]) {
         : "r"(taddr));
 }
 
+// One lane of the (converged) warp: the one that issues the MMAs.
+__device__ __forceinline__ bool tc_elect() {
+    uint32_t pred = 0;
+    asm volatile(
+        "{\n\t.reg .pred P;\n\t"
+        "elect.sync _|P, 0xffffffff;\n\t"
+        "selp.u32 %0, 1, 0, P;\n\t}"
+        : "=r"(pred));
+    return pred != 0;
+}
+
 // Barriers among the 128 threads of one role (id 1: epilogue, id 2: staging);
 // role_all / role_any also combine a flag, so every thread of the role takes
 // the same branch after them.
@@ -581,26 +597,36 @@ struct TcTile {
     int map;  // tensor map that stages the tile, -1: plain loads
 };
 
+// Walks a CTA's contiguous tile range: tile g of the launch lies in item
+// `cur` (tile_start[cur] <= g < tile_start[cur + 1]); g only grows, so the
+// item index only moves forward.
 template <int MAXI>
-__device__ __forceinline__ TcTile tc_tile(const ImgfParamsTc<MAXI>& p, int g) {
-    int lo = 0, hi = p.n_items - 1;
-    while (lo < hi) {
-        const int mid = (lo + hi + 1) >> 1;
-        if (p.tile_start[mid] <= g) lo = mid; else hi = mid - 1;
+struct TcCursor {
+    int cur;
+    __device__ __forceinline__ TcCursor(const ImgfParamsTc<MAXI>& p, int g) {
+        int lo = 0, hi = p.n_items - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (p.tile_start[mid] <= g) lo = mid; else hi = mid - 1;
+        }
+        cur = lo;
     }
-    const pmb_imgf_item& it = p.items[lo];
-    const int local = g - p.tile_start[lo];
-    const int txs = p.tiles_x[lo];
-    const int ty = local / txs, tx = local - ty * txs;
-    TcTile t;
-    t.item = lo;
-    t.c0 = it.c0 + tx * kTcTW;
-    t.r0 = it.r0 + ty * kTcTH;
-    t.tw = min(kTcTW, it.c1 - t.c0);
-    t.rows = min(kTcTH, it.r1 - t.r0);
-    t.map = p.map_of[lo];
-    return t;
-}
+    __device__ __forceinline__ TcTile at(const ImgfParamsTc<MAXI>& p, int g) {
+        while (g >= p.tile_start[cur + 1]) ++cur;
+        const pmb_imgf_item& it = p.items[cur];
+        const int local = g - p.tile_start[cur];
+        const int txs = p.tiles_x[cur];
+        const int ty = local / txs, tx = local - ty * txs;
+        TcTile t;
+        t.item = cur;
+        t.c0 = it.c0 + tx * kTcTW;
+        t.r0 = it.r0 + ty * kTcTH;
+        t.tw = min(kTcTW, it.c1 - t.c0);
+        t.rows = min(kTcTH, it.r1 - t.r0);
+        t.map = p.map_of[cur];
+        return t;
+    }
+};
 
 template <int R, int MODE, int MAXI>
 __global__ void __launch_bounds__(kTcThreads, 1)
@@ -614,21 +640,28 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
     uint8_t* const bsm = smem + G::OFF_B;
     uint64_t* const bars = reinterpret_cast<uint64_t*>(smem + G::OFF_BAR);
     uint64_t* const full = bars;              // [SLOTS]: raw buffer filled
-    uint64_t* const mma_done = bars + 3;      // [2]: accumulator set b written, planes b read
-    uint64_t* const acc_free = bars + 5;      // [2]: accumulator set b drained (4 epilogue warps)
-    uint64_t* const teardown = bars + 7;
-    uint32_t* const tmem_slot = reinterpret_cast<uint32_t*>(bars + 8);
+    uint64_t* const raw_free = bars + 3;      // [SLOTS]: raw buffer drained (4 staging warps)
+    uint64_t* const planes_full = bars + 6;   // [2]: plane buffer b written (4 staging warps)
+    uint64_t* const mma_done = bars + 8;      // [2]: accumulator set b written, planes b read
+    uint64_t* const acc_free = bars + 10;     // [2]: accumulator set b drained (4 epilogue warps)
+    uint64_t* const teardown = bars + 12;
+    uint32_t* const tmem_slot = reinterpret_cast<uint32_t*>(bars + 13);
     __shared__ volatile int s_fail;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int ntiles = (p.total_tiles - static_cast<int>(blockIdx.x) + static_cast<int>(gridDim.x) - 1) /
-                       static_cast<int>(gridDim.x);
-    auto tile_id = [&](int k) { return static_cast<int>(blockIdx.x) + k * static_cast<int>(gridDim.x); };
+    // This CTA's tiles: [t_begin, t_end) of the launch, in order.
+    const int t_begin = static_cast<int>(static_cast<int64_t>(blockIdx.x) * p.total_tiles / gridDim.x);
+    const int t_end = static_cast<int>(static_cast<int64_t>(blockIdx.x + 1) * p.total_tiles / gridDim.x);
+    const int ntiles = t_end - t_begin;
 
     if (tid == 0) {
         s_fail = 0;
-        for (int i = 0; i < SLOTS; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(&full[i])));
+        for (int i = 0; i < SLOTS; ++i) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(&full[i])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(tc_smem(&raw_free[i])));
+        }
         for (int i = 0; i < 2; ++i) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(tc_smem(&planes_full[i])));
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(&mma_done[i])));
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(tc_smem(&acc_free[i])));
         }
@@ -652,7 +685,7 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
         *reinterpret_cast<uint32_t*>(bsm + ky * 512 + off) = word;
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    if (warp == 0) {
+    if (warp == kTcMmaWarp) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(tc_smem(tmem_slot)),
                      "r"(kTcTmemCols)
                      : "memory");
@@ -662,40 +695,84 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
-    int issued = 0;  // tiles whose staging warp 0 has started (warp 0 only)
 
-    if (warp < 4) {
-        // ================= staging and MMAs =================
-        // Warp 0 starts the staging of tile k: one 2-D TMA box into raw slot
-        // k % SLOTS (plain arrival for tiles staged by loads).  Box row j holds
-        // buffer row y0 + j, i.e. image row t.r0 - R + ROWS - 1 - j.
-        auto issue = [&](int k) {
-            if (lane != 0) return;
-            const TcTile t = tc_tile(p, tile_id(k));
-            const int s = k % SLOTS;
-            const uint32_t bar = tc_smem(&full[s]);
-            if (t.map < 0) {
-                tc_arrive(bar);
-                return;
+    if (warp == kTcLoaderWarp) {
+        // ================= loader =================
+        // Tile k goes to raw slot k % SLOTS once the staging warps have
+        // drained the slot's previous tile.  Box row j holds buffer row
+        // y + j, i.e. image row t.r0 - R + ROWS - 1 - j.
+        if (lane == 0) {
+            TcCursor<MAXI> cur(p, t_begin);
+            int issued = 0;
+            for (; issued < ntiles; ++issued) {
+                const int k = issued, s = k % SLOTS;
+                if (s_fail) break;
+                if (k >= SLOTS && !tc_wait(tc_smem(&raw_free[s]), ((k / SLOTS) - 1) & 1)) {
+                    s_fail = 1;
+                    break;
+                }
+                const TcTile t = cur.at(p, t_begin + k);
+                const uint32_t bar = tc_smem(&full[s]);
+                if (t.map < 0) {
+                    tc_arrive(bar);  // staged by the staging warps' own loads
+                    continue;
+                }
+                const pmb_imgf_item& it = p.items[t.item];
+                const int x = 3 * (t.c0 - 16) / 4;                          // u32 elements; 16-byte multiple
+                const int y = it.height - 1 - (t.r0 - R + G::ROWS - 1);     // may be negative: zero-filled rows
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                             "r"(static_cast<uint32_t>(G::ROWS * kRawStride))
+                             : "memory");
+                asm volatile(
+                    "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], "
+                    "[%4];" ::"r"(tc_smem(raws + s * G::RAW)),
+                    "l"(reinterpret_cast<uint64_t>(&p.maps[t.map])), "r"(x), "r"(y), "r"(bar)
+                    : "memory");
             }
-            const pmb_imgf_item& it = p.items[t.item];
-            const int x = 3 * (t.c0 - 16) / 4;                          // u32 elements; 16-byte multiple
-            const int y = it.height - 1 - (t.r0 - R + G::ROWS - 1);     // may be negative: zero-filled rows
-            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
-                         "r"(static_cast<uint32_t>(G::ROWS * kRawStride))
-                         : "memory");
-            asm volatile(
-                "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
-                    tc_smem(raws + s * G::RAW)),
-                "l"(reinterpret_cast<uint64_t>(&p.maps[t.map])), "r"(x), "r"(y), "r"(bar)
-                : "memory");
-        };
-        if (warp == 0)
-            for (; issued < SLOTS - 1 && issued < ntiles; ++issued) issue(issued);
+            // After a failure, copies still in flight must land before the
+            // CTA's shared memory is released: the last tile issued to each
+            // slot completes the slot's latest phase.
+            if (s_fail)
+                for (int k = max(0, issued - SLOTS); k < issued; ++k) tc_wait(tc_smem(&full[k % SLOTS]), (k / SLOTS) & 1);
+        }
+    } else if (warp == kTcMmaWarp) {
+        // ================= MMA issue =================
+        const uint64_t adesc0 = tc_desc(tc_smem(planes), G::CH, 128);
+        const uint64_t bdesc0 = tc_desc(tc_smem(bsm), 256, 128);
+        for (int k = 0; k < ntiles; ++k) {
+            if (__any_sync(0xffffffffu, s_fail != 0)) break;
+            const int b = k & 1;
+            bool ok = tc_wait(tc_smem(&planes_full[b]), (k >> 1) & 1);
+            // Accumulator set b is free once the epilogue has drained tile k - 2.
+            if (ok && k >= 2) ok = tc_wait(tc_smem(&acc_free[b]), ((k - 2) >> 1) & 1);
+            if (!__all_sync(0xffffffffu, ok)) {
+                s_fail = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            if (tc_elect()) {
+                const uint64_t ab = adesc0 + static_cast<uint64_t>((b * G::PLANES) >> 4);
+                const uint32_t acc = tmem + 256u * b;
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+#pragma unroll
+                    for (int tg = 0; tg < 4; ++tg)
+#pragma unroll
+                        for (int ky = 0; ky < G::KD; ++ky)
+                            tc_mma_i8(acc + static_cast<uint32_t>((c * 4 + tg) * 16),
+                                      ab + static_cast<uint64_t>((c * G::PLANE + tg * G::CH + ky * 16) >> 4),
+                                      bdesc0 + static_cast<uint64_t>((ky * 512) >> 4), ky > 0 ? 1u : 0u);
+                tc_commit(tc_smem(&mma_done[b]));
+            }
+            __syncwarp();
+        }
+    } else if (warp >= kTcStageWarp0) {
+        // ================= staging =================
+        const int st = tid - 32 * kTcStageWarp0;  // 0..127
+        TcCursor<MAXI> cur(p, t_begin);
         for (int k = 0; k < ntiles; ++k) {
             if (role_any(2, s_fail != 0)) break;
-            if (warp == 0 && issued < ntiles) issue(issued++);  // SLOTS - 1 tiles ahead
-            const TcTile t = tc_tile(p, tile_id(k));
+            const TcTile t = cur.at(p, t_begin + k);
             const pmb_imgf_item& it = p.items[t.item];
             const int s = k % SLOTS, b = k & 1;
             uint8_t* raw = raws + s * G::RAW;
@@ -705,7 +782,7 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
             if (t.map < 0) {
                 // Plain loads of the needed pixels, clamped to the subscription.
                 const int span = kTcTW + 2 * R;
-                for (int e = tid; e < G::ROWS * span; e += 128) {
+                for (int e = st; e < G::ROWS * span; e += 128) {
                     const int r = e / span, x = 16 - R + (e - r * span);
                     const int m = pmb::clampi(t.r0 - R + r, mlo, mhi);
                     const int n = pmb::clampi(t.c0 - 16 + x, clo, chi);
@@ -725,7 +802,7 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
                     // the image -- repeat the edge pixel.
                     const int x0 = max(0, 16 - t.c0), x1 = min(96, it.width - t.c0 + 16);
                     const int nl = max(0, x0 - (16 - R)), nr = max(0, 80 + R - x1), nx = nl + nr;
-                    for (int e = tid; e < G::ROWS * nx; e += 128) {
+                    for (int e = st; e < G::ROWS * nx; e += 128) {
                         const int j = e / nx, k2 = e - j * nx;
                         const int x = k2 < nl ? 16 - R + k2 : x1 + (k2 - nl);
                         const int xs = x < x0 ? x0 : x1 - 1;
@@ -740,7 +817,7 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
                     role_sync(2);  // edge pixels of the edge rows are in place
                     const int j_top = t.r0 - R + G::ROWS - 1;             // box row of image row 0
                     const int j_bot = t.r0 - R + G::ROWS - it.height;     // box row of image row H - 1
-                    for (int e = tid; e < G::ROWS * (kRawStride / 16); e += 128) {
+                    for (int e = st; e < G::ROWS * (kRawStride / 16); e += 128) {
                         const int j = e / (kRawStride / 16), v = e - j * (kRawStride / 16);
                         const int js = j > j_top ? j_top : (j < j_bot ? j_bot : j);
                         if (js != j)
@@ -755,62 +832,55 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
                 s_fail = 1;
                 break;
             }
+            // De-interleave: item e is plane row r = e % ROWS, chunks 3h .. 3h+2
+            // (h = e / ROWS; chunk 5 does not exist).  Consecutive threads take
+            // consecutive rows: the 16-byte loads (row stride 19 x 16 B) and the
+            // stores (16 B apart) are conflict-free.
             uint8_t* pl = planes + b * G::PLANES;
-            for (int e = tid; e < G::ROWS * kTcChunks; e += 128) {
-                const int q = e / G::ROWS, r = e - q * G::ROWS;
-                const uint8_t* src = raw + (G::ROWS - 1 - r) * kRawStride + 48 * q + 24;  // plane row r
-                uint32_t w[12];
+            for (int e = st; e < 2 * G::ROWS; e += 128) {
+                const int h = e >= G::ROWS ? 1 : 0, r = e - h * G::ROWS;
+                // Raw bytes 48 q + 24 .. 48 q + 71 hold chunk q; the loads cover
+                // 48 q0 + 16 .. 48 q0 + 16 * (3 nq + 1) (16-byte aligned).
+                const uint8_t* src = raw + (G::ROWS - 1 - r) * kRawStride + 144 * h + 16;
+                uint32_t w[3 * 12 + 4];
 #pragma unroll
-                for (int j = 0; j < 6; ++j) {
-                    const uint2 v = *reinterpret_cast<const uint2*>(src + 8 * j);
-                    w[2 * j] = v.x;
-                    w[2 * j + 1] = v.y;
+                for (int j = 0; j < 10; ++j) {
+                    if (h == 1 && j >= 7) break;  // chunks 3, 4: 7 loads
+                    const uint4 v = *reinterpret_cast<const uint4*>(src + 16 * j);
+                    w[4 * j] = v.x;
+                    w[4 * j + 1] = v.y;
+                    w[4 * j + 2] = v.z;
+                    w[4 * j + 3] = v.w;
                 }
-                uint32_t o[3][4];
 #pragma unroll
-                for (int g = 0; g < 4; ++g) deinterleave4(w[3 * g], w[3 * g + 1], w[3 * g + 2], o[0][g], o[1][g], o[2][g]);
+                for (int qq = 0; qq < 3; ++qq) {
+                    if (h == 1 && qq == 2) break;
+                    const int q = 3 * h + qq;
+                    uint32_t o[3][4];
 #pragma unroll
-                for (int c = 0; c < 3; ++c)
-                    *reinterpret_cast<uint4*>(pl + c * G::PLANE + q * G::CH + r * 16) =
-                        make_uint4(o[c][0], o[c][1], o[c][2], o[c][3]);
+                    for (int g = 0; g < 4; ++g)
+                        deinterleave4(w[12 * qq + 2 + 3 * g], w[12 * qq + 3 + 3 * g], w[12 * qq + 4 + 3 * g], o[0][g],
+                                      o[1][g], o[2][g]);
+#pragma unroll
+                    for (int c = 0; c < 3; ++c)
+                        *reinterpret_cast<uint4*>(pl + c * G::PLANE + q * G::CH + r * 16) =
+                            make_uint4(o[c][0], o[c][1], o[c][2], o[c][3]);
+                }
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // planes, then the tensor core reads them
-            role_sync(2);
-            if (tid == 0) {
-                // Accumulator set b is free once the epilogue has drained tile k - 2.
-                // On a timeout no MMAs are issued: the epilogue's wait then runs
-                // out too, and both roles stop at their next iteration.
-                if (k >= 2 && !tc_wait(tc_smem(&acc_free[b]), ((k - 2) >> 1) & 1)) {
-                    s_fail = 1;
-                    continue;
-                }
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t pa = tc_smem(pl), bb = tc_smem(bsm), acc = tmem + 256u * b;
-#pragma unroll 1
-                for (int c = 0; c < 3; ++c)
-#pragma unroll 1
-                    for (int tg = 0; tg < 4; ++tg)
-#pragma unroll
-                        for (int ky = 0; ky < G::KD; ++ky)
-                            tc_mma_i8(acc + static_cast<uint32_t>((c * 4 + tg) * 16),
-                                      tc_desc(pa + c * G::PLANE + tg * G::CH + ky * 16, G::CH, 128),
-                                      tc_desc(bb + ky * 512, 256, 128), ky > 0 ? 1u : 0u);
-                tc_commit(tc_smem(&mma_done[b]));
+            __syncwarp();
+            if (lane == 0) {
+                tc_arrive(tc_smem(&planes_full[b]));
+                tc_arrive(tc_smem(&raw_free[s]));
             }
-        }
-        // Bulk copies started for tiles that will not be consumed (after a
-        // failure) must land before the CTA's shared memory is released.
-        if (warp == 0 && s_fail) {
-            const int consumed_max = issued;
-            for (int k = max(0, consumed_max - (SLOTS - 1)); k < consumed_max; ++k)
-                tc_wait(tc_smem(&full[k % SLOTS]), (k / SLOTS) & 1);
         }
     } else {
         // ================= epilogue =================
-        const int q = warp - 4, row = 32 * q + lane;
+        const int q = warp, row = 32 * q + lane;
+        TcCursor<MAXI> cur(p, t_begin);
         for (int k = 0; k < ntiles; ++k) {
             if (role_any(1, s_fail != 0)) break;
-            const TcTile t = tc_tile(p, tile_id(k));
+            const TcTile t = cur.at(p, t_begin + k);
             const pmb_imgf_item& it = p.items[t.item];
             const int b = k & 1;
             if (!role_all(1, tc_wait(tc_smem(&mma_done[b]), (k >> 1) & 1))) {
@@ -858,20 +928,34 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
                         make_uint4(d[4 * h], d[4 * h + 1], d[4 * h + 2], d[4 * h + 3]);
             }
             role_sync(1);  // the staged tile is complete
-            const int et = tid - 128;
             uint8_t* const obase = it.out + static_cast<int64_t>(t.r0 - it.out_row0) * it.out_pitch +
                                    3 * (t.c0 - it.out_col0);
-            if (t.tw == kTcTW && ((reinterpret_cast<uintptr_t>(obase) | static_cast<uintptr_t>(it.out_pitch)) & 15) == 0) {
-                for (int e = et; e < t.rows * 12; e += 128) {
+            if (t.tw == kTcTW && t.rows == kTcTH &&
+                ((reinterpret_cast<uintptr_t>(obase) | static_cast<uintptr_t>(it.out_pitch)) & 15) == 0) {
+                // Full tile: 12 x 16 B per thread, all loads first.
+                uint4 v[12];
+#pragma unroll
+                for (int i = 0; i < 12; ++i) {
+                    const int e = tid + 128 * i, r = e / 12, c = e - r * 12;
+                    v[i] = *reinterpret_cast<const uint4*>(ost + r * kOutStride + 16 * c);
+                }
+#pragma unroll
+                for (int i = 0; i < 12; ++i) {
+                    const int e = tid + 128 * i, r = e / 12, c = e - r * 12;
+                    *reinterpret_cast<uint4*>(obase + static_cast<int64_t>(r) * it.out_pitch + 16 * c) = v[i];
+                }
+            } else if (t.tw == kTcTW &&
+                       ((reinterpret_cast<uintptr_t>(obase) | static_cast<uintptr_t>(it.out_pitch)) & 15) == 0) {
+                for (int e = tid; e < t.rows * 12; e += 128) {
                     const int r = e / 12, c = e - r * 12;
-                    *reinterpret_cast<uint4*>(obase + r * it.out_pitch + 16 * c) =
+                    *reinterpret_cast<uint4*>(obase + static_cast<int64_t>(r) * it.out_pitch + 16 * c) =
                         *reinterpret_cast<const uint4*>(ost + r * kOutStride + 16 * c);
                 }
             } else {
                 const int nb = 3 * t.tw;
-                for (int e = et; e < t.rows * nb; e += 128) {
+                for (int e = tid; e < t.rows * nb; e += 128) {
                     const int r = e / nb, c = e - r * nb;
-                    obase[r * it.out_pitch + c] = ost[r * kOutStride + c];
+                    obase[static_cast<int64_t>(r) * it.out_pitch + c] = ost[r * kOutStride + c];
                 }
             }
             role_sync(1);  // the staging buffer may be refilled
@@ -880,9 +964,9 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
 
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 0) {
+    if (warp == kTcMmaWarp) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        if (s_fail && lane == 0) {
+        if (s_fail && tc_elect()) {  // the lane that issued the MMAs
             atomicOr(p.err, kImgfErrTimeout);
             tc_commit(tc_smem(teardown));  // every MMA this CTA issued has retired once this arrives
             tc_wait(tc_smem(teardown), 0);
