@@ -984,7 +984,7 @@ def main():
                                "256 subtasks of 512x512 (+2 px halo) in one launch",
                    "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (201 MB in + 201 MB out)"},
         "roofline": {"bound": "hbm", "achieved": round(kernel_gbs, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(kernel_gbs / peak, 4), "traffic": profiled_traffic("imgf_fast_kernel 8192x8192 5x5"),
+                     "frac": round(kernel_gbs / peak, 4), "traffic": profiled_traffic("imgf_tc_kernel 8192x8192 5x5"),
                      "peak_source": f"{peak_kind} hbm_gbs (burst, kernel timed alone)"},
         "e2e": e2e,
         "e2e_c_abi": capi_e2e,

@@ -12,20 +12,19 @@
 // byte is the sum mod 256); CLAMP mode sums unsigned bytes exactly and clamps
 // to [0, 255].
 //
-// Two kernels: imgf_fast_kernel for R <= 4 (every radius the reference's own
-// runs use) and imgf_kernel, the generic form, for 5 <= R <= 15.
+// Two kernels: imgf_tc_kernel (tensor cores, below) for R <= 8 -- every
+// radius the reference's own runs use -- and imgf_kernel, the generic dp4a
+// form, for 9 <= R <= 15.  The batch of subtasks (items) of one or several
+// tasks runs in ONE launch.
 //
-// Design.  One CTA owns a 64 x 32 output tile.  It stages the tile plus halo
-// once into shared memory as three planar byte planes (one per output
-// channel), de-interleaving RGB with byte permutes while loading 12-byte pixel
-// quads with 32-bit loads.  Each thread then produces a 4-pixel x 4-row block:
-// for every staged row it reads a few aligned 32-bit words of a plane and
-// feeds them to dp4a (4 byte multiply-adds per instruction) against filter
-// "pattern" words precomputed on the host (filter row ky shifted so that tap
-// kx lines up with the byte it multiplies).  Every input byte is read from HBM
-// once per tile (halo re-reads hit L2), so the kernel's DRAM traffic is the
-// algorithmic 2 x 3WH bytes per pass.  The batch of subtasks (items) of one or
-// several tasks runs in ONE launch: blockIdx.x is mapped to (item, tile).
+// Generic form.  One CTA owns a 64 x 32 output tile.  It stages the tile
+// plus halo once into shared memory as three planar byte planes (one per
+// output channel), de-interleaving RGB with byte permutes.  Each thread then
+// produces a 4-pixel x 4-row block: for every staged row it reads a few
+// aligned 32-bit words of a plane and feeds them to dp4a (4 byte
+// multiply-adds per instruction) against filter "pattern" words precomputed
+// on the host (filter row ky shifted so that tap kx lines up with the byte it
+// multiplies).  blockIdx.x is mapped to (item, tile).
 #include <algorithm>
 #include <mutex>
 
@@ -204,46 +203,7 @@ imgf_kernel(const __grid_constant__ ImgfParams<R, MAXI> p) {
 }
 
 // ---------------------------------------------------------------------------
-// Fast path for R <= 4 (the reference's default radius 1, its benchmark sweep's
-// 3x3 and 7x7 filters, and the 5x5 configuration).  Same tile and thread map
-// as imgf_kernel, with the per-instruction overhead removed:
-//  - the halo is staged 16 pixels (48 bytes, three 16-byte loads) at a time
-//    and de-interleaved with byte permutes into 16-byte plane stores;
-//  - the filter pattern words stay in the parameter space (constant bank);
-//  - for CB == 3 all three channels accumulate in the same pass over the
-//    staged rows (patterns are shared by the channels);
-//  - results are packed into the RGB byte stream with byte permutes.
-constexpr int kPadF = 16;                 // left halo of the fast planes (pixels)
-constexpr int kPWF = kTW + 2 * kPadF;     // 96 staged bytes per plane row
-// Row stride of the planes: a warp's two half-warps read rows kV apart, so the
-// stride is chosen to put those rows 16 banks apart (28 words * 4 rows = 112
-// words = 16 mod 32): conflict-free window loads.
-constexpr int kRowF = 112;
-static_assert((kRowF / 4 * kV) % 32 == 16 && kRowF % 16 == 0 && kRowF >= kPWF, "plane row stride");
-
-template <int R>
-struct GeoF {
-    static constexpr int KD = 2 * R + 1;
-    static constexpr int WS = (kPadF - R) / 4;   // first window word of group 0
-    static constexpr int OFF = (kPadF - R) % 4;  // first tap byte of pixel 0 in that word
-    static constexpr int NW = (OFF + 2 * R + 3) / 4 + 1;
-    static constexpr int PH = kTH + 2 * R;
-    static_assert(kGX - 1 + WS + NW <= kPWF / 4, "window leaves the plane row");
-};
-
-template <int R>
-__host__ __device__ constexpr bool tap_word_used_f(int k, int w) {
-    return 4 * w <= GeoF<R>::OFF + k + 2 * R && 4 * w + 3 >= GeoF<R>::OFF + k;
-}
-
-template <int R, int MAXI>
-struct ImgfParamsF {
-    uint32_t pat[GeoF<R>::KD][4][GeoF<R>::NW];
-    int n_items;
-    int tile_start[MAXI + 1];
-    int tiles_x[MAXI];
-    pmb_imgf_item items[MAXI];
-};
+// Byte packing shared by the tensor-core path.
 
 // Four 32-bit sums into four bytes (sum k -> byte k): CLAMP saturates to
 // [0, 255] with cvt.pack.sat (two sums per instruction), WRAP keeps the low
@@ -270,201 +230,77 @@ __device__ __forceinline__ void deinterleave4(uint32_t w0, uint32_t w1, uint32_t
     o2 = __byte_perm(__byte_perm(w0, w1, 0x0630), w2, 0x5210);
 }
 
-// One CTA per 64 x 32 tile; blockIdx.y selects the item (subtask), blockIdx.x
-// the tile inside it (CTAs past the item's tile count exit at once).
-template <int R, int MODE, int MAXI, int CB>
-__global__ void __launch_bounds__(kThreads, 4)
-imgf_fast_kernel(const __grid_constant__ ImgfParamsF<R, MAXI> p) {
-    using G = GeoF<R>;
-    __shared__ __align__(16) uint8_t planes[3][G::PH][kRowF];
-
-    const int item = blockIdx.y;
-    const int txs = p.tiles_x[item];
-    const int local = blockIdx.x;
-    if (local >= p.tile_start[item + 1] - p.tile_start[item]) return;
-    const uint8_t* const in = p.items[item].in;
-    uint8_t* const out = p.items[item].out;
-    const int64_t ip = p.items[item].in_pitch, op = p.items[item].out_pitch;
-    const int H = p.items[item].height, Wd = p.items[item].width;
-    const int in_row0 = p.items[item].in_row0, in_col0 = p.items[item].in_col0;
-    const int out_row0 = p.items[item].out_row0, out_col0 = p.items[item].out_col0;
-    const int r0 = p.items[item].r0, r1 = p.items[item].r1, c0 = p.items[item].c0, c1 = p.items[item].c1;
-    const int ty = local / txs, tx = local - ty * txs;
-    const int tile_c0 = c0 + tx * kTW, tile_r0 = r0 + ty * kTH;
-    const int mlo = max(0, r0 - R), mhi = min(H - 1, r1 - 1 + R);
-    const int clo = max(0, c0 - R), chi = min(Wd - 1, c1 - 1 + R);
-    const bool al16 = ((reinterpret_cast<uintptr_t>(in) | static_cast<uintptr_t>(ip)) & 15) == 0;
-    const bool al4 = ((reinterpret_cast<uintptr_t>(in) | static_cast<uintptr_t>(ip)) & 3) == 0;
-
-    // ---- staging: 16-pixel groups, 6 per plane row, straight from HBM -------
-    constexpr int kG16 = kPWF / 16;
-    for (int g = threadIdx.x; g < G::PH * kG16; g += kThreads) {
-        const int yy = g / kG16;
-        const int xg = g - yy * kG16;
-        const int m = pmb::clampi(tile_r0 - R + yy, mlo, mhi);
-        const uint8_t* rowp = in + static_cast<int64_t>(H - 1 - m - in_row0) * ip;
-        const int n0 = tile_c0 - kPadF + 16 * xg;
-        uint32_t o[3][4];
-        if (al16 && n0 >= clo && n0 + 15 <= chi && ((n0 - in_col0) & 15) == 0) {
-            const uint4* sp = reinterpret_cast<const uint4*>(rowp + 3 * (n0 - in_col0));
-            const uint4 a = __ldg(sp), b = __ldg(sp + 1), c = __ldg(sp + 2);
-            deinterleave4(a.x, a.y, a.z, o[0][0], o[1][0], o[2][0]);
-            deinterleave4(a.w, b.x, b.y, o[0][1], o[1][1], o[2][1]);
-            deinterleave4(b.z, b.w, c.x, o[0][2], o[1][2], o[2][2]);
-            deinterleave4(c.y, c.z, c.w, o[0][3], o[1][3], o[2][3]);
-        } else {
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const int nq = n0 + 4 * q;
-                if (al4 && nq >= clo && nq + 3 <= chi && ((nq - in_col0) & 3) == 0) {
-                    const uint32_t* s4 = reinterpret_cast<const uint32_t*>(rowp + 3 * (nq - in_col0));
-                    deinterleave4(__ldg(s4), __ldg(s4 + 1), __ldg(s4 + 2), o[0][q], o[1][q], o[2][q]);
-                } else {
-                    o[0][q] = o[1][q] = o[2][q] = 0;
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) {
-                        const int n = pmb::clampi(nq + e, clo, chi);
-                        const uint8_t* px = rowp + 3 * (n - in_col0);
-                        o[0][q] |= static_cast<uint32_t>(__ldg(px + 2)) << (8 * e);
-                        o[1][q] |= static_cast<uint32_t>(__ldg(px + 1)) << (8 * e);
-                        o[2][q] |= static_cast<uint32_t>(__ldg(px + 0)) << (8 * e);
-                    }
-                }
-            }
-        }
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-            *reinterpret_cast<uint4*>(&planes[c][yy][16 * xg]) = make_uint4(o[c][0], o[c][1], o[c][2], o[c][3]);
-    }
-
-    // The filter pattern words stay in the kernel's parameter space: every
-    // index below is a compile-time constant, so each dp4a reads its pattern
-    // operand from the constant bank and no registers hold the filter.
-    __syncthreads();
-
-    const int gx = threadIdx.x % kGX;
-    const int gy = threadIdx.x / kGX;
-    uint32_t pl[kV][3];  // per output row and plane: the 4 pixels' bytes of that plane
-
-#pragma unroll
-    for (int cb = 0; cb < 3; cb += CB) {
-        int acc[CB][kV][4];
-#pragma unroll
-        for (int c = 0; c < CB; ++c)
-#pragma unroll
-            for (int v = 0; v < kV; ++v)
-#pragma unroll
-                for (int k = 0; k < 4; ++k) acc[c][v][k] = 0;
-#pragma unroll
-        for (int yy = 0; yy < kV + 2 * R; ++yy) {
-            uint32_t win[CB][G::NW];
-#pragma unroll
-            for (int c = 0; c < CB; ++c) {
-                const uint32_t* rp = reinterpret_cast<const uint32_t*>(&planes[cb + c][gy * kV + yy][0]) + gx + G::WS;
-#pragma unroll
-                for (int w = 0; w < G::NW; ++w) win[c][w] = rp[w];
-            }
-#pragma unroll
-            for (int v = 0; v < kV; ++v) {
-                const int ky = yy - v;
-                if (ky < 0 || ky >= G::KD) continue;
-#pragma unroll
-                for (int c = 0; c < CB; ++c)
-#pragma unroll
-                    for (int k = 0; k < 4; ++k)
-#pragma unroll
-                        for (int w = 0; w < G::NW; ++w)
-                            if (tap_word_used_f<R>(k, w))
-                                acc[c][v][k] = dp4a_us(win[c][w], p.pat[ky][k][w], acc[c][v][k]);
-            }
-        }
-#pragma unroll
-        for (int c = 0; c < CB; ++c)
-#pragma unroll
-            for (int v = 0; v < kV; ++v) pl[v][cb + c] = pack4<MODE>(acc[c][v]);
-    }
-
-    const int j0 = tile_c0 + 4 * gx;
-    if (j0 >= c1) return;
-#pragma unroll
-    for (int v = 0; v < kV; ++v) {
-        const int i = tile_r0 + gy * kV + v;
-        if (i >= r1) break;
-        uint8_t* dst = out + static_cast<int64_t>(i - out_row0) * op + 3 * (j0 - out_col0);
-        // pixel k's bytes are (plane 0, plane 1, plane 2) byte k: with P2 = plane 0 and
-        // P0 = plane 2 the permutes below lay out P2.k P1.k P0.k for k = 0..3.
-        const uint32_t P0 = pl[v][2], P1 = pl[v][1], P2 = pl[v][0];
-        if (j0 + 3 < c1 && (reinterpret_cast<uintptr_t>(dst) & 3) == 0) {
-            uint32_t* d = reinterpret_cast<uint32_t*>(dst);
-            d[0] = __byte_perm(__byte_perm(P2, P1, 0x5140), P0, 0x2410);  // P2.0 P1.0 P0.0 P2.1
-            d[1] = __byte_perm(__byte_perm(P1, P0, 0x6251), P2, 0x2610);  // P1.1 P0.1 P2.2 P1.2
-            d[2] = __byte_perm(P0, __byte_perm(P2, P1, 0x0073), 0x3542);  // P0.2 P2.3 P1.3 P0.3
-        } else {
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                if (j0 + k >= c1) break;
-                dst[3 * k + 0] = static_cast<uint8_t>(P2 >> (8 * k));
-                dst[3 * k + 1] = static_cast<uint8_t>(P1 >> (8 * k));
-                dst[3 * k + 2] = static_cast<uint8_t>(P0 >> (8 * k));
-            }
-        }
-    }
-}
-
 // ---------------------------------------------------------------------------
 // Tensor-core path for R <= 8: the stencil as int8 matrix products on the
 // 5th-generation tensor cores (tcgen05.mma kind::i8, u8 pixels x s8 weights,
 // exact s32 sums in tensor memory), so integer parity is unchanged.
 //
-// Output tiles are 128 rows x 64 pixels.  Per channel plane P and filter row
-// ky a tile is D += A_ky * B_ky with
-//   A_ky[i][k] = P[tile_r0 + i + ky - R][tile_c0 - 8 + 16t + k]   (M = 128 rows, K = 32 columns)
+// Output tiles are TH rows x 64 pixels.  Per channel plane P and filter
+// row ky a tile is D += A_ky * B_ky with
+//   A_ky[i][k] = P[i + ky][16t - 8 + k]            (M = 128 rows, K = 32 columns)
 //   B_ky[k][j] = f[ky][k - j + R - 8]  (zero outside [0, 2R])     (N = 16 output columns)
 // for each 16-column group t: the 32-column window of input bytes times a
-// banded Toeplitz slice of the filter row.  A is never materialised per ky:
-// the planes are stored in the canonical K-major no-swizzle layout with the
-// 8-row core groups packed back to back (row r of 16-byte chunk q at q * CH +
-// 16 r), so "rows shifted by ky" is the same descriptor with its start
-// address moved by 16 ky bytes.  B is 512 bytes per ky, built once per CTA.
-// 3 channels x 4 groups x (2R + 1) MMAs of 128 x 16 x 32 fill 12 accumulators
-// (192 TMEM columns).  An MMA of this shape costs about as long as the
-// tensor core takes to read its 4.5 KB of operands from shared memory, so
-// the kernel keeps the rest of its shared-memory traffic conflict-free.
+// banded Toeplitz slice of the filter row (plane row r = image row
+// tile_r0 - R + r, plane column x = pixel tile_c0 + x).  An MMA whose A
+// comes from shared memory costs as long as reading its 4 KB there, so A
+// lives in tensor memory instead: the staging threads de-interleave each
+// input row in registers and write it straight into TMEM (tcgen05.st, one
+// lane per thread: five 16-column chunks = 20 columns per channel), and the
+// ky shift is applied there with tcgen05.shift, which moves every TMEM
+// lane's data to the lane below it -- inside each 32-lane quarter (the last
+// lane of a quarter keeps its data).  So the 128 TMEM lanes hold four bands
+// of 32 plane rows that overlap by 2R rows (band g: plane rows VB g .. VB g
+// + 31, VB = 32 - 2R); after ky shifts lane 32g + l holds plane row VB g + l
+// + ky, exact for l < VB.  A tile therefore has TH = 4 VB output rows (112
+// for 5 x 5 filters); 2R rows of each band overlap are staged twice.  Per
+// channel: 4 (2R + 1) MMAs of 128 x 16 x 32 (B, 512 bytes per ky, built
+// once per CTA, from shared memory) and 3 x 2R shifts of 8 columns; 12
+// accumulators (192 TMEM columns).  Shared memory carries only the raw
+// input rows, the B slices and the staged output rows.
 //
 // Persistent and warp-specialised: one CTA per SM walks a contiguous range
 // of the launch's tiles (horizontal neighbours back to back, so their shared
 // input columns are L2 hits).  Ten warps in four roles:
 //  - loader (warp 8, one lane): loads the tile's input -- 96+ pixels
-//    (tile_c0-16 ..) of 128 + 2R rows of the bottom-up image -- as ONE 2-D
+//    (tile_c0-16 ..) of TH + 2R rows of the bottom-up image -- as ONE 2-D
 //    TMA box (304-byte rows, a tensor map per distinct image) into a ring of
-//    raw buffers, up to SLOTS tiles ahead.  Views a tensor map cannot
-//    describe (not a whole-row NATURAL view, unaligned, or more distinct
-//    images than maps) are staged by the staging warps with plain loads;
-//  - staging (warps 4-7): replace rows and pixels beyond the image (TMA
-//    fills them with zeros) by the edge row / pixel, then de-interleave the
-//    rows by byte permutes into one of two plane buffers;
-//  - MMA (warp 9, one elected lane): issues the tile's MMAs into one of two
-//    accumulator sets and commits them;
+//    raw buffers (2 to 4 slots, as shared memory allows), up to SLOTS tiles
+//    ahead.  Views a tensor map cannot describe (not a whole-row NATURAL
+//    view, unaligned, or more distinct images than maps) are staged by the
+//    staging warps with plain loads;
+//  - staging (warps 4-7, TMEM lane quarter = warp - 4): replace rows and
+//    pixels beyond the image (TMA fills them with zeros) by the edge row /
+//    pixel, then de-interleave thread st's band row by byte permutes and
+//    store its three channels into a ring of five TMEM operand slots;
+//  - MMA (warp 9, one elected lane): per channel issues the MMAs and shifts
+//    on the operand slot into one of two accumulator sets;
 //  - epilogue (warps 0-3, TMEM lane quarter = warp): reads its row's 3 x 64
 //    sums, packs them to bytes (clamp: saturate; wrap: low byte),
 //    re-interleaves RGB into a staged row, frees the accumulator set, and
 //    the four warps write the tile with coalesced 16-byte stores.
-// mbarriers order the roles (raw buffer filled / drained, planes written,
-// MMAs done = planes and accumulators readable, accumulators drained).
-// Every wait is bounded; a wait that expires sets the error word and the
-// CTA stops, waiting (bounded) for its own copies and MMAs before it frees
-// its tensor memory.  Reads outside the subscription but inside the image's
-// rows (NATURAL views hold whole rows) only meet zero filter weights.
-constexpr int kTcTW = 64, kTcTH = 128;
+// mbarriers order the roles (raw buffer filled / drained, operands written,
+// operand slot consumed, MMAs done = accumulators readable, accumulators
+// drained).  Every wait is bounded; a wait that expires sets
+// the error word and the CTA stops, waiting (bounded) for its own copies
+// and MMAs before it frees its tensor memory.  Reads outside the
+// subscription but inside the image's rows (NATURAL views hold whole rows)
+// only meet zero filter weights.
+constexpr int kTcTW = 64;
 constexpr int kTcThreads = 320;     // warps 0-3 epilogue, 4-7 staging, 8 loader, 9 MMA
 constexpr int kTcStageWarp0 = 4, kTcLoaderWarp = 8, kTcMmaWarp = 9;
 constexpr int kTcMaxR = 8;
 constexpr int kTcMaxKD = 2 * kTcMaxR + 1;
-constexpr int kTcChunks = 5;        // plane columns tile_c0-8 .. tile_c0+71 in 16-byte chunks
+constexpr int kTcChunks = 5;        // plane columns tile_c0-8 .. tile_c0+71 in 16-byte chunks (4 TMEM columns each)
 constexpr int kRawStride = 304;     // raw row (a TMA box row): pixels tile_c0-16 .. ; 19 x 16 B (odd: conflict-free)
 constexpr int kImgfMaps = 4;        // distinct images with a tensor map per launch
 constexpr int kOutStride = 208;     // staged output row: 192 B + padding (conflict-free 16-B stores)
-constexpr uint32_t kTcTmemCols = 512;  // two accumulator sets of 192 columns, 256 apart
+// Tensor memory: two accumulator sets of 192 columns (tile k in set k & 1,
+// channel c at 64 c) and a ring of five 24-column operand slots (channel
+// unit u = 3 k + c in slot u % 5; 5 chunks x 4 columns, shifted in 8-column
+// steps).
+constexpr uint32_t kTcTmemCols = 512;
+constexpr uint32_t kTcAccCols = 192, kTcOpCol0 = 2 * kTcAccCols, kTcOpCols = 24, kTcOpSlots = 5;
+static_assert(kTcOpCol0 + kTcOpSlots * kTcOpCols <= kTcTmemCols && 4 * kTcChunks <= kTcOpCols, "tensor memory");
 constexpr uint32_t kTcWaitPolls = 1u << 21;
 constexpr uint32_t kImgfErrTimeout = 1;
 constexpr int kSmemLimit = 227 * 1024 - 256;  // per-block opt-in limit, less the kernel's static shared memory
@@ -472,23 +308,22 @@ constexpr int kSmemLimit = 227 * 1024 - 256;  // per-block opt-in limit, less th
 template <int R>
 struct TcGeo {
     static constexpr int KD = 2 * R + 1;
-    static constexpr int ROWS = kTcTH + 2 * R;        // plane rows
-    static constexpr int CH = ROWS * 16;              // bytes per 16-column chunk of a plane
-    static constexpr int PLANE = kTcChunks * CH;
-    static constexpr int PLANES = 3 * PLANE;          // one buffer of the three planes
+    static constexpr int VB = 32 - 2 * R;             // output rows per 32-lane band
+    static constexpr int TH = 4 * VB;                 // output rows per tile
+    static constexpr int ROWS = TH + 2 * R;           // input rows per tile (TMA box rows)
     static constexpr int RAW = (ROWS * kRawStride + 127) / 128 * 128;  // slot stride (TMA destinations 128-B aligned)
-    static constexpr int OUT = kTcTH * kOutStride;
-    static constexpr int OFF_RAW = (2 * PLANES + 127) / 128 * 128;
-    static constexpr int FIXED = OFF_RAW + OUT + KD * 512 + 128;
-    static constexpr int SLOTS = FIXED + 3 * RAW <= kSmemLimit ? 3 : 2;
+    static constexpr int OUT = TH * kOutStride;
+    static constexpr int OFF_RAW = 0;
+    static constexpr int FIXED = OFF_RAW + OUT + KD * 512 + 256;
+    static constexpr int SLOTS = FIXED + 4 * RAW <= kSmemLimit ? 4 : (FIXED + 3 * RAW <= kSmemLimit ? 3 : 2);
     static constexpr int OFF_OUT = OFF_RAW + SLOTS * RAW;
     static constexpr int OFF_B = OFF_OUT + OUT;
     static constexpr int OFF_BAR = OFF_B + KD * 512;
-    static constexpr int SMEM = OFF_BAR + 128;
-    static_assert(CH % 16 == 0 && OFF_RAW % 128 == 0 && RAW % 128 == 0 && OFF_OUT % 16 == 0 && OFF_B % 16 == 0 &&
+    static constexpr int SMEM = OFF_BAR + 256;
+    static_assert(RAW % 128 == 0 && OFF_OUT % 16 == 0 && OFF_B % 16 == 0 &&
                       OFF_BAR % 8 == 0,
                   "alignment");
-    static_assert(CH / 16 < (1 << 14), "leading byte offset field");
+    static_assert(VB >= 16, "band");
     static_assert(SMEM <= kSmemLimit, "shared memory");
 };
 
@@ -498,7 +333,7 @@ constexpr uint32_t kTcIdesc = (2u << 4) | (0u << 7) | (1u << 10) | ((16u >> 3) <
 
 template <int MAXI>
 struct ImgfParamsTc {
-    CUtensorMap maps[kImgfMaps];  // the input images (u32 elements, 76 x (128 + 2R) boxes)
+    CUtensorMap maps[kImgfMaps];  // the input images (u32 elements, 76 x (TH + 2R) boxes)
     int map_of[MAXI];             // tensor map of each item, -1: plain loads
     int8_t f[kTcMaxKD][kTcMaxKD];
     int n_items;
@@ -542,13 +377,20 @@ __device__ __forceinline__ void tc_arrive(uint32_t bar) {
     asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
-__device__ __forceinline__ void tc_mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t accumulate) {
+// A from tensor memory ([a] = TMEM address of the 128 x 32-byte operand).
+__device__ __forceinline__ void tc_mma_i8_ta(uint32_t tmem_d, uint32_t tmem_a, uint64_t bdesc, uint32_t accumulate) {
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
         "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
-        "l"(adesc), "l"(bdesc), "r"(kTcIdesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u)
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "r"(tmem_a), "l"(bdesc), "r"(kTcIdesc), "r"(accumulate)
         : "memory");
+}
+
+// Every lane of the 8 columns at taddr takes the data of the lane above it
+// (lane + 1) within its 32-lane quarter; the quarter's last lane keeps its own.
+__device__ __forceinline__ void tc_shift(uint32_t taddr) {
+    asm volatile("tcgen05.shift.cta_group::1.down [%0];" ::"r"(taddr) : "memory");
 }
 
 __device__ __forceinline__ void tc_commit(uint32_t bar) {
@@ -592,6 +434,55 @@ __device__ __forceinline__ bool role_all(int id, bool v) {
 }
 __device__ __forceinline__ bool role_any(int id, bool v) { return !role_all(id, !v); }
 
+__device__ __forceinline__ void tc_st8(uint32_t taddr, const uint32_t (&v)[8]) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr), "r"(v[0]),
+                 "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7])
+                 : "memory");
+}
+__device__ __forceinline__ void tc_st4(uint32_t taddr, const uint32_t (&v)[4]) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x4.b32 [%0], {%1,%2,%3,%4};" ::"r"(taddr), "r"(v[0]), "r"(v[1]),
+                 "r"(v[2]), "r"(v[3])
+                 : "memory");
+}
+
+// Chunks Q0 .. Q0 + NQ - 1 of one input row into the warp's TMEM lanes: raw
+// bytes 48 q + 24 .. 48 q + 71 hold chunk q (16 pixels); the 16-byte loads
+// start at raw byte 48 Q0 + 16 (src points at raw byte 16 of the row).
+// Chunk q of channel c goes to columns 4 q .. 4 q + 3 of op[c].  Warp-wide:
+// every lane of the warp calls it.
+template <int Q0, int NQ>
+__device__ __forceinline__ void stage_chunks(const uint8_t* src, const uint32_t (&op)[3]) {
+    constexpr int kLoads = (48 * NQ + 8 + 15) / 16;
+    uint32_t w[4 * kLoads];
+#pragma unroll
+    for (int j = 0; j < kLoads; ++j) {
+        const uint4 v = *reinterpret_cast<const uint4*>(src + 48 * Q0 + 16 * j);
+        w[4 * j] = v.x;
+        w[4 * j + 1] = v.y;
+        w[4 * j + 2] = v.z;
+        w[4 * j + 3] = v.w;
+    }
+    uint32_t o[3][4 * NQ];
+#pragma unroll
+    for (int qq = 0; qq < NQ; ++qq)
+#pragma unroll
+        for (int g = 0; g < 4; ++g)
+            deinterleave4(w[12 * qq + 2 + 3 * g], w[12 * qq + 3 + 3 * g], w[12 * qq + 4 + 3 * g], o[0][4 * qq + g],
+                          o[1][4 * qq + g], o[2][4 * qq + g]);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const uint32_t col = op[c] + 4 * Q0;
+        if constexpr (NQ >= 2) {
+            const uint32_t v[8] = {o[c][0], o[c][1], o[c][2], o[c][3], o[c][4], o[c][5], o[c][6], o[c][7]};
+            tc_st8(col, v);
+        }
+        if constexpr (NQ == 3) {
+            const uint32_t v[4] = {o[c][8], o[c][9], o[c][10], o[c][11]};
+            tc_st4(col + 8, v);
+        }
+    }
+}
+
 struct TcTile {
     int item, r0, c0, tw, rows;
     int map;  // tensor map that stages the tile, -1: plain loads
@@ -600,7 +491,7 @@ struct TcTile {
 // Walks a CTA's contiguous tile range: tile g of the launch lies in item
 // `cur` (tile_start[cur] <= g < tile_start[cur + 1]); g only grows, so the
 // item index only moves forward.
-template <int MAXI>
+template <int MAXI, int TH>
 struct TcCursor {
     int cur;
     __device__ __forceinline__ TcCursor(const ImgfParamsTc<MAXI>& p, int g) {
@@ -620,9 +511,9 @@ struct TcCursor {
         TcTile t;
         t.item = cur;
         t.c0 = it.c0 + tx * kTcTW;
-        t.r0 = it.r0 + ty * kTcTH;
+        t.r0 = it.r0 + ty * TH;
         t.tw = min(kTcTW, it.c1 - t.c0);
-        t.rows = min(kTcTH, it.r1 - t.r0);
+        t.rows = min(TH, it.r1 - t.r0);
         t.map = p.map_of[cur];
         return t;
     }
@@ -634,18 +525,18 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
     using G = TcGeo<R>;
     constexpr int SLOTS = G::SLOTS;
     extern __shared__ __align__(128) uint8_t smem[];
-    uint8_t* const planes = smem;
     uint8_t* const raws = smem + G::OFF_RAW;
     uint8_t* const ost = smem + G::OFF_OUT;
     uint8_t* const bsm = smem + G::OFF_B;
     uint64_t* const bars = reinterpret_cast<uint64_t*>(smem + G::OFF_BAR);
     uint64_t* const full = bars;              // [SLOTS]: raw buffer filled
-    uint64_t* const raw_free = bars + 3;      // [SLOTS]: raw buffer drained (4 staging warps)
-    uint64_t* const planes_full = bars + 6;   // [2]: plane buffer b written (4 staging warps)
-    uint64_t* const mma_done = bars + 8;      // [2]: accumulator set b written, planes b read
-    uint64_t* const acc_free = bars + 10;     // [2]: accumulator set b drained (4 epilogue warps)
-    uint64_t* const teardown = bars + 12;
-    uint32_t* const tmem_slot = reinterpret_cast<uint32_t*>(bars + 13);
+    uint64_t* const raw_free = bars + 4;      // [SLOTS]: raw buffer drained (4 staging warps)
+    uint64_t* const op_full = bars + 8;       // [2]: operands of tile k (k & 1) written (4 staging warps)
+    uint64_t* const mma_done = bars + 10;     // [2]: accumulator set written
+    uint64_t* const acc_free = bars + 12;     // [2]: accumulator set drained (4 epilogue warps)
+    uint64_t* const op_free = bars + 14;      // [5]: operand slot consumed by its unit's MMAs and shifts
+    uint64_t* const teardown = bars + 19;
+    uint32_t* const tmem_slot = reinterpret_cast<uint32_t*>(bars + 20);
     __shared__ volatile int s_fail;
 
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -660,8 +551,10 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(&full[i])));
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(tc_smem(&raw_free[i])));
         }
+        for (int i = 0; i < static_cast<int>(kTcOpSlots); ++i)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(&op_free[i])));
         for (int i = 0; i < 2; ++i) {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(tc_smem(&planes_full[i])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(tc_smem(&op_full[i])));
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(tc_smem(&mma_done[i])));
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(tc_smem(&acc_free[i])));
         }
@@ -702,7 +595,7 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
         // drained the slot's previous tile.  Box row j holds buffer row
         // y + j, i.e. image row t.r0 - R + ROWS - 1 - j.
         if (lane == 0) {
-            TcCursor<MAXI> cur(p, t_begin);
+            TcCursor<MAXI, G::TH> cur(p, t_begin);
             int issued = 0;
             for (; issued < ntiles; ++issued) {
                 const int k = issued, s = k % SLOTS;
@@ -737,12 +630,11 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
         }
     } else if (warp == kTcMmaWarp) {
         // ================= MMA issue =================
-        const uint64_t adesc0 = tc_desc(tc_smem(planes), G::CH, 128);
         const uint64_t bdesc0 = tc_desc(tc_smem(bsm), 256, 128);
         for (int k = 0; k < ntiles; ++k) {
             if (__any_sync(0xffffffffu, s_fail != 0)) break;
             const int b = k & 1;
-            bool ok = tc_wait(tc_smem(&planes_full[b]), (k >> 1) & 1);
+            bool ok = tc_wait(tc_smem(&op_full[b]), (k >> 1) & 1);
             // Accumulator set b is free once the epilogue has drained tile k - 2.
             if (ok && k >= 2) ok = tc_wait(tc_smem(&acc_free[b]), ((k - 2) >> 1) & 1);
             if (!__all_sync(0xffffffffu, ok)) {
@@ -751,17 +643,25 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             if (tc_elect()) {
-                const uint64_t ab = adesc0 + static_cast<uint64_t>((b * G::PLANES) >> 4);
-                const uint32_t acc = tmem + 256u * b;
+#pragma unroll 1
+                for (int c = 0; c < 3; ++c) {
+                    const int u = 3 * k + c;
+                    const uint32_t op = tmem + kTcOpCol0 + kTcOpCols * static_cast<uint32_t>(u % kTcOpSlots);
+                    const uint32_t acc = tmem + kTcAccCols * b + 64u * c;
 #pragma unroll
-                for (int c = 0; c < 3; ++c)
+                    for (int ky = 0; ky < G::KD; ++ky) {
 #pragma unroll
-                    for (int tg = 0; tg < 4; ++tg)
-#pragma unroll
-                        for (int ky = 0; ky < G::KD; ++ky)
-                            tc_mma_i8(acc + static_cast<uint32_t>((c * 4 + tg) * 16),
-                                      ab + static_cast<uint64_t>((c * G::PLANE + tg * G::CH + ky * 16) >> 4),
-                                      bdesc0 + static_cast<uint64_t>((ky * 512) >> 4), ky > 0 ? 1u : 0u);
+                        for (int tg = 0; tg < 4; ++tg)
+                            tc_mma_i8_ta(acc + 16 * tg, op + 4 * tg, bdesc0 + static_cast<uint64_t>((ky * 512) >> 4),
+                                         ky > 0 ? 1u : 0u);
+                        if (ky + 1 < G::KD) {
+                            tc_shift(op);
+                            tc_shift(op + 8);
+                            tc_shift(op + 16);
+                        }
+                    }
+                    tc_commit(tc_smem(&op_free[u % kTcOpSlots]));
+                }
                 tc_commit(tc_smem(&mma_done[b]));
             }
             __syncwarp();
@@ -769,12 +669,12 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
     } else if (warp >= kTcStageWarp0) {
         // ================= staging =================
         const int st = tid - 32 * kTcStageWarp0;  // 0..127
-        TcCursor<MAXI> cur(p, t_begin);
+        TcCursor<MAXI, G::TH> cur(p, t_begin);
         for (int k = 0; k < ntiles; ++k) {
             if (role_any(2, s_fail != 0)) break;
             const TcTile t = cur.at(p, t_begin + k);
             const pmb_imgf_item& it = p.items[t.item];
-            const int s = k % SLOTS, b = k & 1;
+            const int s = k % SLOTS;
             uint8_t* raw = raws + s * G::RAW;
             bool ok = tc_wait(tc_smem(&full[s]), (k / SLOTS) & 1);
             const int mlo = max(0, it.r0 - R), mhi = min(it.height - 1, it.r1 - 1 + R);
@@ -826,58 +726,48 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
                     }
                 }
             }
-            // Planes b are free once the MMAs of tile k - 2 have read them.
-            if (k >= 2) ok = tc_wait(tc_smem(&mma_done[b]), ((k - 2) >> 1) & 1) && ok;
+            // Operand slot of unit u = 3k + c is free once the MMAs and shifts of
+            // unit u - 5 are done.
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                const int u = 3 * k + c;
+                if (u >= static_cast<int>(kTcOpSlots))
+                    ok = ok && tc_wait(tc_smem(&op_free[u % kTcOpSlots]), ((u / static_cast<int>(kTcOpSlots)) - 1) & 1);
+            }
             if (!role_all(2, ok)) {  // also: raw rows complete (loads and edge fills)
                 s_fail = 1;
                 break;
             }
-            // De-interleave: item e is plane row r = e % ROWS, chunks 3h .. 3h+2
-            // (h = e / ROWS; chunk 5 does not exist).  Consecutive threads take
-            // consecutive rows: the 16-byte loads (row stride 19 x 16 B) and the
-            // stores (16 B apart) are conflict-free.
-            uint8_t* pl = planes + b * G::PLANES;
-            for (int e = st; e < 2 * G::ROWS; e += 128) {
-                const int h = e >= G::ROWS ? 1 : 0, r = e - h * G::ROWS;
-                // Raw bytes 48 q + 24 .. 48 q + 71 hold chunk q; the loads cover
-                // 48 q0 + 16 .. 48 q0 + 16 * (3 nq + 1) (16-byte aligned).
-                const uint8_t* src = raw + (G::ROWS - 1 - r) * kRawStride + 144 * h + 16;
-                uint32_t w[3 * 12 + 4];
+            // De-interleave: thread st stages band row st (band st / 32, plane row
+            // VB (st / 32) + st % 32) into TMEM lane st of the three operand
+            // slots.  Consecutive threads take consecutive rows, so the 16-byte
+            // loads (row stride 19 x 16 B) are conflict-free.
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            {
+                const int r = G::VB * (st >> 5) + (st & 31);
+                const uint8_t* const src = raw + (G::ROWS - 1 - r) * kRawStride + 16;
+                const uint32_t lanes = tmem + (static_cast<uint32_t>(st & ~31) << 16);
+                uint32_t op[3];
 #pragma unroll
-                for (int j = 0; j < 10; ++j) {
-                    if (h == 1 && j >= 7) break;  // chunks 3, 4: 7 loads
-                    const uint4 v = *reinterpret_cast<const uint4*>(src + 16 * j);
-                    w[4 * j] = v.x;
-                    w[4 * j + 1] = v.y;
-                    w[4 * j + 2] = v.z;
-                    w[4 * j + 3] = v.w;
-                }
-#pragma unroll
-                for (int qq = 0; qq < 3; ++qq) {
-                    if (h == 1 && qq == 2) break;
-                    const int q = 3 * h + qq;
-                    uint32_t o[3][4];
-#pragma unroll
-                    for (int g = 0; g < 4; ++g)
-                        deinterleave4(w[12 * qq + 2 + 3 * g], w[12 * qq + 3 + 3 * g], w[12 * qq + 4 + 3 * g], o[0][g],
-                                      o[1][g], o[2][g]);
-#pragma unroll
-                    for (int c = 0; c < 3; ++c)
-                        *reinterpret_cast<uint4*>(pl + c * G::PLANE + q * G::CH + r * 16) =
-                            make_uint4(o[c][0], o[c][1], o[c][2], o[c][3]);
-                }
+                for (int c = 0; c < 3; ++c)
+                    op[c] = lanes + kTcOpCol0 + kTcOpCols * static_cast<uint32_t>((3 * k + c) % kTcOpSlots);
+                stage_chunks<0, 3>(src, op);  // raw bytes 16 .. 175
+                stage_chunks<3, 2>(src, op);  // raw bytes 160 .. 271
             }
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // planes, then the tensor core reads them
+            asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
             if (lane == 0) {
-                tc_arrive(tc_smem(&planes_full[b]));
+                tc_arrive(tc_smem(&op_full[k & 1]));
                 tc_arrive(tc_smem(&raw_free[s]));
             }
         }
     } else {
         // ================= epilogue =================
-        const int q = warp, row = 32 * q + lane;
-        TcCursor<MAXI> cur(p, t_begin);
+        // Lane l < VB of quarter q holds output row VB q + l of the tile.
+        const int q = warp, row = G::VB * q + lane;
+        const bool valid_lane = lane < G::VB;
+        TcCursor<MAXI, G::TH> cur(p, t_begin);
         for (int k = 0; k < ntiles; ++k) {
             if (role_any(1, s_fail != 0)) break;
             const TcTile t = cur.at(p, t_begin + k);
@@ -894,8 +784,8 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
                 uint32_t v[4][16];
 #pragma unroll
                 for (int tg = 0; tg < 4; ++tg)
-                    tc_ld16(tmem + 256u * b + (static_cast<uint32_t>(32 * q) << 16) +
-                                static_cast<uint32_t>((c * 4 + tg) * 16),
+                    tc_ld16(tmem + kTcAccCols * b + (static_cast<uint32_t>(32 * q) << 16) +
+                                static_cast<uint32_t>(64 * c + 16 * tg),
                             v[tg]);
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
@@ -913,7 +803,7 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
             if (lane == 0) tc_arrive(tc_smem(&acc_free[b]));
             uint8_t* const orow = ost + row * kOutStride;
 #pragma unroll
-            for (int g = 0; g < 16; g += 4) {
+            for (int g = 0; g < (valid_lane ? 16 : 0); g += 4) {
                 uint32_t d[12];
 #pragma unroll
                 for (int h = 0; h < 4; ++h) {
@@ -930,19 +820,21 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
             role_sync(1);  // the staged tile is complete
             uint8_t* const obase = it.out + static_cast<int64_t>(t.r0 - it.out_row0) * it.out_pitch +
                                    3 * (t.c0 - it.out_col0);
-            if (t.tw == kTcTW && t.rows == kTcTH &&
+            if (t.tw == kTcTW && t.rows == G::TH &&
                 ((reinterpret_cast<uintptr_t>(obase) | static_cast<uintptr_t>(it.out_pitch)) & 15) == 0) {
-                // Full tile: 12 x 16 B per thread, all loads first.
-                uint4 v[12];
+                // Full tile: TH x 12 16-byte pieces, all loads first.
+                constexpr int kPer = (G::TH * 12 + 127) / 128;
+                uint4 v[kPer];
 #pragma unroll
-                for (int i = 0; i < 12; ++i) {
+                for (int i = 0; i < kPer; ++i) {
                     const int e = tid + 128 * i, r = e / 12, c = e - r * 12;
-                    v[i] = *reinterpret_cast<const uint4*>(ost + r * kOutStride + 16 * c);
+                    if (e < G::TH * 12) v[i] = *reinterpret_cast<const uint4*>(ost + r * kOutStride + 16 * c);
                 }
 #pragma unroll
-                for (int i = 0; i < 12; ++i) {
+                for (int i = 0; i < kPer; ++i) {
                     const int e = tid + 128 * i, r = e / 12, c = e - r * 12;
-                    *reinterpret_cast<uint4*>(obase + static_cast<int64_t>(r) * it.out_pitch + 16 * c) = v[i];
+                    if (e < G::TH * 12)
+                        *reinterpret_cast<uint4*>(obase + static_cast<int64_t>(r) * it.out_pitch + 16 * c) = v[i];
                 }
             } else if (t.tw == kTcTW &&
                        ((reinterpret_cast<uintptr_t>(obase) | static_cast<uintptr_t>(it.out_pitch)) & 15) == 0) {
@@ -1077,48 +969,6 @@ int launch_t(const pmb_imgf_item* items, int n, const int8_t* filter, cudaStream
     return PMB_SUCCESS;
 }
 
-template <int R, int MODE, int MAXI>
-int launch_fast(const pmb_imgf_item* items, int n, const int8_t* filter, cudaStream_t s) {
-    using G = GeoF<R>;
-    ImgfParamsF<R, MAXI> p;
-    for (int ky = 0; ky < G::KD; ++ky)
-        for (int k = 0; k < 4; ++k)
-            for (int w = 0; w < G::NW; ++w) {
-                uint32_t word = 0;
-                for (int b = 0; b < 4; ++b) {
-                    const int kx = 4 * w + b - G::OFF - k;
-                    if (kx >= 0 && kx < G::KD)
-                        word |= static_cast<uint32_t>(
-                                    static_cast<uint8_t>(filter[ky * PMB_IMGF_MAX_FILTER_DIM + kx]))
-                                << (8 * b);
-                }
-                p.pat[ky][k][w] = word;
-            }
-    int64_t total = 0;
-    int m = 0;
-    for (int i = 0; i < n; ++i) {
-        const pmb_imgf_item& it = items[i];
-        if (it.r0 == it.r1 || it.c0 == it.c1) continue;
-        const int txs = (it.c1 - it.c0 + kTW - 1) / kTW;
-        const int tys = (it.r1 - it.r0 + kTH - 1) / kTH;
-        p.items[m] = it;
-        p.tiles_x[m] = txs;
-        p.tile_start[m] = static_cast<int>(total);
-        total += static_cast<int64_t>(txs) * tys;
-        ++m;
-    }
-    if (m == 0) return PMB_SUCCESS;
-    if (total > 0x7fffffffLL) return pmb::fail(PMB_BEYOND_LIMITS, "too many tiles: %lld", (long long)total);
-    p.n_items = m;
-    p.tile_start[m] = static_cast<int>(total);
-    constexpr int CB = R <= 2 ? 3 : 1;
-    int max_tiles = 0;
-    for (int i = 0; i < m; ++i) max_tiles = std::max(max_tiles, p.tile_start[i + 1] - p.tile_start[i]);
-    imgf_fast_kernel<R, MODE, MAXI, CB><<<dim3(static_cast<unsigned>(max_tiles), static_cast<unsigned>(m)), kThreads, 0, s>>>(p);
-    PMB_CUDA_TRY(cudaGetLastError());
-    return PMB_SUCCESS;
-}
-
 // Device address of the stencil's error word on the current device.
 __device__ uint32_t g_imgf_err;
 
@@ -1151,7 +1001,7 @@ int launch_tc(const pmb_imgf_item* items, int n, const int8_t* filter, cudaStrea
         const pmb_imgf_item& it = items[i];
         if (it.r0 == it.r1 || it.c0 == it.c1) continue;
         const int txs = (it.c1 - it.c0 + kTcTW - 1) / kTcTW;
-        const int tys = (it.r1 - it.r0 + kTcTH - 1) / kTcTH;
+        const int tys = (it.r1 - it.r0 + G::TH - 1) / G::TH;
         p.items[m] = it;
         p.tiles_x[m] = txs;
         p.tile_start[m] = static_cast<int>(total);
