@@ -488,33 +488,53 @@ struct TcTile {
     int map;  // tensor map that stages the tile, -1: plain loads
 };
 
-// Walks a CTA's contiguous tile range: tile g of the launch lies in item
-// `cur` (tile_start[cur] <= g < tile_start[cur + 1]); g only grows, so the
-// item index only moves forward.
+// Walks a CTA's contiguous tile range, one tile after the other: tile g of
+// the launch lies in item `cur` (tile_start[cur] <= g < tile_start[cur + 1]).
+// The item's description is kept in registers and reloaded only when the
+// walk enters the next item, so a step costs a few register operations, not
+// a chain of dependent loads from the parameter space.
 template <int MAXI, int TH>
 struct TcCursor {
-    int cur;
-    __device__ __forceinline__ TcCursor(const ImgfParamsTc<MAXI>& p, int g) {
+    int cur, g, end_g, tx, ty, txs, map;
+    pmb_imgf_item it;
+    __device__ __forceinline__ void enter(const ImgfParamsTc<MAXI>& p) {
+        it = p.items[cur];
+        txs = p.tiles_x[cur];
+        end_g = p.tile_start[cur + 1];
+        map = p.map_of[cur];
+    }
+    __device__ __forceinline__ TcCursor(const ImgfParamsTc<MAXI>& p, int g0) : g(g0) {
         int lo = 0, hi = p.n_items - 1;
         while (lo < hi) {
             const int mid = (lo + hi + 1) >> 1;
-            if (p.tile_start[mid] <= g) lo = mid; else hi = mid - 1;
+            if (p.tile_start[mid] <= g0) lo = mid; else hi = mid - 1;
         }
         cur = lo;
+        enter(p);
+        const int local = g0 - p.tile_start[cur];
+        ty = local / txs;
+        tx = local - ty * txs;
     }
-    __device__ __forceinline__ TcTile at(const ImgfParamsTc<MAXI>& p, int g) {
-        while (g >= p.tile_start[cur + 1]) ++cur;
-        const pmb_imgf_item& it = p.items[cur];
-        const int local = g - p.tile_start[cur];
-        const int txs = p.tiles_x[cur];
-        const int ty = local / txs, tx = local - ty * txs;
+    __device__ __forceinline__ void next(const ImgfParamsTc<MAXI>& p) {
+        ++g;
+        if (++tx == txs) {
+            tx = 0;
+            ++ty;
+        }
+        if (g >= end_g && cur + 1 < p.n_items) {
+            ++cur;  // every item of the launch has at least one tile
+            enter(p);
+            tx = ty = 0;
+        }
+    }
+    __device__ __forceinline__ TcTile tile() const {
         TcTile t;
         t.item = cur;
         t.c0 = it.c0 + tx * kTcTW;
         t.r0 = it.r0 + ty * TH;
         t.tw = min(kTcTW, it.c1 - t.c0);
         t.rows = min(TH, it.r1 - t.r0);
-        t.map = p.map_of[cur];
+        t.map = map;
         return t;
     }
 };
@@ -599,18 +619,19 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
             int issued = 0;
             for (; issued < ntiles; ++issued) {
                 const int k = issued, s = k % SLOTS;
+                if (k > 0) cur.next(p);
                 if (s_fail) break;
                 if (k >= SLOTS && !tc_wait(tc_smem(&raw_free[s]), ((k / SLOTS) - 1) & 1)) {
                     s_fail = 1;
                     break;
                 }
-                const TcTile t = cur.at(p, t_begin + k);
+                const TcTile t = cur.tile();
                 const uint32_t bar = tc_smem(&full[s]);
                 if (t.map < 0) {
                     tc_arrive(bar);  // staged by the staging warps' own loads
                     continue;
                 }
-                const pmb_imgf_item& it = p.items[t.item];
+                const pmb_imgf_item& it = cur.it;
                 const int x = 3 * (t.c0 - 16) / 4;                          // u32 elements; 16-byte multiple
                 const int y = it.height - 1 - (t.r0 - R + G::ROWS - 1);     // may be negative: zero-filled rows
                 asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
@@ -672,8 +693,9 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
         TcCursor<MAXI, G::TH> cur(p, t_begin);
         for (int k = 0; k < ntiles; ++k) {
             if (role_any(2, s_fail != 0)) break;
-            const TcTile t = cur.at(p, t_begin + k);
-            const pmb_imgf_item& it = p.items[t.item];
+            if (k > 0) cur.next(p);
+            const TcTile t = cur.tile();
+            const pmb_imgf_item& it = cur.it;
             const int s = k % SLOTS;
             uint8_t* raw = raws + s * G::RAW;
             bool ok = tc_wait(tc_smem(&full[s]), (k / SLOTS) & 1);
@@ -770,8 +792,9 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
         TcCursor<MAXI, G::TH> cur(p, t_begin);
         for (int k = 0; k < ntiles; ++k) {
             if (role_any(1, s_fail != 0)) break;
-            const TcTile t = cur.at(p, t_begin + k);
-            const pmb_imgf_item& it = p.items[t.item];
+            if (k > 0) cur.next(p);
+            const TcTile t = cur.tile();
+            const pmb_imgf_item& it = cur.it;
             const int b = k & 1;
             if (!role_all(1, tc_wait(tc_smem(&mma_done[b]), (k >> 1) & 1))) {
                 s_fail = 1;
