@@ -410,6 +410,36 @@ size_t pmb_gemm_workspace_bytes(int M, int N, int K);
 int pmb_sgemm_bf16x3(int M, int N, int K, float alpha, const float* A, int64_t lda, const float* B, int64_t ldb,
                      float beta, float* C, int64_t ldc, void* workspace, size_t ws_bytes, void* stream);
 
+/* One product of a grouped call: C = alpha*A*B + beta*C, row-major fp32
+ * device operands as in pmb_sgemm_bf16x3. */
+typedef struct pmb_gemm_problem {
+    int M, N, K;
+    float alpha;
+    const float* A;
+    int64_t lda;
+    const float* B;
+    int64_t ldb;
+    float beta;
+    float* C;
+    int64_t ldc;
+} pmb_gemm_problem;
+
+/* Device workspace (256-byte aligned) pmb_sgemm_bf16x3_grouped needs for
+ * `count` problems. */
+size_t pmb_gemm_grouped_workspace_bytes(const pmb_gemm_problem* problems, int count);
+
+/* `count` independent BF16x3 products of different shapes (each with the
+ * arithmetic of pmb_sgemm_bf16x3) in one launch of the product kernel per 24
+ * products, after one split launch per product: the tiles of all products
+ * go to the CTA pairs of one grid, so small products share the GPU instead
+ * of each filling a launch of its own.  `problems` is a host array; the
+ * products must not overlap in C.  Word 1 of the workspace is the error word
+ * (pmb_scratch_error).  No counterpart in the reference, whose subtasks each
+ * call cublasSgemm (matrixMultiplyBlasCUDA.cu:54-77); the runtime's batch
+ * hook of the matrixMultiplyBlas app calls it for all subtasks of a task. */
+int pmb_sgemm_bf16x3_grouped(const pmb_gemm_problem* problems, int count, void* workspace, size_t workspace_bytes,
+                             void* stream);
+
 /* Plain GPU form of the same product: FP32 SIMT, 64 x 64 shared-memory
  * tiles, no tensor cores (the one-task-at-a-time FP32 baseline). */
 int pmb_sgemm_plain(int M, int N, int K, float alpha, const float* A, int64_t lda, const float* B, int64_t ldb,

@@ -156,3 +156,37 @@ def test_product_after_producer_on_same_stream(cuda, M, N, K):
     s.synchronize()
     norm, _ = errors(C.cpu().numpy(), A, B)
     assert norm <= NORM_TOL, norm
+
+
+AUTOTUNE_SCRIPT = r"""
+import sys, numpy as np, torch
+sys.path.insert(0, sys.argv[1])
+from unicorn_b200 import ops
+rng = np.random.default_rng(1)
+worst = 0.0
+for (M, N, K) in [(1024, 1024, 1024), (1024, 1024, 1024), (300, 2000, 700), (4096, 512, 256), (96, 96, 4096)]:
+    A = rng.uniform(-1, 1, (M, K)).astype(np.float32)
+    B = rng.uniform(-1, 1, (K, N)).astype(np.float32)
+    C, ws = ops.sgemm(torch.from_numpy(A).cuda(), torch.from_numpy(B).cuda())
+    torch.cuda.synchronize()
+    assert ops.scratch_error(ws) == 0
+    ref = A.astype(np.float64) @ B.astype(np.float64)
+    worst = max(worst, float(np.linalg.norm(C.cpu().numpy() - ref) / np.linalg.norm(ref)))
+print("worst", worst)
+"""
+
+
+def test_autotuned_products_match_fp64():
+    """PMB_GEMM_AUTOTUNE=1: the first product of a shape class times the three
+    product kernels on its own operands (C written by each in turn) and keeps
+    the fastest; every result, tuned or cached, meets the normwise bar."""
+    import os
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    p = subprocess.run([sys.executable, "-c", AUTOTUNE_SCRIPT, root], capture_output=True, text=True, timeout=600,
+                       env=dict(os.environ, PMB_GEMM_AUTOTUNE="1"))
+    assert p.returncode == 0, p.stdout + p.stderr
+    worst = float(p.stdout.split("worst")[-1])
+    assert worst <= NORM_TOL, worst

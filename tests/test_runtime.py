@@ -44,8 +44,9 @@ def selftest():
     return SELFTEST
 
 
-def run(cmd, timeout=300):
-    p = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout)
+def run(cmd, timeout=300, env=None):
+    p = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout,
+                       env=None if env is None else dict(os.environ, **env))
     return p.returncode, p.stdout + p.stderr
 
 
@@ -124,13 +125,17 @@ def test_reference_int_matrix_multiply_app_cpu_mode(n):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("batch", ["grouped", "per_subtask"])
 @pytest.mark.parametrize("n", ["1024", "4096"])
-def test_reference_matrix_multiply_app_gpu_mode(n):
+def test_reference_matrix_multiply_app_gpu_mode(n, batch):
     """The unchanged matrixMultiplyBlas app, parallel mode 2 (local GPU): its
-    subtasks run matrixMultiply_cudaLaunchFunc of libpmb_app_matrixMultiplyBlas
-    (the tcgen05 BF16x3 GEMM) and the app compares them with its serial
-    cblas_sgemm at relative 1e-5 per element."""
-    rc, out = run([app_or_skip(MM_APP), "1", "2", "0", n], timeout=600)
+    subtasks run on the tcgen05 BF16x3 GEMM of libpmb_app_matrixMultiplyBlas --
+    through its batch hook (each half of a task's C blocks as one grouped
+    product launch) or, with PMB_NO_BATCH=1, through matrixMultiply_cudaLaunchFunc
+    per subtask -- and the app compares them with its serial cblas_sgemm at
+    relative 1e-5 per element."""
+    env = {"PMB_NO_BATCH": "1"} if batch == "per_subtask" else None
+    rc, out = run([app_or_skip(MM_APP), "1", "2", "0", n], timeout=600, env=env)
     assert rc == 0 and "Serial Comparison Test Passed" in out and "Failed" not in out, out
 
 

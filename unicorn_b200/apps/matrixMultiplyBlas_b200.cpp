@@ -7,12 +7,21 @@
 // product runs on the tcgen05 BF16x3 kernel instead of cublasSgemm.  The split
 // buffers the kernel needs are cached per stream, so a callback allocates
 // only when a stream first sees a larger problem.
+//
+// A batch hook lets the runtime run the subtasks of a task (NATURAL views) in
+// groups: the C blocks of a group are one grouped product launch
+// (pmb_sgemm_bf16x3_grouped) instead of one split + product launch pair per
+// subtask.  Two groups per task, so the second group's staging overlaps the
+// first group's products.
 #include "matrixMultiplyBlas_b200.h"
 
 #include <map>
 #include <mutex>
+#include <vector>
 
 #include "pmb_capi.h"
+
+extern "C" int pmb_runtime_register_batch_groups(void* subtask_gpu_custom, void* batch_fn, int groups);
 
 namespace matrixMultiplyBlas {
 
@@ -46,6 +55,54 @@ int workspace_for(void* stream, size_t need, void** out) {
     *out = w.ptr;
     return PMB_SUCCESS;
 }
+
+// The C block of one subtask as a product (false: the subtask has no block).
+bool problem_for(const matrixMultiplyTaskConf* conf, const pmSubtaskInfo& si, pmb_gemm_problem& q) {
+    size_t offset = 0, height = 0;
+    pmSplitInfo split = si.splitInfo;
+    if (!GetSplitData(&offset, &height, const_cast<matrixMultiplyTaskConf*>(conf), split)) return false;
+    const int n = static_cast<int>(conf->matrixDim), bd = static_cast<int>(conf->blockDim);
+    const pmMemInfo& a = si.memInfo[kMatrixA];
+    const pmMemInfo& b = si.memInfo[kMatrixB];
+    const pmMemInfo& c = si.memInfo[kMatrixC];
+    q.M = static_cast<int>(height);
+    q.N = bd;
+    q.K = n;
+    q.alpha = 1.0f;
+    q.A = static_cast<const float*>(a.ptr);
+    q.lda = n;
+    q.B = static_cast<const float*>(b.ptr);
+    q.ldb = b.visibilityType == SUBSCRIPTION_NATURAL ? n : bd;
+    q.beta = 0.0f;
+    q.C = static_cast<float*>(c.ptr);
+    q.ldc = c.visibilityType == SUBSCRIPTION_NATURAL ? n : bd;
+    return true;
+}
+
+pmStatus matrixMultiply_batch(const pmTaskInfo* task, const pmDeviceInfo*, const pmSubtaskInfo* subtasks,
+                              unsigned long count, void* stream) {
+    const matrixMultiplyTaskConf* conf = static_cast<const matrixMultiplyTaskConf*>(task->taskConf);
+    std::vector<pmb_gemm_problem> probs;
+    probs.reserve(count);
+    for (unsigned long i = 0; i < count; ++i) {
+        pmb_gemm_problem q;
+        if (problem_for(conf, subtasks[i], q)) probs.push_back(q);
+    }
+    if (probs.empty()) return pmSuccess;
+    const size_t need = pmb_gemm_grouped_workspace_bytes(probs.data(), static_cast<int>(probs.size()));
+    void* ws = nullptr;
+    int st = workspace_for(stream, need, &ws);
+    if (st == PMB_SUCCESS)
+        st = pmb_sgemm_bf16x3_grouped(probs.data(), static_cast<int>(probs.size()), ws, need, stream);
+    return st == PMB_SUCCESS ? pmSuccess : static_cast<pmStatus>(st);
+}
+
+struct Registrar {
+    Registrar() {
+        pmb_runtime_register_batch_groups(reinterpret_cast<void*>(&matrixMultiply_cudaLaunchFunc),
+                                          reinterpret_cast<void*>(&matrixMultiply_batch), 2);
+    }
+} g_registrar;
 
 }  // namespace
 

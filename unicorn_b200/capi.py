@@ -38,6 +38,24 @@ class PmbError(RuntimeError):
         self.status = status
 
 
+class GemmProblem(ctypes.Structure):
+    """Mirror of pmb_gemm_problem (include/pmb_capi.h)."""
+
+    _fields_ = [
+        ("M", ctypes.c_int32),
+        ("N", ctypes.c_int32),
+        ("K", ctypes.c_int32),
+        ("alpha", ctypes.c_float),
+        ("A", c_void_p),
+        ("lda", c_int64),
+        ("B", c_void_p),
+        ("ldb", c_int64),
+        ("beta", ctypes.c_float),
+        ("C", c_void_p),
+        ("ldc", c_int64),
+    ]
+
+
 class ImgfItem(ctypes.Structure):
     """Mirror of pmb_imgf_item (include/pmb_capi.h)."""
 
@@ -146,6 +164,8 @@ _SIGS = {
     "pmb_gemm_workspace_bytes": (c_size_t, [c_int, c_int, c_int]),
     "pmb_sgemm_bf16x3": (c_int, [c_int, c_int, c_int, ctypes.c_float, c_void_p, c_int64, c_void_p, c_int64,
                                  ctypes.c_float, c_void_p, c_int64, c_void_p, c_size_t, c_void_p]),
+    "pmb_gemm_grouped_workspace_bytes": (c_size_t, [c_void_p, c_int]),
+    "pmb_sgemm_bf16x3_grouped": (c_int, [c_void_p, c_int, c_void_p, c_size_t, c_void_p]),
     "pmb_sgemm_plain": (c_int, [c_int, c_int, c_int, ctypes.c_float, c_void_p, c_int64, c_void_p, c_int64,
                                 ctypes.c_float, c_void_p, c_int64, c_void_p]),
     "pmb_lu_workspace_bytes": (c_size_t, [c_int, c_int]),

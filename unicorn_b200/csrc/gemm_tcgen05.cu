@@ -42,8 +42,10 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <map>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "pmb_common.cuh"
 
@@ -397,9 +399,8 @@ __device__ __forceinline__ void umma_commit_pair(uint32_t bar) {
 // Grouped tile order of the 2-SM kernels: CTA pair blockIdx.x / 2 -> 256 x tn
 // tile (pm, pn).  Consecutive pairs sweep the columns of a band of kGroupRows
 // tile rows.
-__device__ __forceinline__ void pair_tile(int M, int N, int tn, int& pm, int& pn) {
+__device__ __forceinline__ void pair_tile(int M, int N, int tn, int pid, int& pm, int& pn) {
     const int num_pm = (M + 255) / 256, num_pn = (N + tn - 1) / tn;
-    const int pid = static_cast<int>(blockIdx.x >> 1);
     const int per_group = kGroupRows * num_pn;
     const int first = (pid / per_group) * kGroupRows;
     const int rows = min(num_pm - first, kGroupRows);
@@ -408,13 +409,14 @@ __device__ __forceinline__ void pair_tile(int M, int N, int tn, int& pm, int& pn
     pn = in_group / rows;
 }
 
+// One 256 x TN tile of one product, computed by a CTA pair: `pid` is the
+// pair's tile index within the product.  `maps` must live in the parameter
+// (or global) space: its address goes to the TMA loads.
 template <int TN>
-__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
-gemm_bf16x3_2sm_kernel(const __grid_constant__ GemmMaps maps, int M, int N, int KT, float alpha, float beta,
-                       float* __restrict__ C, int64_t ldc, uint32_t* __restrict__ err) {
+__device__ __forceinline__ void gemm2_tile(const GemmMaps& maps, int M, int N, int KT, float alpha, float beta,
+                                           float* __restrict__ C, int64_t ldc, uint32_t* __restrict__ err, int pid) {
     using P = Pair2<TN>;
     constexpr int kStages2 = P::kStages, kStage2Bytes = P::kStageBytes, kBHalf = P::kBHalf;
-    asm volatile("griddepcontrol.wait;" ::: "memory");  // the split pass launched before it
     extern __shared__ uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     float* stage_out = reinterpret_cast<float*>(smem + kStages2 * kStage2Bytes);
@@ -434,7 +436,7 @@ gemm_bf16x3_2sm_kernel(const __grid_constant__ GemmMaps maps, int M, int N, int 
     // panels (read once from HBM, then from L2) instead of each wave reading
     // every row panel of A.
     int pm, pn;
-    pair_tile(M, N, TN, pm, pn);
+    pair_tile(M, N, TN, pid, pm, pn);
     const int m0 = pm * 256 + 128 * static_cast<int>(rank);     // this CTA's rows of A and C
     const int n0 = pn * TN;                                     // the pair's columns
     const int nb0 = n0 + (TN / 2) * static_cast<int>(rank);     // this CTA's rows of B^T
@@ -593,6 +595,44 @@ gemm_bf16x3_2sm_kernel(const __grid_constant__ GemmMaps maps, int M, int N, int 
     }
 }
 
+template <int TN>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
+gemm_bf16x3_2sm_kernel(const __grid_constant__ GemmMaps maps, int M, int N, int KT, float alpha, float beta,
+                       float* __restrict__ C, int64_t ldc, uint32_t* __restrict__ err) {
+    asm volatile("griddepcontrol.wait;" ::: "memory");  // the split pass launched before it
+    gemm2_tile<TN>(maps, M, N, KT, alpha, beta, C, ldc, err, static_cast<int>(blockIdx.x >> 1));
+}
+
+// Grouped products: one launch over the tiles of up to kMaxGroup products of
+// different shapes (the subtasks of a task, or the products of concurrent
+// tasks).  Pair p takes tile p - tile_start[g] of product g, where g is the
+// product whose range [tile_start[g], tile_start[g + 1]) holds p.
+constexpr int kMaxGroup = 24;
+struct Gemm2Product {
+    GemmMaps maps;
+    float* C;
+    int64_t ldc;
+    int M, N, KT;
+    float alpha, beta;
+};
+struct Gemm2Group {
+    Gemm2Product prod[kMaxGroup];
+    int tile_start[kMaxGroup + 1];
+    int count;
+};
+static_assert(sizeof(Gemm2Group) <= 32000, "kernel parameter space");
+
+template <int TN>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(kThreads, 1)
+gemm_bf16x3_2sm_grouped_kernel(const __grid_constant__ Gemm2Group grp, uint32_t* __restrict__ err) {
+    asm volatile("griddepcontrol.wait;" ::: "memory");  // the split passes launched before it
+    const int pid = static_cast<int>(blockIdx.x >> 1);
+    int g = 0;
+    while (g + 1 < grp.count && pid >= grp.tile_start[g + 1]) ++g;
+    const Gemm2Product& pr = grp.prod[g];
+    gemm2_tile<TN>(pr.maps, pr.M, pr.N, pr.KT, pr.alpha, pr.beta, pr.C, pr.ldc, err, pid - grp.tile_start[g]);
+}
+
 // ---- 2-SM update kernel for short products (K <= 64) ------------------------
 // With a single 64-deep K slice per tile (the LU trailing update, K = block
 // size) the product is bound by reading and writing C, not by the MMAs.  The
@@ -639,7 +679,7 @@ gemm_update_2sm_kernel(const __grid_constant__ GemmMaps maps, const __grid_const
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t rank = cluster_rank();
     int pm, pn;
-    pair_tile(M, N, 256, pm, pn);
+    pair_tile(M, N, 256, static_cast<int>(blockIdx.x >> 1), pm, pn);
     const int m0 = pm * 256 + 128 * static_cast<int>(rank);
     const int n0 = pn * 256;
     const int nb0 = n0 + 128 * static_cast<int>(rank);
@@ -1000,6 +1040,160 @@ extern "C" int pmb_sgemm_bf16x3(int M, int N, int K, float alpha, const float* A
                                     static_cast<cudaStream_t>(stream), true);
 }
 
+namespace {
+
+// Product kernels of the BF16x3 GEMM: 128 x 256 tiles per CTA, or 256 x 256 /
+// 256 x 128 tiles per CTA pair.
+enum class GemmCfg : int { kOneSm = 0, kPair256 = 1, kPair128 = 2 };
+
+int launch_product(GemmCfg cfg, int M, int N, int kp, float alpha, const __nv_bfloat16* ah, const __nv_bfloat16* al,
+                   const __nv_bfloat16* bh, const __nv_bfloat16* bl, float beta, float* C, int64_t ldc, uint32_t* err,
+                   cudaStream_t s) {
+    GemmMaps maps;
+    int st;
+    if (cfg != GemmCfg::kOneSm) {
+        const int tn = cfg == GemmCfg::kPair128 ? 128 : 256;
+        if ((st = make_map(&maps.ah, ah, M, kp, 128, BK2)) != PMB_SUCCESS) return st;
+        if ((st = make_map(&maps.al, al, M, kp, 128, BK2)) != PMB_SUCCESS) return st;
+        if ((st = make_map(&maps.bh, bh, N, kp, tn / 2, BK2)) != PMB_SUCCESS) return st;
+        if ((st = make_map(&maps.bl, bl, N, kp, tn / 2, BK2)) != PMB_SUCCESS) return st;
+        static std::once_flag attr2_once;
+        static cudaError_t attr2_err = cudaSuccess;
+        std::call_once(attr2_once, [] {
+            attr2_err = cudaFuncSetAttribute(gemm_bf16x3_2sm_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             Pair2<256>::kSmemBytes);
+            if (attr2_err == cudaSuccess)
+                attr2_err = cudaFuncSetAttribute(gemm_bf16x3_2sm_kernel<128>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, Pair2<128>::kSmemBytes);
+            if (attr2_err == cudaSuccess &&
+                (pmb::tmem_exclusive(reinterpret_cast<const void*>(gemm_bf16x3_2sm_kernel<256>), kThreads,
+                                     Pair2<256>::kSmemBytes, "gemm_bf16x3_2sm_kernel<256>") != PMB_SUCCESS ||
+                 pmb::tmem_exclusive(reinterpret_cast<const void*>(gemm_bf16x3_2sm_kernel<128>), kThreads,
+                                     Pair2<128>::kSmemBytes, "gemm_bf16x3_2sm_kernel<128>") != PMB_SUCCESS))
+                attr2_err = cudaErrorInvalidConfiguration;
+        });
+        PMB_CUDA_TRY(attr2_err);
+        const dim3 grid2(2 * ((M + 255) / 256) * ((N + tn - 1) / tn));
+        if (tn == 128)
+            PMB_CUDA_TRY(launch_dep(gemm_bf16x3_2sm_kernel<128>, grid2, kThreads, Pair2<128>::kSmemBytes, s, true, maps,
+                                    M, N, (kp + BK2 - 1) / BK2, alpha, beta, C, ldc, err));
+        else
+            PMB_CUDA_TRY(launch_dep(gemm_bf16x3_2sm_kernel<256>, grid2, kThreads, Pair2<256>::kSmemBytes, s, true, maps,
+                                    M, N, (kp + BK2 - 1) / BK2, alpha, beta, C, ldc, err));
+        return PMB_SUCCESS;
+    }
+    if ((st = make_map(&maps.ah, ah, M, kp, BM)) != PMB_SUCCESS) return st;
+    if ((st = make_map(&maps.al, al, M, kp, BM)) != PMB_SUCCESS) return st;
+    if ((st = make_map(&maps.bh, bh, N, kp, BN)) != PMB_SUCCESS) return st;
+    if ((st = make_map(&maps.bl, bl, N, kp, BN)) != PMB_SUCCESS) return st;
+    static std::once_flag attr_once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(attr_once, [] {
+        attr_err = cudaFuncSetAttribute(gemm_bf16x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
+        if (attr_err == cudaSuccess &&
+            pmb::tmem_exclusive(reinterpret_cast<const void*>(gemm_bf16x3_kernel), kThreads, kSmemBytes,
+                                "gemm_bf16x3_kernel") != PMB_SUCCESS)
+            attr_err = cudaErrorInvalidConfiguration;
+    });
+    PMB_CUDA_TRY(attr_err);
+    const dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
+    PMB_CUDA_TRY(launch_dep(gemm_bf16x3_kernel, grid, kThreads, kSmemBytes, s, true, maps, M, N, kp / BK, alpha, beta, C,
+                            ldc, err));
+    return PMB_SUCCESS;
+}
+
+int sm_pair_count() {
+    static const int pairs = [] {
+        int dev = 0, sms = 148;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+            cudaGetLastError();
+            sms = 148;
+        }
+        return sms / 2;
+    }();
+    return pairs;
+}
+
+// The fixed rule: CTA pairs for M > 128, with 256 x 128 tiles when 256 x 256
+// ones would leave at least half the SM pairs without a tile (e.g. 1024 x
+// 1024: 16 tiles for 74 pairs); one CTA per 128 x 256 tile otherwise.
+GemmCfg rule_cfg(int M, int N) {
+    if (M <= BM) return GemmCfg::kOneSm;
+    const int64_t tiles256 = static_cast<int64_t>((M + 255) / 256) * ((N + 255) / 256);
+    return 2 * tiles256 <= sm_pair_count() ? GemmCfg::kPair128 : GemmCfg::kPair256;
+}
+
+int ceil_log2(int64_t x) {
+    int l = 0;
+    while ((int64_t{1} << l) < x) ++l;
+    return l;
+}
+
+// Autotuner (PMB_GEMM_AUTOTUNE=1): the first product of each shape class
+// (ceil log2 of M, N and the padded K) times the three product kernels on the
+// call's own operands -- only when C is write-only (beta = 0) and the stream
+// is not being captured -- and remembers the fastest; later products of the
+// class use it.  Each timed kernel writes all of C, so the call's result is
+// the last one's.  Off (the default), or for a class not tuned, the fixed rule.
+GemmCfg choose_cfg(int M, int N, int kp, float alpha, const __nv_bfloat16* ah, const __nv_bfloat16* al,
+                   const __nv_bfloat16* bh, const __nv_bfloat16* bl, float beta, float* C, int64_t ldc, uint32_t* err,
+                   cudaStream_t s) {
+    static const bool tune = [] {
+        const char* v = getenv("PMB_GEMM_AUTOTUNE");
+        return v && v[0] == '1';
+    }();
+    const GemmCfg rule = rule_cfg(M, N);
+    if (!tune) return rule;
+    const uint32_t key = (static_cast<uint32_t>(ceil_log2(M)) << 16) | (static_cast<uint32_t>(ceil_log2(N)) << 8) |
+                         static_cast<uint32_t>(ceil_log2(kp));
+    static std::mutex mu;
+    static std::map<uint32_t, GemmCfg> best;
+    {
+        std::lock_guard<std::mutex> g(mu);
+        auto it = best.find(key);
+        if (it != best.end()) return it->second;
+    }
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (beta != 0.0f || cudaStreamIsCapturing(s, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) {
+        cudaGetLastError();
+        return rule;
+    }
+    const GemmCfg cand[3] = {GemmCfg::kOneSm, GemmCfg::kPair256, GemmCfg::kPair128};
+    cudaEvent_t ev[4] = {};
+    for (cudaEvent_t& e : ev)
+        if (cudaEventCreate(&e) != cudaSuccess) {
+            cudaGetLastError();
+            for (cudaEvent_t& x : ev)
+                if (x) cudaEventDestroy(x);
+            return rule;
+        }
+    bool ok = launch_product(rule, M, N, kp, alpha, ah, al, bh, bl, beta, C, ldc, err, s) == PMB_SUCCESS;  // warm-up
+    ok = ok && cudaEventRecord(ev[0], s) == cudaSuccess;
+    for (int i = 0; i < 3 && ok; ++i) {
+        ok = launch_product(cand[i], M, N, kp, alpha, ah, al, bh, bl, beta, C, ldc, err, s) == PMB_SUCCESS;
+        ok = ok && cudaEventRecord(ev[i + 1], s) == cudaSuccess;
+    }
+    GemmCfg pick = rule;
+    if (ok && cudaEventSynchronize(ev[3]) == cudaSuccess) {
+        float best_ms = 0.0f;
+        for (int i = 0; i < 3; ++i) {
+            float ms = 0.0f;
+            if (cudaEventElapsedTime(&ms, ev[i], ev[i + 1]) != cudaSuccess) continue;
+            if (i == 0 || ms < best_ms) {
+                best_ms = ms;
+                pick = cand[i];
+            }
+        }
+        std::lock_guard<std::mutex> g(mu);
+        best[key] = pick;
+    }
+    cudaGetLastError();
+    for (cudaEvent_t& e : ev) cudaEventDestroy(e);
+    return pick;
+}
+
+}  // namespace
+
 int pmb::sgemm_bf16x3_launch(int M, int N, int K, float alpha, const float* A, int64_t lda, const float* B,
                              int64_t ldb, float beta, float* C, int64_t ldc, void* workspace, size_t ws_bytes,
                              cudaStream_t s, bool clear_error) {
@@ -1041,71 +1235,9 @@ int pmb::sgemm_bf16x3_launch(int M, int N, int K, float alpha, const float* A, i
     if (kp <= BK2 && c_map_ok(C, ldc) && !force_1sm)
         return launch_update(M, N, kp, alpha, ah, al, bh, bl, beta, C, ldc, err, s, true);
 
-    GemmMaps maps;
-    int st;
-    // Tiles of 256 rows per CTA pair for M > 128.
-    if (M > BM && !force_1sm) {
-        // 256 x 128 tiles when 256 x 256 ones would leave at least half the SM
-        // pairs without a tile (e.g. 1024 x 1024: 16 tiles for 74 pairs).
-        static const int sm_pairs = [] {
-            int dev = 0, sms = 148;
-            if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
-                cudaGetLastError();
-                sms = 148;
-            }
-            return sms / 2;
-        }();
-        const int64_t tiles256 = static_cast<int64_t>((M + 255) / 256) * ((N + 255) / 256);
-        const bool narrow = 2 * tiles256 <= sm_pairs;
-        const int tn = narrow ? 128 : 256;
-        if ((st = make_map(&maps.ah, ah, M, kp, 128, BK2)) != PMB_SUCCESS) return st;
-        if ((st = make_map(&maps.al, al, M, kp, 128, BK2)) != PMB_SUCCESS) return st;
-        if ((st = make_map(&maps.bh, bh, N, kp, tn / 2, BK2)) != PMB_SUCCESS) return st;
-        if ((st = make_map(&maps.bl, bl, N, kp, tn / 2, BK2)) != PMB_SUCCESS) return st;
-        static std::once_flag attr2_once;
-        static cudaError_t attr2_err = cudaSuccess;
-        std::call_once(attr2_once, [] {
-            attr2_err = cudaFuncSetAttribute(gemm_bf16x3_2sm_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             Pair2<256>::kSmemBytes);
-            if (attr2_err == cudaSuccess)
-                attr2_err = cudaFuncSetAttribute(gemm_bf16x3_2sm_kernel<128>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, Pair2<128>::kSmemBytes);
-            if (attr2_err == cudaSuccess &&
-                (pmb::tmem_exclusive(reinterpret_cast<const void*>(gemm_bf16x3_2sm_kernel<256>), kThreads,
-                                     Pair2<256>::kSmemBytes, "gemm_bf16x3_2sm_kernel<256>") != PMB_SUCCESS ||
-                 pmb::tmem_exclusive(reinterpret_cast<const void*>(gemm_bf16x3_2sm_kernel<128>), kThreads,
-                                     Pair2<128>::kSmemBytes, "gemm_bf16x3_2sm_kernel<128>") != PMB_SUCCESS))
-                attr2_err = cudaErrorInvalidConfiguration;
-        });
-        PMB_CUDA_TRY(attr2_err);
-        const dim3 grid2(2 * ((M + 255) / 256) * ((N + tn - 1) / tn));
-        if (narrow)
-            PMB_CUDA_TRY(launch_dep(gemm_bf16x3_2sm_kernel<128>, grid2, kThreads, Pair2<128>::kSmemBytes, s, true, maps,
-                                    M, N, (kp + BK2 - 1) / BK2, alpha, beta, C, ldc, err));
-        else
-            PMB_CUDA_TRY(launch_dep(gemm_bf16x3_2sm_kernel<256>, grid2, kThreads, Pair2<256>::kSmemBytes, s, true, maps,
-                                    M, N, (kp + BK2 - 1) / BK2, alpha, beta, C, ldc, err));
-        return PMB_SUCCESS;
-    }
-    if ((st = make_map(&maps.ah, ah, M, kp, BM)) != PMB_SUCCESS) return st;
-    if ((st = make_map(&maps.al, al, M, kp, BM)) != PMB_SUCCESS) return st;
-    if ((st = make_map(&maps.bh, bh, N, kp, BN)) != PMB_SUCCESS) return st;
-    if ((st = make_map(&maps.bl, bl, N, kp, BN)) != PMB_SUCCESS) return st;
-
-    static std::once_flag attr_once;
-    static cudaError_t attr_err = cudaSuccess;
-    std::call_once(attr_once, [] {
-        attr_err = cudaFuncSetAttribute(gemm_bf16x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSmemBytes);
-        if (attr_err == cudaSuccess &&
-            pmb::tmem_exclusive(reinterpret_cast<const void*>(gemm_bf16x3_kernel), kThreads, kSmemBytes,
-                                "gemm_bf16x3_kernel") != PMB_SUCCESS)
-            attr_err = cudaErrorInvalidConfiguration;
-    });
-    PMB_CUDA_TRY(attr_err);
-    const dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
-    PMB_CUDA_TRY(launch_dep(gemm_bf16x3_kernel, grid, kThreads, kSmemBytes, s, true, maps, M, N, kp / BK, alpha, beta, C,
-                            ldc, err));
-    return PMB_SUCCESS;
+    if (force_1sm) return launch_product(GemmCfg::kOneSm, M, N, kp, alpha, ah, al, bh, bl, beta, C, ldc, err, s);
+    return launch_product(choose_cfg(M, N, kp, alpha, ah, al, bh, bl, beta, C, ldc, err, s), M, N, kp, alpha, ah, al,
+                          bh, bl, beta, C, ldc, err, s);
 }
 
 extern "C" int pmb_sgemm_plain(int M, int N, int K, float alpha, const float* A, int64_t lda, const float* B,
@@ -1116,5 +1248,151 @@ extern "C" int pmb_sgemm_plain(int M, int N, int K, float alpha, const float* A,
     sgemm_plain_kernel<<<dim3((N + 63) / 64, (M + 63) / 64), 256, 0, static_cast<cudaStream_t>(stream)>>>(
         M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
     PMB_CUDA_TRY(cudaGetLastError());
+    return PMB_SUCCESS;
+}
+
+// ---------------------------------------------------------------------------
+// Grouped products: many C = alpha A B + beta C of different shapes in one
+// launch of the product kernel (after one split pass per product), instead of
+// a split + product launch pair per product.
+
+namespace {
+
+size_t grouped_ws_bytes(const pmb_gemm_problem* probs, int count) {
+    size_t total = 256;
+    for (int i = 0; i < count; ++i) {
+        const pmb_gemm_problem& q = probs[i];
+        if (q.M <= 0 || q.N <= 0 || q.K <= 0) continue;
+        total += pmb_gemm_workspace_bytes(q.M, q.N, q.K) - 256;
+    }
+    return total;
+}
+
+}  // namespace
+
+extern "C" size_t pmb_gemm_grouped_workspace_bytes(const pmb_gemm_problem* problems, int count) {
+    if (!problems || count <= 0) return 256;
+    return grouped_ws_bytes(problems, count);
+}
+
+extern "C" int pmb_sgemm_bf16x3_grouped(const pmb_gemm_problem* problems, int count, void* workspace,
+                                        size_t workspace_bytes, void* stream) {
+    PMB_CHECK_ARG(problems && count >= 0, "null problem list");
+    PMB_CHECK_ARG(workspace && (reinterpret_cast<uintptr_t>(workspace) & 255) == 0,
+                  "workspace must be non-null and 256-byte aligned");
+    PMB_CHECK_ARG(workspace_bytes >= grouped_ws_bytes(problems, count), "grouped GEMM workspace %zu bytes, need %zu",
+                  workspace_bytes, grouped_ws_bytes(problems, count));
+    for (int i = 0; i < count; ++i) {
+        const pmb_gemm_problem& q = problems[i];
+        PMB_CHECK_ARG(q.M >= 0 && q.N >= 0 && q.K >= 0, "problem %d: negative size", i);
+        if (q.M == 0 || q.N == 0) continue;
+        PMB_CHECK_ARG(q.C && (q.K == 0 || (q.A && q.B)), "problem %d: null pointer", i);
+        PMB_CHECK_ARG(q.ldc >= q.N && (q.K == 0 || (q.lda >= q.K && q.ldb >= q.N)),
+                      "problem %d: leading dimension too small", i);
+    }
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    char* ws = static_cast<char*>(workspace);
+    uint32_t* err = reinterpret_cast<uint32_t*>(ws) + 1;
+    PMB_CUDA_TRY(cudaMemsetAsync(ws, 0, 256, s));
+    static std::once_flag attr_once;
+    static cudaError_t attr_err = cudaSuccess;
+    std::call_once(attr_once, [] {
+        attr_err = cudaFuncSetAttribute(gemm_bf16x3_2sm_grouped_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        Pair2<256>::kSmemBytes);
+        if (attr_err == cudaSuccess)
+            attr_err = cudaFuncSetAttribute(gemm_bf16x3_2sm_grouped_kernel<128>,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, Pair2<128>::kSmemBytes);
+        if (attr_err == cudaSuccess &&
+            (pmb::tmem_exclusive(reinterpret_cast<const void*>(gemm_bf16x3_2sm_grouped_kernel<256>), kThreads,
+                                 Pair2<256>::kSmemBytes, "gemm_bf16x3_2sm_grouped_kernel<256>") != PMB_SUCCESS ||
+             pmb::tmem_exclusive(reinterpret_cast<const void*>(gemm_bf16x3_2sm_grouped_kernel<128>), kThreads,
+                                 Pair2<128>::kSmemBytes, "gemm_bf16x3_2sm_grouped_kernel<128>") != PMB_SUCCESS))
+            attr_err = cudaErrorInvalidConfiguration;
+    });
+    PMB_CUDA_TRY(attr_err);
+    static const int sm_pairs = [] {
+        int dev = 0, sms = 148;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+            cudaGetLastError();
+            sms = 148;
+        }
+        return sms / 2;
+    }();
+
+    // Split every product into its bf16 hi/lo operands (workspace laid out in
+    // problem order); K == 0 products only scale C.
+    struct Split {
+        const __nv_bfloat16 *ah, *al, *bh, *bl;
+        int kp;
+    };
+    std::vector<Split> split(static_cast<size_t>(count));
+    std::vector<int> live;
+    size_t off = 256;
+    for (int i = 0; i < count; ++i) {
+        const pmb_gemm_problem& q = problems[i];
+        if (q.M == 0 || q.N == 0) continue;
+        if (q.K == 0) {
+            scale_kernel<<<256, 256, 0, s>>>(q.C, q.ldc, q.M, q.N, q.beta);
+            PMB_CUDA_TRY(cudaGetLastError());
+            continue;
+        }
+        const int kp = padded_k(q.K);
+        const size_t a_bytes = align256(static_cast<size_t>(q.M) * kp * 2);
+        const size_t b_bytes = align256(static_cast<size_t>(q.N) * kp * 2);
+        __nv_bfloat16* ah = reinterpret_cast<__nv_bfloat16*>(ws + off);
+        __nv_bfloat16* al = reinterpret_cast<__nv_bfloat16*>(ws + off + a_bytes);
+        __nv_bfloat16* bh = reinterpret_cast<__nv_bfloat16*>(ws + off + 2 * a_bytes);
+        __nv_bfloat16* bl = reinterpret_cast<__nv_bfloat16*>(ws + off + 2 * a_bytes + b_bytes);
+        off += 2 * a_bytes + 2 * b_bytes;
+        const int64_t row_elems = static_cast<int64_t>(q.M) * kp;
+        const int row_blocks = static_cast<int>(std::min<int64_t>(1184, (row_elems + 255) / 256));
+        const int tiles = ((q.N + 31) / 32) * ((kp + 31) / 32);
+        split_both_kernel<<<row_blocks + tiles, 256, 0, s>>>(q.A, q.lda, q.M, q.B, q.ldb, q.N, q.K, kp, row_blocks, ah,
+                                                             al, bh, bl);
+        PMB_CUDA_TRY(cudaGetLastError());
+        split[i] = Split{ah, al, bh, bl, kp};
+        live.push_back(i);
+    }
+    // The products, kMaxGroup per launch, each launch a programmatic
+    // dependent of the work before it on the stream.
+    for (size_t g0 = 0; g0 < live.size(); g0 += kMaxGroup) {
+        const size_t g1 = std::min(live.size(), g0 + kMaxGroup);
+        int64_t tiles256 = 0;
+        for (size_t j = g0; j < g1; ++j) {
+            const pmb_gemm_problem& q = problems[live[j]];
+            tiles256 += static_cast<int64_t>((q.M + 255) / 256) * ((q.N + 255) / 256);
+        }
+        // 256 x 128 tiles when 256 x 256 ones would leave at least half the SM pairs idle.
+        const bool narrow = 2 * tiles256 <= sm_pairs;
+        const int tn = narrow ? 128 : 256;
+        Gemm2Group grp;
+        grp.count = static_cast<int>(g1 - g0);
+        int total = 0, st;
+        for (int j = 0; j < grp.count; ++j) {
+            const pmb_gemm_problem& q = problems[live[g0 + j]];
+            const Split& sp = split[live[g0 + j]];
+            Gemm2Product& pr = grp.prod[j];
+            if ((st = make_map(&pr.maps.ah, sp.ah, q.M, sp.kp, 128, BK2)) != PMB_SUCCESS) return st;
+            if ((st = make_map(&pr.maps.al, sp.al, q.M, sp.kp, 128, BK2)) != PMB_SUCCESS) return st;
+            if ((st = make_map(&pr.maps.bh, sp.bh, q.N, sp.kp, tn / 2, BK2)) != PMB_SUCCESS) return st;
+            if ((st = make_map(&pr.maps.bl, sp.bl, q.N, sp.kp, tn / 2, BK2)) != PMB_SUCCESS) return st;
+            pr.C = q.C;
+            pr.ldc = q.ldc;
+            pr.M = q.M;
+            pr.N = q.N;
+            pr.KT = (sp.kp + BK2 - 1) / BK2;
+            pr.alpha = q.alpha;
+            pr.beta = q.beta;
+            grp.tile_start[j] = total;
+            total += ((q.M + 255) / 256) * ((q.N + tn - 1) / tn);
+        }
+        grp.tile_start[grp.count] = total;
+        if (narrow)
+            PMB_CUDA_TRY(launch_dep(gemm_bf16x3_2sm_grouped_kernel<128>, dim3(2 * total), kThreads,
+                                    Pair2<128>::kSmemBytes, s, true, grp, err));
+        else
+            PMB_CUDA_TRY(launch_dep(gemm_bf16x3_2sm_grouped_kernel<256>, dim3(2 * total), kThreads,
+                                    Pair2<256>::kSmemBytes, s, true, grp, err));
+    }
     return PMB_SUCCESS;
 }

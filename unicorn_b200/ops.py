@@ -212,6 +212,34 @@ def sgemm(A, B, C=None, alpha: float = 1.0, beta: float = 0.0, plain: bool = Fal
     return C, workspace
 
 
+def sgemm_grouped(products, workspace=None, stream=None):
+    """Several row-major fp32 products C = alpha*A@B + beta*C in one grouped
+    BF16x3 call.  products: list of (A, B, C, alpha, beta) CUDA tensors /
+    floats (2-D, unit column stride).  Returns the workspace."""
+    import torch
+
+    arr = (capi.GemmProblem * len(products))()
+    for i, (A, B, C, alpha, beta) in enumerate(products):
+        for t in (A, B, C):
+            if t.dtype != torch.float32 or not t.is_cuda or t.stride(1) != 1:
+                raise ValueError("fp32 CUDA matrices with unit column stride expected")
+        M, K = A.shape
+        K2, N = B.shape
+        if K != K2 or tuple(C.shape) != (M, N):
+            raise ValueError(f"product {i}: shapes {tuple(A.shape)} x {tuple(B.shape)} -> {tuple(C.shape)}")
+        q = arr[i]
+        q.M, q.N, q.K = M, N, K
+        q.alpha, q.beta = alpha, beta
+        q.A, q.lda, q.B, q.ldb, q.C, q.ldc = A.data_ptr(), A.stride(0), B.data_ptr(), B.stride(0), C.data_ptr(), C.stride(0)
+    L = capi.lib()
+    need = L.pmb_gemm_grouped_workspace_bytes(arr, len(products))
+    if workspace is None or workspace.numel() < need:
+        workspace = _scratch(need)
+    capi.check(L.pmb_sgemm_bf16x3_grouped(arr, len(products), workspace.data_ptr(), workspace.numel(),
+                                          _stream_ptr(stream)))
+    return workspace
+
+
 def lu_decompose(d_A, nb: int = 64, plain: bool = False, workspace=None, stream=None):
     """In-place Crout LU of a square fp32 CUDA matrix stored column-major.
 

@@ -191,7 +191,11 @@ struct Controller {
     std::vector<std::unique_ptr<CallbackSet>> callbacks;
     std::set<AddressSpace*> spaces;
     std::set<Task*> tasks;
-    std::map<void*, BatchFn> batch;
+    struct BatchHook {
+        BatchFn fn = nullptr;
+        size_t groups = 0;  // launches per task; 0: batch_groups
+    };
+    std::map<void*, BatchHook> batch;
     // stub
     std::thread stub, completer;
     std::mutex qmu;
@@ -214,6 +218,7 @@ struct Controller {
     size_t max_inflight = 64;              // GPU tasks on the device at once (admission slots)
     std::atomic<bool> eager_writeback{false};  // copy written bytes to the host at task end
     size_t batch_groups = 16;              // launches a batched task is split into (pipelined staging)
+    bool batch_off = false;                // PMB_NO_BATCH: every subtask through its own callback
     // pinned host buffers of released address spaces, kept for reuse
     std::mutex pin_mu;
     std::multimap<size_t, char*> pin_free;
@@ -232,9 +237,9 @@ static Controller& ctl() {
     return *c;
 }
 
-void register_batch(pmSubtaskCallback_GPU_Custom callback, BatchFn batch) {
+void register_batch(pmSubtaskCallback_GPU_Custom callback, BatchFn batch, size_t groups) {
     std::lock_guard<std::mutex> g(ctl().mu);
-    ctl().batch[reinterpret_cast<void*>(callback)] = batch;
+    ctl().batch[reinterpret_cast<void*>(callback)] = Controller::BatchHook{batch, groups};
 }
 
 // Data-distribution context of the calling thread.
@@ -1249,10 +1254,14 @@ static pmStatus stage_and_launch_gpu(Task* t) {
     }
 
     BatchFn batch = nullptr;
-    if (cb.subtask_gpu_custom) {
+    size_t groups = c.batch_groups;
+    if (cb.subtask_gpu_custom && !c.batch_off) {
         std::lock_guard<std::mutex> g(c.mu);
         auto it = c.batch.find(reinterpret_cast<void*>(cb.subtask_gpu_custom));
-        if (it != c.batch.end()) batch = it->second;
+        if (it != c.batch.end()) {
+            batch = it->second.fn;
+            if (it->second.groups) groups = it->second.groups;
+        }
         for (size_t i = 0; i < ns && batch; ++i)
             if (t->views[i] != SUBSCRIPTION_NATURAL) batch = nullptr;
         for (Subtask& s : t->subtasks)
@@ -1278,7 +1287,7 @@ static pmStatus stage_and_launch_gpu(Task* t) {
     std::vector<void*> group_staged;
     if (batch) {
         const size_t nsub = t->subtasks.size();
-        const size_t per = (nsub + std::max<size_t>(c.batch_groups, 1) - 1) / std::max<size_t>(c.batch_groups, 1);
+        const size_t per = (nsub + std::max<size_t>(groups, 1) - 1) / std::max<size_t>(groups, 1);
         for (size_t g0 = 0; g0 < nsub; g0 += std::max<size_t>(per, 1)) group_begin.push_back(g0);
         group_begin.push_back(nsub);
     }
@@ -1834,6 +1843,7 @@ pmStatus pmInitialize() {
         c.eager_writeback = env_flag("PMB_EAGER_WRITEBACK");
         const char* bg = getenv("PMB_BATCH_GROUPS");
         c.batch_groups = bg && atoi(bg) > 0 ? static_cast<size_t>(atoi(bg)) : 16;
+        c.batch_off = env_flag("PMB_NO_BATCH");
         const char* mv = getenv("PMB_MAX_INFLIGHT");
         c.max_inflight = mv && atoi(mv) > 0 ? static_cast<size_t>(atoi(mv)) : 64;
     }
@@ -2309,10 +2319,17 @@ pmStatus pmUnmapFiles(const char* const* pPaths, uint pFileCount) {
 
 }  // namespace pm
 
+extern "C" int pmb_runtime_register_batch_groups(void* subtask_gpu_custom, void* batch_fn, int groups) {
+    if (!subtask_gpu_custom || !batch_fn || groups < 0) return pm::pmInvalidIndex;
+    pmr::register_batch(reinterpret_cast<pm::pmSubtaskCallback_GPU_Custom>(subtask_gpu_custom),
+                        reinterpret_cast<pmr::BatchFn>(batch_fn), static_cast<size_t>(groups));
+    return pm::pmSuccess;
+}
+
 extern "C" int pmb_runtime_register_batch(void* subtask_gpu_custom, void* batch_fn) {
     if (!subtask_gpu_custom || !batch_fn) return pm::pmInvalidIndex;
     pmr::register_batch(reinterpret_cast<pm::pmSubtaskCallback_GPU_Custom>(subtask_gpu_custom),
-                        reinterpret_cast<pmr::BatchFn>(batch_fn));
+                        reinterpret_cast<pmr::BatchFn>(batch_fn), 0);
     return pm::pmSuccess;
 }
 

@@ -150,14 +150,18 @@ struct Task {
 
 // Registers a whole-task GPU implementation for a subtask_gpu_custom callback:
 // when every subtask of a task uses that callback with NATURAL views, the
-// CUDA stub calls `batch` once for all of them instead of once per subtask.
-void register_batch(pmSubtaskCallback_GPU_Custom callback, BatchFn batch);
+// CUDA stub calls `batch` once per group of consecutive subtasks instead of
+// once per subtask -- `groups` groups per task (0: PMB_BATCH_GROUPS, 16 by
+// default), each launched as soon as its own inputs are staged.
+// PMB_NO_BATCH=1 turns every hook off (per-subtask callbacks).
+void register_batch(pmSubtaskCallback_GPU_Custom callback, BatchFn batch, size_t groups);
 
 }  // namespace pmr
 
 extern "C" {
-// C entry for apps libraries (see register_batch).
+// C entries for apps libraries (see register_batch).
 int pmb_runtime_register_batch(void* subtask_gpu_custom, void* batch_fn);
+int pmb_runtime_register_batch_groups(void* subtask_gpu_custom, void* batch_fn, int groups);
 // Runtime statistics: bytes moved host->device / device->host, GPU callback
 // invocations, batched launches; for tests and benchmarks.
 void pmb_runtime_stats(unsigned long long* h2d_bytes, unsigned long long* d2h_bytes,
