@@ -464,7 +464,12 @@ size_t pmb_lu_workspace_bytes(int n, int nb);
  * and the trailing updates run as BF16x3 tensor-core GEMMs.  Word 1 of the
  * workspace gets flags (pmb_scratch_error): 1 = partial pivoting (FP64
  * comparison) would have exchanged rows in some column, 2 = a zero pivot,
- * 4 = a kernel's bounded wait expired (the result is not valid). */
+ * 4 = a kernel's bounded wait expired (the result is not valid).  For
+ * nb <= 64 the serial chain of each step (diagonal block, panels, the next
+ * block column of the update) runs on a high-priority stream the library
+ * keeps per (device, `stream`) while the rest of the update runs on `stream`
+ * (PMB_LU_LOOKAHEAD=0: everything on `stream`); calls that share `stream`
+ * must come from one host thread at a time. */
 int pmb_lu_decompose(float* d_A, int n, int64_t lda, int nb, void* d_workspace, size_t ws_bytes, void* stream);
 
 /* Same factorization with FP32 SIMT GEMMs (the plain one-task-at-a-time form). */

@@ -34,6 +34,9 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <cstdlib>
+#include <map>
+#include <mutex>
 
 #include "pmb_common.cuh"
 
@@ -597,6 +600,49 @@ LuWs carve(void* ws, int n, int nb) {
     return w;
 }
 
+// Look-ahead: per caller stream (and device) a high-priority stream that runs
+// the serial chain -- diagonal block, panel solves, the next block column of
+// the update -- while the rest of each trailing update runs on the caller's
+// stream, so the block scheduler hands the chain's small grids the next free
+// SM ahead of the update's tiles.  Reusable events order them (chain ready ->
+// rest of the update may start; rest done -> next panel may start; start and
+// end hand-offs with the caller's stream); each wait is enqueued before its
+// event is recorded again, so one set of events serves every step.
+struct SideStream {
+    cudaStream_t hi = nullptr;
+    cudaEvent_t panel_done = nullptr, rest_done = nullptr, start = nullptr, end = nullptr;
+};
+
+bool side_stream_for(cudaStream_t s, SideStream& out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    static std::mutex mu;
+    static std::map<std::pair<int, cudaStream_t>, SideStream> sides;
+    std::lock_guard<std::mutex> g(mu);
+    auto it = sides.find({dev, s});
+    if (it != sides.end()) {
+        out = it->second;
+        return true;
+    }
+    SideStream ss;
+    int least = 0, greatest = 0;
+    if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess ||
+        cudaStreamCreateWithPriority(&ss.hi, cudaStreamNonBlocking, greatest) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ss.panel_done, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ss.rest_done, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ss.start, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ss.end, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    sides[{dev, s}] = ss;
+    out = ss;
+    return true;
+}
+
 }  // namespace
 
 extern "C" size_t pmb_lu_workspace_bytes(int n, int nb) {
@@ -609,7 +655,11 @@ extern "C" size_t pmb_lu_workspace_bytes(int n, int nb) {
 // Blocked LU.  Block sizes up to 64 take three launches a step: the FP64
 // diagonal factorization (with the in-block pivot check), the panel solves
 // (U12, L21 and the rest of the pivot check) and the trailing update
-// A22 -= L21 U12.  Larger blocks form explicit inverses W = L11^-1 and
+// A22 -= L21 U12.  With look-ahead (block sizes up to 64, tcgen05 path, the
+// stream not being captured, PMB_LU_LOOKAHEAD not 0) the update is split: the
+// next block column first, on the high-priority chain stream, so the next
+// diagonal block can start; the rest on the caller's stream, overlapping that
+// diagonal factorization, and the next panel solve waits for it.  Larger blocks form explicit inverses W = L11^-1 and
 // V = U11^-1 and solve the panels as products.  `plain` selects FP32 solves
 // and the FP32 SIMT GEMM (the one-task-at-a-time baseline) instead of FP64
 // solves and the tcgen05 BF16x3 GEMM.
@@ -625,6 +675,26 @@ static int lu_impl(float* A, int n, int64_t lda, int nb, void* workspace, size_t
     LuWs w = carve(workspace, n, nb);
     PMB_CUDA_TRY(cudaMemsetAsync(workspace, 0, 256, s));
     if (!plain) PMB_CUDA_TRY(cudaMemsetAsync(w.gemm, 0, 256, s));  // the products' error word, cleared once
+    static const bool lookahead_on = [] {
+        const char* v = getenv("PMB_LU_LOOKAHEAD");
+        return !(v && v[0] == '0');
+    }();
+    SideStream side;
+    bool lookahead = false;
+    if (lookahead_on && !plain && nb <= kPanelNb) {
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(s, &cap) == cudaSuccess && cap == cudaStreamCaptureStatusNone)
+            lookahead = side_stream_for(s, side);
+        cudaGetLastError();
+    }
+    bool rest_pending = false;  // the caller's stream holds the rest of the previous update
+    cudaStream_t const caller = s;
+    if (lookahead) {
+        // The chain starts after everything before it on the caller's stream.
+        PMB_CUDA_TRY(cudaEventRecord(side.start, caller));
+        PMB_CUDA_TRY(cudaStreamWaitEvent(side.hi, side.start, 0));
+        s = side.hi;
+    }
     for (int k0 = 0; k0 < n; k0 += nb) {
         const int kb = n - k0 < nb ? n - k0 : nb;
         const int rest = n - k0 - kb;
@@ -639,6 +709,12 @@ static int lu_impl(float* A, int n, int64_t lda, int nb, void* workspace, size_t
             PMB_CUDA_TRY(launch_chained(lu_diag64_kernel, 1, 256, s, k0 > 0, A11, lda, kb, w.F, &w.flags[1]));
             if (rest == 0) continue;
             const int half = std::min((rest + 7) / 8, 4 * 148);  // blocks per side, 8 warps (items) each
+            if (rest_pending) {
+                // The panel solve reads what the rest of the previous update writes,
+                // and overwrites the split operands that update reads.
+                PMB_CUDA_TRY(cudaStreamWaitEvent(s, side.rest_done, 0));
+                rest_pending = false;
+            }
             if (plain) {
                 PMB_CUDA_TRY(launch_chained(lu_panel_kernel<float>, 2 * half, 256, s, true, A, lda, k0, kb, rest, half,
                                             w.F, &w.flags[1], static_cast<__nv_bfloat16*>(nullptr),
@@ -653,8 +729,22 @@ static int lu_impl(float* A, int n, int64_t lda, int nb, void* workspace, size_t
                                             half, w.F, &w.flags[1], direct ? w.uh : nullptr, w.ul, w.lh, w.ll));
                 if (direct) {
                     // A22 -= L21 * U12 == row-major (U12^T)(L21^T); a timed-out wait shows as flag 4.
-                    st = pmb::gemm_presplit_launch(rest, rest, kPanelNb, -1.0f, w.uh, w.ul, w.lh, w.ll, 1.0f, A22,
-                                                   lda, &w.flags[1], s, true);
+                    // Row-major rows of C are columns of A22; rows of the U12^T operand
+                    // are kPanelNb split elements apart.
+                    const int kn = lookahead ? std::min(nb, rest) : rest;
+                    if (kn < rest) {
+                        PMB_CUDA_TRY(cudaEventRecord(side.panel_done, s));
+                        PMB_CUDA_TRY(cudaStreamWaitEvent(caller, side.panel_done, 0));
+                        const size_t off = static_cast<size_t>(kn) * kPanelNb;
+                        st = pmb::gemm_presplit_launch(rest - kn, rest, kPanelNb, -1.0f, w.uh + off, w.ul + off, w.lh,
+                                                       w.ll, 1.0f, A22 + static_cast<int64_t>(kn) * lda, lda,
+                                                       &w.flags[1], caller, false);
+                        if (st != PMB_SUCCESS) return st;
+                        PMB_CUDA_TRY(cudaEventRecord(side.rest_done, caller));
+                        rest_pending = true;
+                    }
+                    st = pmb::gemm_presplit_launch(kn, rest, kPanelNb, -1.0f, w.uh, w.ul, w.lh, w.ll, 1.0f, A22, lda,
+                                                   &w.flags[1], s, true);
                     if (st != PMB_SUCCESS) return st;
                     continue;
                 }
@@ -695,6 +785,11 @@ static int lu_impl(float* A, int n, int64_t lda, int nb, void* workspace, size_t
         else st = pmb::sgemm_bf16x3_launch(rest, rest, kb, -1.0f, A12, lda, A21, lda, 1.0f, A22, lda, w.gemm,
                                            w.gemm_bytes, s, false);
         if (st != PMB_SUCCESS) return st;
+    }
+    // The caller's stream completes only after the chain's last kernel.
+    if (lookahead) {
+        PMB_CUDA_TRY(cudaEventRecord(side.end, s));
+        PMB_CUDA_TRY(cudaStreamWaitEvent(caller, side.end, 0));
     }
     return PMB_SUCCESS;
 }
