@@ -277,7 +277,7 @@ __device__ __forceinline__ void deinterleave4(uint32_t w0, uint32_t w1, uint32_t
 //  - epilogue (warps 0-3, TMEM lane quarter = warp): reads its row's 3 x 64
 //    sums, packs them to bytes (clamp: saturate; wrap: low byte),
 //    re-interleaves RGB into a staged row, frees the accumulator set, and
-//    the four warps write the tile with coalesced 16-byte stores.
+//    each warp writes its own rows out with coalesced 16-byte stores.
 // mbarriers order the roles (raw buffer filled / drained, operands written,
 // operand slot consumed, MMAs done = accumulators readable, accumulators
 // drained).  Every wait is bounded; a wait that expires sets
@@ -417,8 +417,8 @@ __device__ __forceinline__ bool tc_elect() {
 }
 
 // Barriers among the 128 threads of one role (id 1: epilogue, id 2: staging);
-// role_all / role_any also combine a flag, so every thread of the role takes
-// the same branch after them.
+// role_all also combines a flag, so every thread of the role takes the same
+// branch after it.
 __device__ __forceinline__ void role_sync(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
 __device__ __forceinline__ bool role_all(int id, bool v) {
     uint32_t r;
@@ -432,7 +432,6 @@ __device__ __forceinline__ bool role_all(int id, bool v) {
         : "memory");
     return r != 0;
 }
-__device__ __forceinline__ bool role_any(int id, bool v) { return !role_all(id, !v); }
 
 __device__ __forceinline__ void tc_st8(uint32_t taddr, const uint32_t (&v)[8]) {
     asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr), "r"(v[0]),
@@ -692,13 +691,14 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
         const int st = tid - 32 * kTcStageWarp0;  // 0..127
         TcCursor<MAXI, G::TH> cur(p, t_begin);
         for (int k = 0; k < ntiles; ++k) {
-            if (role_any(2, s_fail != 0)) break;
             if (k > 0) cur.next(p);
             const TcTile t = cur.tile();
             const pmb_imgf_item& it = cur.it;
             const int s = k % SLOTS;
             uint8_t* raw = raws + s * G::RAW;
-            bool ok = tc_wait(tc_smem(&full[s]), (k / SLOTS) & 1);
+            // After a failure elsewhere (s_fail) this thread stops waiting; the
+            // role_all below then takes every staging thread out together.
+            bool ok = s_fail == 0 && tc_wait(tc_smem(&full[s]), (k / SLOTS) & 1);
             const int mlo = max(0, it.r0 - R), mhi = min(it.height - 1, it.r1 - 1 + R);
             const int clo = max(0, it.c0 - R), chi = min(it.width - 1, it.c1 - 1 + R);
             if (t.map < 0) {
@@ -791,12 +791,11 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
         const bool valid_lane = lane < G::VB;
         TcCursor<MAXI, G::TH> cur(p, t_begin);
         for (int k = 0; k < ntiles; ++k) {
-            if (role_any(1, s_fail != 0)) break;
             if (k > 0) cur.next(p);
             const TcTile t = cur.tile();
             const pmb_imgf_item& it = cur.it;
             const int b = k & 1;
-            if (!role_all(1, tc_wait(tc_smem(&mma_done[b]), (k >> 1) & 1))) {
+            if (!role_all(1, s_fail == 0 && tc_wait(tc_smem(&mma_done[b]), (k >> 1) & 1))) {
                 s_fail = 1;
                 break;
             }
@@ -824,7 +823,8 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
             __syncwarp();
             if (lane == 0) tc_arrive(tc_smem(&acc_free[b]));
-            uint8_t* const orow = ost + row * kOutStride;
+            uint8_t* const ostb = ost;
+            uint8_t* const orow = ostb + row * kOutStride;
 #pragma unroll
             for (int g = 0; g < (valid_lane ? 16 : 0); g += 4) {
                 uint32_t d[12];
@@ -840,40 +840,37 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
                     *reinterpret_cast<uint4*>(orow + 12 * g + 16 * h) =
                         make_uint4(d[4 * h], d[4 * h + 1], d[4 * h + 2], d[4 * h + 3]);
             }
-            role_sync(1);  // the staged tile is complete
+            // Each warp writes out the rows it staged (tile rows VB q .. VB q +
+            // VB - 1): 12 16-byte pieces per row, consecutive lanes on
+            // consecutive pieces.  Only the warp's own rows are read, so a warp
+            // barrier orders the staging and the copy, and the next tile's
+            // staging of the same rows comes after this copy in program order.
+            __syncwarp();
+            const int r_lo = G::VB * q, r_hi = min(r_lo + G::VB, t.rows);
             uint8_t* const obase = it.out + static_cast<int64_t>(t.r0 - it.out_row0) * it.out_pitch +
                                    3 * (t.c0 - it.out_col0);
-            if (t.tw == kTcTW && t.rows == G::TH &&
-                ((reinterpret_cast<uintptr_t>(obase) | static_cast<uintptr_t>(it.out_pitch)) & 15) == 0) {
-                // Full tile: TH x 12 16-byte pieces, all loads first.
-                constexpr int kPer = (G::TH * 12 + 127) / 128;
+            if (t.tw == kTcTW && ((reinterpret_cast<uintptr_t>(obase) | static_cast<uintptr_t>(it.out_pitch)) & 15) == 0) {
+                constexpr int kPer = (G::VB * 12 + 31) / 32;
+                const int n = (r_hi - r_lo) * 12;
                 uint4 v[kPer];
 #pragma unroll
                 for (int i = 0; i < kPer; ++i) {
-                    const int e = tid + 128 * i, r = e / 12, c = e - r * 12;
-                    if (e < G::TH * 12) v[i] = *reinterpret_cast<const uint4*>(ost + r * kOutStride + 16 * c);
+                    const int e = lane + 32 * i, r = r_lo + e / 12, c = e % 12;
+                    if (e < n) v[i] = *reinterpret_cast<const uint4*>(ostb + r * kOutStride + 16 * c);
                 }
 #pragma unroll
                 for (int i = 0; i < kPer; ++i) {
-                    const int e = tid + 128 * i, r = e / 12, c = e - r * 12;
-                    if (e < G::TH * 12)
-                        *reinterpret_cast<uint4*>(obase + static_cast<int64_t>(r) * it.out_pitch + 16 * c) = v[i];
-                }
-            } else if (t.tw == kTcTW &&
-                       ((reinterpret_cast<uintptr_t>(obase) | static_cast<uintptr_t>(it.out_pitch)) & 15) == 0) {
-                for (int e = tid; e < t.rows * 12; e += 128) {
-                    const int r = e / 12, c = e - r * 12;
-                    *reinterpret_cast<uint4*>(obase + static_cast<int64_t>(r) * it.out_pitch + 16 * c) =
-                        *reinterpret_cast<const uint4*>(ost + r * kOutStride + 16 * c);
+                    const int e = lane + 32 * i, r = r_lo + e / 12, c = e % 12;
+                    if (e < n) *reinterpret_cast<uint4*>(obase + static_cast<int64_t>(r) * it.out_pitch + 16 * c) = v[i];
                 }
             } else {
                 const int nb = 3 * t.tw;
-                for (int e = tid; e < t.rows * nb; e += 128) {
-                    const int r = e / nb, c = e - r * nb;
-                    obase[static_cast<int64_t>(r) * it.out_pitch + c] = ost[r * kOutStride + c];
+                for (int e = lane; e < (r_hi - r_lo) * nb; e += 32) {
+                    const int r = r_lo + e / nb, c = e % nb;
+                    obase[static_cast<int64_t>(r) * it.out_pitch + c] = ostb[r * kOutStride + c];
                 }
             }
-            role_sync(1);  // the staging buffer may be refilled
+            __syncwarp();
         }
     }
 
