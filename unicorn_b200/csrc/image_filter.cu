@@ -795,7 +795,8 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
             const TcTile t = cur.tile();
             const pmb_imgf_item& it = cur.it;
             const int b = k & 1;
-            if (!role_all(1, s_fail == 0 && tc_wait(tc_smem(&mma_done[b]), (k >> 1) & 1))) {
+            // Each epilogue warp decides for itself (no role barrier follows).
+            if (!__all_sync(0xffffffffu, s_fail == 0 && tc_wait(tc_smem(&mma_done[b]), (k >> 1) & 1))) {
                 s_fail = 1;
                 break;
             }
