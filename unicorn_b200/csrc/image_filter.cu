@@ -416,22 +416,8 @@ __device__ __forceinline__ bool tc_elect() {
     return pred != 0;
 }
 
-// Barriers among the 128 threads of one role (id 1: epilogue, id 2: staging);
-// role_all also combines a flag, so every thread of the role takes the same
-// branch after it.
+// Barrier among the 128 staging threads (id 2).
 __device__ __forceinline__ void role_sync(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
-__device__ __forceinline__ bool role_all(int id, bool v) {
-    uint32_t r;
-    asm volatile(
-        "{\n\t.reg .pred p, q;\n\t"
-        "setp.ne.u32 p, %1, 0;\n\t"
-        "bar.red.and.pred q, %2, 128, p;\n\t"
-        "selp.u32 %0, 1, 0, q;\n\t}"
-        : "=r"(r)
-        : "r"(static_cast<uint32_t>(v)), "r"(id)
-        : "memory");
-    return r != 0;
-}
 
 __device__ __forceinline__ void tc_st8(uint32_t taddr, const uint32_t (&v)[8]) {
     asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr), "r"(v[0]),
@@ -696,11 +682,18 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
             const pmb_imgf_item& it = cur.it;
             const int s = k % SLOTS;
             uint8_t* raw = raws + s * G::RAW;
-            // After a failure elsewhere (s_fail) this thread stops waiting; the
-            // role_all below then takes every staging thread out together.
+            // After a failure (s_fail) a staging warp stops waiting and stops
+            // working, but keeps walking the tiles and taking part in the role's
+            // barriers, so the other staging warps never wait for it there.
             bool ok = s_fail == 0 && tc_wait(tc_smem(&full[s]), (k / SLOTS) & 1);
             const int mlo = max(0, it.r0 - R), mhi = min(it.height - 1, it.r1 - 1 + R);
             const int clo = max(0, it.c0 - R), chi = min(it.width - 1, it.c1 - 1 + R);
+            const bool top = t.r0 - R < 0, bottom = t.r0 - R + G::ROWS > it.height;
+            const bool left = t.c0 < 16, right = t.c0 + 80 + R > it.width + 16;
+            // Raw rows written by the staging threads themselves (plain loads, edge
+            // fills) need a role barrier before other threads read them; rows that
+            // only TMA wrote are visible to every thread after its own wait.
+            const bool shared_writes = t.map < 0 || left || right || top || bottom;
             if (t.map < 0) {
                 // Plain loads of the needed pixels, clamped to the subscription.
                 const int span = kTcTW + 2 * R;
@@ -716,8 +709,6 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
                     d[2] = __ldg(src + 2);
                 }
             } else {
-                const bool top = t.r0 - R < 0, bottom = t.r0 - R + G::ROWS > it.height;
-                const bool left = t.c0 < 16, right = t.c0 + 80 + R > it.width + 16;
                 if (left || right) {
                     // Needed pixels (x in [16 - R, 80 + R)) beyond the image's left or
                     // right edge -- the halo, or the part of a tile that overhangs
@@ -756,9 +747,11 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
                 if (u >= static_cast<int>(kTcOpSlots))
                     ok = ok && tc_wait(tc_smem(&op_free[u % kTcOpSlots]), ((u / static_cast<int>(kTcOpSlots)) - 1) & 1);
             }
-            if (!role_all(2, ok)) {  // also: raw rows complete (loads and edge fills)
+            ok = __all_sync(0xffffffffu, ok);
+            if (shared_writes) role_sync(2);  // raw rows complete (loads and edge fills)
+            if (!ok) {
                 s_fail = 1;
-                break;
+                continue;
             }
             // De-interleave: thread st stages band row st (band st / 32, plane row
             // VB (st / 32) + st % 32) into TMEM lane st of the three operand
