@@ -166,6 +166,16 @@ typedef struct pmb_imgf_item {
 int pmb_image_filter(const pmb_imgf_item* items, int n_items,
                      const int8_t* filter, int radius, int mode, void* stream);
 
+/* The rectangles one pmb_image_filter call filters for `items` (host only,
+ * no device work): items whose views are whole-row layouts (in_pitch =
+ * out_pitch = 3W) of the same input and output images and whose output
+ * rectangles are adjacent -- same rows with touching columns, or same columns
+ * with touching rows -- are merged into one item covering both; empty
+ * rectangles are dropped; other items are kept as they are.  Writes at most
+ * n_items items to `out` and their count to `*n_out`.  No counterpart in the
+ * reference. */
+int pmb_image_filter_cover(const pmb_imgf_item* items, int n_items, pmb_imgf_item* out, int* n_out);
+
 /* Error word of the stencil kernels on the current device (synchronous copy;
  * `clear` resets it): 0 = clean; 1 = a bounded wait of a tensor-core stencil
  * launch (tile staging or its matrix products) expired, and that launch's

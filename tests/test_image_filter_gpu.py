@@ -94,6 +94,44 @@ def test_batched_subtask_rectangles(cuda, oracle, T):
     assert (got[~covered] == 0).all(), "kernel wrote outside its rectangles"
 
 
+@pytest.mark.parametrize("T", [96, 64, 45])
+def test_checkerboard_items_two_outputs(cuda, oracle, pmb, T):
+    """Neighbouring subtasks write to two different output images, so no two
+    items of the launch merge: the kernel walks many tensor-map items (item
+    changes inside a CTA's tile range, partial tiles at every seam)."""
+    from unicorn_b200 import capi
+
+    W, H, R = 1024, 700, 3
+    img, f = make_case(W, H, R, 500 + T, 1)
+    ref = run_oracle(oracle, img, W, H, R, f, 1).reshape(H, W, 3)
+    d_in = cuda.from_numpy(img).cuda()
+    outs = [cuda.zeros_like(d_in), cuda.zeros_like(d_in)]
+    rects = tiles(W, H, T)[:256]
+    items = (capi.ImgfItem * len(rects))()
+    for k, (r0, r1, c0, c1) in enumerate(rects):
+        it = items[k]
+        it.in_ = d_in.data_ptr()
+        it.out = outs[((r0 // T) + (c0 // T)) & 1].data_ptr()
+        it.in_pitch = it.out_pitch = 3 * W
+        it.width, it.height = W, H
+        it.in_row0 = it.in_col0 = it.out_row0 = it.out_col0 = 0
+        it.r0, it.r1, it.c0, it.c1 = r0, r1, c0, c1
+    cover = (capi.ImgfItem * len(rects))()
+    n = ctypes.c_int(0)
+    assert pmb.pmb_image_filter_cover(items, len(rects), cover, ctypes.byref(n)) == 0
+    assert n.value == len(rects)
+    capi.check(pmb.pmb_image_filter(items, len(rects), ptr(f), R, 1, None))
+    cuda.cuda.synchronize()
+    got = [o.cpu().numpy().reshape(H, W, 3) for o in outs]
+    written = [np.zeros((H, W), bool), np.zeros((H, W), bool)]
+    for (r0, r1, c0, c1) in rects:
+        o = ((r0 // T) + (c0 // T)) & 1
+        written[o][r0:r1, c0:c1] = True
+        assert np.array_equal(got[o][r0:r1, c0:c1], ref[r0:r1, c0:c1]), (r0, c0)
+    for o in range(2):
+        assert (got[o][~written[o]] == 0).all(), "kernel wrote outside its rectangles"
+
+
 @pytest.mark.parametrize("R", [1, 2, 7])
 def test_compact_views(cuda, oracle, pmb, R):
     """Each subtask reads a compact copy of its input subscription and writes a

@@ -130,6 +130,8 @@ _SIGS = {
     "pmb_image_filter_host": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p, c_int, c_int,
                                       c_int, c_void_p]),
     "pmb_image_filter_error": (c_int, [c_int, ctypes.POINTER(ctypes.c_uint32)]),
+    "pmb_image_filter_cover": (c_int, [ctypes.POINTER(ImgfItem), c_int, ctypes.POINTER(ImgfItem),
+                                       ctypes.POINTER(c_int)]),
     "pmb_trsm_workspace_bytes": (c_size_t, [c_int, c_int, c_int]),
     "pmb_lu_refine_workspace_bytes": (c_size_t, [c_int]),
     "pmb_lu_solve_refined": (c_int, [c_void_p, c_int64, c_void_p, c_int64, c_int, c_void_p, c_void_p, c_int, c_void_p,

@@ -27,6 +27,7 @@
 // multiplies).  blockIdx.x is mapped to (item, tile).
 #include <algorithm>
 #include <mutex>
+#include <vector>
 
 #include "pmb_common.cuh"
 
@@ -726,16 +727,21 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
                     }
                 }
                 if (top || bottom) {
-                    // Rows beyond the image's top or bottom repeat the edge row.
+                    // The R rows beyond the image's top or bottom repeat the edge
+                    // row; rows further out feed only output rows outside the
+                    // image, which are not written.
                     role_sync(2);  // edge pixels of the edge rows are in place
                     const int j_top = t.r0 - R + G::ROWS - 1;             // box row of image row 0
                     const int j_bot = t.r0 - R + G::ROWS - it.height;     // box row of image row H - 1
-                    for (int e = st; e < G::ROWS * (kRawStride / 16); e += 128) {
-                        const int j = e / (kRawStride / 16), v = e - j * (kRawStride / 16);
-                        const int js = j > j_top ? j_top : (j < j_bot ? j_bot : j);
-                        if (js != j)
-                            *reinterpret_cast<uint4*>(raw + j * kRawStride + 16 * v) =
-                                *reinterpret_cast<const uint4*>(raw + js * kRawStride + 16 * v);
+                    const int nt = top ? min(R, G::ROWS - 1 - j_top) : 0;  // box rows j_top + 1 .. j_top + nt
+                    const int nb = bottom ? min(R, j_bot) : 0;             // box rows j_bot - nb .. j_bot - 1
+                    constexpr int kV = kRawStride / 16;
+                    for (int e = st; e < (nt + nb) * kV; e += 128) {
+                        const int i = e / kV, v = e - i * kV;
+                        const int j = i < nt ? j_top + 1 + i : j_bot - nb + (i - nt);
+                        const int js = i < nt ? j_top : j_bot;
+                        *reinterpret_cast<uint4*>(raw + j * kRawStride + 16 * v) =
+                            *reinterpret_cast<const uint4*>(raw + js * kRawStride + 16 * v);
                     }
                 }
             }
@@ -944,6 +950,94 @@ int validate_item(const pmb_imgf_item& it, int R, int idx) {
     return PMB_SUCCESS;
 }
 
+// Pixel (m, n) of an item's input is read at in_base + (H-1-m) * in_pitch + 3n
+// and written at out_base + m * out_pitch + 3n: two items with the same
+// bases, whole-row pitches and image size address every pixel identically,
+// so where their output rectangles are adjacent (same rows and touching
+// columns, or same columns and touching rows) one item covering both
+// computes the same bytes, and it reads and writes only memory inside the
+// two items' views.
+struct ItemKey {
+    uintptr_t in_base, out_base;
+    int width, height;
+    bool operator<(const ItemKey& o) const {
+        if (in_base != o.in_base) return in_base < o.in_base;
+        if (out_base != o.out_base) return out_base < o.out_base;
+        if (width != o.width) return width < o.width;
+        return height < o.height;
+    }
+    bool operator==(const ItemKey& o) const {
+        return in_base == o.in_base && out_base == o.out_base && width == o.width && height == o.height;
+    }
+};
+
+ItemKey key_of(const pmb_imgf_item& it) {
+    ItemKey k;
+    k.in_base = reinterpret_cast<uintptr_t>(it.in) - static_cast<uintptr_t>(it.in_row0 * it.in_pitch) -
+                3u * static_cast<uintptr_t>(it.in_col0);
+    k.out_base = reinterpret_cast<uintptr_t>(it.out) - static_cast<uintptr_t>(it.out_row0 * it.out_pitch) -
+                 3u * static_cast<uintptr_t>(it.out_col0);
+    k.width = it.width;
+    k.height = it.height;
+    return k;
+}
+
+// Merges adjacent items in two sorted passes (rows of touching column
+// ranges, then columns of touching row ranges); drops empty rectangles.
+// Items with a pitch other than 3W (COMPACT views) are kept as they are.
+// Returns the number of items written to `out`.
+int coalesce_items(const pmb_imgf_item* items, int n, pmb_imgf_item* out) {
+    struct Entry {
+        ItemKey key;
+        pmb_imgf_item it;
+    };
+    std::vector<Entry> e;
+    int m = 0;
+    e.reserve(n);
+    for (int i = 0; i < n; ++i) {
+        const pmb_imgf_item& it = items[i];
+        if (it.r0 == it.r1 || it.c0 == it.c1) continue;
+        if (it.in_pitch == 3LL * it.width && it.out_pitch == 3LL * it.width)
+            e.push_back({key_of(it), it});
+        else
+            out[m++] = it;
+    }
+    auto merge_pass = [&e](bool rows) {
+        std::sort(e.begin(), e.end(), [rows](const Entry& a, const Entry& b) {
+            if (!(a.key == b.key)) return a.key < b.key;
+            const int a1 = rows ? a.it.r0 : a.it.c0, b1 = rows ? b.it.r0 : b.it.c0;
+            const int a2 = rows ? a.it.r1 : a.it.c1, b2 = rows ? b.it.r1 : b.it.c1;
+            const int a3 = rows ? a.it.c0 : a.it.r0, b3 = rows ? b.it.c0 : b.it.r0;
+            if (a1 != b1) return a1 < b1;
+            if (a2 != b2) return a2 < b2;
+            return a3 < b3;
+        });
+        size_t w = 0;
+        for (size_t i = 0; i < e.size(); ++i) {
+            if (w > 0) {
+                pmb_imgf_item& p = e[w - 1].it;
+                const pmb_imgf_item& c = e[i].it;
+                if (e[w - 1].key == e[i].key) {
+                    if (rows && p.r0 == c.r0 && p.r1 == c.r1 && p.c1 == c.c0) {
+                        p.c1 = c.c1;
+                        continue;
+                    }
+                    if (!rows && p.c0 == c.c0 && p.c1 == c.c1 && p.r1 == c.r0) {
+                        p.r1 = c.r1;
+                        continue;
+                    }
+                }
+            }
+            e[w++] = e[i];
+        }
+        e.resize(w);
+    };
+    merge_pass(true);
+    merge_pass(false);
+    for (const Entry& x : e) out[m++] = x.it;
+    return m;
+}
+
 template <int R, int MODE, int MAXI>
 int launch_t(const pmb_imgf_item* items, int n, const int8_t* filter, cudaStream_t s) {
     using G = Geo<R>;
@@ -1121,8 +1215,21 @@ extern "C" int pmb_image_filter(const pmb_imgf_item* items, int n_items, const i
         if (st != PMB_SUCCESS) return st;
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    return n_items <= 8 ? launch_radius<8>(items, n_items, filter, radius, mode, s)
-                        : launch_radius<PMB_IMGF_MAX_ITEMS>(items, n_items, filter, radius, mode, s);
+    // Subtasks that tile a larger rectangle of the same whole-row views are
+    // filtered as that rectangle: same bytes, one tile grid (no partial tiles
+    // at the subtask seams) and a smaller launch.
+    pmb_imgf_item merged[PMB_IMGF_MAX_ITEMS];
+    const int n = coalesce_items(items, n_items, merged);
+    return n <= 8 ? launch_radius<8>(merged, n, filter, radius, mode, s)
+                  : launch_radius<PMB_IMGF_MAX_ITEMS>(merged, n, filter, radius, mode, s);
+}
+
+extern "C" int pmb_image_filter_cover(const pmb_imgf_item* items, int n_items, pmb_imgf_item* out, int* n_out) {
+    PMB_CHECK_ARG(items && out && n_out, "null items/out/n_out");
+    PMB_CHECK_ARG(n_items >= 1 && n_items <= PMB_IMGF_MAX_ITEMS, "n_items %d outside [1,%d]", n_items,
+                  PMB_IMGF_MAX_ITEMS);
+    *n_out = coalesce_items(items, n_items, out);
+    return PMB_SUCCESS;
 }
 
 extern "C" int pmb_image_filter_full(const uint8_t* d_in, uint8_t* d_out, int width, int height,
