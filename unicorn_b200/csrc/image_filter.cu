@@ -594,6 +594,12 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tmem_slot;
+    // Launched as a programmatic dependent of the stream's previous kernel:
+    // the set-up above (barriers, filter slices, tensor memory) overlaps that
+    // kernel's tail, and global memory is touched only from here on, once
+    // that kernel is complete and its writes are visible.
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 
     if (warp == kTcLoaderWarp) {
         // ================= loader =================
@@ -1170,8 +1176,17 @@ int launch_tc(const pmb_imgf_item* items, int n, const int8_t* filter, cudaStrea
     PMB_CUDA_TRY(cudaGetDevice(&dev));
     PMB_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     const unsigned grid = static_cast<unsigned>(std::min<int64_t>(total, sms));  // persistent: one CTA per SM
-    imgf_tc_kernel<R, MODE, MAXI><<<grid, kTcThreads, G::SMEM, s>>>(p);
-    PMB_CUDA_TRY(cudaGetLastError());
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(kTcThreads);
+    cfg.dynamicSmemBytes = G::SMEM;
+    cfg.stream = s;
+    cudaLaunchAttribute pdl[1];
+    pdl[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    pdl[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = pdl;
+    cfg.numAttrs = 1;
+    PMB_CUDA_TRY(cudaLaunchKernelEx(&cfg, imgf_tc_kernel<R, MODE, MAXI>, p));
     return PMB_SUCCESS;
 }
 
