@@ -259,6 +259,20 @@ __device__ __forceinline__ void deinterleave4(uint32_t w0, uint32_t w1, uint32_t
 // accumulators (192 TMEM columns).  Shared memory carries only the raw
 // input rows, the B slices and the staged output rows.
 //
+// Interleaved form, R <= 2 (the reference's own runs use 5 x 5): the MMAs
+// read the RGB bytes as they lie in the row, with no planes.  Output byte
+// o = 3j + c of a row (pixel j, channel c, reading input byte 2 - c) is
+//   sum_kx f[ky][kx] * in[o - 2c + 2 + 3 (kx - R)],
+// so for the 16 output bytes 16t .. 16t + 15 the inputs lie in the 32-byte
+// window 16t - 8 .. 16t + 23 (19 + 6R <= 32 bytes) and
+//   B_{ky,ph}[k][n] = f[ky][kx]  where k = n - 2c + 3 (kx - R) + 10, c = (ph + n) % 3,
+// with ph = t mod 3 (16 = 1 mod 3): three slices per filter row.  A tile is
+// then 12 (2R + 1) MMAs on ONE operand slot of 52 columns (input bytes
+// 3 tile_c0 - 8 .. 3 tile_c0 + 199, copied from the raw row unchanged) and
+// 7 x 2R shifts; the accumulator columns are the output bytes in order, so
+// the epilogue packs four sums to a word with no re-interleave.  The staging
+// threads only copy, and the operand slot is double-buffered per tile.
+//
 // Persistent and warp-specialised: one CTA per SM walks a contiguous range
 // of the launch's tiles (horizontal neighbours back to back, so their shared
 // input columns are L2 hits).  Ten warps in four roles:
@@ -302,6 +316,14 @@ constexpr int kOutStride = 208;     // staged output row: 192 B + padding (confl
 constexpr uint32_t kTcTmemCols = 512;
 constexpr uint32_t kTcAccCols = 192, kTcOpCol0 = 2 * kTcAccCols, kTcOpCols = 24, kTcOpSlots = 5;
 static_assert(kTcOpCol0 + kTcOpSlots * kTcOpCols <= kTcTmemCols && 4 * kTcChunks <= kTcOpCols, "tensor memory");
+// Interleaved form (R <= kTcIlMaxR): one operand slot per tile, double
+// buffered: raw bytes 40 .. 247 of each band row (input bytes 3 tile_c0 - 8 ..
+// 3 tile_c0 + 199) in 52 columns, shifted as 7 groups of 8.  Output bytes
+// 16 t .. 16 t + 15 read columns 4 t .. 4 t + 7.
+constexpr int kTcIlMaxR = 2;
+constexpr uint32_t kTcIlOpCols = 56, kTcIlUsedCols = 52;
+static_assert(kTcOpCol0 + 2 * kTcIlOpCols <= kTcTmemCols && kTcIlOpCols % 8 == 0 && kTcIlUsedCols <= kTcIlOpCols,
+              "tensor memory (interleaved)");
 constexpr uint32_t kTcWaitPolls = 1u << 21;
 constexpr uint32_t kImgfErrTimeout = 1;
 constexpr int kSmemLimit = 227 * 1024 - 256;  // per-block opt-in limit, less the kernel's static shared memory
@@ -309,17 +331,21 @@ constexpr int kSmemLimit = 227 * 1024 - 256;  // per-block opt-in limit, less th
 template <int R>
 struct TcGeo {
     static constexpr int KD = 2 * R + 1;
+    // R <= 2: the MMAs read the interleaved RGB bytes (no planes), with one
+    // banded filter slice per filter row and output-byte phase (16 t mod 3).
+    static constexpr bool IL = R <= kTcIlMaxR;
+    static constexpr int NB = (IL ? 3 : 1) * KD * 512;   // filter slices in shared memory
     static constexpr int VB = 32 - 2 * R;             // output rows per 32-lane band
     static constexpr int TH = 4 * VB;                 // output rows per tile
     static constexpr int ROWS = TH + 2 * R;           // input rows per tile (TMA box rows)
     static constexpr int RAW = (ROWS * kRawStride + 127) / 128 * 128;  // slot stride (TMA destinations 128-B aligned)
     static constexpr int OUT = TH * kOutStride;
     static constexpr int OFF_RAW = 0;
-    static constexpr int FIXED = OFF_RAW + OUT + KD * 512 + 256;
+    static constexpr int FIXED = OFF_RAW + OUT + NB + 256;
     static constexpr int SLOTS = FIXED + 4 * RAW <= kSmemLimit ? 4 : (FIXED + 3 * RAW <= kSmemLimit ? 3 : 2);
     static constexpr int OFF_OUT = OFF_RAW + SLOTS * RAW;
     static constexpr int OFF_B = OFF_OUT + OUT;
-    static constexpr int OFF_BAR = OFF_B + KD * 512;
+    static constexpr int OFF_BAR = OFF_B + NB;
     static constexpr int SMEM = OFF_BAR + 256;
     static_assert(RAW % 128 == 0 && OFF_OUT % 16 == 0 && OFF_B % 16 == 0 &&
                       OFF_BAR % 8 == 0,
@@ -569,19 +595,21 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
     }
     // B: per filter row, the 16 x 32 banded slice, K-major core matrices
     // (8 output columns x 16 bytes; column groups 128 B, K chunks 256 B apart).
-    for (int w = tid; w < G::KD * 128; w += kTcThreads) {
-        const int ky = w >> 7, off = (w & 127) * 4;
-        uint32_t word = 0;
-#pragma unroll
-        for (int b = 0; b < 4; ++b) {
-            const int o = off + b;
-            const int k = (o >> 8) * 16 + (o & 15);
-            const int j = ((o >> 7) & 1) * 8 + ((o >> 4) & 7);
-            const int kx = k - j + R - 8;
-            const int v = (kx >= 0 && kx <= 2 * R) ? p.f[ky][kx] : 0;
-            word |= static_cast<uint32_t>(static_cast<uint8_t>(v)) << (8 * b);
-        }
-        *reinterpret_cast<uint32_t*>(bsm + ky * 512 + off) = word;
+    // B: per filter row (and, interleaved, per output-byte phase ph), the
+    // 16 x 32 banded slice, K-major core matrices (8 output columns x 16
+    // bytes; column groups 128 B, K chunks 256 B apart): byte (k, n) at
+    // (k / 16) 256 + (n / 8) 128 + (n % 8) 16 + k % 16.  Zeroed, then each
+    // tap placed: planar, output column n reads plane column k = n + kx - R + 8
+    // of its window; interleaved, output byte n (channel c = (ph + n) % 3)
+    // reads window byte k = n - 2c + 3 (kx - R) + 10.
+    for (int w = tid; w < G::NB / 4; w += kTcThreads) reinterpret_cast<uint32_t*>(bsm)[w] = 0;
+    __syncthreads();
+    for (int e = tid; e < (G::NB / 512) * 16 * G::KD; e += kTcThreads) {
+        const int kx = e % G::KD, n = (e / G::KD) & 15, slice = e / (16 * G::KD);
+        const int ky = G::IL ? slice / 3 : slice;
+        const int k = G::IL ? n - 2 * ((slice % 3 + n) % 3) + 3 * (kx - R) + 10 : n + kx - R + 8;
+        bsm[slice * 512 + (k >> 4) * 256 + (n >> 3) * 128 + (n & 7) * 16 + (k & 15)] =
+            static_cast<uint8_t>(p.f[ky][kx]);
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     if (warp == kTcMmaWarp) {
@@ -655,7 +683,25 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            if (tc_elect()) {
+            if (G::IL && tc_elect()) {
+                // Interleaved: 12 output-byte groups per filter row, all on the
+                // tile's operand slot; one shift of the slot per filter row.
+                const uint32_t op = tmem + kTcOpCol0 + kTcIlOpCols * static_cast<uint32_t>(k & 1);
+                const uint32_t acc = tmem + kTcAccCols * b;
+#pragma unroll
+                for (int ky = 0; ky < G::KD; ++ky) {
+#pragma unroll
+                    for (int tg = 0; tg < 12; ++tg)
+                        tc_mma_i8_ta(acc + 16 * tg, op + 4 * tg,
+                                     bdesc0 + static_cast<uint64_t>(((3 * ky + tg % 3) * 512) >> 4), ky > 0 ? 1u : 0u);
+                    if (ky + 1 < G::KD) {
+#pragma unroll
+                        for (uint32_t sc = 0; sc < kTcIlOpCols; sc += 8) tc_shift(op + sc);
+                    }
+                }
+                tc_commit(tc_smem(&op_free[k & 1]));
+                tc_commit(tc_smem(&mma_done[b]));
+            } else if (!G::IL && tc_elect()) {
 #pragma unroll 1
                 for (int c = 0; c < 3; ++c) {
                     const int u = 3 * k + c;
@@ -751,13 +797,19 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
                     }
                 }
             }
-            // Operand slot of unit u = 3k + c is free once the MMAs and shifts of
-            // unit u - 5 are done.
+            if (G::IL) {
+                // The tile's operand slot is free once tile k - 2's MMAs and shifts are done.
+                if (k >= 2) ok = ok && tc_wait(tc_smem(&op_free[k & 1]), ((k >> 1) - 1) & 1);
+            } else {
+                // Operand slot of unit u = 3k + c is free once the MMAs and shifts of
+                // unit u - 5 are done.
 #pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                const int u = 3 * k + c;
-                if (u >= static_cast<int>(kTcOpSlots))
-                    ok = ok && tc_wait(tc_smem(&op_free[u % kTcOpSlots]), ((u / static_cast<int>(kTcOpSlots)) - 1) & 1);
+                for (int c = 0; c < 3; ++c) {
+                    const int u = 3 * k + c;
+                    if (u >= static_cast<int>(kTcOpSlots))
+                        ok = ok &&
+                             tc_wait(tc_smem(&op_free[u % kTcOpSlots]), ((u / static_cast<int>(kTcOpSlots)) - 1) & 1);
+                }
             }
             ok = __all_sync(0xffffffffu, ok);
             if (shared_writes) role_sync(2);  // raw rows complete (loads and edge fills)
@@ -770,7 +822,36 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
             // slots.  Consecutive threads take consecutive rows, so the 16-byte
             // loads (row stride 19 x 16 B) are conflict-free.
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            {
+            if (G::IL) {
+                // Interleaved: raw bytes 40 .. 247 of band row st, as they are,
+                // into TMEM lane st of the tile's slot (16-byte loads from raw
+                // byte 32; words 2 .. 53 go to columns 0 .. 51).
+                const int r = G::VB * (st >> 5) + (st & 31);
+                const uint4* const src = reinterpret_cast<const uint4*>(raw + (G::ROWS - 1 - r) * kRawStride + 32);
+                const uint32_t col0 = tmem + (static_cast<uint32_t>(st & ~31) << 16) + kTcOpCol0 +
+                                      kTcIlOpCols * static_cast<uint32_t>(k & 1);
+                // Two rounds (loads 0-7, then 8-13) keep fewer words live.
+                uint32_t w[56];
+#pragma unroll
+                for (int half = 0; half < 2; ++half) {
+#pragma unroll
+                    for (int j = 8 * half; j < (half ? 14 : 8); ++j) {
+                        const uint4 v = src[j];
+                        w[4 * j] = v.x;
+                        w[4 * j + 1] = v.y;
+                        w[4 * j + 2] = v.z;
+                        w[4 * j + 3] = v.w;
+                    }
+#pragma unroll
+                    for (int g = 3 * half; g < (half ? 6 : 3); ++g) {
+                        const uint32_t v[8] = {w[8 * g + 2], w[8 * g + 3], w[8 * g + 4], w[8 * g + 5],
+                                               w[8 * g + 6], w[8 * g + 7], w[8 * g + 8], w[8 * g + 9]};
+                        tc_st8(col0 + 8 * g, v);
+                    }
+                }
+                const uint32_t v4[4] = {w[50], w[51], w[52], w[53]};
+                tc_st4(col0 + 48, v4);
+            } else {
                 const int r = G::VB * (st >> 5) + (st & 31);
                 const uint8_t* const src = raw + (G::ROWS - 1 - r) * kRawStride + 16;
                 const uint32_t lanes = tmem + (static_cast<uint32_t>(st & ~31) << 16);
@@ -806,45 +887,79 @@ imgf_tc_kernel(const __grid_constant__ ImgfParamsTc<MAXI> p) {
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            uint32_t pw[3][16];
-#pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                uint32_t v[4][16];
-#pragma unroll
-                for (int tg = 0; tg < 4; ++tg)
-                    tc_ld16(tmem + kTcAccCols * b + (static_cast<uint32_t>(32 * q) << 16) +
-                                static_cast<uint32_t>(64 * c + 16 * tg),
-                            v[tg]);
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-                for (int tg = 0; tg < 4; ++tg)
-#pragma unroll
-                    for (int g = 0; g < 4; ++g) {
-                        const int a[4] = {static_cast<int>(v[tg][4 * g]), static_cast<int>(v[tg][4 * g + 1]),
-                                          static_cast<int>(v[tg][4 * g + 2]), static_cast<int>(v[tg][4 * g + 3])};
-                        pw[c][4 * tg + g] = pack4<MODE>(a);
-                    }
-            }
-            // The accumulator set is drained: the MMAs of tile k + 2 may start.
-            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            __syncwarp();
-            if (lane == 0) tc_arrive(tc_smem(&acc_free[b]));
             uint8_t* const ostb = ost;
             uint8_t* const orow = ostb + row * kOutStride;
+            if constexpr (G::IL) {
+                // Interleaved: accumulator column 16 t + n is output byte 16 t + n
+                // of the row, so four sums pack into a word in place.
+                uint32_t pw[48];
 #pragma unroll
-            for (int g = 0; g < (valid_lane ? 16 : 0); g += 4) {
-                uint32_t d[12];
+                for (int h = 0; h < 3; ++h) {
+                    uint32_t v[4][16];
 #pragma unroll
-                for (int h = 0; h < 4; ++h) {
-                    const uint32_t A = pw[0][g + h], B = pw[1][g + h], C = pw[2][g + h];
-                    d[3 * h + 0] = __byte_perm(__byte_perm(A, B, 0x0140), C, 0x2410);  // a0 b0 c0 a1
-                    d[3 * h + 1] = __byte_perm(__byte_perm(B, C, 0x0251), A, 0x2610);  // b1 c1 a2 b2
-                    d[3 * h + 2] = __byte_perm(C, __byte_perm(A, B, 0x0073), 0x3542);  // c2 a3 b3 c3
+                    for (int tg = 0; tg < 4; ++tg)
+                        tc_ld16(tmem + kTcAccCols * b + (static_cast<uint32_t>(32 * q) << 16) +
+                                    static_cast<uint32_t>(64 * h + 16 * tg),
+                                v[tg]);
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                    for (int tg = 0; tg < 4; ++tg)
+#pragma unroll
+                        for (int g = 0; g < 4; ++g) {
+                            const int a[4] = {static_cast<int>(v[tg][4 * g]), static_cast<int>(v[tg][4 * g + 1]),
+                                              static_cast<int>(v[tg][4 * g + 2]), static_cast<int>(v[tg][4 * g + 3])};
+                            pw[16 * h + 4 * tg + g] = pack4<MODE>(a);
+                        }
                 }
+                // The accumulator set is drained: the MMAs of tile k + 2 may start.
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) tc_arrive(tc_smem(&acc_free[b]));
+                if (valid_lane) {
 #pragma unroll
-                for (int h = 0; h < 3; ++h)
-                    *reinterpret_cast<uint4*>(orow + 12 * g + 16 * h) =
-                        make_uint4(d[4 * h], d[4 * h + 1], d[4 * h + 2], d[4 * h + 3]);
+                    for (int i = 0; i < 12; ++i)
+                        *reinterpret_cast<uint4*>(orow + 16 * i) =
+                            make_uint4(pw[4 * i], pw[4 * i + 1], pw[4 * i + 2], pw[4 * i + 3]);
+                }
+            } else {
+                uint32_t pw[3][16];
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    uint32_t v[4][16];
+#pragma unroll
+                    for (int tg = 0; tg < 4; ++tg)
+                        tc_ld16(tmem + kTcAccCols * b + (static_cast<uint32_t>(32 * q) << 16) +
+                                    static_cast<uint32_t>(64 * c + 16 * tg),
+                                v[tg]);
+                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+                    for (int tg = 0; tg < 4; ++tg)
+#pragma unroll
+                        for (int g = 0; g < 4; ++g) {
+                            const int a[4] = {static_cast<int>(v[tg][4 * g]), static_cast<int>(v[tg][4 * g + 1]),
+                                              static_cast<int>(v[tg][4 * g + 2]), static_cast<int>(v[tg][4 * g + 3])};
+                            pw[c][4 * tg + g] = pack4<MODE>(a);
+                        }
+                }
+                // The accumulator set is drained: the MMAs of tile k + 2 may start.
+                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+                __syncwarp();
+                if (lane == 0) tc_arrive(tc_smem(&acc_free[b]));
+#pragma unroll
+                for (int g = 0; g < (valid_lane ? 16 : 0); g += 4) {
+                    uint32_t d[12];
+#pragma unroll
+                    for (int h = 0; h < 4; ++h) {
+                        const uint32_t A = pw[0][g + h], B = pw[1][g + h], C = pw[2][g + h];
+                        d[3 * h + 0] = __byte_perm(__byte_perm(A, B, 0x0140), C, 0x2410);  // a0 b0 c0 a1
+                        d[3 * h + 1] = __byte_perm(__byte_perm(B, C, 0x0251), A, 0x2610);  // b1 c1 a2 b2
+                        d[3 * h + 2] = __byte_perm(C, __byte_perm(A, B, 0x0073), 0x3542);  // c2 a3 b3 c3
+                    }
+#pragma unroll
+                    for (int h = 0; h < 3; ++h)
+                        *reinterpret_cast<uint4*>(orow + 12 * g + 16 * h) =
+                            make_uint4(d[4 * h], d[4 * h + 1], d[4 * h + 2], d[4 * h + 3]);
+                }
             }
             // Each warp writes out the rows it staged (tile rows VB q .. VB q +
             // VB - 1): 12 16-byte pieces per row, consecutive lanes on
