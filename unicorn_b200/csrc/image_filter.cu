@@ -27,7 +27,6 @@
 // multiplies).  blockIdx.x is mapped to (item, tile).
 #include <algorithm>
 #include <mutex>
-#include <vector>
 
 #include "pmb_common.cuh"
 
@@ -1081,12 +1080,6 @@ int validate_item(const pmb_imgf_item& it, int R, int idx) {
 struct ItemKey {
     uintptr_t in_base, out_base;
     int width, height;
-    bool operator<(const ItemKey& o) const {
-        if (in_base != o.in_base) return in_base < o.in_base;
-        if (out_base != o.out_base) return out_base < o.out_base;
-        if (width != o.width) return width < o.width;
-        return height < o.height;
-    }
     bool operator==(const ItemKey& o) const {
         return in_base == o.in_base && out_base == o.out_base && width == o.width && height == o.height;
     }
@@ -1108,37 +1101,43 @@ ItemKey key_of(const pmb_imgf_item& it) {
 // Items with a pitch other than 3W (COMPACT views) are kept as they are.
 // Returns the number of items written to `out`.
 int coalesce_items(const pmb_imgf_item* items, int n, pmb_imgf_item* out) {
-    struct Entry {
-        ItemKey key;
-        pmb_imgf_item it;
+    // Small records sorted in place (no allocation): the item's group of
+    // identical keys, its rectangle and its index.
+    struct Rect {
+        int g, idx, r0, r1, c0, c1;
     };
-    std::vector<Entry> e;
-    int m = 0;
-    e.reserve(n);
+    Rect e[PMB_IMGF_MAX_ITEMS];
+    ItemKey keys[PMB_IMGF_MAX_ITEMS];
+    int ne = 0, nk = 0, m = 0;
     for (int i = 0; i < n; ++i) {
         const pmb_imgf_item& it = items[i];
         if (it.r0 == it.r1 || it.c0 == it.c1) continue;
-        if (it.in_pitch == 3LL * it.width && it.out_pitch == 3LL * it.width)
-            e.push_back({key_of(it), it});
-        else
+        if (it.in_pitch != 3LL * it.width || it.out_pitch != 3LL * it.width) {
             out[m++] = it;
+            continue;
+        }
+        const ItemKey k = key_of(it);
+        int g = 0;
+        while (g < nk && !(keys[g] == k)) ++g;
+        if (g == nk) keys[nk++] = k;
+        e[ne++] = {g, i, it.r0, it.r1, it.c0, it.c1};
     }
-    auto merge_pass = [&e](bool rows) {
-        std::sort(e.begin(), e.end(), [rows](const Entry& a, const Entry& b) {
-            if (!(a.key == b.key)) return a.key < b.key;
-            const int a1 = rows ? a.it.r0 : a.it.c0, b1 = rows ? b.it.r0 : b.it.c0;
-            const int a2 = rows ? a.it.r1 : a.it.c1, b2 = rows ? b.it.r1 : b.it.c1;
-            const int a3 = rows ? a.it.c0 : a.it.r0, b3 = rows ? b.it.c0 : b.it.r0;
+    auto merge_pass = [&e, &ne](bool rows) {
+        std::sort(e, e + ne, [rows](const Rect& a, const Rect& b) {
+            if (a.g != b.g) return a.g < b.g;
+            const int a1 = rows ? a.r0 : a.c0, b1 = rows ? b.r0 : b.c0;
+            const int a2 = rows ? a.r1 : a.c1, b2 = rows ? b.r1 : b.c1;
+            const int a3 = rows ? a.c0 : a.r0, b3 = rows ? b.c0 : b.r0;
             if (a1 != b1) return a1 < b1;
             if (a2 != b2) return a2 < b2;
             return a3 < b3;
         });
-        size_t w = 0;
-        for (size_t i = 0; i < e.size(); ++i) {
+        int w = 0;
+        for (int i = 0; i < ne; ++i) {
             if (w > 0) {
-                pmb_imgf_item& p = e[w - 1].it;
-                const pmb_imgf_item& c = e[i].it;
-                if (e[w - 1].key == e[i].key) {
+                Rect& p = e[w - 1];
+                const Rect& c = e[i];
+                if (p.g == c.g) {
                     if (rows && p.r0 == c.r0 && p.r1 == c.r1 && p.c1 == c.c0) {
                         p.c1 = c.c1;
                         continue;
@@ -1151,11 +1150,18 @@ int coalesce_items(const pmb_imgf_item* items, int n, pmb_imgf_item* out) {
             }
             e[w++] = e[i];
         }
-        e.resize(w);
+        ne = w;
     };
     merge_pass(true);
     merge_pass(false);
-    for (const Entry& x : e) out[m++] = x.it;
+    for (int i = 0; i < ne; ++i) {
+        pmb_imgf_item it = items[e[i].idx];
+        it.r0 = e[i].r0;
+        it.r1 = e[i].r1;
+        it.c0 = e[i].c0;
+        it.c1 = e[i].c1;
+        out[m++] = it;
+    }
     return m;
 }
 
