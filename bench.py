@@ -904,12 +904,15 @@ def main():
     max_over_ranks = ranks.max
 
     # ---- device-resident timing -----------------------------------------
-    with torch.cuda.stream(stream):
-        for _ in range(args.warmup):
-            step()
-    barrier()
+    # The clock sampler starts first (its start-up pause would otherwise leave
+    # the GPU idle right before the timed steps); then the warm-up steps, the
+    # barrier + synchronize, and at once the timed steps.
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
+        with torch.cuda.stream(stream):
+            for _ in range(args.warmup):
+                step()
+        barrier()
         ev0.record(stream)
         for _ in range(args.steps):
             step()
