@@ -94,15 +94,17 @@ def test_batched_subtask_rectangles(cuda, oracle, T):
     assert (got[~covered] == 0).all(), "kernel wrote outside its rectangles"
 
 
+@pytest.mark.parametrize("R", [2, 3])
 @pytest.mark.parametrize("T", [96, 64, 45])
-def test_checkerboard_items_two_outputs(cuda, oracle, pmb, T):
+def test_checkerboard_items_two_outputs(cuda, oracle, pmb, T, R):
     """Neighbouring subtasks write to two different output images, so no two
     items of the launch merge: the kernel walks many tensor-map items (item
-    changes inside a CTA's tile range, partial tiles at every seam)."""
+    changes inside a CTA's tile range, partial tiles at every seam), in the
+    interleaved-byte form (R = 2) and the planar form (R = 3)."""
     from unicorn_b200 import capi
 
-    W, H, R = 1024, 700, 3
-    img, f = make_case(W, H, R, 500 + T, 1)
+    W, H = 1024, 700
+    img, f = make_case(W, H, R, 500 + T + R, 1)
     ref = run_oracle(oracle, img, W, H, R, f, 1).reshape(H, W, 3)
     d_in = cuda.from_numpy(img).cuda()
     outs = [cuda.zeros_like(d_in), cuda.zeros_like(d_in)]
